@@ -1,0 +1,292 @@
+// Test harness over the UNMODIFIED reference BG_Flood sources (compiled in
+// place by oracle/ref/Makefile).  It is test infrastructure: tests/ and the
+// CPU-baseline leg of bench.py load oracle/_ref/libbgf_ref.so to run the
+// reference's own FlowCPU (src/FlowCPU.cu:15) -- and, on a GPU box, its
+// FlowGPU (src/FlowGPU.cu:14) -- on in-memory setups, exactly the way the
+// reference's own tests drive it (src/Testing.cu:418-629: Param built in
+// memory, a flat bathymetry, checkparamsanity, InitMesh, InitialConditions,
+// then the evolving fields overwritten before the time loop).
+//
+// The harness exposes a small extern "C" surface (ref_*) with plain pointers.
+#include "General.h"
+#include "Param.h"
+#include "Arrays.h"
+#include "Forcing.h"
+#include "ReadInput.h"
+#include "Mesh.h"
+#include "InitialConditions.h"
+#include "FlowCPU.h"
+#include "FlowGPU.h"
+#include "Setup_GPU.h"
+#include "Mainloop.h"
+#include "Adaptation.h"
+#include "Updateforcing.h"
+#include "Gradients.h"
+#include "Halo.h"
+
+#include <memory>
+#include <sstream>
+
+namespace {
+
+struct RefBase {
+    virtual ~RefBase() {}
+    virtual int step(int nsteps, double* dts) = 0;
+    virtual int get(const char* name, double* out) = 0;
+    virtual int get_blocks(int* level, double* xo, double* yo, int* nbr8) = 0;
+    virtual int adapt() = 0;
+    Param P;
+    Forcing<float> F;
+    double totaltime = 0.0, nextoutputtime = 0.0, dtmax = 0.0;
+    int gpu = -1;
+};
+
+template <class T> struct RefModel : RefBase {
+    Model<T> M;
+    Model<T> Mg;
+    Loop<T> L;
+    Loop<T> Lg;
+
+    int setup(const char* paramtext, int nx, int ny, double dx, double xo, double yo,
+              const double* zb, const double* h, const double* u, const double* v,
+              const double* cf, double nextout)
+    {
+        // Parameters through the reference's own key parser (src/ReadInput.cu:162).
+        std::istringstream ss(paramtext ? paramtext : "");
+        std::string line;
+        int engine_override = -1;
+        while (std::getline(ss, line)) {
+            if (line.empty()) continue;
+            // The reference parser maps every "engine" value other than 1 to engine 5
+            // (src/ReadInput.cu:193-213), so engine 2 (Kurganov) can only be chosen in
+            // code, as src/Testing.cu does; "harness_engine = N" does that here.
+            if (line.rfind("harness_engine", 0) == 0) {
+                engine_override = std::stoi(line.substr(line.find('=') + 1));
+                continue;
+            }
+            P = readparamstr(line, P);
+            F = readparamstr(line, F);
+        }
+        if (engine_override > 0) P.engine = engine_override;
+        P.dx = dx;
+        P.xo = xo;
+        P.yo = yo;
+        P.xmax = xo + nx * dx;
+        P.ymax = yo + ny * dx;
+        gpu = P.GPUDEVICE;
+
+        // Flat 3x3 bathymetry covering the domain, as src/Testing.cu:490-513.
+        StaticForcingP<float> bathy;
+        F.Bathy.push_back(bathy);
+        F.Bathy[0].xo = xo - dx;
+        F.Bathy[0].yo = yo - dx;
+        F.Bathy[0].nx = 3;
+        F.Bathy[0].ny = 3;
+        F.Bathy[0].dx = (nx * dx + 2 * dx) / 2.0;
+        F.Bathy[0].dy = F.Bathy[0].dx;
+        F.Bathy[0].xmax = F.Bathy[0].xo + 2 * F.Bathy[0].dx;
+        F.Bathy[0].ymax = F.Bathy[0].yo + 2 * F.Bathy[0].dx;
+        AllocateCPU(3, 3, F.Bathy[0].val);
+        for (int k = 0; k < 9; k++) F.Bathy[0].val[k] = 0.0f;
+
+        checkparamsanity(P, F);
+        InitMesh(P, F, M);
+        InitialConditions(P, F, M);
+
+        // Overwrite the fields on interior cells (row-major global cell grid).
+        int nbx = nx / 16;
+        for (int ibl = 0; ibl < P.nblk; ibl++) {
+            int ib = M.blocks.active[ibl];
+            int bx = (int)llround(M.blocks.xo[ib] / (16.0 * dx));
+            int by = (int)llround(M.blocks.yo[ib] / (16.0 * dx));
+            (void)nbx;
+            for (int iy = 0; iy < 16; iy++)
+                for (int ix = 0; ix < 16; ix++) {
+                    int n = memloc(P, ix, iy, ib);
+                    size_t g = (size_t)(by * 16 + iy) * nx + (bx * 16 + ix);
+                    M.zb[n] = T(zb[g]);
+                    M.evolv.h[n] = T(h[g]);
+                    M.evolv.u[n] = T(u[g]);
+                    M.evolv.v[n] = T(v[g]);
+                    M.evolv.zs[n] = M.zb[n] + M.evolv.h[n];
+                    if (cf) M.cf[n] = T(cf[g]);
+                }
+        }
+        // Bed halo and gradients, as src/Testing.cu:583-588.
+        fillHaloC(P, M.blocks, M.zb);
+        gradientC(P, M.blocks, M.zb, M.grad.dzbdx, M.grad.dzbdy);
+        gradientHalo(P, M.blocks, M.zb, M.grad.dzbdx, M.grad.dzbdy);
+        refine_linear(P, M.blocks, M.zb, M.grad.dzbdx, M.grad.dzbdy);
+        gradientHalo(P, M.blocks, M.zb, M.grad.dzbdx, M.grad.dzbdy);
+
+        L.hugenegval = std::numeric_limits<T>::min();
+        L.hugeposval = std::numeric_limits<T>::max();
+        L.epsilon = std::numeric_limits<T>::epsilon();
+        L.totaltime = 0.0;
+        L.nextoutputtime = nextout;
+        L.dtmax = initdt(P, L, M);
+        if (gpu >= 0) {
+            SetupGPU(P, M, F, Mg);
+            Lg.hugenegval = L.hugenegval;
+            Lg.hugeposval = L.hugeposval;
+            Lg.epsilon = L.epsilon;
+            Lg.totaltime = L.totaltime;
+            Lg.nextoutputtime = L.nextoutputtime;
+            Lg.dtmax = L.dtmax;
+            // SetupGPU copies the model state; the bed halo/gradients computed above are
+            // copied again explicitly so the GPU starts from the same arrays.
+            CopytoGPU(P.nblkmem, P.blksize, M.zb, Mg.zb);
+            CopytoGPU(P.nblkmem, P.blksize, M.grad.dzbdx, Mg.grad.dzbdx);
+            CopytoGPU(P.nblkmem, P.blksize, M.grad.dzbdy, Mg.grad.dzbdy);
+        }
+        return 0;
+    }
+
+    int step(int nsteps, double* dts) override
+    {
+        for (int s = 0; s < nsteps; s++) {
+            if (gpu >= 0) {
+                updateforcing(P, Lg, F);
+                FlowGPU(P, Lg, F, Mg);
+                Lg.totaltime = Lg.totaltime + Lg.dt;
+                if (dts) dts[s] = Lg.dt;
+            } else {
+                updateforcing(P, L, F);
+                FlowCPU(P, L, F, M);
+                L.totaltime = L.totaltime + L.dt;
+                if (dts) dts[s] = L.dt;
+            }
+        }
+        return 0;
+    }
+
+    T* field(const char* name, bool devicecopy)
+    {
+        Model<T>& X = M;
+        std::string s(name);
+        T* p = nullptr;
+        if (s == "zs") p = X.evolv.zs;
+        else if (s == "h") p = X.evolv.h;
+        else if (s == "u") p = X.evolv.u;
+        else if (s == "v") p = X.evolv.v;
+        else if (s == "zb") p = X.zb;
+        else if (s == "dzbdx") p = X.grad.dzbdx;
+        else if (s == "dzbdy") p = X.grad.dzbdy;
+        else if (s == "cf") p = X.cf;
+        if (p && devicecopy && gpu >= 0) {
+            T* pg = nullptr;
+            if (s == "zs") pg = Mg.evolv.zs;
+            else if (s == "h") pg = Mg.evolv.h;
+            else if (s == "u") pg = Mg.evolv.u;
+            else if (s == "v") pg = Mg.evolv.v;
+            else if (s == "zb") pg = Mg.zb;
+            else if (s == "dzbdx") pg = Mg.grad.dzbdx;
+            else if (s == "dzbdy") pg = Mg.grad.dzbdy;
+            else if (s == "cf") pg = Mg.cf;
+            if (pg) cudaMemcpy(p, pg, sizeof(T) * (size_t)P.nblkmem * P.blksize, cudaMemcpyDeviceToHost);
+        }
+        return p;
+    }
+
+    // Full 18x18 tiles of every allocated block, in block-index order.
+    int get(const char* name, double* out) override
+    {
+        T* p = field(name, true);
+        if (!p) return -1;
+        size_t n = (size_t)P.nblk * P.blksize;
+        for (int ibl = 0; ibl < P.nblk; ibl++) {
+            int ib = M.blocks.active[ibl];
+            for (int k = 0; k < P.blksize; k++)
+                out[(size_t)ibl * P.blksize + k] = double(p[(size_t)ib * P.blksize + k]);
+        }
+        (void)n;
+        return 0;
+    }
+
+    int get_blocks(int* level, double* xo, double* yo, int* nbr8) override
+    {
+        for (int ibl = 0; ibl < P.nblk; ibl++) {
+            int ib = M.blocks.active[ibl];
+            if (level) level[ibl] = M.blocks.level[ib];
+            if (xo) xo[ibl] = double(M.blocks.xo[ib]);
+            if (yo) yo[ibl] = double(M.blocks.yo[ib]);
+            if (nbr8) {
+                int* q = nbr8 + 8 * ibl;
+                q[0] = M.blocks.LeftBot[ib];  q[1] = M.blocks.LeftTop[ib];
+                q[2] = M.blocks.RightBot[ib]; q[3] = M.blocks.RightTop[ib];
+                q[4] = M.blocks.BotLeft[ib];  q[5] = M.blocks.BotRight[ib];
+                q[6] = M.blocks.TopLeft[ib];  q[7] = M.blocks.TopRight[ib];
+            }
+        }
+        return P.nblk;
+    }
+
+    int adapt() override { return -1; }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Creates an in-memory reference model on a uniform nx*ny cell grid (multiples of 16),
+// overwriting bed and state with the given row-major cell arrays.
+void* ref_create(const char* paramtext, int use_double, int nx, int ny, double dx, double xo,
+                 double yo, const double* zb, const double* h, const double* u, const double* v,
+                 const double* cf, double nextoutputtime)
+{
+    if (use_double) {
+        auto* m = new RefModel<double>();
+        m->setup(paramtext, nx, ny, dx, xo, yo, zb, h, u, v, cf, nextoutputtime);
+        return m;
+    }
+    auto* m = new RefModel<float>();
+    m->setup(paramtext, nx, ny, dx, xo, yo, zb, h, u, v, cf, nextoutputtime);
+    return m;
+}
+
+// Adds a boundary segment on one side BEFORE ref_create is not possible through this
+// surface; segments are instead declared in paramtext with the reference's own keys
+// ("left = 2,file" needs a file), so uniform series are injected here after creation.
+int ref_set_segment_series(void* hdl, int iseg, int n, const double* t, const double* wl)
+{
+    RefBase* m = (RefBase*)hdl;
+    if (iseg < 0 || iseg >= (int)m->F.bndseg.size()) return -1;
+    bndsegment& s = m->F.bndseg[iseg];
+    s.data.clear();
+    for (int k = 0; k < n; k++) {
+        Windin w;
+        w.time = t[k];
+        w.wspeed = wl[k];
+        s.data.push_back(w);
+    }
+    s.on = true;
+    s.uniform = true;
+    return 0;
+}
+
+int ref_set_rain_series(void* hdl, int n, const double* t, const double* r)
+{
+    RefBase* m = (RefBase*)hdl;
+    m->F.Rain.inputfile = "uniform_rain_series";
+    m->F.Rain.uniform = true;
+    m->F.Rain.unidata.clear();
+    for (int k = 0; k < n; k++) {
+        Windin w;
+        w.time = t[k];
+        w.wspeed = r[k];
+        m->F.Rain.unidata.push_back(w);
+    }
+    return 0;
+}
+
+int ref_step(void* hdl, int nsteps, double* dts) { return ((RefBase*)hdl)->step(nsteps, dts); }
+int ref_nblk(void* hdl) { return ((RefBase*)hdl)->P.nblk; }
+int ref_nseg(void* hdl) { return (int)((RefBase*)hdl)->F.bndseg.size(); }
+int ref_get(void* hdl, const char* name, double* out) { return ((RefBase*)hdl)->get(name, out); }
+int ref_get_blocks(void* hdl, int* level, double* xo, double* yo, int* nbr8)
+{
+    return ((RefBase*)hdl)->get_blocks(level, xo, yo, nbr8);
+}
+void ref_destroy(void* hdl) { delete (RefBase*)hdl; }
+
+}

@@ -1,0 +1,301 @@
+#!/usr/bin/env python
+"""Flow-step benchmark: cell-updates/s of the B200 library on the wet/dry run-up
+workload (1024x1024 cells of 16x16 blocks, dx = 0.05 m, conical island, Manning
+n = 0.01, solitary wave entering from the west), one JSON line on stdout.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+A step is one full flow step (predictor + corrector) of the whole grid.
+* value:   device time of K steps (CUDA events around the two kernels on the
+           library's stream), L2 flushed before every step, max over ranks.
+* e2e:     the same K steps through the C ABI with host buffers: state upload
+           from host, K bgf_flow_step calls (each returns dt to the host), state
+           download; wall clock.
+* roofline: the dominant kernel's algorithmic bytes per launch / its mean event
+           time, against the measured HBM copy bandwidth.
+* cpu_baseline: the reference BG_Flood FlowCPU (built from its sources,
+           oracle/_ref) on a 256x256 window of the same workload.
+With N > 1 (torchrun) every rank runs its own replica of the scenario: the path
+has no exchange step between independent scenarios (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "cell-updates/s"
+UNIT = "cell-updates/s"
+WORKLOAD = "wet/dry run-up 1024x1024 cells (16x16 blocks), dx=0.05 m, conical island, solitary wave, Manning n=0.01"
+ALG_BYTES_FLUX = 28    # h,u,v,zb read + dh,dhu,dhv written (FP32)
+ALG_BYTES_UPDATE = 40  # h,u,v,dh,dhu,dhv,zb read + h,u,v written (FP32)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=1024, help="grid cells per side")
+    ap.add_argument("--engine", type=int, default=1)
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons with NVML while the timed region runs."""
+
+    def __init__(self, dev: int):
+        self.samples, self.reasons = [], set()
+        self.stop_ev = threading.Event()
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(dev)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        names = {}
+        for attr in ("HW_SLOWDOWN", "HW_THERMAL_SLOWDOWN", "SW_THERMAL_SLOWDOWN", "SW_POWER_CAP", "HW_POWER_BRAKE_SLOWDOWN"):
+            v = getattr(nv, "nvmlClocksEventReason" + "".join(w.title() for w in attr.split("_")), None) or \
+                getattr(nv, "nvmlClocksThrottleReason" + "".join(w.title() for w in attr.split("_")), None)
+            if v is not None:
+                names[attr.lower()] = v
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                try:
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except Exception:
+                    r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                for n, bit in names.items():
+                    if r & bit:
+                        self.reasons.add(n)
+            except Exception:
+                pass
+            time.sleep(0.05)
+
+    def __enter__(self):
+        if self.nv:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.nv:
+            self.stop_ev.set()
+            self.t.join()
+
+    def summary(self):
+        med = float(np.median(self.samples)) if self.samples else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def workload_case(n: int, engine: int, dev: int):
+    import cases
+    case = cases.conical_island(n, engine=engine, dx=0.05 * 1024 / n if n != 1024 else 0.05)
+    case.param.GPUDEVICE = dev
+    return case
+
+
+def cpu_reference_sample(steps: int, warmup: int, engine: int):
+    """The reference FlowCPU on a 256x256 window of the workload (oracle/_ref), or the
+    C restatement when the reference build is absent.  Returns (cells/s, kind, steps)."""
+    import cases
+    from oracle.pyoracle import ref_available
+    case = cases.conical_island(256, engine=engine, dx=0.05)
+    ncell = 256 * 256
+    if ref_available():
+        from runners import make_reference
+        r = make_reference(case)
+        r.step(warmup)
+        t0 = time.perf_counter()
+        r.step(steps)
+        dt = time.perf_counter() - t0
+        return ncell * steps / dt, "reference", dt
+    from runners import make_oracle
+    o, _ = make_oracle(case)
+    o.step(warmup)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return ncell * steps / dt, "port", dt
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    nthreads = min(8, os.cpu_count() or 1)
+    steps = max(1, args.steps if args.steps <= 20 else 10)
+    val, kind, secs = cpu_reference_sample(steps, min(args.warmup, 3), args.engine)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": min(args.warmup, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": "256x256 window of the workload", "engine": args.engine},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthreads, "kind": kind,
+                         "sample": f"{steps} FlowCPU steps on a 256x256 window ({secs:.1f} s)"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from runners import make_gpu
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    case = workload_case(args.n, args.engine, local)
+    f, mesh, loop = make_gpu(case)
+    ncell = mesh.nblk * 256
+
+    for _ in range(args.warmup):
+        loop.totaltime += f.flow_step(loop)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    f.set_profiling(True)
+    launches0 = f.kernel_launches()
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with clocks:
+        for _ in range(args.steps):
+            flush.zero_()                 # L2 (126 MB) flushed before every timed step
+            torch.cuda.synchronize()
+            loop.totaltime += f.flow_step(loop)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    flux_ms, update_ms, nprof = f.kernel_timing()
+    launches = f.kernel_launches() - launches0
+    f.set_profiling(False)
+    step_ms = (flux_ms + update_ms) / max(nprof, 1)
+    tot_ms = torch.tensor([flux_ms + update_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(tot_ms, op=dist.ReduceOp.MAX)
+    tmax_s = float(tot_ms.item()) / 1e3
+    value = world * ncell * args.steps / tmax_s
+
+    # dominant kernel roofline
+    peak, peak_kind = measured_peak_hbm()
+    kern = {"flux_kernel": (flux_ms / nprof, ALG_BYTES_FLUX), "update_kernel": (update_ms / nprof, ALG_BYTES_UPDATE)}
+    dom = max(kern, key=lambda k: kern[k][0])
+    dom_ms, dom_b = kern[dom]
+    achieved = dom_b * ncell / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", f"{dom}_traffic.txt")
+    if os.path.exists(tfile):
+        for ln in open(tfile):
+            if ln.startswith("dram_bytes_per_cell:"):
+                traffic = float(ln.split(":")[1]) * ncell
+
+    # end to end through the C ABI with host buffers
+    zs, h, u, v = f.get_state()
+    e2e_loop = type(loop)(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=case.nextoutputtime)
+    f.init_dt(e2e_loop)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f.set_state(h, u, v)
+    for _ in range(args.steps):
+        e2e_loop.totaltime += f.flow_step(e2e_loop)
+    zs2, h2, u2, v2 = f.get_state()
+    e2e_s = time.perf_counter() - t0
+    tslot = 80
+    h2d = (3 * ncell * 4 + args.steps * (tslot + 8)) / args.steps
+    d2h = ((3 * ncell + mesh.nblk * 324) * 4 + args.steps * tslot) / args.steps
+    e2e_val = world * ncell * args.steps / e2e_s
+
+    extra = {}
+    if not args.no_extra and rank == 0:
+        # production mode: the device-resident loop (CUDA graphs), L2-warm, same workload
+        l2 = type(loop)(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=1e30)
+        f.init_dt(l2)
+        f.run(l2, endtime=1e30, maxsteps=20)
+        f.run(l2, endtime=1e30, maxsteps=400)
+        ms, nl = f.last_run_timing()
+        extra["device_loop_L2_resident"] = {"value": ncell * 400 / (ms / 1e3), "steps": 400, "ms": ms}
+        del f
+        # a grid well above L2 (4096^2 cells, ~1 GB of state): HBM-bound device loop
+        big = workload_case(4096, args.engine, local)
+        fb, mb, lb = make_gpu(big)
+        fb.run(lb, endtime=1e30, maxsteps=10)
+        fb.run(lb, endtime=1e30, maxsteps=100)
+        msb, _ = fb.last_run_timing()
+        extra["device_loop_4096x4096"] = {"value": mb.nblk * 256 * 100 / (msb / 1e3), "steps": 100, "ms": msb}
+        del fb
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cv, kind, secs = cpu_reference_sample(8, 1, args.engine)
+        cpu = {"value": cv, "unit": UNIT, "cores": min(8, os.cpu_count() or 1), "kind": kind,
+               "sample": f"8 FlowCPU steps on a 256x256 window of the workload ({secs:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": ncell, "blocks": mesh.nblk, "engine": args.engine,
+                       "l2": "flushed (256 MB write) before every timed step", "parallelism":
+                       f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "alg_bytes_per_cell": dom_b},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "kernels_ms_per_step": {"flux_kernel": flux_ms / nprof, "update_kernel": update_ms / nprof},
+            "extra": extra,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,863 @@
+// C-ABI of the flow-step library (include/bg_flood_b200.h): handle life cycle,
+// BUQ-layout uploads/downloads, boundary segments, the single-step entry point
+// that stands in for FlowGPU, and the device-resident time loop.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/bg_flood_b200.h"
+#include "bgf_flow.cuh"
+#include "bgf_internal.h"
+
+using namespace bgf;
+
+static thread_local std::string g_last_error;
+
+#define BGF_CUDA(call)                                                                 \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);         \
+            return BGF_ECUDA;                                                          \
+        }                                                                              \
+    } while (0)
+
+struct HostSeg {
+    int type;
+    std::vector<double> t, wl;
+    std::vector<int> blk[4];
+};
+
+struct bgf_handle {
+    bgf_param P;
+    int nblkmem = 0, nblk = 0, dbl = 0, dev = 0;
+    size_t esz = 4;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // host copies of the tables
+    std::vector<int> active, level, nbr;  // nbr as [8][nblkmem]
+    std::vector<HostSeg> segs;
+    std::vector<double> rain_t, rain_r;
+    // device buffers
+    int *d_active = nullptr, *d_level = nullptr, *d_nbr = nullptr, *d_bndseg = nullptr, *d_err = nullptr;
+    void *d_zb = nullptr, *d_dzbdx = nullptr, *d_dzbdy = nullptr, *d_cf = nullptr;
+    uint8_t* d_rainmask = nullptr;
+    float* d_qmean = nullptr;
+    SegDev* d_segs = nullptr;
+    double *d_seg_t = nullptr, *d_seg_wl = nullptr, *d_rain_t = nullptr, *d_rain_r = nullptr;
+    void *d_h[2] = {nullptr, nullptr}, *d_u[2] = {nullptr, nullptr}, *d_v[2] = {nullptr, nullptr};
+    void *d_dh = nullptr, *d_dhu = nullptr, *d_dhv = nullptr;
+    TimeState* d_time = nullptr;
+    unsigned long long* d_dtmin = nullptr;
+    double* d_scratch = nullptr;
+    TimeState* h_time = nullptr;  // pinned
+    int cur = 0, parity = 0;
+    bool has_blocks = false, has_bed = false, has_state = false, has_cf = false, has_rainmask = false;
+    int nseg_dev = 0, rain_n_dev = 0;
+    int64_t launches = 0;
+    // graph of two consecutive steps (parities p, p^1)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graph_valid = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_run_ms = 0.0;
+    int64_t last_run_launches = 0;
+    // per-kernel timing of bgf_flow_step (CUDA events on the handle's stream)
+    int profiling = 0;
+    cudaEvent_t pev[3] = {nullptr, nullptr, nullptr};
+    double flux_ms = 0.0, update_ms = 0.0;
+    int64_t profiled_steps = 0;
+    // pinned staging buffer for host <-> device copies of BUQ fields
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+// ---------------------------------------------------------------- helpers
+
+template <class T> static DevModel<T> dev_model(bgf_handle* h)
+{
+    DevModel<T> m;
+    m.nblk = h->nblk;
+    m.nblkmem = h->nblkmem;
+    m.active = h->d_active;
+    m.level = h->d_level;
+    m.nbr = h->d_nbr;
+    m.zb = (const T*)h->d_zb;
+    m.dzbdx = (const T*)h->d_dzbdx;
+    m.dzbdy = (const T*)h->d_dzbdy;
+    m.cf = h->has_cf ? (const T*)h->d_cf : nullptr;
+    m.rainmask = h->has_rainmask ? h->d_rainmask : nullptr;
+    m.bndseg = h->d_bndseg;
+    m.qmean = h->d_qmean;
+    m.segs = h->d_segs;
+    m.seg_t = h->d_seg_t;
+    m.seg_wl = h->d_seg_wl;
+    m.rain_t = h->d_rain_t;
+    m.rain_r = h->d_rain_r;
+    for (int k = 0; k < 2; k++) {
+        m.h[k] = (T*)h->d_h[k];
+        m.u[k] = (T*)h->d_u[k];
+        m.v[k] = (T*)h->d_v[k];
+    }
+    m.dh = (T*)h->d_dh;
+    m.dhu = (T*)h->d_dhu;
+    m.dhv = (T*)h->d_dhv;
+    m.time = h->d_time;
+    m.dtmin = h->d_dtmin;
+    m.err = h->d_err;
+    return m;
+}
+
+template <class T> static StepParams<T> step_params(const bgf_handle* h)
+{
+    const bgf_param& P = h->P;
+    StepParams<T> p;
+    p.g = (T)P.g;
+    p.eps = (T)P.eps;
+    p.CFL = (T)P.CFL;
+    p.theta = (T)P.theta;
+    p.delta0 = (T)P.delta;
+    p.epsi = std::nextafter((T)1.0, (T)2.0) - (T)1.0;
+    p.epsface = (T)P.eps + p.epsi;
+    // Coriolis factor of updateEVCPU (src/Advection.cu:187) for a Cartesian grid
+    p.fc = (T)((double)std::sin((T)(P.lat * 3.14159265 / 180.0)) * 3.14159265 / (double)(T)21600.0);
+    p.eps_d = P.eps;
+    p.dtparam = P.dt;
+    p.bndfiltertime = P.bndfiltertime;
+    p.bndrelaxtime = P.bndrelaxtime;
+    p.bndtaper = P.bndtaper;
+    p.inittime = P.inittime;
+    p.zsinit = P.zsinit;
+    p.zsoffset = std::isnan(P.zsoffset) ? 0.0 : P.zsoffset;
+    p.dtmin = P.dtmin;
+    p.cf = (T)P.cf;
+    p.frictionmodel = P.frictionmodel;
+    p.forcemass = P.ForceMassConserve;
+    p.has_cf = h->has_cf ? 1 : 0;
+    p.has_rain = h->rain_n_dev > 0 ? 1 : 0;
+    p.nseg = h->nseg_dev;
+    p.rain_n = h->rain_n_dev;
+    return p;
+}
+
+static int set_device(bgf_handle* h)
+{
+    BGF_CUDA(cudaSetDevice(h->dev));
+    return BGF_OK;
+}
+
+template <class T> static T epsi_of() { return std::nextafter((T)1.0, (T)2.0) - (T)1.0; }
+
+static unsigned long long dt_init_bits(int dbl)
+{
+    if (dbl) {
+        double v = 1.0 / epsi_of<double>();
+        unsigned long long b;
+        memcpy(&b, &v, 8);
+        return b;
+    }
+    float v = 1.0f / epsi_of<float>();
+    unsigned int b;
+    memcpy(&b, &v, 4);
+    return (unsigned long long)b;
+}
+
+static void free_graphs(bgf_handle* h)
+{
+    for (int k = 0; k < 2; k++)
+        if (h->graph[k]) {
+            cudaGraphExecDestroy(h->graph[k]);
+            h->graph[k] = nullptr;
+        }
+    h->graph_valid = false;
+}
+
+// Reads a BUQ field of the caller's precision into a T vector.
+template <class T> static void buq_to(const void* src, int dbl, size_t n, std::vector<T>& out)
+{
+    out.resize(n);
+    if (dbl) for (size_t k = 0; k < n; k++) out[k] = (T)((const double*)src)[k];
+    else for (size_t k = 0; k < n; k++) out[k] = (T)((const float*)src)[k];
+}
+
+// Pinned staging area of at least `bytes` (grown on demand, kept for the handle).
+static void* staging(bgf_handle* h, size_t bytes)
+{
+    if (h->pinned_bytes < bytes) {
+        if (h->pinned) cudaFreeHost(h->pinned);
+        h->pinned = nullptr;
+        h->pinned_bytes = 0;
+        if (cudaMallocHost(&h->pinned, bytes) != cudaSuccess) return nullptr;
+        h->pinned_bytes = bytes;
+    }
+    return h->pinned;
+}
+
+// ---------------------------------------------------------------- C ABI
+// (C linkage comes from the declarations in include/bg_flood_b200.h)
+
+
+void bgf_param_default(bgf_param* p)
+{
+    memset(p, 0, sizeof(*p));
+    p->g = 9.81;
+    p->eps = 0.0001;
+    p->dt = 0.0;
+    p->CFL = 0.5;
+    p->theta = 1.3;
+    p->cf = 0.0001;
+    p->dx = NAN;
+    p->delta = NAN;
+    p->xo = 0.0;
+    p->yo = 0.0;
+    p->lat = 0.0;
+    p->zsinit = NAN;
+    p->zsoffset = 0.0;
+    p->bndtaper = 0.0;
+    p->bndrelaxtime = 3600.0;
+    p->bndfiltertime = 60.0;
+    p->inittime = 0.0;
+    p->dtmin = 0.0005;
+    p->dtinit = -1;
+    p->mask = 9999.0;
+    p->engine = 1;
+    p->frictionmodel = 0;
+    p->ForceMassConserve = 0;
+    p->wetdryfix = 1;
+    p->conserveElevation = 0;
+    p->doubleprecision = 0;
+    p->minlevel = 0;
+    p->maxlevel = 0;
+    p->initlevel = 0;
+    p->aoibnd = 0;
+    p->rainbnd = 0;
+    p->GPUDEVICE = 0;
+}
+
+const char* bgf_strerror(int s)
+{
+    switch (s) {
+        case BGF_OK: return "ok";
+        case BGF_EINVAL: return "invalid argument or unsupported configuration";
+        case BGF_ECUDA: return "CUDA runtime error";
+        case BGF_ENOMEM: return "device allocation failed";
+        case BGF_EDT_UNDERFLOW: return "time step fell below dtmin (model crash)";
+        case BGF_ENAN: return "non-finite value in the state";
+        case BGF_ESTATE: return "call out of order";
+        case BGF_EBUDGET: return "request exceeds the memory budget";
+        case BGF_ETIMEOUT: return "bounded wait gave up";
+        case BGF_ENOKERNEL: return "CUDA kernels unavailable on this device";
+    }
+    return "unknown status";
+}
+
+const char* bgf_last_error(void) { return g_last_error.c_str(); }
+
+int bgf_device_supported(int dev)
+{
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return 0;
+    return prop.major == 10 && prop.minor == 0;
+}
+
+int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
+{
+    if (!p || !out || nblkmem <= 0) return BGF_EINVAL;
+    if (p->engine != 1 && p->engine != 2) return BGF_EINVAL;
+    if (p->conserveElevation) return BGF_EINVAL;
+    if (!(p->delta > 0.0)) return BGF_EINVAL;
+    *out = nullptr;
+    bgf_handle* h = new bgf_handle();
+    h->P = *p;
+    h->nblkmem = nblkmem;
+    h->dbl = p->doubleprecision ? 1 : 0;
+    h->esz = h->dbl ? 8 : 4;
+    h->dev = p->GPUDEVICE;
+    int rc;
+    if ((rc = set_device(h)) != BGF_OK) { delete h; return rc; }
+    if (!bgf_device_supported(h->dev)) {
+        g_last_error = "device is not sm_100 (the library is built for sm_100a)";
+        delete h;
+        return BGF_ENOKERNEL;
+    }
+    cudaError_t e = h->dbl ? configure_kernels<double>() : configure_kernels<float>();
+    if (e != cudaSuccess) {
+        g_last_error = std::string("configure kernels: ") + cudaGetErrorString(e);
+        delete h;
+        return BGF_ENOKERNEL;
+    }
+    if (stream) h->stream = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return BGF_ECUDA; }
+        h->own_stream = true;
+    }
+    size_t nb = (size_t)nblkmem;
+    size_t es = h->esz;
+    struct A { void** p; size_t bytes; } allocs[] = {
+        {(void**)&h->d_active, nb * sizeof(int)},        {(void**)&h->d_level, nb * sizeof(int)},
+        {(void**)&h->d_nbr, 8 * nb * sizeof(int)},       {(void**)&h->d_bndseg, 4 * nb * sizeof(int)},
+        {(void**)&h->d_err, sizeof(int)},                {&h->d_zb, nb * 324 * es},
+        {&h->d_dzbdx, nb * 324 * es},                    {&h->d_dzbdy, nb * 324 * es},
+        {&h->d_cf, nb * 256 * es},                       {(void**)&h->d_rainmask, nb * 256},
+        {(void**)&h->d_qmean, nb * 64 * sizeof(float)},  {&h->d_h[0], nb * 256 * es},
+        {&h->d_h[1], nb * 256 * es},                     {&h->d_u[0], nb * 256 * es},
+        {&h->d_u[1], nb * 256 * es},                     {&h->d_v[0], nb * 256 * es},
+        {&h->d_v[1], nb * 256 * es},                     {&h->d_dh, nb * 256 * es},
+        {&h->d_dhu, nb * 256 * es},                      {&h->d_dhv, nb * 256 * es},
+        {(void**)&h->d_time, 2 * sizeof(TimeState)},     {(void**)&h->d_dtmin, 2 * sizeof(unsigned long long)},
+        {(void**)&h->d_scratch, 8 * sizeof(double)},
+    };
+    for (auto& a : allocs) {
+        if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
+            g_last_error = "cudaMalloc failed";
+            bgf_destroy(h);
+            return BGF_ENOMEM;
+        }
+    }
+    cudaMemsetAsync(h->d_bndseg, 0xff, 4 * nb * sizeof(int), h->stream);
+    cudaMemsetAsync(h->d_qmean, 0, nb * 64 * sizeof(float), h->stream);
+    cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
+    cudaMemsetAsync(h->d_dh, 0, nb * 256 * es, h->stream);
+    cudaMemsetAsync(h->d_dhu, 0, nb * 256 * es, h->stream);
+    cudaMemsetAsync(h->d_dhv, 0, nb * 256 * es, h->stream);
+    if (cudaMallocHost((void**)&h->h_time, 2 * sizeof(TimeState)) != cudaSuccess) {
+        bgf_destroy(h);
+        return BGF_ENOMEM;
+    }
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    for (int k = 0; k < 3; k++) cudaEventCreate(&h->pev[k]);
+    *out = h;
+    return BGF_OK;
+}
+
+int bgf_destroy(bgf_handle* h)
+{
+    if (!h) return BGF_EINVAL;
+    cudaSetDevice(h->dev);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_graphs(h);
+    void* ptrs[] = {h->d_active, h->d_level, h->d_nbr, h->d_bndseg, h->d_err, h->d_zb, h->d_dzbdx, h->d_dzbdy,
+                    h->d_cf, h->d_rainmask, h->d_qmean, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t,
+                    h->d_rain_r, h->d_h[0], h->d_h[1], h->d_u[0], h->d_u[1], h->d_v[0], h->d_v[1], h->d_dh,
+                    h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->h_time) cudaFreeHost(h->h_time);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    for (int k = 0; k < 3; k++)
+        if (h->pev[k]) cudaEventDestroy(h->pev[k]);
+    if (h->pinned) cudaFreeHost(h->pinned);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return BGF_OK;
+}
+
+static int rebuild_segments(bgf_handle* h);
+
+int bgf_set_blocks(bgf_handle* h, const bgf_blockp* b)
+{
+    if (!h || !b || b->nblk <= 0 || b->nblk > h->nblkmem || !b->active || !b->level) return BGF_EINVAL;
+    const int* tabs[8] = {b->LeftBot, b->LeftTop, b->RightBot, b->RightTop, b->BotLeft, b->BotRight, b->TopLeft, b->TopRight};
+    for (int k = 0; k < 8; k++)
+        if (!tabs[k]) return BGF_EINVAL;
+    int nb = h->nblkmem;
+    h->nblk = b->nblk;
+    h->active.assign(b->active, b->active + b->nblk);
+    h->level.assign(b->level, b->level + nb);
+    h->nbr.assign((size_t)8 * nb, 0);
+    for (int k = 0; k < 8; k++)
+        for (int ib = 0; ib < nb; ib++) h->nbr[(size_t)k * nb + ib] = tabs[k][ib];
+    for (int ibl = 0; ibl < b->nblk; ibl++) {
+        int ib = b->active[ibl];
+        if (ib < 0 || ib >= nb) return BGF_EINVAL;
+        for (int k = 0; k < 8; k++) {
+            int q = tabs[k][ib];
+            if (q < 0 || q >= nb) return BGF_EINVAL;
+        }
+    }
+    int rc = set_device(h);
+    if (rc) return rc;
+    BGF_CUDA(cudaMemcpyAsync(h->d_active, h->active.data(), sizeof(int) * b->nblk, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_level, h->level.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_nbr, h->nbr.data(), sizeof(int) * 8 * nb, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    h->has_blocks = true;
+    free_graphs(h);
+    return rebuild_segments(h);
+}
+
+template <class T>
+static int set_bed_t(bgf_handle* h, const void* zb, const void* dzbdx, const void* dzbdy, const void* cf,
+                     const int* activeCell)
+{
+    size_t nb = h->nblkmem;
+    std::vector<T> z, gx, gy;
+    buq_to<T>(zb, h->dbl, nb * 324, z);
+    if (dzbdx && dzbdy) {
+        buq_to<T>(dzbdx, h->dbl, nb * 324, gx);
+        buq_to<T>(dzbdy, h->dbl, nb * 324, gy);
+    } else {
+        gx.assign(nb * 324, (T)0);
+        gy.assign(nb * 324, (T)0);
+        int rc = host_bed_gradients<T>(h->nblk, h->active.data(), h->level.data(), h->nbr.data(), h->nblkmem,
+                                       h->P.delta, h->P.theta, z.data(), gx.data(), gy.data());
+        if (rc) return rc;
+    }
+    BGF_CUDA(cudaMemcpy(h->d_zb, z.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
+    BGF_CUDA(cudaMemcpy(h->d_dzbdx, gx.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
+    BGF_CUDA(cudaMemcpy(h->d_dzbdy, gy.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
+    h->has_cf = cf != nullptr;
+    if (cf) {
+        std::vector<T> c(nb * 256);
+        for (size_t ib = 0; ib < nb; ib++)
+            for (int j = 0; j < 16; j++)
+                for (int i = 0; i < 16; i++) {
+                    size_t s = ib * 324 + (i + 1) + (j + 1) * 18;
+                    c[ib * 256 + j * 16 + i] = h->dbl ? (T)((const double*)cf)[s] : (T)((const float*)cf)[s];
+                }
+        BGF_CUDA(cudaMemcpy(h->d_cf, c.data(), nb * 256 * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    h->has_rainmask = activeCell != nullptr;
+    if (activeCell) {
+        std::vector<uint8_t> r(nb * 256);
+        for (size_t ib = 0; ib < nb; ib++)
+            for (int j = 0; j < 16; j++)
+                for (int i = 0; i < 16; i++) r[ib * 256 + j * 16 + i] = (uint8_t)(activeCell[ib * 324 + (i + 1) + (j + 1) * 18] != 0);
+        BGF_CUDA(cudaMemcpy(h->d_rainmask, r.data(), nb * 256, cudaMemcpyHostToDevice));
+    }
+    h->has_bed = true;
+    free_graphs(h);
+    return BGF_OK;
+}
+
+int bgf_set_bed(bgf_handle* h, const void* zb, const void* dzbdx, const void* dzbdy, const void* cf,
+                const int* activeCell)
+{
+    if (!h || !zb) return BGF_EINVAL;
+    if (!h->has_blocks) return BGF_ESTATE;
+    int rc = set_device(h);
+    if (rc) return rc;
+    return h->dbl ? set_bed_t<double>(h, zb, dzbdx, dzbdy, cf, activeCell)
+                  : set_bed_t<float>(h, zb, dzbdx, dzbdy, cf, activeCell);
+}
+
+// Per-block side -> segment table.  A block belongs to one segment; each of its
+// domain-edge sides is handled by that segment, in the segment order of
+// FlowbndFlux (src/Boundary.cu:108-195).
+static int rebuild_segments(bgf_handle* h)
+{
+    int nb = h->nblkmem;
+    std::vector<int> side(4 * (size_t)nb, -1);
+    std::vector<SegDev> sd;
+    std::vector<double> st, swl;
+    for (size_t k = 0; k < h->segs.size(); k++) {
+        const HostSeg& s = h->segs[k];
+        SegDev d;
+        d.type = s.type;
+        d.n = (int)s.t.size();
+        d.off = (int)st.size();
+        d.pad = 0;
+        sd.push_back(d);
+        st.insert(st.end(), s.t.begin(), s.t.end());
+        swl.insert(swl.end(), s.wl.begin(), s.wl.end());
+        for (int sidx = 0; sidx < 4; sidx++)
+            for (int ib : s.blk[sidx]) {
+                if (ib < 0 || ib >= nb) return BGF_EINVAL;
+                side[(size_t)ib * 4 + sidx] = (int)k;
+            }
+    }
+    int rc = set_device(h);
+    if (rc) return rc;
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->d_segs) { cudaFree(h->d_segs); h->d_segs = nullptr; }
+    if (h->d_seg_t) { cudaFree(h->d_seg_t); h->d_seg_t = nullptr; }
+    if (h->d_seg_wl) { cudaFree(h->d_seg_wl); h->d_seg_wl = nullptr; }
+    size_t ns = std::max<size_t>(1, sd.size()), nt = std::max<size_t>(1, st.size());
+    BGF_CUDA(cudaMalloc((void**)&h->d_segs, ns * sizeof(SegDev)));
+    BGF_CUDA(cudaMalloc((void**)&h->d_seg_t, nt * sizeof(double)));
+    BGF_CUDA(cudaMalloc((void**)&h->d_seg_wl, nt * sizeof(double)));
+    if (!sd.empty()) BGF_CUDA(cudaMemcpy(h->d_segs, sd.data(), sd.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
+    if (!st.empty()) {
+        BGF_CUDA(cudaMemcpy(h->d_seg_t, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
+        BGF_CUDA(cudaMemcpy(h->d_seg_wl, swl.data(), swl.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    BGF_CUDA(cudaMemcpy(h->d_bndseg, side.data(), side.size() * sizeof(int), cudaMemcpyHostToDevice));
+    h->nseg_dev = (int)sd.size();
+    free_graphs(h);
+    return BGF_OK;
+}
+
+int bgf_add_bnd_segment(bgf_handle* h, int type, int n, const double* t, const double* wl, const int nblk_side[4],
+                        const int* const blk_side[4])
+{
+    if (!h || type < 0 || type > 3 || n < 0 || (n > 0 && (!t || !wl)) || n == 1) return BGF_EINVAL;
+    HostSeg s;
+    s.type = type;
+    for (int k = 0; k < n; k++) {
+        s.t.push_back(t[k]);
+        s.wl.push_back(wl[k]);
+    }
+    for (int sd = 0; sd < 4; sd++) {
+        int c = nblk_side ? nblk_side[sd] : 0;
+        if (c < 0) return BGF_EINVAL;
+        for (int k = 0; k < c; k++) s.blk[sd].push_back(blk_side[sd][k]);
+    }
+    h->segs.push_back(s);
+    return rebuild_segments(h);
+}
+
+int bgf_set_rain_series(bgf_handle* h, int n, const double* t, const double* r)
+{
+    if (!h || n < 0 || n == 1 || (n > 0 && (!t || !r))) return BGF_EINVAL;
+    int rc = set_device(h);
+    if (rc) return rc;
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->d_rain_t) { cudaFree(h->d_rain_t); h->d_rain_t = nullptr; }
+    if (h->d_rain_r) { cudaFree(h->d_rain_r); h->d_rain_r = nullptr; }
+    h->rain_n_dev = n;
+    if (n > 0) {
+        BGF_CUDA(cudaMalloc((void**)&h->d_rain_t, n * sizeof(double)));
+        BGF_CUDA(cudaMalloc((void**)&h->d_rain_r, n * sizeof(double)));
+        BGF_CUDA(cudaMemcpy(h->d_rain_t, t, n * sizeof(double), cudaMemcpyHostToDevice));
+        BGF_CUDA(cudaMemcpy(h->d_rain_r, r, n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    free_graphs(h);
+    return BGF_OK;
+}
+
+template <class T> static int set_state_t(bgf_handle* h, const bgf_evolving* ev)
+{
+    size_t nb = h->nblkmem;
+    T* a = (T*)staging(h, 3 * nb * 256 * sizeof(T));
+    if (!a) return BGF_ENOMEM;
+    void* dst[3] = {h->d_h[h->cur], h->d_u[h->cur], h->d_v[h->cur]};
+    const void* src[3] = {ev->h, ev->u, ev->v};
+    for (int f = 0; f < 3; f++) {
+        T* o = a + f * nb * 256;
+        for (size_t ib = 0; ib < nb; ib++)
+            for (int j = 0; j < 16; j++)
+                for (int i = 0; i < 16; i++) {
+                    size_t s = ib * 324 + (i + 1) + (j + 1) * 18;
+                    o[ib * 256 + j * 16 + i] = h->dbl ? (T)((const double*)src[f])[s] : (T)((const float*)src[f])[s];
+                }
+        BGF_CUDA(cudaMemcpyAsync(dst[f], o, nb * 256 * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    }
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    h->has_state = true;
+    return BGF_OK;
+}
+
+int bgf_set_state(bgf_handle* h, const bgf_evolving* ev)
+{
+    if (!h || !ev || !ev->h || !ev->u || !ev->v) return BGF_EINVAL;
+    int rc = set_device(h);
+    if (rc) return rc;
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    return h->dbl ? set_state_t<double>(h, ev) : set_state_t<float>(h, ev);
+}
+
+template <class T> static int get_state_t(bgf_handle* h, bgf_evolving* ev)
+{
+    size_t nb = h->nblkmem;
+    T* a = (T*)staging(h, (3 * nb * 256 + nb * 324) * sizeof(T));
+    if (!a) return BGF_ENOMEM;
+    T *hh = a, *uu = a + nb * 256, *vv = a + 2 * nb * 256, *zb = a + 3 * nb * 256;
+    BGF_CUDA(cudaMemcpyAsync(hh, h->d_h[h->cur], nb * 256 * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(uu, h->d_u[h->cur], nb * 256 * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(vv, h->d_v[h->cur], nb * 256 * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(zb, h->d_zb, nb * 324 * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    for (int ibl = 0; ibl < h->nblk; ibl++) {
+        size_t ib = h->active[ibl];
+        for (int j = 0; j < 16; j++)
+            for (int i = 0; i < 16; i++) {
+                size_t d = ib * 324 + (i + 1) + (j + 1) * 18, s = ib * 256 + j * 16 + i;
+                T z = zb[d] + hh[s];
+                if (h->dbl) {
+                    if (ev->h) ((double*)ev->h)[d] = (double)hh[s];
+                    if (ev->u) ((double*)ev->u)[d] = (double)uu[s];
+                    if (ev->v) ((double*)ev->v)[d] = (double)vv[s];
+                    if (ev->zs) ((double*)ev->zs)[d] = (double)z;
+                } else {
+                    if (ev->h) ((float*)ev->h)[d] = (float)hh[s];
+                    if (ev->u) ((float*)ev->u)[d] = (float)uu[s];
+                    if (ev->v) ((float*)ev->v)[d] = (float)vv[s];
+                    if (ev->zs) ((float*)ev->zs)[d] = (float)z;
+                }
+            }
+    }
+    return BGF_OK;
+}
+
+int bgf_get_state(bgf_handle* h, bgf_evolving* ev)
+{
+    if (!h || !ev) return BGF_EINVAL;
+    if (!h->has_state) return BGF_ESTATE;
+    int rc = set_device(h);
+    if (rc) return rc;
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    return h->dbl ? get_state_t<double>(h, ev) : get_state_t<float>(h, ev);
+}
+
+static int check_ready(bgf_handle* h)
+{
+    if (!h) return BGF_EINVAL;
+    if (!h->has_blocks || !h->has_bed || !h->has_state) return BGF_ESTATE;
+    return set_device(h);
+}
+
+static int check_err_word(bgf_handle* h)
+{
+    int err = 0;
+    BGF_CUDA(cudaMemcpy(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        g_last_error = "mesh has cross-level neighbours, which this build does not support yet";
+        return BGF_EINVAL;
+    }
+    return BGF_OK;
+}
+
+template <class T> static int init_dt_t(bgf_handle* h, bgf_loop* loop)
+{
+    unsigned long long init = dt_init_bits(h->dbl);
+    BGF_CUDA(cudaMemcpyAsync(h->d_dtmin, &init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
+    DevModel<T> m = dev_model<T>(h);
+    StepParams<T> p = step_params<T>(h);
+    launch_initdt<T>(m, p, h->cur, h->d_dtmin, h->stream);
+    h->launches++;
+    BGF_CUDA(cudaGetLastError());
+    unsigned long long bits = 0;
+    BGF_CUDA(cudaMemcpyAsync(&bits, h->d_dtmin, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    T dt;
+    if (sizeof(T) == 8) memcpy(&dt, &bits, 8);
+    else { unsigned int b = (unsigned int)bits; memcpy(&dt, &b, 4); }
+    // initdt (src/Mainloop.cu:515-554) on a local copy of the loop
+    int maxlevel = h->P.maxlevel;
+    double dtmaxloc = h->P.dtinit > 0 ? h->P.dtinit / 1.5
+                                      : (maxlevel < 0 ? h->P.delta * (double)(1 << (-maxlevel)) : h->P.delta / (double)(1 << maxlevel)) /
+                                            (sqrt(h->P.g * 10.0));
+    T one_over_epsi = (T)1.0 / epsi_of<T>();
+    if (one_over_epsi < dt) dt = one_over_epsi;  // reduction starts at 1/epsi (timestepreductionCPU)
+    if ((double)dt > (1.5 * dtmaxloc)) dt = (T)(1.5 * dtmaxloc);
+    if (ceil((loop->nextoutputtime - loop->totaltime) / (double)dt) > 0.0)
+        dt = (T)((loop->nextoutputtime - loop->totaltime) / ceil((loop->nextoutputtime - loop->totaltime) / (double)dt));
+    loop->dtmax = (double)dt;
+    return BGF_OK;
+}
+
+int bgf_init_dt(bgf_handle* h, bgf_loop* loop)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!loop) return BGF_EINVAL;
+    return h->dbl ? init_dt_t<double>(h, loop) : init_dt_t<float>(h, loop);
+}
+
+template <class T> static void enqueue_step(bgf_handle* h, int parity)
+{
+    DevModel<T> m = dev_model<T>(h);
+    StepParams<T> p = step_params<T>(h);
+    launch_flux<T>(m, p, h->P.engine, parity, h->stream);
+    launch_update<T>(m, p, h->P.engine, parity, h->stream);
+}
+
+static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep, long long maxsteps)
+{
+    TimeState ts;
+    memset(&ts, 0, sizeof(ts));
+    ts.totaltime = loop->totaltime;
+    ts.dt = loop->dt;
+    ts.dtmax = loop->dtmax;
+    ts.nextoutputtime = loop->nextoutputtime;
+    ts.endtime = endtime;
+    ts.outputtimestep = outputtimestep;
+    ts.nstep = 0;
+    ts.maxsteps = maxsteps;
+    ts.cur = h->cur;
+    ts.done = 0;
+    ts.status = 0;
+    h->h_time[0] = ts;
+    unsigned long long init = dt_init_bits(h->dbl);
+    BGF_CUDA(cudaMemcpyAsync(h->d_time + h->parity, &h->h_time[0], sizeof(TimeState), cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_dtmin + h->parity, &init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
+    // the pinned staging slot must not be reused before the copy has executed
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    return BGF_OK;
+}
+
+int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!loop) return BGF_EINVAL;
+    rc = write_time_slot(h, loop, INFINITY, 0.0, 1);
+    if (rc) return rc;
+    if (h->profiling) {
+        BGF_CUDA(cudaEventRecord(h->pev[0], h->stream));
+        if (h->dbl) {
+            launch_flux<double>(dev_model<double>(h), step_params<double>(h), h->P.engine, h->parity, h->stream);
+            BGF_CUDA(cudaEventRecord(h->pev[1], h->stream));
+            launch_update<double>(dev_model<double>(h), step_params<double>(h), h->P.engine, h->parity, h->stream);
+        } else {
+            launch_flux<float>(dev_model<float>(h), step_params<float>(h), h->P.engine, h->parity, h->stream);
+            BGF_CUDA(cudaEventRecord(h->pev[1], h->stream));
+            launch_update<float>(dev_model<float>(h), step_params<float>(h), h->P.engine, h->parity, h->stream);
+        }
+        BGF_CUDA(cudaEventRecord(h->pev[2], h->stream));
+    } else if (h->dbl) {
+        enqueue_step<double>(h, h->parity);
+    } else {
+        enqueue_step<float>(h, h->parity);
+    }
+    h->launches += 2;
+    BGF_CUDA(cudaGetLastError());
+    BGF_CUDA(cudaMemcpyAsync(&h->h_time[1], h->d_time + (h->parity ^ 1), sizeof(TimeState), cudaMemcpyDeviceToHost,
+                             h->stream));
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->profiling) {
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, h->pev[0], h->pev[1]);
+        cudaEventElapsedTime(&b, h->pev[1], h->pev[2]);
+        h->flux_ms += a;
+        h->update_ms += b;
+        h->profiled_steps++;
+    }
+    rc = check_err_word(h);
+    if (rc) return rc;
+    const TimeState& nt = h->h_time[1];
+    loop->dt = nt.dt;
+    loop->dtmax = nt.dtmax;
+    h->cur = nt.cur;
+    h->parity ^= 1;
+    return BGF_OK;
+}
+
+static int build_graphs(bgf_handle* h)
+{
+    free_graphs(h);
+    for (int p0 = 0; p0 < 2; p0++) {
+        cudaGraph_t g;
+        BGF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < 2; k++) {
+            if (h->dbl) enqueue_step<double>(h, p0 ^ k);
+            else enqueue_step<float>(h, p0 ^ k);
+        }
+        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        if (e != cudaSuccess) {
+            g_last_error = std::string("graph capture: ") + cudaGetErrorString(e);
+            return BGF_ECUDA;
+        }
+        e = cudaGraphInstantiate(&h->graph[p0], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            g_last_error = std::string("graph instantiate: ") + cudaGetErrorString(e);
+            return BGF_ECUDA;
+        }
+    }
+    h->graph_valid = true;
+    return BGF_OK;
+}
+
+int bgf_run(bgf_handle* h, bgf_loop* loop, double endtime, double outputtimestep, int maxsteps, int* nsteps)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!loop || maxsteps < 0) return BGF_EINVAL;
+    if (nsteps) *nsteps = 0;
+    if (!h->graph_valid) {
+        rc = build_graphs(h);
+        if (rc) return rc;
+    }
+    rc = write_time_slot(h, loop, endtime, outputtimestep, maxsteps);
+    if (rc) return rc;
+    const int p0 = h->parity;
+    double gpu_ms = 0.0;
+    int64_t launched = 0;
+    TimeState ts = h->h_time[0];
+    double dtguess = loop->dtmax > 0 ? loop->dtmax : 1.0;
+    while (true) {
+        double remaining = (endtime - ts.totaltime) / (dtguess > 0 ? dtguess : 1.0);
+        long long left = (long long)maxsteps - ts.nstep;
+        long long want = (long long)std::min<double>(remaining * 1.02 + 2.0, (double)left);
+        int batch = (int)std::max<long long>(1, std::min<long long>((want + 1) / 2, 512));
+        BGF_CUDA(cudaEventRecord(h->ev0, h->stream));
+        for (int b = 0; b < batch; b++) BGF_CUDA(cudaGraphLaunch(h->graph[p0], h->stream));
+        BGF_CUDA(cudaEventRecord(h->ev1, h->stream));
+        launched += 4LL * batch;
+        // after whole graphs the latest time state is in slot p0
+        BGF_CUDA(cudaMemcpyAsync(&h->h_time[1], h->d_time + p0, sizeof(TimeState), cudaMemcpyDeviceToHost, h->stream));
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        gpu_ms += ms;
+        ts = h->h_time[1];
+        if (ts.dt > 0) dtguess = ts.dt;
+        if (ts.done || ts.totaltime >= endtime || ts.nstep >= maxsteps) break;
+    }
+    h->launches += launched;
+    h->last_run_ms = gpu_ms;
+    h->last_run_launches = launched;
+    rc = check_err_word(h);
+    if (rc) return rc;
+    loop->totaltime = ts.totaltime;
+    loop->dt = ts.dt;
+    loop->dtmax = ts.dtmax;
+    loop->nextoutputtime = ts.nextoutputtime;
+    h->cur = ts.cur;
+    // parity stays p0: every graph replay advances it by two
+    if (nsteps) *nsteps = (int)ts.nstep;
+    if (ts.status == BGF_EDT_UNDERFLOW) return BGF_EDT_UNDERFLOW;
+    return BGF_OK;
+}
+
+int bgf_volume(bgf_handle* h, double* volume)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!volume) return BGF_EINVAL;
+    BGF_CUDA(cudaMemsetAsync(h->d_scratch, 0, sizeof(double), h->stream));
+    if (h->dbl) launch_volume<double>(dev_model<double>(h), (double)h->P.delta, h->cur, h->d_scratch, h->stream);
+    else launch_volume<float>(dev_model<float>(h), (float)h->P.delta, h->cur, h->d_scratch, h->stream);
+    h->launches++;
+    BGF_CUDA(cudaGetLastError());
+    BGF_CUDA(cudaMemcpyAsync(volume, h->d_scratch, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    return BGF_OK;
+}
+
+int64_t bgf_kernel_launches(bgf_handle* h) { return h ? h->launches : -1; }
+
+int bgf_set_profiling(bgf_handle* h, int on)
+{
+    if (!h) return BGF_EINVAL;
+    h->profiling = on ? 1 : 0;
+    h->flux_ms = h->update_ms = 0.0;
+    h->profiled_steps = 0;
+    return BGF_OK;
+}
+
+int bgf_kernel_timing(bgf_handle* h, double* flux_ms, double* update_ms, int64_t* steps)
+{
+    if (!h) return BGF_EINVAL;
+    if (flux_ms) *flux_ms = h->flux_ms;
+    if (update_ms) *update_ms = h->update_ms;
+    if (steps) *steps = h->profiled_steps;
+    return BGF_OK;
+}
+
+int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches)
+{
+    if (!h) return BGF_EINVAL;
+    if (gpu_ms) *gpu_ms = h->last_run_ms;
+    if (launches) *launches = h->last_run_launches;
+    return BGF_OK;
+}

@@ -1,0 +1,465 @@
+// Flow-step kernels (see bgf_flow.cuh for the design) and their launchers.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include "bgf_flow.cuh"
+#include "bgf_internal.h"
+
+namespace bgf {
+
+// ---------------------------------------------------------------- tile assembly
+
+// Loads the bed halo tile and (engine 1) the bed-gradient rows/columns.
+template <class T, int ENGINE>
+__device__ __forceinline__ void load_bed(Smem<T>& s, const DevModel<T>& m, int ib, int tid)
+{
+    const T* zbt = m.zb + (size_t)ib * 324;
+    for (int k = tid; k < 324; k += NTHREADS) s.zb[k] = zbt[k];
+    if (ENGINE == 1) {
+        const T* gx = m.dzbdx + (size_t)ib * 324;
+        const T* gy = m.dzbdy + (size_t)ib * 324;
+        for (int k = tid; k < 18 * 16; k += NTHREADS) {
+            int x = k % 18 - 1, y = k / 18;
+            s.dzbx[k] = gx[hi18(x, y)];
+            int xx = k % 16, yy = k / 16 - 1;
+            s.dzby[k] = gy[hi18(xx, yy)];
+        }
+    }
+}
+
+// zs of a tile cell: ring 1 and the interior use the block's own bed tile
+// (RecalculateZs, src/Halo.cu:72-107); ring 2 uses the bed under its source cell,
+// as the neighbour's own RecalculateZs does before gradientHalo reads it.
+template <class T>
+__device__ __forceinline__ T tile_zb(const Smem<T>& s, const DevModel<T>& m, int x, int y, int sb, int sx, int sy)
+{
+    bool ring2 = x < -1 || x > BW || y < -1 || y > BW;
+    if (!ring2) return s.zb[hi18(x, y)];
+    return m.zb[(size_t)sb * 324 + hi18(sx, sy)];
+}
+
+// Predictor tile: state n of the block and its two-cell ring.
+template <class T>
+__device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m, int ib, int cur, int tid)
+{
+    const T* H = m.h[cur];
+    const T* U = m.u[cur];
+    const T* V = m.v[cur];
+    {
+        int x = tid & 15, y = tid >> 4;
+        size_t g = (size_t)ib * 256 + tid;
+        T hv = H[g], uv = U[g], vv = V[g];
+        int c = ti(x, y);
+        s.h[c] = hv; s.u[c] = uv; s.v[c] = vv;
+        s.zs[c] = s.zb[hi18(x, y)] + hv;
+        int c18 = hi18(x, y);
+        s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
+    }
+    if (tid < 128) {
+        int x, y, sb, sx, sy;
+        ring_pos(tid, x, y);
+        if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy)) {
+            atomicOr(m.err, 1);
+            sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
+        }
+        size_t g = (size_t)sb * 256 + sy * 16 + sx;
+        T hv = H[g], uv = U[g], vv = V[g];
+        int c = ti(x, y);
+        s.h[c] = hv; s.u[c] = uv; s.v[c] = vv;
+        s.zs[c] = tile_zb(s, m, x, y, sb, sx, sy) + hv;
+        if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
+            int c18 = hi18(x, y);
+            s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
+        }
+    }
+}
+
+// Corrector tile: half-step state h* = Advance(state n, adv, dt/2) at every tile
+// cell, evaluated from the source cell's state and flux divergence; state n is kept
+// on the 18x18 tile for the boundary fluxes and the full-step advance.
+template <class T>
+__device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
+                                               int cur, T halfdt, int tid)
+{
+    const T* H = m.h[cur];
+    const T* U = m.u[cur];
+    const T* V = m.v[cur];
+    for (int k = tid; k < 256 + 128; k += NTHREADS) {
+        int x, y, sb = ib, sx, sy;
+        if (k < 256) {
+            x = k & 15; y = k >> 4; sx = x; sy = y;
+        } else {
+            ring_pos(k - 256, x, y);
+            if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy)) {
+                atomicOr(m.err, 1);
+                sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
+            }
+        }
+        size_t g = (size_t)sb * 256 + sy * 16 + sx;
+        T hv = H[g], uv = U[g], vv = V[g];
+        T ho, uo, vo;
+        advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, m.dh[g], m.dhu[g], m.dhv[g], ho, uo, vo);
+        int c = ti(x, y);
+        s.h[c] = ho; s.u[c] = uo; s.v[c] = vo;
+        s.zs[c] = tile_zb(s, m, x, y, sb, sx, sy) + ho;
+        if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
+            int c18 = hi18(x, y);
+            s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- boundaries
+
+// interptime (src/Util_CPU.cu:107-110) over a uniform series, stepping as
+// FlowbndFlux does (src/Boundary.cu:130-143).
+__device__ __forceinline__ double series_at(const double* t, const double* v, int n, double time)
+{
+    int st = 1;
+    while (st < n - 1 && t[st] - time < 0.0) st++;
+    return v[st - 1] + (time - t[st - 1]) / (t[st] - t[st - 1]) * (v[st] - v[st - 1]);
+}
+
+// bndFluxGPUSideCPU (src/Boundary.cu:587-745) for the four sides of one block.
+// Face arrays in s are modified in place; state n comes from s.h0/u0/v0 and the
+// bed tile (zs = zb + h, as RecalculateZs leaves it).
+template <class T>
+__device__ __forceinline__ void apply_boundaries(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
+                                                 double tbnd, int tid)
+{
+    if (tid >= 64) return;
+    int side = tid >> 4, t = tid & 15;
+    int k = m.bndseg[ib * 4 + side];
+    if (k < 0) return;
+    SegDev sg = m.segs[k];
+    if (sg.type == 1) return;
+    double zsbnd = 0.0;
+    if (!isnan(p.zsinit)) zsbnd = p.zsinit;
+    T taper = (T)1.0;
+    if (sg.n > 0) {
+        if (p.bndtaper > 0.0) taper = (T)fmin((tbnd - p.inittime) / p.bndtaper, 1.0);
+        zsbnd = series_at(m.seg_t + sg.off, m.seg_wl + sg.off, sg.n, tbnd);
+    }
+    int isright = side == 0 ? -1 : side == 1 ? 1 : 0;
+    int istop = side == 2 ? 1 : side == 3 ? -1 : 0;
+    int ix, iy, inx, iny;
+    if (isright == 0) { ix = t; iy = istop < 0 ? 0 : BW; }
+    else { iy = t; ix = isright < 0 ? 0 : BW; }
+    if (isright < 0) { inx = ix + 1; iny = iy; }
+    else if (isright > 0) { inx = ix - 1; iny = iy; }
+    else if (istop < 0) { inx = ix; iny = iy + 1; }
+    else { inx = ix; iny = iy - 1; }
+    T sign = (T)isright + (T)istop;
+    float zsb = (float)zsbnd;
+    zsb = (float)((double)zsb + p.zsoffset);
+    int ci = hi18(ix, iy), cin = hi18(inx, iny);
+    T zsi = s.zb[ci] + s.h0[ci];
+    T zsinside = s.zb[cin] + s.h0[cin];
+    T hinside = s.h0[cin];
+    T uninside = isright != 0 ? s.u0[cin] : s.v0[cin];
+    T hface = s.h0[ci];
+    T zsX = (T)(((double)((T)zsb + (T)0.0) - 0.5 * (double)(zsi + zsinside)) * (double)taper + 0.5 * (double)(zsi + zsinside));
+    float* qm = m.qmean + ib * 64 + side * 16 + t;
+    T qmean = (T)*qm;
+    T *Fh, *Fq, *Ss;
+    int fi, fin;
+    if (isright != 0) {
+        Fh = s.Fhu; Fq = s.Fqux; Ss = s.Su;
+        fi = fxi(ix, iy); fin = fxi(inx, iny);
+    } else {
+        Fh = s.Fhv; Fq = s.Fqvy; Ss = s.Sv;
+        fi = fyi(ix, iy); fin = fyi(inx, iny);
+    }
+    T F, G, S;
+    bool lowside = isright < 0 || istop < 0;
+    if (lowside) { F = Fh[fi]; G = Fq[fi]; S = Ss[fin]; }
+    else { F = Fh[fi]; G = Ss[fi]; S = Fq[fin]; }
+    T factime = M<T>::fmin_((T)(p.dtparam / p.bndfiltertime), (T)1.0);
+    T facrel = (T)1.0 - M<T>::fmin_((T)(p.dtparam / p.bndrelaxtime), (T)1.0);
+    if (sg.type == 0) {
+        F = (T)0.0;
+        S = G;
+    } else if (sg.type == 3) {
+        if ((double)hface > p.eps_d || zsX > zsi) {
+            abs1dq<T>(p.g, sign, factime, facrel, zsi, zsX, hface, qmean, F);
+        } else {
+            F = (T)0.0; S = G; qmean = (T)0.0;
+        }
+        *qm = (float)qmean;
+    } else if (sg.type == 2) {
+        if ((double)hface > p.eps_d || zsX > zsi) {
+            dirichlet1q<T>(p.g, sign, zsX, zsinside, hinside, uninside, F);
+        } else {
+            F = (T)0.0; S = G; qmean = (T)0.0;
+        }
+        *qm = (float)qmean;
+    }
+    if (lowside) { Fh[fi] = F; Fq[fi] = G; Ss[fin] = S; }
+    else { Fh[fi] = F; Ss[fi] = G; Fq[fin] = S; }
+}
+
+// updateEVCPU (src/Advection.cu:160-254), Cartesian.  Returns dh, dhu, dhv of the
+// thread's cell from the face arrays.
+template <class T>
+__device__ __forceinline__ void flux_divergence(const Smem<T>& s, const StepParams<T>& p, T delta, int x, int y, T hi,
+                                                T uui, T vvi, T& dh, T& dhu, T& dhv)
+{
+    T cmdinv = (T)1.0 / ((T)1.0 * delta);
+    T ga = (T)0.5 * p.g;
+    T dmdl = ((T)1.0 - (T)1.0) / ((T)1.0 * delta);
+    T dmdt = ((T)1.0 - (T)1.0) / ((T)1.0 * delta);
+    T fG = vvi * dmdl - uui * dmdt;
+    int fi = fxi(x, y), fr = fxi(x + 1, y);
+    int gi = fyi(x, y), gt = fyi(x, y + 1);
+    dh = (T)-1.0 * (s.Fhu[fr] - s.Fhu[fi] + s.Fhv[gt] - s.Fhv[gi]) * cmdinv;
+    dhu = (s.Fqux[fi] + s.Fquy[gi] - s.Su[fr] - s.Fquy[gt]) * cmdinv + p.fc * hi * vvi;
+    dhv = (s.Fqvy[gi] + s.Fqvx[fi] - s.Sv[gt] - s.Fqvx[fr]) * cmdinv - p.fc * hi * uui;
+    dhu += hi * (ga * hi * dmdl + fG * vvi);
+    dhv += hi * (ga * hi * dmdt - fG * uui);
+}
+
+// ---------------------------------------------------------------- kernels
+
+// Whether this step runs (the reference loop condition totaltime < endtime plus
+// the step budget); identical in both kernels of a step.
+__device__ __forceinline__ bool step_live(const TimeState& ts)
+{
+    return !ts.done && ts.totaltime < ts.endtime && ts.nstep < ts.maxsteps;
+}
+
+template <class T, int ENGINE>
+__global__ void __launch_bounds__(NTHREADS) flux_kernel(DevModel<T> m, StepParams<T> p, int parity)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
+    const TimeState ts = m.time[parity];
+    if (!step_live(ts)) return;
+    const int tid = threadIdx.x;
+    const int ib = m.active[blockIdx.x];
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    const int cur = ts.cur;
+
+    load_bed<T, ENGINE>(s, m, ib, tid);
+    __syncthreads();
+    load_state_tile<T>(s, m, ib, cur, tid);
+    __syncthreads();
+    T celldt = tile_fluxes<T, ENGINE>(s, p, delta, tid);
+    __syncthreads();
+    // CFL minimum: the interior dtmax values reduced with the warp shuffle, then one
+    // atomic per block on the float bit pattern (dt > 0, so integer order == float order).
+    T v = celldt;
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    if ((tid & 31) == 0) s.red[tid >> 5] = v;
+    // Boundary segments (FlowbndFlux) after the dt, at t + dt_prev/2 as FlowCPU does.
+    apply_boundaries<T>(s, m, p, ib, ts.totaltime + ts.dt * 0.5, tid);
+    __syncthreads();
+    if (tid == 0) {
+        T b = s.red[0];
+        for (int k = 1; k < NTHREADS / 32; k++) b = s.red[k] < b ? s.red[k] : b;
+        atomicMin(&m.dtmin[parity], dt_bits(b));
+    }
+    const int x = tid & 15, y = tid >> 4;
+    const int c = ti(x, y);
+    T dh, dhu, dhv;
+    flux_divergence<T>(s, p, delta, x, y, s.h[c], s.u[c], s.v[c], dh, dhu, dhv);
+    size_t g = (size_t)ib * 256 + tid;
+    m.dh[g] = dh;
+    m.dhu[g] = dhu;
+    m.dhv[g] = dhv;
+}
+
+// dt of the step from the reduced minimum (CalctimestepGPU, src/Advection.cu:549-620
+// and CalctimestepCPU, :511-535): clamp to 1.5 * the previous dt, then split the
+// time to the next output into an integer number of equal steps.
+template <class T> __device__ __forceinline__ T step_dt(const TimeState& ts, unsigned long long minbits)
+{
+    T dt = dt_from_bits<T>(minbits);
+    if ((double)dt > (1.5 * ts.dtmax)) dt = (T)(1.5 * ts.dtmax);
+    if (ceil((ts.nextoutputtime - ts.totaltime) / (double)dt) > 0.0)
+        dt = (T)((ts.nextoutputtime - ts.totaltime) / ceil((ts.nextoutputtime - ts.totaltime) / (double)dt));
+    return dt;
+}
+
+template <class T, int ENGINE>
+__global__ void __launch_bounds__(NTHREADS) update_kernel(DevModel<T> m, StepParams<T> p, int parity)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
+    const TimeState ts = m.time[parity];
+    const int tid = threadIdx.x;
+    if (!step_live(ts)) {
+        if (blockIdx.x == 0 && tid == 0) {
+            TimeState nt = ts;
+            nt.done = 1;
+            m.time[parity ^ 1] = nt;
+        }
+        return;
+    }
+    const int ib = m.active[blockIdx.x];
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    const int cur = ts.cur;
+    const T dt = step_dt<T>(ts, m.dtmin[parity]);
+    const double dtd = (double)dt;
+
+    load_bed<T, ENGINE>(s, m, ib, tid);
+    __syncthreads();
+    load_half_tile<T>(s, m, p, ib, cur, dt * (T)0.5, tid);
+    __syncthreads();
+    (void)tile_fluxes<T, ENGINE>(s, p, delta, tid);
+    __syncthreads();
+    apply_boundaries<T>(s, m, p, ib, ts.totaltime + dtd, tid);
+    __syncthreads();
+    const int x = tid & 15, y = tid >> 4;
+    const int c = ti(x, y);
+    T dh, dhu, dhv;
+    flux_divergence<T>(s, p, delta, x, y, s.h[c], s.u[c], s.v[c], dh, dhu, dhv);
+    // full step from state n (AdvkernelCPU with evolv), then friction on the result
+    const int c18 = hi18(x, y);
+    T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];
+    T ho, uo, vo;
+    advance<T>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+    size_t g = (size_t)ib * 256 + tid;
+    T cfv = p.has_cf ? m.cf[g] : p.cf;
+    bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);
+    if (p.has_rain) {
+        // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): uniform rain rate
+        // interpolated at the start of the step (updateforcing)
+        double rnow = series_at(m.rain_t, m.rain_r, p.rain_n, ts.totaltime);
+        T Rainhh = (T)rnow;
+        T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
+        Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
+        T hi = ho;
+        T qvol = hi / (hi + Rainhh);
+        ho = hi + Rainhh;
+        if ((double)hi > p.eps_d) {
+            uo = uo * qvol;
+            vo = vo * qvol;
+        }
+    }
+    const int nxt = cur ^ 1;
+    m.h[nxt][g] = ho;
+    m.u[nxt][g] = uo;
+    m.v[nxt][g] = vo;
+    if (blockIdx.x == 0 && tid == 0) {
+        TimeState nt = ts;
+        nt.dt = dtd;
+        nt.dtmax = dtd;
+        nt.totaltime = ts.totaltime + dtd;
+        nt.nstep = ts.nstep + 1;
+        nt.cur = nxt;
+        if (dtd < p.dtmin && nt.totaltime < ts.endtime) {
+            nt.status = 4;  // BGF_EDT_UNDERFLOW (CrashDetection, src/Mainloop.cu:648-719)
+            nt.done = 1;
+        }
+        if (ts.outputtimestep > 0.0 && nt.nextoutputtime - nt.totaltime <= dtd * 0.00001) {
+            nt.nextoutputtime = fmin(nt.nextoutputtime + ts.outputtimestep, ts.endtime);
+        }
+        m.time[parity ^ 1] = nt;
+        // the next step reduces into the other slot
+        T epsi = M<T>::epsi();
+        m.dtmin[parity ^ 1] = dt_bits((T)1.0 / epsi);
+    }
+}
+
+// initdt (src/Mainloop.cu:515-554): CalcInitdtCPU per cell, block minimum, atomic.
+template <class T> __global__ void initdt_kernel(DevModel<T> m, StepParams<T> p, int cur, unsigned long long* out)
+{
+    __shared__ T red[NTHREADS / 32];
+    const int tid = threadIdx.x;
+    const int ib = m.active[blockIdx.x];
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    T hv = m.h[cur][(size_t)ib * 256 + tid];
+    T epsT = (T)p.eps_d;
+    T hm = hv < epsT ? epsT : hv;
+    T v = delta / M<T>::sqrt_(p.g * hm);
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+        T b = red[0];
+        for (int k = 1; k < NTHREADS / 32; k++) b = red[k] < b ? red[k] : b;
+        atomicMin(out, dt_bits(b));
+    }
+}
+
+// Volume sum_h h * delta^2 over active interior cells in double.
+template <class T> __global__ void volume_kernel(DevModel<T> m, T delta0, int cur, double* out)
+{
+    __shared__ double red[NTHREADS / 32];
+    const int tid = threadIdx.x;
+    const int ib = m.active[blockIdx.x];
+    double d = (double)calcres<T>(delta0, m.level[ib]);
+    double v = (double)m.h[cur][(size_t)ib * 256 + tid] * d * d;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+        double b = 0;
+        for (int k = 0; k < NTHREADS / 32; k++) b += red[k];
+        atomicAdd(out, b);
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+
+template <class T> size_t smem_bytes() { return sizeof(Smem<T>); }
+
+template <class T, int ENGINE> cudaError_t configure_engine()
+{
+    cudaError_t e = cudaFuncSetAttribute(flux_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_bytes<T>());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(update_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes<T>());
+}
+
+template <class T> cudaError_t configure_kernels()
+{
+    cudaError_t e = configure_engine<T, 1>();
+    if (e != cudaSuccess) return e;
+    return configure_engine<T, 2>();
+}
+
+template <class T>
+void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st)
+{
+    if (engine == 1) flux_kernel<T, 1><<<m.nblk, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+    else flux_kernel<T, 2><<<m.nblk, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+}
+
+template <class T>
+void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st)
+{
+    if (engine == 1) update_kernel<T, 1><<<m.nblk, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+    else update_kernel<T, 2><<<m.nblk, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+}
+
+template <class T>
+void launch_initdt(const DevModel<T>& m, const StepParams<T>& p, int cur, unsigned long long* out, cudaStream_t st)
+{
+    initdt_kernel<T><<<m.nblk, NTHREADS, 0, st>>>(m, p, cur, out);
+}
+
+template <class T> void launch_volume(const DevModel<T>& m, T delta0, int cur, double* out, cudaStream_t st)
+{
+    volume_kernel<T><<<m.nblk, NTHREADS, 0, st>>>(m, delta0, cur, out);
+}
+
+template cudaError_t configure_kernels<float>();
+template cudaError_t configure_kernels<double>();
+template void launch_flux<float>(const DevModel<float>&, const StepParams<float>&, int, int, cudaStream_t);
+template void launch_flux<double>(const DevModel<double>&, const StepParams<double>&, int, int, cudaStream_t);
+template void launch_update<float>(const DevModel<float>&, const StepParams<float>&, int, int, cudaStream_t);
+template void launch_update<double>(const DevModel<double>&, const StepParams<double>&, int, int, cudaStream_t);
+template void launch_initdt<float>(const DevModel<float>&, const StepParams<float>&, int, unsigned long long*, cudaStream_t);
+template void launch_initdt<double>(const DevModel<double>&, const StepParams<double>&, int, unsigned long long*, cudaStream_t);
+template void launch_volume<float>(const DevModel<float>&, float, int, double*, cudaStream_t);
+template void launch_volume<double>(const DevModel<double>&, double, int, double*, cudaStream_t);
+
+}  // namespace bgf

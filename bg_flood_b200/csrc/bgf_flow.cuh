@@ -1,0 +1,263 @@
+// Fused flow-step kernels for sm_100a.
+//
+// One step of the reference (FlowGPU, src/FlowGPU.cu:14-315) is two launches:
+//
+//   flux_kernel   (predictor): per 16x16 block, assemble the state tile with a
+//                 two-cell ring from the neighbour tables (fillHalo + the
+//                 stencils of gradientHalo), limited gradients, wet-slope reset,
+//                 X/Y face fluxes, boundary-segment fluxes, the per-cell dtmax and
+//                 the block's share of the global CFL minimum, then the flux
+//                 divergence (updateEV).  Writes dh, dhu, dhv only.
+//
+//   update_kernel (corrector): turns the global minimum into dt with the
+//                 reference clamps (CalctimestepGPU), rebuilds the half-step state
+//                 h* = Advance(h, dh, dt/2) on the fly for its tile and ring (the
+//                 predictor advance is pointwise, so the ring values equal what a
+//                 halo exchange of h* would deliver), repeats gradients / fluxes /
+//                 boundaries on h*, and applies the full-step advance, friction and
+//                 rain, writing the next state into the other ping-pong buffer.
+//
+// Per cell-update HBM traffic is h,u,v,zb read + dh,dhu,dhv written (predictor)
+// and h,u,v,dh,dhu,dhv,zb read + h,u,v written (corrector): 68 B in FP32 with a
+// uniform friction coefficient, the algorithmic minimum of the two-stage scheme.
+#pragma once
+#include <stdint.h>
+
+#include "bgf_numerics.cuh"
+
+namespace bgf {
+
+constexpr int BW = 16;      // block width in cells
+constexpr int TW = 20;      // tile width: 16 interior + 2 rings each side
+constexpr int NTHREADS = 256;
+
+// Device time-loop state (reference Loop<T> members, src/Arrays.h:359-404), kept in
+// two slots that alternate with the step parity.
+struct TimeState {
+    double totaltime;
+    double dt;          // dt of the last step taken (the "previous dt" of the next one)
+    double dtmax;       // clamp reference for the next dt (XLoop.dtmax)
+    double nextoutputtime;
+    double endtime;
+    double outputtimestep;
+    long long nstep;
+    long long maxsteps;
+    int cur;            // state buffer holding the current state
+    int done;           // 1: the loop condition failed; further steps are no-ops
+    int status;         // 0 ok, BGF_EDT_UNDERFLOW
+    int pad;
+};
+
+struct SegDev {
+    int type;  // 0 wall, 1 Neumann, 2 Dirichlet, 3 absorbing
+    int n;     // series length (0: no series, zsbnd from zsinit)
+    int off;   // offset in the series arrays
+    int pad;
+};
+
+template <class T> struct StepParams {
+    T g, eps, CFL, theta, delta0, epsi, epsface, fc;
+    double eps_d, dtparam, bndfiltertime, bndrelaxtime, bndtaper, inittime, zsinit, zsoffset, dtmin;
+    T cf;        // uniform friction coefficient
+    int frictionmodel, forcemass, has_cf, has_rain, nseg, rain_n;
+};
+
+template <class T> struct DevModel {
+    int nblk, nblkmem;
+    const int* active;
+    const int* level;
+    const int* nbr;  // [8][nblkmem]: LB, LT, RB, RT, BL, BR, TL, TR
+    const T* zb;     // 324 per block (halo filled)
+    const T* dzbdx;  // 324 per block (engine 1)
+    const T* dzbdy;
+    const T* cf;     // 256 per block (optional)
+    const uint8_t* rainmask;  // 256 per block (optional)
+    const int* bndseg;        // 4 per block: segment index per side or -1
+    float* qmean;             // 64 per block
+    const SegDev* segs;
+    const double* seg_t;
+    const double* seg_wl;
+    const double* rain_t;
+    const double* rain_r;
+    T* h[2];
+    T* u[2];
+    T* v[2];
+    T* dh;
+    T* dhu;
+    T* dhv;
+    TimeState* time;       // [2]
+    unsigned long long* dtmin;  // [2] bit patterns of the running minimum (dt > 0: integer order)
+    int* err;              // device error word (0 ok)
+};
+
+// Positive floating-point values order like their bit patterns.
+__device__ __forceinline__ unsigned long long dt_bits(float v) { return (unsigned long long)__float_as_uint(v); }
+__device__ __forceinline__ unsigned long long dt_bits(double v) { return (unsigned long long)__double_as_longlong(v); }
+template <class T> __device__ __forceinline__ T dt_from_bits(unsigned long long b);
+template <> __device__ __forceinline__ float dt_from_bits<float>(unsigned long long b) { return __uint_as_float((unsigned int)b); }
+template <> __device__ __forceinline__ double dt_from_bits<double>(unsigned long long b) { return __longlong_as_double((long long)b); }
+
+__device__ __forceinline__ int ti(int x, int y) { return (y + 2) * TW + (x + 2); }
+__device__ __forceinline__ int hi18(int x, int y) { return (y + 1) * 18 + (x + 1); }  // memloc within a tile
+__device__ __forceinline__ int gxi(int x, int y) { return y * 18 + (x + 1); }          // x-gradients, x=-1..16
+__device__ __forceinline__ int gyi(int x, int y) { return (y + 1) * 16 + x; }          // y-gradients, y=-1..16
+__device__ __forceinline__ int fxi(int x, int y) { return y * 17 + x; }                // X faces x=0..16
+__device__ __forceinline__ int fyi(int x, int y) { return y * 16 + x; }                // Y faces y=0..16
+
+// Source cell of tile position (x, y) for a single-level neighbourhood: the
+// interior cell whose value fillHalo copies into ring 1 (src/Halo.cu:2083-2286)
+// and whose value gradientHalo uses as the outer stencil point for ring 2
+// (src/Gradients.cu:2713-3290).  At a domain edge (neighbour == self) both rings
+// take the block's own edge cell.  Returns false for cross-level sides.
+__device__ __forceinline__ bool tile_source(const int* nbr, int nblkmem, const int* level, int ib, int x, int y,
+                                            int& sb, int& sx, int& sy)
+{
+    sb = ib;
+    sx = x;
+    sy = y;
+    if (x < 0) {
+        int nb = nbr[0 * nblkmem + ib];
+        if (nb == ib) { sx = 0; return nbr[1 * nblkmem + ib] == ib; }
+        if (level[nb] != level[ib]) return false;
+        sb = nb; sx = BW + x;
+    } else if (x >= BW) {
+        int nb = nbr[2 * nblkmem + ib];
+        if (nb == ib) { sx = BW - 1; return nbr[3 * nblkmem + ib] == ib; }
+        if (level[nb] != level[ib]) return false;
+        sb = nb; sx = x - BW;
+    } else if (y < 0) {
+        int nb = nbr[4 * nblkmem + ib];
+        if (nb == ib) { sy = 0; return nbr[5 * nblkmem + ib] == ib; }
+        if (level[nb] != level[ib]) return false;
+        sb = nb; sy = BW + y;
+    } else if (y >= BW) {
+        int nb = nbr[6 * nblkmem + ib];
+        if (nb == ib) { sy = BW - 1; return nbr[7 * nblkmem + ib] == ib; }
+        if (level[nb] != level[ib]) return false;
+        sb = nb; sy = y - BW;
+    }
+    return true;
+}
+
+// Ring position k in [0,128): side = k/32 (left, right, bot, top), ring = (k/16)&1, t = k&15.
+__device__ __forceinline__ void ring_pos(int k, int& x, int& y)
+{
+    int side = k >> 5, ring = (k >> 4) & 1, t = k & 15;
+    if (side == 0) { x = -1 - ring; y = t; }
+    else if (side == 1) { x = BW + ring; y = t; }
+    else if (side == 2) { x = t; y = -1 - ring; }
+    else { x = t; y = BW + ring; }
+}
+
+template <class T> struct Smem {
+    T h[TW * TW], u[TW * TW], v[TW * TW], zs[TW * TW];
+    T zb[18 * 18];
+    T dhx[18 * 16], dzsx[18 * 16], dux[18 * 16], dvx[18 * 16];  // x-gradients
+    T dhy[16 * 18], dzsy[16 * 18], duy[16 * 18], dvy[16 * 18];  // y-gradients
+    T dzbx[18 * 16], dzby[16 * 18];
+    T Fhu[17 * 16], Fqux[17 * 16], Su[17 * 16], Fqvx[17 * 16];
+    T Fhv[16 * 17], Fqvy[16 * 17], Sv[16 * 17], Fquy[16 * 17];
+    // state n on the 18x18 tile (corrector: evolv for the boundary and the advance)
+    T h0[18 * 18], u0[18 * 18], v0[18 * 18];
+    T red[NTHREADS / 32];
+    double dt_d;
+    T dt;
+    int ok;
+};
+
+// One X (isx) or Y face of the tile, written to the face arrays of s.
+template <class T, int ENGINE>
+__device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p, T delta, bool isx, int x, int y)
+{
+    FaceIn<T, ENGINE> f;
+    int ci = ti(x, y), cn = isx ? ti(x - 1, y) : ti(x, y - 1);
+    f.hi = s.h[ci]; f.hn = s.h[cn];
+    f.zsi = s.zs[ci]; f.zsn = s.zs[cn];
+    if (isx) {
+        int gi = gxi(x, y), gn = gxi(x - 1, y);
+        f.uni = s.u[ci]; f.unn = s.u[cn]; f.uti = s.v[ci]; f.utn = s.v[cn];
+        f.dhi = s.dhx[gi]; f.dhn = s.dhx[gn]; f.dzsi = s.dzsx[gi]; f.dzsn = s.dzsx[gn];
+        f.duni = s.dux[gi]; f.dunn = s.dux[gn]; f.duti = s.dvx[gi]; f.dutn = s.dvx[gn];
+    } else {
+        int gi = gyi(x, y), gn = gyi(x, y - 1);
+        f.uni = s.v[ci]; f.unn = s.v[cn]; f.uti = s.u[ci]; f.utn = s.u[cn];
+        f.dhi = s.dhy[gi]; f.dhn = s.dhy[gn]; f.dzsi = s.dzsy[gi]; f.dzsn = s.dzsy[gn];
+        f.duni = s.dvy[gi]; f.dunn = s.dvy[gn]; f.duti = s.duy[gi]; f.dutn = s.duy[gn];
+    }
+    f.hsi = f.hi;
+    f.hsn = f.hn;
+    if (ENGINE == 1) {
+        f.zbi = s.zb[hi18(x, y)];
+        f.zbn = isx ? s.zb[hi18(x - 1, y)] : s.zb[hi18(x, y - 1)];
+        f.zsrci = f.zbi;
+        f.zsrcn = f.zbn;
+    } else {
+        f.zsrci = f.zsi - f.hi;
+        f.zsrcn = f.zsn - f.hn;
+    }
+    Face<T> r = face_flux<T, ENGINE>(f, p.g, p.CFL, p.epsi, p.epsface, delta);
+    if (isx) {
+        int fi = fxi(x, y);
+        s.Fhu[fi] = r.Fh; s.Fqux[fi] = r.Fq; s.Su[fi] = r.S; s.Fqvx[fi] = r.Ft;
+    } else {
+        int fi = fyi(x, y);
+        s.Fhv[fi] = r.Fh; s.Fqvy[fi] = r.Fq; s.Sv[fi] = r.S; s.Fquy[fi] = r.Ft;
+    }
+    return r;
+}
+
+// Gradients, wet-slope reset and face fluxes on an assembled tile (s.h/u/v/zs/zb).
+// Restates gradientCPU (src/Gradients.cu:971-1054) on a single-level tile, then
+// the engine's X and Y sweeps.  Returns this thread's cell dtmax (the value the
+// reference leaves in dtmax[i] after both sweeps).
+template <class T, int ENGINE>
+__device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T delta, int tid)
+{
+    const T theta = p.theta;
+    // x-gradients at x=-1..16 (rows 0..15) and y-gradients at y=-1..16 (cols 0..15)
+    for (int k = tid; k < 18 * 16; k += NTHREADS) {
+        int x = k % 18 - 1, y = k / 18;
+        int c = ti(x, y), l = ti(x - 1, y), r = ti(x + 1, y);
+        s.dhx[k] = minmod2(theta, s.h[l], s.h[c], s.h[r]) / delta;
+        s.dzsx[k] = minmod2(theta, s.zs[l], s.zs[c], s.zs[r]) / delta;
+        s.dux[k] = minmod2(theta, s.u[l], s.u[c], s.u[r]) / delta;
+        s.dvx[k] = minmod2(theta, s.v[l], s.v[c], s.v[r]) / delta;
+        int xx = k % 16, yy = k / 16 - 1;
+        int cy = ti(xx, yy), b = ti(xx, yy - 1), t = ti(xx, yy + 1);
+        s.dhy[k] = minmod2(theta, s.h[b], s.h[cy], s.h[t]) / delta;
+        s.dzsy[k] = minmod2(theta, s.zs[b], s.zs[cy], s.zs[t]) / delta;
+        s.duy[k] = minmod2(theta, s.u[b], s.u[cy], s.u[t]) / delta;
+        s.dvy[k] = minmod2(theta, s.v[b], s.v[cy], s.v[t]) / delta;
+    }
+    __syncthreads();
+    if (ENGINE == 1) {
+        // Wet-slope reset: interior cells follow WetsloperesetCPU (its y test compares
+        // both reconstructions with zs[yminus]); ring-1 cells follow the halo variants.
+        for (int k = tid; k < 18 * 16; k += NTHREADS) {
+            int x = k % 18 - 1, y = k / 18;
+            int c = ti(x, y);
+            s.dzsx[k] = wetslope(delta, s.zs[c], s.h[c], s.zs[ti(x - 1, y)], s.zs[ti(x + 1, y)], s.dzsx[k], s.dhx[k],
+                                 s.dzbx[k]);
+            int xx = k % 16, yy = k / 16 - 1;
+            int cy = ti(xx, yy);
+            bool interior = (yy >= 0 && yy < BW);
+            T zsm = s.zs[ti(xx, yy - 1)];
+            T zsp = interior ? zsm : s.zs[ti(xx, yy + 1)];
+            s.dzsy[k] = wetslope(delta, s.zs[cy], s.h[cy], zsm, zsp, s.dzsy[k], s.dhy[k], s.dzby[k]);
+        }
+        __syncthreads();
+    }
+    const int tx = tid & 15, ty = tid >> 4;
+    // Thread (tx,ty) owns the left (X) and bottom (Y) faces of its cell; threads
+    // 0..15 also take X face x=16 and threads 16..31 Y face y=16 (the faces the
+    // reference computes in the right / top halo column).
+    Face<T> fx = tile_face<T, ENGINE>(s, p, delta, true, tx, ty);
+    T celldt = fx.dt;  // dtmax after the X sweep (hugeposval exceeds any finite dt)
+    Face<T> fy = tile_face<T, ENGINE>(s, p, delta, false, tx, ty);
+    celldt = fy.wet ? (fy.dt < celldt ? fy.dt : celldt) : fy.dt;
+    if (tid < 16) tile_face<T, ENGINE>(s, p, delta, true, BW, tid);
+    else if (tid < 32) tile_face<T, ENGINE>(s, p, delta, false, tid - 16, BW);
+    return celldt;
+}
+
+}  // namespace bgf

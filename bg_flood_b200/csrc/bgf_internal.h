@@ -1,0 +1,28 @@
+// Internal declarations shared by the C-ABI layer and the kernel launchers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+namespace bgf {
+
+struct TimeState;
+struct SegDev;
+template <class T> struct DevModel;
+template <class T> struct StepParams;
+
+template <class T> cudaError_t configure_kernels();
+template <class T> void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st);
+template <class T> void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st);
+template <class T> void launch_initdt(const DevModel<T>& m, const StepParams<T>& p, int cur, unsigned long long* out, cudaStream_t st);
+template <class T> void launch_volume(const DevModel<T>& m, T delta0, int cur, double* out, cudaStream_t st);
+
+// Host restatement of the bed preparation the reference performs once at
+// initialisation (src/InitialConditions.cu:140-144): bed halo fill and bed
+// gradients including halo cells, on BUQ tiles.
+template <class T>
+int host_bed_gradients(int nblk, const int* active, const int* level, const int* nbr8soa, int nblkmem, double delta,
+                       double theta, const T* zb, T* dzbdx, T* dzbdy);
+
+}  // namespace bgf

@@ -1,0 +1,203 @@
+/*
+ * bg_flood_b200.h -- C ABI of the B200 implementation of BG_Flood's explicit
+ * shallow-water flow step on the block-uniform quadtree (BUQ).
+ *
+ * The library is a drop-in for the flow step that BG_Flood's time loop calls
+ * once per step, FlowGPU / FlowCPU (src/FlowGPU.cu:14-315, src/FlowCPU.cu:15-253,
+ * called from src/Mainloop.cu:43-57).  Every entry point takes plain pointers and
+ * sizes, returns a status code (BGF_OK == 0) and never exits the process.
+ *
+ * Data layout at this boundary is the reference's own: each block is an 18x18
+ * tile of 16x16 cells plus a one-cell halo, cell (i, j) of block ib at index
+ * (i + 1) + (j + 1) * 18 + ib * 324 (memloc, src/MemManagement.cu:37-40).
+ * Block tables are the reference BlockP arrays (src/Arrays.h:234-250).
+ *
+ * Precision follows the reference's "doubleprecision" key: with
+ * bgf_param.doubleprecision == 0 all field pointers are float*, otherwise
+ * double*.  Simulated time, dt and the output-time clamp are always double.
+ *
+ * Thread safety: a handle may be used from one host thread at a time; distinct
+ * handles are independent.  All work of a handle is ordered on its CUDA stream.
+ */
+#ifndef BG_FLOOD_B200_H
+#define BG_FLOOD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+enum {
+    BGF_OK = 0,
+    BGF_EINVAL = 1,        /* bad argument or unsupported configuration        */
+    BGF_ECUDA = 2,         /* a CUDA runtime call failed (see bgf_last_error)   */
+    BGF_ENOMEM = 3,        /* device allocation failed                          */
+    BGF_EDT_UNDERFLOW = 4, /* dt fell below dtmin before endtime (CrashDetection) */
+    BGF_ENAN = 5,          /* non-finite value detected in the state            */
+    BGF_ESTATE = 6,        /* call out of order (e.g. step before state upload) */
+    BGF_EBUDGET = 7,       /* serving: request exceeds the HBM budget           */
+    BGF_ETIMEOUT = 8,      /* bounded wait gave up                              */
+    BGF_ENOKERNEL = 9      /* the CUDA kernels are not available on this device */
+};
+
+/* ------------------------------------------------------------ parameters */
+/* Subset of the reference Param class (src/Param.h:10-239) used by the flow
+ * step, with the reference's member names, meanings and defaults
+ * (bgf_param_default fills them). */
+typedef struct bgf_param {
+    double g;             /* gravity, 9.81                                    */
+    double eps;           /* drying height, 1e-4                              */
+    double dt;            /* "dt" key (boundary filter/relax factors), 0      */
+    double CFL;           /* 0.5                                              */
+    double theta;         /* minmod limiter parameter, 1.3                    */
+    double cf;            /* uniform friction coefficient, 1e-4               */
+    double dx;            /* level-0 resolution                               */
+    double delta;         /* resolution used by the solver (== dx, Cartesian) */
+    double xo, yo;        /* domain origin                                    */
+    double lat;           /* latitude for the Coriolis term, 0                */
+    double zsinit;        /* NaN if unset                                     */
+    double zsoffset;      /* 0                                                */
+    double bndtaper;      /* 0                                                */
+    double bndrelaxtime;  /* 3600                                             */
+    double bndfiltertime; /* 60                                               */
+    double inittime;      /* 0                                                */
+    double dtmin;         /* 5e-4                                             */
+    double dtinit;        /* -1                                               */
+    double mask;          /* 9999                                             */
+    int engine;           /* 1 HLLC (Buttinger-Kreuzhuber), 2 Kurganov        */
+    int frictionmodel;    /* -1 Manning, 0 quadratic, 1 smart                 */
+    int ForceMassConserve;/* 0                                                */
+    int wetdryfix;        /* 1                                                */
+    int conserveElevation;/* 0 (only 0 is supported)                          */
+    int doubleprecision;  /* 0 float state, 1 double state                    */
+    int minlevel, maxlevel, initlevel;
+    int aoibnd;           /* boundary type of the remainder segment, 0 wall   */
+    int rainbnd;          /* 0: no rain on the two outermost cell rows        */
+    int GPUDEVICE;        /* CUDA device ordinal                              */
+} bgf_param;
+
+/* Reference Loop<T> members the step reads and writes (src/Arrays.h:359-404). */
+typedef struct bgf_loop {
+    double nextoutputtime;
+    double dt;        /* in: previous dt; out: dt of this step               */
+    double dtmax;     /* in: previous dt (or initdt); out: dt of this step   */
+    double totaltime; /* in: time at the start of the step                   */
+} bgf_loop;
+
+/* Reference BlockP<T> tables (src/Arrays.h:234-250).  xo/yo are float when
+ * doubleprecision == 0, double otherwise (same rule as the fields). */
+typedef struct bgf_blockp {
+    int nblk;                   /* active blocks                              */
+    const int* active;          /* nblk active block ids                      */
+    const int* level;           /* nblkmem                                    */
+    const int *BotLeft, *BotRight, *TopLeft, *TopRight;
+    const int *LeftBot, *LeftTop, *RightBot, *RightTop;
+    const void *xo, *yo;        /* block origins relative to Param.xo/yo     */
+} bgf_blockp;
+
+/* Reference EvolvingP<T> (src/Arrays.h:67-77): four BUQ arrays. */
+typedef struct bgf_evolving {
+    void *zs, *h, *u, *v;
+} bgf_evolving;
+
+typedef struct bgf_handle bgf_handle;
+
+/* Fills p with the reference defaults (src/Param.h). */
+void bgf_param_default(bgf_param* p);
+const char* bgf_strerror(int status);
+/* Text of the last CUDA error seen by this thread, or "". */
+const char* bgf_last_error(void);
+/* 1 when the sm_100a kernels can run on device `dev` (the library was built for sm_100a). */
+int bgf_device_supported(int dev);
+
+/* Creates a handle holding device memory for nblkmem blocks.  stream may be
+ * NULL (the handle creates its own non-blocking stream). Replaces SetupGPU /
+ * AllocateGPU (src/Setup_GPU.cu:15-36, src/MemManagement.cu:804). */
+int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out);
+int bgf_destroy(bgf_handle* h);
+
+/* Block tables (BlockP).  Replaces the block part of CopytoGPU
+ * (src/Setup_GPU.cu:196-375). */
+int bgf_set_blocks(bgf_handle* h, const bgf_blockp* blocks);
+
+/* Bed elevation and per-cell inputs in BUQ layout (nblkmem tiles).
+ * zb: bed with its halo already filled (as after fillHaloC on zb,
+ *     src/Testing.cu:583).  dzbdx/dzbdy: bed gradients incl. halo cells
+ *     (src/InitialConditions.cu:140-144); NULL to let the library compute them.
+ * cf: friction coefficient per cell, NULL for the uniform Param.cf.
+ * activeCell: rain mask per cell (int), NULL for all ones. */
+int bgf_set_bed(bgf_handle* h, const void* zb, const void* dzbdx, const void* dzbdy, const void* cf,
+                const int* activeCell);
+
+/* Boundary segment (reference bndsegment, src/Forcing.h:120-144): type 0 wall,
+ * 1 Neumann, 2 Dirichlet water level, 3 absorbing 1D; an optional uniform
+ * water-level series (n points of time t and level wl); and for each side
+ * (0 left, 1 right, 2 top, 3 bot) the blocks it applies to.  Segments are
+ * applied in the order they are added, as FlowbndFlux does per segment
+ * (src/Boundary.cu:108-195). */
+int bgf_add_bnd_segment(bgf_handle* h, int type, int n, const double* t, const double* wl,
+                        const int nblk_side[4], const int* const blk_side[4]);
+
+/* Uniform rain series in mm/h (reference Forcing.Rain with unidata). */
+int bgf_set_rain_series(bgf_handle* h, int n, const double* t, const double* rain_mmh);
+
+/* Uploads / downloads the evolving state (EvolvingP) in BUQ layout.  zs is
+ * ignored on upload (the step recomputes zs = zb + h everywhere, as
+ * RecalculateZs does, src/Halo.cu:72-107); on download only the 16x16
+ * interior of each active block is written. */
+int bgf_set_state(bgf_handle* h, const bgf_evolving* ev);
+int bgf_get_state(bgf_handle* h, bgf_evolving* ev);
+
+/* initdt (src/Mainloop.cu:515-554): writes loop->dtmax. */
+int bgf_init_dt(bgf_handle* h, bgf_loop* loop);
+
+/* One flow step, the equivalent of FlowGPU(XParam, XLoop, XForcing, XModel)
+ * (src/FlowGPU.cu:14-315) with the dt reduction of CalctimestepGPU
+ * (src/Advection.cu:549-620): reads loop->{totaltime, dt, dtmax,
+ * nextoutputtime}, writes loop->dt and loop->dtmax.  Like the reference it
+ * leaves loop->totaltime to the caller.  Synchronises the stream (dt is
+ * returned to the host). */
+int bgf_flow_step(bgf_handle* h, bgf_loop* loop);
+
+/* Device-resident time loop: repeats {flow step; totaltime += dt} while
+ * totaltime < endtime, at most maxsteps steps, without host synchronisation
+ * between steps (steps are captured in CUDA graphs).  nextoutputtime in loop
+ * clamps dt exactly like the reference; it is advanced by outputtimestep
+ * (if > 0) each time it is reached.  On return loop holds the final state
+ * of the time loop and *nsteps the number of steps taken.
+ * Returns BGF_EDT_UNDERFLOW if dt < dtmin before endtime (CrashDetection,
+ * src/Mainloop.cu:648-719). */
+int bgf_run(bgf_handle* h, bgf_loop* loop, double endtime, double outputtimestep, int maxsteps,
+            int* nsteps);
+
+/* Sum of h * delta_l^2 over active interior cells, accumulated in double on the
+ * device (the volume total of the reference tests, src/Testing.cu:1111-1129). */
+int bgf_volume(bgf_handle* h, double* volume);
+
+/* Number of kernel launches this handle has issued so far. */
+int64_t bgf_kernel_launches(bgf_handle* h);
+/* Per-kernel timing of bgf_flow_step: when on, CUDA events recorded on the
+ * handle's stream around the flux (predictor) and update (corrector) kernels
+ * accumulate their device times; turning it on resets the totals. */
+int bgf_set_profiling(bgf_handle* h, int on);
+int bgf_kernel_timing(bgf_handle* h, double* flux_ms, double* update_ms, int64_t* steps);
+/* Device time (ms) and kernel launches of the last bgf_run (events around its graphs). */
+int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches);
+
+/* ------------------------------------------------------------ mesh helpers */
+/* Uniform BUQ mesh as InitBlockxoyo / InitBlockneighbours build it
+ * (src/Mesh.cu:257-433): nbx*nby candidate blocks in row-major order, blocks
+ * whose present[] entry is 0 are skipped (masked), ids are assigned in order,
+ * neighbours are matched by position and default to the block itself at the
+ * domain edge.  Outputs are sized nbx*nby; returns the block count in *nblk.
+ * xo/yo (double) are the block origins relative to the domain origin. */
+int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* present, int* nblk, int* level,
+                     int* nbr8, double* xo, double* yo);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,196 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the CPU oracle on the
+same inputs.
+
+Bit-exact (dt sequence and h, u, v) wherever the reference path uses only IEEE
++ - * / sqrt (the library is built with --fmad=false).  Cases with Manning
+friction call cbrtf, which glibc (reference, oracle) and CUDA round differently
+in the last place; those are compared with the tolerance written in the test.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from runners import interior, make_gpu, make_oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+EXACT = [
+    ("gauss48_e1_b3", lambda: cases.gauss(48, 1, 3), 40),
+    ("gauss48_e2_b3", lambda: cases.gauss(48, 2, 3), 40),
+    ("gauss32_e1_b0", lambda: cases.gauss(32, 1, 0), 40),
+    ("hump64_e2", lambda: cases.hump_walls(64, 2), 30),
+    ("hump48_e1", lambda: cases.hump_walls(48, 1), 30),
+    ("dam48_e1", lambda: cases.dam_break(48, 1), 40),
+    ("dam32_e2", lambda: cases.dam_break(32, 2), 40),
+    ("island64_e1_still", lambda: cases.conical_island(64, 1, wave=False), 20),
+]
+# Manning friction (cbrtf): relative dt and absolute field tolerances
+TOLERANT = [
+    ("island64_e1", lambda: cases.conical_island(64, 1), 40),
+    ("island48_e2", lambda: cases.conical_island(48, 2), 40),
+    ("rain48_e1", lambda: cases.rain_on_terrain(48, 1), 30),
+]
+FIELD_TOL = 1e-5   # m or m/s after the stated number of steps
+DT_RTOL = 1e-5
+
+
+def _compare(f, o, exact):
+    zs, h, u, v = f.get_state()
+    for name, a in (("h", h), ("u", u), ("v", v)):
+        b = o.get(name)
+        ga, gb = interior(a).astype(np.float64), interior(b)
+        if exact:
+            assert np.array_equal(ga, gb), (name, float(np.abs(ga - gb).max()))
+        else:
+            assert float(np.abs(ga - gb).max()) <= FIELD_TOL, name
+
+
+@pytest.mark.parametrize("name,mk,nsteps", EXACT, ids=[c[0] for c in EXACT])
+def test_flow_step_bitexact_vs_oracle(name, mk, nsteps):
+    case = mk()
+    f, mesh, loop = make_gpu(case)
+    o, _ = make_oracle(case)
+    for s in range(nsteps):
+        dt = f.flow_step(loop)
+        loop.totaltime += dt
+        do = o.step(1)[0]
+        assert dt == do, (s, dt, do)
+    _compare(f, o, True)
+    assert f.kernel_launches() >= 2 * nsteps
+
+
+@pytest.mark.parametrize("name,mk,nsteps", TOLERANT, ids=[c[0] for c in TOLERANT])
+def test_flow_step_close_to_oracle(name, mk, nsteps):
+    case = mk()
+    f, mesh, loop = make_gpu(case)
+    o, _ = make_oracle(case)
+    for s in range(nsteps):
+        dt = f.flow_step(loop)
+        loop.totaltime += dt
+        do = o.step(1)[0]
+        assert abs(dt - do) <= DT_RTOL * do, (s, dt, do)
+    _compare(f, o, False)
+
+
+@pytest.mark.parametrize("name,mk,nsteps", EXACT[:4], ids=[c[0] for c in EXACT[:4]])
+def test_device_loop_equals_single_steps(name, mk, nsteps):
+    """bgf_run (device-resident loop in CUDA graphs) == nsteps calls of bgf_flow_step."""
+    case = mk()
+    f1, _, l1 = make_gpu(case)
+    f2, _, l2 = make_gpu(case)
+    for _ in range(nsteps):
+        l1.totaltime += f1.flow_step(l1)
+    n = f2.run(l2, endtime=1e30, maxsteps=nsteps)
+    assert n == nsteps
+    assert l2.totaltime == l1.totaltime and l2.dt == l1.dt
+    for a, b in zip(f1.get_state()[1:], f2.get_state()[1:]):
+        assert np.array_equal(interior(a), interior(b))
+
+
+def test_device_loop_stops_at_endtime_and_hits_output_times():
+    """The device loop clamps dt onto the output times and stops at endtime exactly
+    like the oracle driven with the same output schedule."""
+    case = cases.hump_walls(64, 2)
+    f, _, loop = make_gpu(case)
+    o, _ = make_oracle(case)
+    o.set_loop(0.0, 2.0, loop.dtmax)
+    loop.nextoutputtime = 2.0
+    n = f.run(loop, endtime=5.0, outputtimestep=2.0)
+    t, steps, next_out = 0.0, 0, 2.0
+    while t < 5.0:
+        dt = float(o.step(1)[0])
+        t = o.totaltime
+        steps += 1
+        if next_out - t <= dt * 1e-5:
+            next_out = min(next_out + 2.0, 5.0)
+            o.set_loop(t, next_out, dt)
+    assert steps == n
+    assert loop.totaltime == t
+    zs, h, u, v = f.get_state()
+    assert np.array_equal(interior(h), interior(o.get("h")))
+
+
+@pytest.mark.parametrize("name", ["gauss48_e1_b3", "gauss48_e2_b3", "hump64_e2", "dam48_e1"])
+def test_gpu_matches_reference_fixture(name):
+    mk = {"gauss48_e1_b3": lambda: cases.gauss(48, 1, 3), "gauss48_e2_b3": lambda: cases.gauss(48, 2, 3),
+          "hump64_e2": lambda: cases.hump_walls(64, 2), "dam48_e1": lambda: cases.dam_break(48, 1)}[name]
+    g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    f, _, loop = make_gpu(mk())
+    for s in range(int(g["nsteps"])):
+        dt = f.flow_step(loop)
+        loop.totaltime += dt
+        assert dt == g["dts"][s]
+    zs, h, u, v = f.get_state()
+    for k, a in (("h", h), ("u", u), ("v", v)):
+        assert np.array_equal(interior(a).astype(np.float32), g[k]), k
+
+
+def test_gaussian_hump_known_answer_on_gpu():
+    ref = json.load(open(os.path.join(GOLDEN, "zs_verif_buttinger.json")))
+    case = cases.gauss(256, engine=1, aoibnd=3)
+    f, mesh, loop = make_gpu(case)
+    f.run(loop, endtime=0.1)
+    zs = f.get_state()[0]
+    for k, expect in enumerate(ref["zs"]):
+        ii, jj = 16 * (k + 1) - 1, 127
+        ib = int(np.flatnonzero((mesh.bx == ii // 16) & (mesh.by == jj // 16))[0])
+        assert abs(float(zs[ib, jj % 16 + 1, ii % 16 + 1]) - expect) <= ref["tolerance"]
+
+
+def test_double_precision_bitexact_vs_oracle():
+    case = cases.dam_break(32, 1)
+    case.param.doubleprecision = 1
+    f, _, loop = make_gpu(case)
+    o, _ = make_oracle(case, use_double=True)
+    for s in range(30):
+        dt = f.flow_step(loop)
+        loop.totaltime += dt
+        assert dt == o.step(1)[0]
+    zs, h, u, v = f.get_state()
+    for name, a in (("h", h), ("u", u), ("v", v)):
+        assert np.array_equal(interior(a), interior(o.get(name))), name
+
+
+# ---------------------------------------------------------------- full-size properties
+
+def test_mass_conservation_with_walls_full_size():
+    """256x256 hump in a closed basin: volume constant to float32 round-off."""
+    case = cases.hump_walls(256, 2)
+    f, _, loop = make_gpu(case)
+    v0 = f.volume()
+    f.run(loop, endtime=10.0)
+    v1 = f.volume()
+    assert abs(v1 - v0) / v0 < 2e-6
+
+
+def test_lake_at_rest_is_preserved():
+    """Still water around the conical island stays still (well-balanced scheme)."""
+    for engine in (1, 2):
+        case = cases.conical_island(128, engine, wave=False)
+        case.param.frictionmodel = 0
+        case.param.cf = 0.0
+        f, _, loop = make_gpu(case)
+        f.run(loop, endtime=2.0)
+        zs, h, u, v = f.get_state()
+        assert float(np.abs(interior(u)).max()) < 1e-5
+        assert float(np.abs(interior(v)).max()) < 1e-5
+
+
+def test_symmetric_hump_stays_symmetric():
+    """Engine 2 on a centred hump: the X and Y sweeps are the same formula, so the
+    solution is symmetric under x <-> y."""
+    from bg_flood_b200.mesh import buq_to_grid
+    case = cases.hump_walls(128, 2)
+    f, mesh, loop = make_gpu(case)
+    f.run(loop, endtime=5.0)
+    zs, h, u, v = f.get_state()
+    H = buq_to_grid(h, mesh)
+    U = buq_to_grid(u, mesh)
+    V = buq_to_grid(v, mesh)
+    assert np.array_equal(H, H.T)
+    assert np.array_equal(U, V.T)

@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=1024, help="grid cells per side")
     ap.add_argument("--engine", type=int, default=1)
+    ap.add_argument("--fastmath", type=int, default=1, help="1: fast-math kernels, 0: bit-exact kernels")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     return ap.parse_args()
 
@@ -123,11 +124,25 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def workload_case(n: int, engine: int, dev: int):
+def workload_case(n: int, engine: int, dev: int, fastmath: int = 1):
     import cases
     case = cases.conical_island(n, engine=engine, dx=0.05 * 1024 / n if n != 1024 else 0.05)
     case.param.GPUDEVICE = dev
+    case.param.fastmath = fastmath
     return case
+
+
+def flushed_steps(f, loop, steps, flush):
+    """K flow steps, L2 flushed before each; returns (flux_ms, update_ms) summed."""
+    import torch
+    f.set_profiling(True)
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        loop.totaltime += f.flow_step(loop)
+    a, b, n = f.kernel_timing()
+    f.set_profiling(False)
+    return a, b
 
 
 def cpu_reference_sample(steps: int, warmup: int, engine: int):
@@ -187,7 +202,7 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
 
-    case = workload_case(args.n, args.engine, local)
+    case = workload_case(args.n, args.engine, local, args.fastmath)
     f, mesh, loop = make_gpu(case)
     ncell = mesh.nblk * 256
 
@@ -250,6 +265,16 @@ def main():
 
     extra = {}
     if not args.no_extra and rank == 0:
+        # the other kernel variant on the same workload, same protocol
+        other = workload_case(args.n, args.engine, local, 1 - args.fastmath)
+        fo, _, lo = make_gpu(other)
+        for _ in range(3):
+            lo.totaltime += fo.flow_step(lo)
+        a, b = flushed_steps(fo, lo, min(args.steps, 50), flush)
+        extra["bitexact_kernels" if args.fastmath else "fastmath_kernels"] = {
+            "value": ncell * min(args.steps, 50) / ((a + b) / 1e3), "flux_ms": a / min(args.steps, 50),
+            "update_ms": b / min(args.steps, 50)}
+        del fo
         # production mode: the device-resident loop (CUDA graphs), L2-warm, same workload
         l2 = type(loop)(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=1e30)
         f.init_dt(l2)
@@ -259,7 +284,7 @@ def main():
         extra["device_loop_L2_resident"] = {"value": ncell * 400 / (ms / 1e3), "steps": 400, "ms": ms}
         del f
         # a grid well above L2 (4096^2 cells, ~1 GB of state): HBM-bound device loop
-        big = workload_case(4096, args.engine, local)
+        big = workload_case(4096, args.engine, local, args.fastmath)
         fb, mb, lb = make_gpu(big)
         fb.run(lb, endtime=1e30, maxsteps=10)
         fb.run(lb, endtime=1e30, maxsteps=100)
@@ -279,6 +304,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "cells": ncell, "blocks": mesh.nblk, "engine": args.engine,
+                       "kernels": "fast-math (tolerance parity)" if args.fastmath else "bit-exact",
                        "l2": "flushed (256 MB write) before every timed step", "parallelism":
                        f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -20,7 +20,14 @@ LIBNAME = "libbgflood_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
            "-Xcompiler", "-ffp-contract=off"]
-SOURCES = ["bgf_flow.cu", "bgf_capi.cu", "bgf_host.cpp"]
+# (source, object name, extra flags): the flow kernels are built twice
+SOURCES = [
+    ("bgf_flow.cu", "bgf_flow_exact.o", ["-DBGF_VARIANT=exact"]),
+    ("bgf_flow.cu", "bgf_flow_fast.o", ["-DBGF_VARIANT=fast", "-DBGF_FAST=1", "--fmad=true", "-prec-div=false", "-prec-sqrt=false",
+                                        "-ftz=true"]),
+    ("bgf_capi.cu", "bgf_capi.o", []),
+    ("bgf_host.cpp", "bgf_host.o", ["-x", "cu"]),
+]
 
 
 def nvcc() -> str:
@@ -45,11 +52,10 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     if not force and not _stale(out, deps):
         return out
     objs = []
-    for src in SOURCES:
-        obj = os.path.join(LIBDIR, src + ".o")
-        cmd = [nvcc(), *ARCH, *NVFLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
-        if src.endswith(".cpp"):
-            cmd = [nvcc(), "-x", "cu", *ARCH, *NVFLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+    for src, oname, extra in SOURCES:
+        obj = os.path.join(LIBDIR, oname)
+        # later flags override the defaults (--fmad, -prec-div, ...)
+        cmd = [nvcc(), *ARCH, *NVFLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         if verbose:

@@ -17,6 +17,8 @@
 #include "bgf_internal.h"
 
 using namespace bgf;
+namespace ex = bgf::exact;
+namespace fa = bgf::fast;
 
 static thread_local std::string g_last_error;
 
@@ -37,7 +39,7 @@ struct HostSeg {
 
 struct bgf_handle {
     bgf_param P;
-    int nblkmem = 0, nblk = 0, dbl = 0, dev = 0;
+    int nblkmem = 0, nblk = 0, dbl = 0, dev = 0, fast = 0;
     size_t esz = 4;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -238,6 +240,7 @@ void bgf_param_default(bgf_param* p)
     p->aoibnd = 0;
     p->rainbnd = 0;
     p->GPUDEVICE = 0;
+    p->fastmath = 0;
 }
 
 const char* bgf_strerror(int s)
@@ -286,7 +289,9 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         delete h;
         return BGF_ENOKERNEL;
     }
-    cudaError_t e = h->dbl ? configure_kernels<double>() : configure_kernels<float>();
+    h->fast = p->fastmath ? 1 : 0;
+    cudaError_t e = h->dbl ? (h->fast ? fa::configure_kernels<double>() : ex::configure_kernels<double>())
+                           : (h->fast ? fa::configure_kernels<float>() : ex::configure_kernels<float>());
     if (e != cudaSuccess) {
         g_last_error = std::string("configure kernels: ") + cudaGetErrorString(e);
         delete h;
@@ -631,7 +636,8 @@ template <class T> static int init_dt_t(bgf_handle* h, bgf_loop* loop)
     BGF_CUDA(cudaMemcpyAsync(h->d_dtmin, &init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
     DevModel<T> m = dev_model<T>(h);
     StepParams<T> p = step_params<T>(h);
-    launch_initdt<T>(m, p, h->cur, h->d_dtmin, h->stream);
+    if (h->fast) fa::launch_initdt<T>(m, p, h->cur, h->d_dtmin, h->stream);
+    else ex::launch_initdt<T>(m, p, h->cur, h->d_dtmin, h->stream);
     h->launches++;
     BGF_CUDA(cudaGetLastError());
     unsigned long long bits = 0;
@@ -662,12 +668,22 @@ int bgf_init_dt(bgf_handle* h, bgf_loop* loop)
     return h->dbl ? init_dt_t<double>(h, loop) : init_dt_t<float>(h, loop);
 }
 
+template <class T> static void enqueue_flux(bgf_handle* h, int parity)
+{
+    if (h->fast) fa::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
+    else ex::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
+}
+
+template <class T> static void enqueue_update(bgf_handle* h, int parity)
+{
+    if (h->fast) fa::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
+    else ex::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
+}
+
 template <class T> static void enqueue_step(bgf_handle* h, int parity)
 {
-    DevModel<T> m = dev_model<T>(h);
-    StepParams<T> p = step_params<T>(h);
-    launch_flux<T>(m, p, h->P.engine, parity, h->stream);
-    launch_update<T>(m, p, h->P.engine, parity, h->stream);
+    enqueue_flux<T>(h, parity);
+    enqueue_update<T>(h, parity);
 }
 
 static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep, long long maxsteps)
@@ -704,13 +720,13 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
     if (h->profiling) {
         BGF_CUDA(cudaEventRecord(h->pev[0], h->stream));
         if (h->dbl) {
-            launch_flux<double>(dev_model<double>(h), step_params<double>(h), h->P.engine, h->parity, h->stream);
+            enqueue_flux<double>(h, h->parity);
             BGF_CUDA(cudaEventRecord(h->pev[1], h->stream));
-            launch_update<double>(dev_model<double>(h), step_params<double>(h), h->P.engine, h->parity, h->stream);
+            enqueue_update<double>(h, h->parity);
         } else {
-            launch_flux<float>(dev_model<float>(h), step_params<float>(h), h->P.engine, h->parity, h->stream);
+            enqueue_flux<float>(h, h->parity);
             BGF_CUDA(cudaEventRecord(h->pev[1], h->stream));
-            launch_update<float>(dev_model<float>(h), step_params<float>(h), h->P.engine, h->parity, h->stream);
+            enqueue_update<float>(h, h->parity);
         }
         BGF_CUDA(cudaEventRecord(h->pev[2], h->stream));
     } else if (h->dbl) {
@@ -825,8 +841,8 @@ int bgf_volume(bgf_handle* h, double* volume)
     if (rc) return rc;
     if (!volume) return BGF_EINVAL;
     BGF_CUDA(cudaMemsetAsync(h->d_scratch, 0, sizeof(double), h->stream));
-    if (h->dbl) launch_volume<double>(dev_model<double>(h), (double)h->P.delta, h->cur, h->d_scratch, h->stream);
-    else launch_volume<float>(dev_model<float>(h), (float)h->P.delta, h->cur, h->d_scratch, h->stream);
+    if (h->dbl) ex::launch_volume<double>(dev_model<double>(h), (double)h->P.delta, h->cur, h->d_scratch, h->stream);
+    else ex::launch_volume<float>(dev_model<float>(h), (float)h->P.delta, h->cur, h->d_scratch, h->stream);
     h->launches++;
     BGF_CUDA(cudaGetLastError());
     BGF_CUDA(cudaMemcpyAsync(volume, h->d_scratch, sizeof(double), cudaMemcpyDeviceToHost, h->stream));

@@ -1,11 +1,21 @@
 // Flow-step kernels (see bgf_flow.cuh for the design) and their launchers.
+//
+// This file is compiled twice: with BGF_VARIANT=exact (--fmad=false, IEEE
+// division and square root: bit-identical to the reference CPU build) and with
+// BGF_VARIANT=fast (FMA contraction, approximate division and square root,
+// flush-to-zero).  Each build puts its kernels and launchers in its own namespace.
 #include <cuda_runtime.h>
 #include <stdio.h>
 
 #include "bgf_flow.cuh"
 #include "bgf_internal.h"
 
+#ifndef BGF_VARIANT
+#define BGF_VARIANT exact
+#endif
+
 namespace bgf {
+namespace BGF_VARIANT {
 
 // ---------------------------------------------------------------- tile assembly
 
@@ -50,8 +60,8 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
         size_t g = (size_t)ib * 256 + tid;
         T hv = H[g], uv = U[g], vv = V[g];
         int c = ti(x, y);
-        s.h[c] = hv; s.u[c] = uv; s.v[c] = vv;
-        s.zs[c] = s.zb[hi18(x, y)] + hv;
+        s.t[VH][c] = hv; s.t[VU][c] = uv; s.t[VV][c] = vv;
+        s.t[VZS][c] = s.zb[hi18(x, y)] + hv;
         int c18 = hi18(x, y);
         s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
     }
@@ -65,8 +75,8 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
         size_t g = (size_t)sb * 256 + sy * 16 + sx;
         T hv = H[g], uv = U[g], vv = V[g];
         int c = ti(x, y);
-        s.h[c] = hv; s.u[c] = uv; s.v[c] = vv;
-        s.zs[c] = tile_zb(s, m, x, y, sb, sx, sy) + hv;
+        s.t[VH][c] = hv; s.t[VU][c] = uv; s.t[VV][c] = vv;
+        s.t[VZS][c] = tile_zb(s, m, x, y, sb, sx, sy) + hv;
         if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
             int c18 = hi18(x, y);
             s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
@@ -100,8 +110,8 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
         T ho, uo, vo;
         advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, m.dh[g], m.dhu[g], m.dhv[g], ho, uo, vo);
         int c = ti(x, y);
-        s.h[c] = ho; s.u[c] = uo; s.v[c] = vo;
-        s.zs[c] = tile_zb(s, m, x, y, sb, sx, sy) + ho;
+        s.t[VH][c] = ho; s.t[VU][c] = uo; s.t[VV][c] = vo;
+        s.t[VZS][c] = tile_zb(s, m, x, y, sb, sx, sy) + ho;
         if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
             int c18 = hi18(x, y);
             s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
@@ -201,21 +211,16 @@ __device__ __forceinline__ void apply_boundaries(Smem<T>& s, const DevModel<T>& 
 // updateEVCPU (src/Advection.cu:160-254), Cartesian.  Returns dh, dhu, dhv of the
 // thread's cell from the face arrays.
 template <class T>
-__device__ __forceinline__ void flux_divergence(const Smem<T>& s, const StepParams<T>& p, T delta, int x, int y, T hi,
+__device__ __forceinline__ void flux_divergence(const Smem<T>& s, const StepParams<T>& p, T cmdinv, int x, int y, T hi,
                                                 T uui, T vvi, T& dh, T& dhu, T& dhv)
 {
-    T cmdinv = (T)1.0 / ((T)1.0 * delta);
-    T ga = (T)0.5 * p.g;
-    T dmdl = ((T)1.0 - (T)1.0) / ((T)1.0 * delta);
-    T dmdt = ((T)1.0 - (T)1.0) / ((T)1.0 * delta);
-    T fG = vvi * dmdl - uui * dmdt;
-    int fi = fxi(x, y), fr = fxi(x + 1, y);
-    int gi = fyi(x, y), gt = fyi(x, y + 1);
+    // Cartesian grid: the metric terms dmdl, dmdt and fG of the reference are zero
+    // and their products only add signed zeros.
+    int fi = fxi(x, y), fr = fi + 1;
+    int gi = fyi(x, y), gt = gi + 16;
     dh = (T)-1.0 * (s.Fhu[fr] - s.Fhu[fi] + s.Fhv[gt] - s.Fhv[gi]) * cmdinv;
     dhu = (s.Fqux[fi] + s.Fquy[gi] - s.Su[fr] - s.Fquy[gt]) * cmdinv + p.fc * hi * vvi;
     dhv = (s.Fqvy[gi] + s.Fqvx[fi] - s.Sv[gt] - s.Fqvx[fr]) * cmdinv - p.fc * hi * uui;
-    dhu += hi * (ga * hi * dmdl + fG * vvi);
-    dhv += hi * (ga * hi * dmdt - fG * uui);
 }
 
 // ---------------------------------------------------------------- kernels
@@ -228,7 +233,7 @@ __device__ __forceinline__ bool step_live(const TimeState& ts)
 }
 
 template <class T, int ENGINE>
-__global__ void __launch_bounds__(NTHREADS) flux_kernel(DevModel<T> m, StepParams<T> p, int parity)
+__global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepParams<T> p, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
@@ -264,7 +269,7 @@ __global__ void __launch_bounds__(NTHREADS) flux_kernel(DevModel<T> m, StepParam
     const int x = tid & 15, y = tid >> 4;
     const int c = ti(x, y);
     T dh, dhu, dhv;
-    flux_divergence<T>(s, p, delta, x, y, s.h[c], s.u[c], s.v[c], dh, dhu, dhv);
+    flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, s.t[VH][c], s.t[VU][c], s.t[VV][c], dh, dhu, dhv);
     size_t g = (size_t)ib * 256 + tid;
     m.dh[g] = dh;
     m.dhu[g] = dhu;
@@ -284,7 +289,7 @@ template <class T> __device__ __forceinline__ T step_dt(const TimeState& ts, uns
 }
 
 template <class T, int ENGINE>
-__global__ void __launch_bounds__(NTHREADS) update_kernel(DevModel<T> m, StepParams<T> p, int parity)
+__global__ void __launch_bounds__(NTHREADS, 4) update_kernel(DevModel<T> m, StepParams<T> p, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
@@ -315,7 +320,7 @@ __global__ void __launch_bounds__(NTHREADS) update_kernel(DevModel<T> m, StepPar
     const int x = tid & 15, y = tid >> 4;
     const int c = ti(x, y);
     T dh, dhu, dhv;
-    flux_divergence<T>(s, p, delta, x, y, s.h[c], s.u[c], s.v[c], dh, dhu, dhv);
+    flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, s.t[VH][c], s.t[VU][c], s.t[VV][c], dh, dhu, dhv);
     // full step from state n (AdvkernelCPU with evolv), then friction on the result
     const int c18 = hi18(x, y);
     T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];
@@ -359,8 +364,7 @@ __global__ void __launch_bounds__(NTHREADS) update_kernel(DevModel<T> m, StepPar
         }
         m.time[parity ^ 1] = nt;
         // the next step reduces into the other slot
-        T epsi = M<T>::epsi();
-        m.dtmin[parity ^ 1] = dt_bits((T)1.0 / epsi);
+        m.dtmin[parity ^ 1] = dt_bits(inv_epsi<T>());
     }
 }
 
@@ -462,4 +466,5 @@ template void launch_initdt<double>(const DevModel<double>&, const StepParams<do
 template void launch_volume<float>(const DevModel<float>&, float, int, double*, cudaStream_t);
 template void launch_volume<double>(const DevModel<double>&, double, int, double*, cudaStream_t);
 
+}  // namespace BGF_VARIANT
 }  // namespace bgf

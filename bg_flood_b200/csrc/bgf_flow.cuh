@@ -149,21 +149,53 @@ __device__ __forceinline__ void ring_pos(int k, int& x, int& y)
     else { x = t; y = BW + ring; }
 }
 
+// Variables of the state tile / gradient arrays
+enum { VH = 0, VZS = 1, VU = 2, VV = 3 };
+
 template <class T> struct Smem {
-    T h[TW * TW], u[TW * TW], v[TW * TW], zs[TW * TW];
+    T t[4][TW * TW];           // h, zs, u, v on the 20x20 tile
     T zb[18 * 18];
-    T dhx[18 * 16], dzsx[18 * 16], dux[18 * 16], dvx[18 * 16];  // x-gradients
-    T dhy[16 * 18], dzsy[16 * 18], duy[16 * 18], dvy[16 * 18];  // y-gradients
+    T gx[4][18 * 16];          // x-gradients at x=-1..16, rows 0..15
+    T gy[4][16 * 18];          // y-gradients at y=-1..16, cols 0..15
     T dzbx[18 * 16], dzby[16 * 18];
     T Fhu[17 * 16], Fqux[17 * 16], Su[17 * 16], Fqvx[17 * 16];
     T Fhv[16 * 17], Fqvy[16 * 17], Sv[16 * 17], Fquy[16 * 17];
     // state n on the 18x18 tile (corrector: evolv for the boundary and the advance)
     T h0[18 * 18], u0[18 * 18], v0[18 * 18];
     T red[NTHREADS / 32];
-    double dt_d;
-    T dt;
-    int ok;
 };
+
+// Correctly rounded quotient x / d for a divisor shared by a whole block, from the
+// precomputed r = RN(1/d): one product and two Newton-Raphson correction steps with
+// exact residuals (Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; the last step is
+// Markstein's correctly-rounding theorem).  Tiny numerators, whose residual could
+// underflow, take the IEEE division.
+template <class T> __device__ __forceinline__ T div_by(T x, T d, T r);
+#if BGF_FAST
+// fast-math build: one product with the rounded reciprocal (within about an ulp)
+template <> __device__ __forceinline__ float div_by<float>(float x, float d, float r) { return x * r; }
+template <> __device__ __forceinline__ double div_by<double>(double x, double d, double r) { return x * r; }
+#else
+template <> __device__ __forceinline__ float div_by<float>(float x, float d, float r)
+{
+    if (fabsf(x) < 0x1p-90f) return x / d;
+    float q = x * r;
+    float e = fmaf(-q, d, x);
+    q = fmaf(e, r, q);
+    e = fmaf(-q, d, x);
+    return fmaf(e, r, q);
+}
+template <> __device__ __forceinline__ double div_by<double>(double x, double d, double r)
+{
+    if (fabs(x) < 0x1p-960) return x / d;
+    double q = x * r;
+    double e = fma(-q, d, x);
+    q = fma(e, r, q);
+    e = fma(-q, d, x);
+    return fma(e, r, q);
+}
+#endif
 
 // One X (isx) or Y face of the tile, written to the face arrays of s.
 template <class T, int ENGINE>
@@ -171,18 +203,18 @@ __device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p,
 {
     FaceIn<T, ENGINE> f;
     int ci = ti(x, y), cn = isx ? ti(x - 1, y) : ti(x, y - 1);
-    f.hi = s.h[ci]; f.hn = s.h[cn];
-    f.zsi = s.zs[ci]; f.zsn = s.zs[cn];
+    f.hi = s.t[VH][ci]; f.hn = s.t[VH][cn];
+    f.zsi = s.t[VZS][ci]; f.zsn = s.t[VZS][cn];
     if (isx) {
-        int gi = gxi(x, y), gn = gxi(x - 1, y);
-        f.uni = s.u[ci]; f.unn = s.u[cn]; f.uti = s.v[ci]; f.utn = s.v[cn];
-        f.dhi = s.dhx[gi]; f.dhn = s.dhx[gn]; f.dzsi = s.dzsx[gi]; f.dzsn = s.dzsx[gn];
-        f.duni = s.dux[gi]; f.dunn = s.dux[gn]; f.duti = s.dvx[gi]; f.dutn = s.dvx[gn];
+        int gi = gxi(x, y), gn = gi - 1;
+        f.uni = s.t[VU][ci]; f.unn = s.t[VU][cn]; f.uti = s.t[VV][ci]; f.utn = s.t[VV][cn];
+        f.dhi = s.gx[VH][gi]; f.dhn = s.gx[VH][gn]; f.dzsi = s.gx[VZS][gi]; f.dzsn = s.gx[VZS][gn];
+        f.duni = s.gx[VU][gi]; f.dunn = s.gx[VU][gn]; f.duti = s.gx[VV][gi]; f.dutn = s.gx[VV][gn];
     } else {
-        int gi = gyi(x, y), gn = gyi(x, y - 1);
-        f.uni = s.v[ci]; f.unn = s.v[cn]; f.uti = s.u[ci]; f.utn = s.u[cn];
-        f.dhi = s.dhy[gi]; f.dhn = s.dhy[gn]; f.dzsi = s.dzsy[gi]; f.dzsn = s.dzsy[gn];
-        f.duni = s.dvy[gi]; f.dunn = s.dvy[gn]; f.duti = s.duy[gi]; f.dutn = s.duy[gn];
+        int gi = gyi(x, y), gn = gi - 16;
+        f.uni = s.t[VV][ci]; f.unn = s.t[VV][cn]; f.uti = s.t[VU][ci]; f.utn = s.t[VU][cn];
+        f.dhi = s.gy[VH][gi]; f.dhn = s.gy[VH][gn]; f.dzsi = s.gy[VZS][gi]; f.dzsn = s.gy[VZS][gn];
+        f.duni = s.gy[VV][gi]; f.dunn = s.gy[VV][gn]; f.duti = s.gy[VU][gi]; f.dutn = s.gy[VU][gn];
     }
     f.hsi = f.hi;
     f.hsn = f.hn;
@@ -214,40 +246,53 @@ template <class T, int ENGINE>
 __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T delta, int tid)
 {
     const T theta = p.theta;
-    // x-gradients at x=-1..16 (rows 0..15) and y-gradients at y=-1..16 (cols 0..15)
-    for (int k = tid; k < 18 * 16; k += NTHREADS) {
-        int x = k % 18 - 1, y = k / 18;
-        int c = ti(x, y), l = ti(x - 1, y), r = ti(x + 1, y);
-        s.dhx[k] = minmod2(theta, s.h[l], s.h[c], s.h[r]) / delta;
-        s.dzsx[k] = minmod2(theta, s.zs[l], s.zs[c], s.zs[r]) / delta;
-        s.dux[k] = minmod2(theta, s.u[l], s.u[c], s.u[r]) / delta;
-        s.dvx[k] = minmod2(theta, s.v[l], s.v[c], s.v[r]) / delta;
-        int xx = k % 16, yy = k / 16 - 1;
-        int cy = ti(xx, yy), b = ti(xx, yy - 1), t = ti(xx, yy + 1);
-        s.dhy[k] = minmod2(theta, s.h[b], s.h[cy], s.h[t]) / delta;
-        s.dzsy[k] = minmod2(theta, s.zs[b], s.zs[cy], s.zs[t]) / delta;
-        s.duy[k] = minmod2(theta, s.u[b], s.u[cy], s.u[t]) / delta;
-        s.dvy[k] = minmod2(theta, s.v[b], s.v[cy], s.v[t]) / delta;
+    const T rdelta = (T)1.0 / delta;
+    const int tx = tid & 15, ty = tid >> 4;
+    {
+        // interior cell of this thread: x- and y-gradients of h, zs, u, v
+        const int c = ti(tx, ty), gi = gxi(tx, ty), gj = gyi(tx, ty);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const T* a = s.t[k];
+            s.gx[k][gi] = div_by(minmod2(theta, a[c - 1], a[c], a[c + 1]), delta, rdelta);
+            s.gy[k][gj] = div_by(minmod2(theta, a[c - TW], a[c], a[c + TW]), delta, rdelta);
+        }
+        // one ring gradient per thread: ring cell r = tid/4 (64 cells), variable tid%4;
+        // x-gradients on the left/right ring columns, y-gradients on the bottom/top rows
+        const int r = tid >> 2, k = tid & 3, side = r >> 4, q = r & 15;
+        const T* a = s.t[k];
+        int cr, st, o;
+        T* out;
+        if (side == 0) { cr = ti(-1, q); st = 1; out = &s.gx[k][gxi(-1, q)]; }
+        else if (side == 1) { cr = ti(BW, q); st = 1; out = &s.gx[k][gxi(BW, q)]; }
+        else if (side == 2) { cr = ti(q, -1); st = TW; out = &s.gy[k][gyi(q, -1)]; }
+        else { cr = ti(q, BW); st = TW; out = &s.gy[k][gyi(q, BW)]; }
+        (void)o;
+        *out = div_by(minmod2(theta, a[cr - st], a[cr], a[cr + st]), delta, rdelta);
     }
     __syncthreads();
     if (ENGINE == 1) {
         // Wet-slope reset: interior cells follow WetsloperesetCPU (its y test compares
         // both reconstructions with zs[yminus]); ring-1 cells follow the halo variants.
-        for (int k = tid; k < 18 * 16; k += NTHREADS) {
-            int x = k % 18 - 1, y = k / 18;
-            int c = ti(x, y);
-            s.dzsx[k] = wetslope(delta, s.zs[c], s.h[c], s.zs[ti(x - 1, y)], s.zs[ti(x + 1, y)], s.dzsx[k], s.dhx[k],
-                                 s.dzbx[k]);
-            int xx = k % 16, yy = k / 16 - 1;
-            int cy = ti(xx, yy);
-            bool interior = (yy >= 0 && yy < BW);
-            T zsm = s.zs[ti(xx, yy - 1)];
-            T zsp = interior ? zsm : s.zs[ti(xx, yy + 1)];
-            s.dzsy[k] = wetslope(delta, s.zs[cy], s.h[cy], zsm, zsp, s.dzsy[k], s.dhy[k], s.dzby[k]);
+        const T* zs = s.t[VZS];
+        const T* hh = s.t[VH];
+        {
+            const int c = ti(tx, ty), gi = gxi(tx, ty), gj = gyi(tx, ty);
+            s.gx[VZS][gi] = wetslope(delta, zs[c], hh[c], zs[c - 1], zs[c + 1], s.gx[VZS][gi], s.gx[VH][gi], s.dzbx[gi]);
+            s.gy[VZS][gj] = wetslope(delta, zs[c], hh[c], zs[c - TW], zs[c - TW], s.gy[VZS][gj], s.gy[VH][gj], s.dzby[gj]);
+        }
+        if (tid < 64) {
+            const int side = tid >> 4, q = tid & 15;
+            if (side < 2) {
+                const int x = side == 0 ? -1 : BW, c = ti(x, q), g = gxi(x, q);
+                s.gx[VZS][g] = wetslope(delta, zs[c], hh[c], zs[c - 1], zs[c + 1], s.gx[VZS][g], s.gx[VH][g], s.dzbx[g]);
+            } else {
+                const int y = side == 2 ? -1 : BW, c = ti(q, y), g = gyi(q, y);
+                s.gy[VZS][g] = wetslope(delta, zs[c], hh[c], zs[c - TW], zs[c + TW], s.gy[VZS][g], s.gy[VH][g], s.dzby[g]);
+            }
         }
         __syncthreads();
     }
-    const int tx = tid & 15, ty = tid >> 4;
     // Thread (tx,ty) owns the left (X) and bottom (Y) faces of its cell; threads
     // 0..15 also take X face x=16 and threads 16..31 Y face y=16 (the faces the
     // reference computes in the right / top halo column).

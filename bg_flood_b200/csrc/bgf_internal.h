@@ -12,11 +12,24 @@ struct SegDev;
 template <class T> struct DevModel;
 template <class T> struct StepParams;
 
-template <class T> cudaError_t configure_kernels();
-template <class T> void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st);
-template <class T> void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st);
-template <class T> void launch_initdt(const DevModel<T>& m, const StepParams<T>& p, int cur, unsigned long long* out, cudaStream_t st);
-template <class T> void launch_volume(const DevModel<T>& m, T delta0, int cur, double* out, cudaStream_t st);
+// Kernel launchers, built twice (bgf_flow.cu): "exact" reproduces the reference
+// CPU arithmetic bit for bit, "fast" trades the last bits for speed.
+#define BGF_DECLARE_LAUNCHERS                                                                                   \
+    template <class T> cudaError_t configure_kernels();                                                        \
+    template <class T>                                                                                         \
+    void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st);   \
+    template <class T>                                                                                         \
+    void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st); \
+    template <class T>                                                                                         \
+    void launch_initdt(const DevModel<T>& m, const StepParams<T>& p, int cur, unsigned long long* out,         \
+                       cudaStream_t st);                                                                       \
+    template <class T> void launch_volume(const DevModel<T>& m, T delta0, int cur, double* out, cudaStream_t st);
+namespace exact {
+BGF_DECLARE_LAUNCHERS
+}
+namespace fast {
+BGF_DECLARE_LAUNCHERS
+}
 
 // Host restatement of the bed preparation the reference performs once at
 // initialisation (src/InitialConditions.cu:140-144): bed halo fill and bed

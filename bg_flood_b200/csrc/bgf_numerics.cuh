@@ -29,6 +29,11 @@ template <> struct M<double> {
     static __device__ __forceinline__ double epsi() { return nextafter(1.0, 2.0) - 1.0; }
 };
 
+// 1 / (nextafter(1, 2) - 1): the "dry" time step of the reference sweeps
+template <class T> __device__ __forceinline__ T inv_epsi();
+template <> __device__ __forceinline__ float inv_epsi<float>() { return 8388608.0f; }
+template <> __device__ __forceinline__ double inv_epsi<double>() { return 4503599627370496.0; }
+
 // calcres (src/Util_CPU.cu:193-198)
 template <class T> __device__ __forceinline__ T calcres(T dx, int level)
 {
@@ -40,13 +45,13 @@ template <class T> __device__ __forceinline__ T minmod2(T theta, T s0, T s1, T s
 {
     if (s0 < s1 && s1 < s2) {
         T d1 = theta * (s1 - s0);
-        T d2 = (s2 - s0) / (T)2.0;
+        T d2 = (s2 - s0) * (T)0.5;  // == (s2 - s0) / 2, exactly
         T d3 = theta * (s2 - s1);
         if (d2 < d1) d1 = d2;
         return M<T>::fmin_(d1, d3);
     }
     if (s0 > s1 && s1 > s2) {
-        T d1 = theta * (s1 - s0), d2 = (s2 - s0) / (T)2.0, d3 = theta * (s2 - s1);
+        T d1 = theta * (s1 - s0), d2 = (s2 - s0) * (T)0.5, d3 = theta * (s2 - s1);
         if (d2 > d1) d1 = d2;
         return M<T>::fmax_(d1, d3);
     }
@@ -72,12 +77,11 @@ __device__ __forceinline__ T kurg_solver(T g, T delta, T epsi, T CFL, T hp, T hm
         T apm = ap * am;
         fh = (ap * qm - am * qp + apm * (hp - hm)) * ad;
         fu = (ap * (qm * um + ga * (hm * hm)) - am * (qp * up + ga * (hp * hp)) + apm * (qp - qm)) * ad;
-        T dlt = delta * (T)1.0 / (T)1.0;
-        return CFL * dlt / a;
+        return CFL * delta / a;  // dlt = delta * cm / fm with cm = fm = 1
     }
     fh = (T)0.0;
     fu = (T)0.0;
-    return (T)1.0 / epsi;
+    return inv_epsi<T>();
 }
 
 // hllc (src/Reimann.cu:838-877), Cartesian metric.
@@ -86,30 +90,29 @@ __device__ __forceinline__ T hllc(T g, T delta, T epsi, T CFL, T hm, T hp, T um,
 {
     T cmo = M<T>::sqrt_(g * hm);
     T cp = M<T>::sqrt_(g * hp);
-    T ustar = (um + up) / (T)2. + cmo - cp;
-    T cstar = (cmo + cp) / (T)2. + (um - up) / (T)4.;
+    T ustar = (um + up) * (T)0.5 + cmo - cp;  // halving and quartering are exact
+    T cstar = (cmo + cp) * (T)0.5 + (um - up) * (T)0.25;
     T SL = hm == (T)0. ? up - (T)2. * cp : M<T>::fmin_(um - cmo, ustar - cstar);
     T SR = hp == (T)0. ? um + (T)2. * cmo : M<T>::fmax_(up + cp, ustar + cstar);
     if ((T)0. <= SL) {
         fh = um * hm;
-        fq = hm * (um * um + g * hm / (T)2.);
+        fq = hm * (um * um + g * hm * (T)0.5);
     } else if ((T)0. >= SR) {
         fh = up * hp;
-        fq = hp * (up * up + g * hp / (T)2.);
+        fq = hp * (up * up + g * hp * (T)0.5);
     } else {
         T fhm = um * hm;
-        T fum = hm * (um * um + g * hm / (T)2.);
+        T fum = hm * (um * um + g * hm * (T)0.5);
         T fhp = up * hp;
-        T fup = hp * (up * up + g * hp / (T)2.);
+        T fup = hp * (up * up + g * hp * (T)0.5);
         fh = (SR * fhm - SL * fhp + SL * SR * (hp - hm)) / (SR - SL);
         fq = (SR * fum - SL * fup + SL * SR * (hp * up - hm * um)) / (SR - SL);
     }
     double a = (double)M<T>::fmax_(M<T>::fabs_(SL), M<T>::fabs_(SR));
     if (a > (double)epsi) {
-        T dlt = delta * (T)1.0 / (T)1.0;
-        return CFL * dlt / (T)a;
+        return CFL * delta / (T)a;
     }
-    return (T)1.0 / epsi;
+    return inv_epsi<T>();
 }
 
 // Result of one face of the X or Y sweep (reference FluxP members for that face).
@@ -194,7 +197,7 @@ __device__ __forceinline__ Face<T> face_flux(const FaceIn<T, ENGINE>& f, T g, T 
         r.Ft = fv;
         r.wet = true;
     } else {
-        r.dt = (T)1.0 / epsi;
+        r.dt = inv_epsi<T>();
         r.Fh = (T)0.0;
         r.Fq = (T)0.0;
         r.S = (T)0.0;

@@ -23,7 +23,7 @@ class CParam(ctypes.Structure):
         "bndtaper", "bndrelaxtime", "bndfiltertime", "inittime", "dtmin", "dtinit", "mask")] + \
         [(n, ctypes.c_int) for n in (
             "engine", "frictionmodel", "ForceMassConserve", "wetdryfix", "conserveElevation",
-            "doubleprecision", "minlevel", "maxlevel", "initlevel", "aoibnd", "rainbnd", "GPUDEVICE")]
+            "doubleprecision", "minlevel", "maxlevel", "initlevel", "aoibnd", "rainbnd", "GPUDEVICE", "fastmath")]
 
 
 @dataclass
@@ -54,6 +54,7 @@ class Param:
     lat: float = 0.0
     GPUDEVICE: int = 0
     doubleprecision: int = 0
+    fastmath: int = 0  # library option, not a reference key: 1 selects the fast-math kernels
     engine: int = 1
     dx: float = math.nan
     xo: float = math.nan

@@ -77,6 +77,11 @@ typedef struct bgf_param {
     int aoibnd;           /* boundary type of the remainder segment, 0 wall   */
     int rainbnd;          /* 0: no rain on the two outermost cell rows        */
     int GPUDEVICE;        /* CUDA device ordinal                              */
+    int fastmath;         /* 0: kernels reproduce the reference CPU arithmetic
+                             bit for bit (no FMA contraction, IEEE division and
+                             square root); 1: FMA contraction and approximate
+                             division / square root (results within the
+                             tolerances of the parity tests)                   */
 } bgf_param;
 
 /* Reference Loop<T> members the step reads and writes (src/Arrays.h:359-404). */

@@ -183,7 +183,8 @@ def test_lake_at_rest_is_preserved():
 
 def test_symmetric_hump_stays_symmetric():
     """Engine 2 on a centred hump: the X and Y sweeps are the same formula, so the
-    solution is symmetric under x <-> y."""
+    solution is symmetric under x <-> y up to the summation order of the flux
+    divergence (X then Y terms), i.e. to float32 rounding."""
     from bg_flood_b200.mesh import buq_to_grid
     case = cases.hump_walls(128, 2)
     f, mesh, loop = make_gpu(case)
@@ -192,5 +193,52 @@ def test_symmetric_hump_stays_symmetric():
     H = buq_to_grid(h, mesh)
     U = buq_to_grid(u, mesh)
     V = buq_to_grid(v, mesh)
-    assert np.array_equal(H, H.T)
-    assert np.array_equal(U, V.T)
+    assert float(np.abs(H - H.T).max()) <= 1e-6 * float(np.abs(H).max())
+    assert float(np.abs(U - V.T).max()) <= 1e-5 * float(np.abs(U).max())
+
+
+# ---------------------------------------------------------------- fast-math kernels
+
+FAST_CASES = [
+    ("gauss48_e1_b3", lambda: cases.gauss(48, 1, 3), 40),
+    ("hump64_e2", lambda: cases.hump_walls(64, 2), 30),
+    ("dam48_e1", lambda: cases.dam_break(48, 1), 40),
+    ("island64_e1", lambda: cases.conical_island(64, 1), 40),
+    ("rain48_e1", lambda: cases.rain_on_terrain(48, 1), 30),
+]
+FAST_FIELD_TOL = 2e-4   # m, m/s after the stated number of steps
+FAST_DT_RTOL = 1e-4
+
+
+@pytest.mark.parametrize("name,mk,nsteps", FAST_CASES, ids=[c[0] for c in FAST_CASES])
+def test_fastmath_kernels_close_to_oracle(name, mk, nsteps):
+    case = mk()
+    case.param.fastmath = 1
+    f, _, loop = make_gpu(case)
+    o, _ = make_oracle(case)
+    for s in range(nsteps):
+        dt = f.flow_step(loop)
+        loop.totaltime += dt
+        do = o.step(1)[0]
+        assert abs(dt - do) <= FAST_DT_RTOL * do, (s, dt, do)
+    zs, h, u, v = f.get_state()
+    for nm, a in (("h", h), ("u", u), ("v", v)):
+        assert float(np.abs(interior(a).astype(np.float64) - interior(o.get(nm))).max()) <= FAST_FIELD_TOL, nm
+
+
+@pytest.mark.parametrize("fast", [0, 1])
+def test_fp32_eta_error_against_fp64_oracle(fast):
+    """Both kernel variants in FP32 stay within 1e-3 m of the FP64 oracle on the
+    wet/dry run-up case (2 s of simulated time, 128x128)."""
+    case = cases.conical_island(128, 1)
+    case.param.fastmath = fast
+    f, mesh, loop = make_gpu(case)
+    o, _ = make_oracle(case, use_double=True)
+    loop.nextoutputtime = 2.0
+    f.run(loop, endtime=2.0)
+    o.set_loop(0.0, 2.0, o.init_loop(0.0, 2.0))
+    while o.totaltime < 2.0:
+        o.step(1)
+    zs, h, u, v = f.get_state()
+    err = float(np.abs(interior(zs).astype(np.float64) - interior(o.get("zs"))).max())
+    assert err <= 1e-3, err

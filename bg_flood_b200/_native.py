@@ -41,6 +41,7 @@ SIGNATURES = {
     "bgf_set_profiling": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "bgf_kernel_timing": (ctypes.c_int, [c_void_p, c_double_p, c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "bgf_run_timing": (ctypes.c_int, [c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "bgf_flow_step_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "bgf_mesh_uniform": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, c_void_p, c_int_p, c_int_p,
                                         c_int_p, c_double_p, c_double_p]),
 }

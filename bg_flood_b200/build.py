@@ -26,6 +26,7 @@ SOURCES = [
     ("bgf_flow.cu", "bgf_flow_fast.o", ["-DBGF_VARIANT=fast", "-DBGF_FAST=1", "--fmad=true", "-prec-div=false", "-prec-sqrt=false",
                                         "-ftz=true"]),
     ("bgf_capi.cu", "bgf_capi.o", []),
+    ("bgf_noalloc.cu", "bgf_noalloc.o", []),
     ("bgf_host.cpp", "bgf_host.o", ["-x", "cu"]),
 ]
 

@@ -22,6 +22,8 @@ namespace fa = bgf::fast;
 
 static thread_local std::string g_last_error;
 
+void bgf::set_last_error(const std::string& msg) { g_last_error = msg; }
+
 #define BGF_CUDA(call)                                                                 \
     do {                                                                               \
         cudaError_t e_ = (call);                                                       \

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
 #include <vector>
 
 namespace bgf {
@@ -30,6 +31,9 @@ BGF_DECLARE_LAUNCHERS
 namespace fast {
 BGF_DECLARE_LAUNCHERS
 }
+
+// Records the text returned by bgf_last_error() for this thread.
+void set_last_error(const std::string& msg);
 
 // Host restatement of the bed preparation the reference performs once at
 // initialisation (src/InitialConditions.cu:140-144): bed halo fill and bed

@@ -192,6 +192,44 @@ int bgf_kernel_timing(bgf_handle* h, double* flux_ms, double* update_ms, int64_t
 /* Device time (ms) and kernel launches of the last bgf_run (events around its graphs). */
 int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches);
 
+/* ------------------------------------------------------------ allocation-free step */
+/* No counterpart in the reference.  One flow step (the two kernels of
+ * bgf_flow_step) for callers that cannot allocate device memory once they are
+ * running -- e.g. a service that reserves its GPU memory pool at start-up and
+ * treats any later cudaMalloc as a fault, or a host model that owns all its
+ * device arrays (like BG_Flood's Model<T>) and may not trigger the device-wide
+ * synchronisation of cudaMalloc / cudaFree.  It calls no allocating routine: the
+ * caller passes device pointers to its inputs and outputs, and the kernels'
+ * scratch (flux divergence, dt reduction, time slots, boundary running means)
+ * lives in one static device array sized for BGF_NOALLOC_MAX_BLOCKS blocks in
+ * double precision (about 3.3 MB), which every GPU that loads the library keeps
+ * until the process exits.
+ * - The first call on a device finds the array's device address and writes its
+ *   constant part; make that first call before any stream capture.
+ * - Every call shares the array and it keeps the last call's contents; the parts
+ *   that must start at zero are cleared on each call.  Calls whose GPU work
+ *   overlaps (other streams, other threads) race on it.
+ * - nblkmem > BGF_NOALLOC_MAX_BLOCKS is rejected with BGF_EINVAL.
+ * - Single-level meshes only; no rain, uniform friction coefficient.  Boundary
+ *   sides carry a type (0 wall, 1 Neumann, 2 Dirichlet at Param.zsinit,
+ *   3 absorbing 1D) or -1 for a side with a neighbour.
+ * State layout here is the kernels' own: 256 values per block slot, cell
+ * (i, j) at j * 16 + i; the output arrays must not alias the inputs.
+ * Synchronises `stream` (dt is returned to the host, as bgf_flow_step does). */
+#define BGF_NOALLOC_MAX_BLOCKS 512
+typedef struct bgf_noalloc_args {
+    int nblk, nblkmem;
+    const int* active;    /* device: nblk active block ids                     */
+    const int* level;     /* device: nblkmem                                   */
+    const int* nbr;       /* device: [8][nblkmem] LeftBot, LeftTop, RightBot,
+                             RightTop, BotLeft, BotRight, TopLeft, TopRight    */
+    const int* bndtype;   /* device: [nblkmem][4] side type (left, right, top, bot) */
+    const void *zb, *dzbdx, *dzbdy; /* device BUQ tiles, 324 per block slot    */
+    const void *h_in, *u_in, *v_in; /* device, 256 per block slot              */
+    void *h_out, *u_out, *v_out;    /* device, 256 per block slot              */
+} bgf_noalloc_args;
+int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* args, bgf_loop* loop, void* stream);
+
 /* ------------------------------------------------------------ mesh helpers */
 /* Uniform BUQ mesh as InitBlockxoyo / InitBlockneighbours build it
  * (src/Mesh.cu:257-433): nbx*nby candidate blocks in row-major order, blocks

@@ -18,16 +18,16 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIBNAME = "libbgflood_b200.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
            "-Xcompiler", "-ffp-contract=off"]
 # (source, object name, extra flags): the flow kernels are built twice
 SOURCES = [
-    ("bgf_flow.cu", "bgf_flow_exact.o", ["-DBGF_VARIANT=exact"]),
+    ("bgf_flow.cu", "bgf_flow_exact.o", ["-DBGF_VARIANT=exact", "--fmad=false"]),
     ("bgf_flow.cu", "bgf_flow_fast.o", ["-DBGF_VARIANT=fast", "-DBGF_FAST=1", "--fmad=true", "-prec-div=false", "-prec-sqrt=false",
                                         "-ftz=true"]),
-    ("bgf_capi.cu", "bgf_capi.o", []),
-    ("bgf_noalloc.cu", "bgf_noalloc.o", []),
-    ("bgf_host.cpp", "bgf_host.o", ["-x", "cu"]),
+    ("bgf_capi.cu", "bgf_capi.o", ["--fmad=false"]),
+    ("bgf_noalloc.cu", "bgf_noalloc.o", ["--fmad=false"]),
+    ("bgf_host.cpp", "bgf_host.o", ["-x", "cu", "--fmad=false"]),
 ]
 
 

@@ -19,6 +19,8 @@
 #define LOG logf
 #define SIN sinf
 #define NEXTAFTER nextafterf
+#define CEIL ceilf
+#define FLOOR floorf
 #define HUGEPOS FLT_MAX
 #include "bgf_oracle_impl.inc"
 #undef REAL
@@ -31,6 +33,8 @@
 #undef LOG
 #undef SIN
 #undef NEXTAFTER
+#undef CEIL
+#undef FLOOR
 #undef HUGEPOS
 #undef ML
 #undef BW
@@ -45,6 +49,8 @@
 #define LOG log
 #define SIN sin
 #define NEXTAFTER nextafter
+#define CEIL ceil
+#define FLOOR floor
 #define HUGEPOS DBL_MAX
 #include "bgf_oracle_impl.inc"
 

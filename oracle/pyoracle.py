@@ -80,6 +80,10 @@ def ref_lib():
         l.ref_set_segment_series.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D, D]
         l.ref_set_rain_series.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         l.ref_destroy.argtypes = [ctypes.c_void_p]
+        l.ref_adapt.argtypes = [ctypes.c_void_p]
+        l.ref_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, D]
+        l.ref_reinit.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        l.ref_get_active.argtypes = [ctypes.c_void_p, I]
         _rlib = l
     return _rlib
 
@@ -222,3 +226,30 @@ class Reference:
         dts = np.zeros(n)
         self.lib.ref_step(self.h, n, _dp(dts))
         return dts
+
+    def adapt(self) -> int:
+        """Runs the reference's own Adaptation() with the "Adaptation" key of paramtext."""
+        self.nblk = self.lib.ref_adapt(self.h)
+        return self.nblk
+
+    def active(self) -> np.ndarray:
+        a = np.zeros(self.nblk, np.int32)
+        self.lib.ref_get_active(self.h, a.ctypes.data_as(I))
+        return a
+
+    def set(self, name: str, buq):
+        a = np.ascontiguousarray(buq, np.float64).reshape(-1)
+        assert a.size == self.nblk * 324
+        if self.lib.ref_set(self.h, name.encode(), _dp(a)):
+            raise KeyError(name)
+
+    def reinit(self, nextoutputtime: float):
+        self.lib.ref_reinit(self.h, nextoutputtime)
+
+    def mesh_active_order(self):
+        """Block tables renumbered to active order: (level, nbr (nblk, 8), xo, yo)."""
+        act = self.active()
+        pos = {int(b): k for k, b in enumerate(act)}
+        lev, nb, xo, yo = self.blocks()
+        nbr = np.vectorize(lambda b: pos[int(b)])(nb).astype(np.int32)
+        return lev, nbr, xo, yo

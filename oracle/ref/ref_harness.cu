@@ -35,6 +35,9 @@ struct RefBase {
     virtual int get(const char* name, double* out) = 0;
     virtual int get_blocks(int* level, double* xo, double* yo, int* nbr8) = 0;
     virtual int adapt() = 0;
+    virtual int set(const char* name, const double* buq) = 0;
+    virtual int reinit(double nextout) = 0;
+    virtual int get_active(int* out) = 0;
     Param P;
     Forcing<float> F;
     double totaltime = 0.0, nextoutputtime = 0.0, dtmax = 0.0;
@@ -221,7 +224,59 @@ template <class T> struct RefModel : RefBase {
         return P.nblk;
     }
 
-    int adapt() override { return -1; }
+    // The reference's own initial mesh adaptation (InitialAdaptation,
+    // src/Adaptation.cu:133-146: Adaptation then InitialConditions, which also
+    // rebuilds the boundary block lists) on the current state, with the criterion
+    // given by the "Adaptation" key.
+    int adapt() override
+    {
+        CopyArrayBUQ(P, M.blocks, M.evolv, M.evolv_o);
+        InitialAdaptation(P, F, M);
+        return P.nblk;
+    }
+
+    // Whole 18x18 tiles in active-block order (the layout of get()).
+    int set(const char* name, const double* buq) override
+    {
+        T* p = field(name, false);
+        if (!p) return -1;
+        for (int ibl = 0; ibl < P.nblk; ibl++) {
+            int ib = M.blocks.active[ibl];
+            for (int k = 0; k < P.blksize; k++) p[(size_t)ib * P.blksize + k] = T(buq[(size_t)ibl * P.blksize + k]);
+        }
+        return 0;
+    }
+
+    // After fields were set on an adapted mesh: bed halo and gradients as
+    // src/Testing.cu:583-588 does, zs = zb + h, state copy, fresh loop and initdt.
+    int reinit(double nextout) override
+    {
+        fillHaloC(P, M.blocks, M.zb);
+        gradientC(P, M.blocks, M.zb, M.grad.dzbdx, M.grad.dzbdy);
+        gradientHalo(P, M.blocks, M.zb, M.grad.dzbdx, M.grad.dzbdy);
+        refine_linear(P, M.blocks, M.zb, M.grad.dzbdx, M.grad.dzbdy);
+        gradientHalo(P, M.blocks, M.zb, M.grad.dzbdx, M.grad.dzbdy);
+        for (int ibl = 0; ibl < P.nblk; ibl++) {
+            int ib = M.blocks.active[ibl];
+            for (int iy = 0; iy < 16; iy++)
+                for (int ix = 0; ix < 16; ix++) {
+                    int n = memloc(P, ix, iy, ib);
+                    M.evolv.zs[n] = M.zb[n] + M.evolv.h[n];
+                }
+        }
+        CopyArrayBUQ(P, M.blocks, M.evolv, M.evolv_o);
+        L.totaltime = 0.0;
+        L.dt = 0.0;
+        L.nextoutputtime = nextout;
+        L.dtmax = initdt(P, L, M);
+        return 0;
+    }
+
+    int get_active(int* out) override
+    {
+        for (int ibl = 0; ibl < P.nblk; ibl++) out[ibl] = M.blocks.active[ibl];
+        return P.nblk;
+    }
 };
 
 }  // namespace
@@ -280,6 +335,10 @@ int ref_set_rain_series(void* hdl, int n, const double* t, const double* r)
 }
 
 int ref_step(void* hdl, int nsteps, double* dts) { return ((RefBase*)hdl)->step(nsteps, dts); }
+int ref_adapt(void* hdl) { return ((RefBase*)hdl)->adapt(); }
+int ref_set(void* hdl, const char* name, const double* buq) { return ((RefBase*)hdl)->set(name, buq); }
+int ref_reinit(void* hdl, double nextout) { return ((RefBase*)hdl)->reinit(nextout); }
+int ref_get_active(void* hdl, int* out) { return ((RefBase*)hdl)->get_active(out); }
 int ref_nblk(void* hdl) { return ((RefBase*)hdl)->P.nblk; }
 int ref_nseg(void* hdl) { return (int)((RefBase*)hdl)->F.bndseg.size(); }
 int ref_get(void* hdl, const char* name, double* out) { return ((RefBase*)hdl)->get(name, out); }

@@ -162,3 +162,75 @@ def dam_break(n: int = 64, engine: int = 1, seed: int = 3) -> Case:
     v = np.where(h > 0, 0.2 * rng.standard_normal((n, n)), 0.0).astype(np.float32)
     p = Param(dx=dx, xo=0.0, yo=0.0, engine=engine, aoibnd=0, cf=0.002, frictionmodel=0)
     return Case(f"dam{n}_e{engine}", p, _param_text(p), dx, 0.0, 0.0, zb, h, u, v)
+
+
+# ---------------------------------------------------------------- multi-level meshes
+
+@dataclass
+class AMRCase:
+    """A case on a mesh refined by the reference's own Adaptation(): fields are
+    functions of cell-centre coordinates, sampled on the level-0 grid before the
+    adaptation and again on every block of the adapted mesh."""
+    name: str
+    param: Param
+    paramtext: str
+    n0: int                 # level-0 cells per side
+    dx: float               # level-0 resolution
+    xo: float
+    yo: float
+    zb_fn: object
+    eta_fn: object
+    uv_fn: object = None
+    nextoutputtime: float = 1e30
+    adapt_eta_fn: object = None   # surface used only to drive the adaptation (default eta_fn)
+
+
+def _amr_text(p: Param, crit: str, maxlevel: int) -> str:
+    p.initlevel, p.minlevel, p.maxlevel = 0, 0, maxlevel
+    return _param_text(p) + f"initlevel = 0\nminlevel = 0\nmaxlevel = {maxlevel}\nAdaptation = {crit}\n"
+
+
+def amr_hump(n0: int = 32, engine: int = 1, maxlevel: int = 1, off: float = 0.5) -> AMRCase:
+    """Gaussian hump on a flat bed, refined where the surface exceeds 0.13 m; the hump
+    sits at fraction `off` of the domain (off-centre gives a mixed-level mesh)."""
+    dx = 1.0 / 64
+    p = Param(dx=dx, xo=0.0, yo=0.0, engine=engine, aoibnd=0, cf=0.0, frictionmodel=0)
+    c = n0 * dx * off
+    eta = lambda x, y: 0.1 + 0.5 * np.exp(-((x - c) ** 2 + (y - c) ** 2) / (2 * 0.05 ** 2))
+    return AMRCase(f"amrhump{n0}_e{engine}_l{maxlevel}", p, _amr_text(p, "Threshold,0.13,zs", maxlevel), n0, dx, 0.0,
+                   0.0, lambda x, y: np.zeros_like(x), eta)
+
+
+def amr_island(n0: int = 32, engine: int = 1, maxlevel: int = 2, off: float = 0.5) -> AMRCase:
+    """Conical island with a wet/dry shoreline, refined on the island (bed above
+    -0.2 m), quadratic friction, a small tilted surface to drive a flow."""
+    dx = 0.4
+    p = Param(dx=dx, xo=0.0, yo=0.0, engine=engine, aoibnd=0, cf=0.001, frictionmodel=0)
+    c = n0 * dx * off
+
+    def zb(x, y):
+        r = np.sqrt((x - c) ** 2 + (y - c) ** 2)
+        return -0.32 + np.clip((3.6 - r) / 2.5, 0.0, 1.0) * 0.625
+
+    eta = lambda x, y: 0.01 * (x - c) / c
+    return AMRCase(f"amrisland{n0}_e{engine}_l{maxlevel}", p, _amr_text(p, "Threshold,-0.2,zb", maxlevel), n0, dx,
+                   0.0, 0.0, zb, eta)
+
+
+def amr_dambreak(n0: int = 64, engine: int = 1, maxlevel: int = 2, seed: int = 5) -> AMRCase:
+    """Wet/dry on a three-level mesh: a noisy sloping bed, water up to 1.2 m left of
+    x = 0.45 L and dry land beyond; the mesh is refined around the left third, so the
+    wet/dry front crosses level interfaces."""
+    dx = 0.5
+    L = n0 * dx
+    p = Param(dx=dx, xo=0.0, yo=0.0, engine=engine, aoibnd=0, cf=0.002, frictionmodel=0)
+    rng = np.random.default_rng(seed)
+    noise = rng.standard_normal(64)
+
+    def zb(x, y):
+        return 0.02 * x + 0.05 * np.sin(x * 1.3 + noise[0]) * np.cos(y * 0.7 + noise[1])
+
+    eta = lambda x, y: np.where(x < 0.45 * L, 1.2, -10.0)
+    crit = lambda x, y: np.where(x < 0.33 * L, 2.0, -10.0)
+    return AMRCase(f"amrdam{n0}_e{engine}_l{maxlevel}", p, _amr_text(p, "Threshold,0.5,zs", maxlevel), n0, dx, 0.0,
+                   0.0, zb, eta, adapt_eta_fn=crit)

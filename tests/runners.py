@@ -68,3 +68,50 @@ def oracle_fields(o: Oracle) -> dict:
 
 def maxdiff(a, b) -> float:
     return float(np.max(np.abs(interior(a).astype(np.float64) - interior(b).astype(np.float64))))
+
+
+def _sample(fn, level, xo, yo, case, zb=None):
+    """fn at the cell centres of every block (tiles (nblk, 18, 18), halo left 0)."""
+    n = len(level)
+    out = np.zeros((n, 18, 18))
+    ii = np.arange(16)
+    for b in range(n):
+        d = case.dx / (2.0 ** level[b])
+        X, Y = np.meshgrid(case.xo + xo[b] + ii * d, case.yo + yo[b] + ii * d)
+        out[b, 1:17, 1:17] = fn(X, Y) if zb is None else fn(X, Y, zb[b, 1:17, 1:17])
+    return out.astype(np.float32).astype(np.float64)
+
+
+def make_amr_pair(case):
+    """The reference adapts the mesh; the oracle gets the same tables and fields.
+    Returns (reference, oracle, (level, nbr, xo, yo))."""
+    n0 = case.n0
+    ii = (np.arange(n0) + 0.5) * case.dx
+    X, Y = np.meshgrid(case.xo + ii, case.yo + ii)
+    zb0 = case.zb_fn(X, Y).astype(np.float32)
+    eta0 = case.adapt_eta_fn if case.adapt_eta_fn is not None else case.eta_fn
+    h0 = np.maximum(eta0(X, Y) - zb0, 0).astype(np.float32)
+    z0 = np.zeros_like(zb0)
+    r = Reference(case.paramtext, n0, n0, case.dx, case.xo, case.yo, zb0, h0, z0, z0, None, case.nextoutputtime)
+    r.adapt()
+    lev, nbr, xo, yo = r.mesh_active_order()
+    zb = _sample(case.zb_fn, lev, xo, yo, case)
+    h = _sample(lambda X, Y, Z: np.maximum(case.eta_fn(X, Y) - Z, 0.0), lev, xo, yo, case, zb=zb)
+    zero = np.zeros_like(zb)
+    for name, a in (("zb", zb), ("h", h), ("u", zero), ("v", zero)):
+        r.set(name, a)
+    r.reinit(case.nextoutputtime)
+    o = Oracle(case.param, len(lev))
+    o.set_blocks(lev, nbr, xo, yo)
+    for name, a in (("zb", zb), ("h", h), ("u", zero), ("v", zero)):
+        o.set(name, a)
+    o.set("zs", (zb + h).astype(np.float32))
+    from bg_flood_b200.mesh import Mesh
+    from bg_flood_b200.mesh import boundary_segments
+    m = Mesh(n0 // 16, n0 // 16, case.dx, len(lev), lev, nbr, xo, yo, np.zeros(len(lev), np.int32),
+             np.zeros(len(lev), np.int32))
+    for typ, times, levels, sides in boundary_segments(m, case.param.segments, case.param.aoibnd, case.xo, case.yo):
+        o.add_segment(typ, times, levels, sides)
+    o.init_bed()
+    o.init_loop(0.0, case.nextoutputtime)
+    return r, o, (lev, nbr, xo, yo)

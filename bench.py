@@ -241,7 +241,8 @@ def main():
     dom_ms, dom_b = kern[dom]
     achieved = dom_b * ncell / (dom_ms / 1e3) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", f"{dom}_traffic.txt")
+    variant = "fastmath" if args.fastmath else "exact"
+    tfile = os.path.join(ROOT, "profiles", f"{dom}_runup{args.n}_{variant}.md")
     if os.path.exists(tfile):
         for ln in open(tfile):
             if ln.startswith("dram_bytes_per_cell:"):

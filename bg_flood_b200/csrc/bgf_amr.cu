@@ -1,0 +1,556 @@
+// Multi-level flow step and the bed preparation (see bgf_amr.cuh for the design).
+//
+// One stage (predictor or corrector) of a step on a mesh with several refinement
+// levels is this chain of launches over all active blocks:
+//
+//   amr_halo_kernel     halo of h, u, v from the neighbours' interiors (fillHalo),
+//                       wet/dry restriction next to finer blocks, zs = zb + h, and
+//                       the interior gradients of h, u, v of blocks that have a
+//                       finer neighbour (what the neighbour's prolongation reads)
+//   amr_refine_kernel   halos next to coarser blocks rebuilt by linear
+//                       reconstruction in the coarse cell (refine_linear)
+//   amr_wetdry_kernel   wet/dry prolongation decisions, one launch per level
+//                       above the coarsest (the reference visits blocks in order,
+//                       so a decision may see a coarser block's halo that the
+//                       same pass already changed)
+//   amr_apply_kernel    the decisions applied (depth and bed of the parent), zs
+//                       recomputed on the prolongated halo
+//   amr_flux_kernel     tile with its outer stencil ring, gradients, wet-slope
+//                       reset, faces with the coarse/fine source substitution,
+//                       cell dtmax and the block minimum (predictor only);
+//                       faces written to the stage face arrays
+//   amr_update_kernel   faces next to finer blocks replaced by the mean of the two
+//                       fine faces, boundary segments, flux divergence, advance
+//                       (predictor: half step into the scratch arrays; corrector:
+//                       full step, friction, rain, next state, time slot)
+//
+// The reference counterpart is FlowGPU/FlowCPU with its fillHalo, gradient,
+// refine_linear, WetDryProlongation and HaloFlux calls (src/FlowCPU.cu:15-253).
+#include <cuda_runtime.h>
+
+#include "bgf_amr.cuh"
+#include "bgf_internal.h"
+
+#ifndef BGF_VARIANT
+#define BGF_VARIANT exact
+#endif
+
+namespace bgf {
+namespace BGF_VARIANT {
+
+#include "bgf_stage.cuh"
+
+__device__ __forceinline__ bool has_coarser_side(const int* nbr, int nbm, const int* lv, int ib)
+{
+    const int l = lv[ib];
+    return lv[nbr[0 * nbm + ib]] < l || lv[nbr[2 * nbm + ib]] < l || lv[nbr[4 * nbm + ib]] < l ||
+           lv[nbr[6 * nbm + ib]] < l;
+}
+
+__device__ __forceinline__ bool has_finer_neighbour(const int* nbr, int nbm, const int* lv, int ib)
+{
+    const int l = lv[ib];
+    bool f = false;
+#pragma unroll
+    for (int k = 0; k < 8; k++) f |= lv[nbr[k * nbm + ib]] > l;
+    return f;
+}
+
+// wetdryrestriction (src/ConserveElevation.cu:676-726): a halo cell next to a finer
+// neighbour whose four cells are partly wet takes the depth-weighted surface of the
+// wet ones minus its own bed.  hv is the restricted depth from the halo fill.
+template <class T>
+__device__ __forceinline__ T wetdry_restrict(const Acc256<T>& h, const Acc324<T>& zb, T eps, T zbw, int nb, int s, int j,
+                                             T hv)
+{
+    const int jj = j < BW / 2 ? 2 * j : (j - BW / 2) * 2;
+    int x0, y0;
+    if (s == 0) { x0 = BW - 2; y0 = jj; }
+    else if (s == 1) { x0 = 0; y0 = jj; }
+    else if (s == 2) { x0 = jj; y0 = BW - 2; }
+    else { x0 = jj; y0 = 0; }
+    const T hii = h(nb, x0, y0), hir = h(nb, x0 + 1, y0), hit = h(nb, x0, y0 + 1), hitr = h(nb, x0 + 1, y0 + 1);
+    const T iiwet = hii > eps ? (T)1.0 : (T)0.0;
+    const T irwet = hir > eps ? (T)1.0 : (T)0.0;
+    const T itwet = hit > eps ? (T)1.0 : (T)0.0;
+    const T itrwet = hitr > eps ? (T)1.0 : (T)0.0;
+    const T cwet = (iiwet + irwet + itwet + itrwet);
+    T hwet = (iiwet * hii + irwet * hir + itwet * hit + itrwet * hitr);
+    T zswet = (iiwet * hii) * (zb(nb, x0, y0) + hii) + (irwet * hir) * (zb(nb, x0 + 1, y0) + hir) +
+              (itwet * hit) * (zb(nb, x0, y0 + 1) + hit) + (itrwet * hitr) * (zb(nb, x0 + 1, y0 + 1) + hitr);
+    if (cwet > (T)0.0 && cwet < (T)4.0) {
+        zswet = zswet / hwet;
+        return ((T)0.0 < zswet - zbw) ? zswet - zbw : (T)0.0;
+    }
+    return hv;
+}
+
+// ---------------------------------------------------------------- stage kernels
+
+template <class T>
+__global__ void __launch_bounds__(NTHREADS) amr_halo_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+                                                             int stage)
+{
+    __shared__ T th[3][324];
+    const TimeState ts = m.time[parity];
+    if (!step_live(ts)) return;
+    const int tid = threadIdx.x;
+    const int ib = m.active[blockIdx.x];
+    const int nbm = m.nblkmem;
+    const T* src[3] = {stage == 0 ? m.h[ts.cur] : m.dh, stage == 0 ? m.u[ts.cur] : m.dhu,
+                       stage == 0 ? m.v[ts.cur] : m.dhv};
+    T* const* W = a.W[stage];
+    const size_t base = (size_t)ib * 324;
+    const int x = tid & 15, y = tid >> 4, c = hi18(x, y);
+    {
+        const size_t g = (size_t)ib * 256 + tid;
+#pragma unroll
+        for (int f = 0; f < 3; f++) th[f][c] = src[f][g];
+        W[0][base + c] = th[0][c];
+        W[2][base + c] = th[1][c];
+        W[3][base + c] = th[2][c];
+        W[1][base + c] = a.zb[base + c] + th[0][c];
+    }
+    if (tid < 64) {
+        const int s = tid >> 4, j = tid & 15;
+        const CellRule<T> r = halo_rule<T>(m.nbr, nbm, m.level, ib, s, j);
+        T hv = rule_eval(r, Acc256<T>{src[0]});
+        const T uv = rule_eval(r, Acc256<T>{src[1]});
+        const T vv = rule_eval(r, Acc256<T>{src[2]});
+        int hx, hy;
+        halo_xy(s, j, hx, hy);
+        const int hc = hi18(hx, hy);
+        const int nbh = m.nbr[(2 * s + (j >= BW / 2 ? 1 : 0)) * nbm + ib];
+        if (a.wetdryfix && m.level[nbh] > m.level[ib])
+            hv = wetdry_restrict<T>(Acc256<T>{src[0]}, Acc324<T>{a.zb}, p.eps, a.zb[base + hc], nbh, s, j, hv);
+        th[0][hc] = hv;
+        th[1][hc] = uv;
+        th[2][hc] = vv;
+        W[0][base + hc] = hv;
+        W[2][base + hc] = uv;
+        W[3][base + hc] = vv;
+        W[1][base + hc] = a.zb[base + hc] + hv;
+    }
+    // gradientC (src/Gradients.cu:921-957) of h, u, v for the prolongation of the
+    // finer neighbours' halos
+    if (!has_finer_neighbour(m.nbr, nbm, m.level, ib)) return;
+    __syncthreads();
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    const T rdelta = (T)1.0 / delta;
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+        const T* t = th[f];
+        a.G0[2 * f][base + c] = div_by(minmod2(p.theta, t[c - 1], t[c], t[c + 1]), delta, rdelta);
+        a.G0[2 * f + 1][base + c] = div_by(minmod2(p.theta, t[c - 18], t[c], t[c + 18]), delta, rdelta);
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(64) amr_refine_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+                                                        int stage)
+{
+    const TimeState ts = m.time[parity];
+    if (!step_live(ts)) return;
+    const int ib = m.active[blockIdx.x];
+    const int s = threadIdx.x >> 4, j = threadIdx.x & 15;
+    int pb, px, py;
+    if (!parent_cell(m.nbr, m.nblkmem, m.level, ib, s, j, pb, px, py)) return;
+    int hx, hy;
+    halo_xy(s, j, hx, hy);
+    const size_t o = (size_t)ib * 324 + hi18(hx, hy);
+    T* const* W = a.W[stage];
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+        const int wf = f == 0 ? 0 : f + 1;  // h, u, v in W order h, zs, u, v
+        W[wf][o] = refine_value<T>(Acc324<T>{W[wf]}, Acc324<T>{a.G0[2 * f]}, Acc324<T>{a.G0[2 * f + 1]}, s, j, pb, px,
+                                   py, m.level[ib], p.delta0, p.delta0_d);
+    }
+}
+
+// WetDryProlongation (src/ConserveElevation.cu:80-203) for the blocks of one level:
+// a halo cell next to a coarser block whose parent or any of the parent's four
+// neighbours is dry takes the parent's depth and bed.  The reference visits the
+// blocks in active-list order and changes halos as it goes, so the four neighbours
+// of a parent that lie in the coarse block's own halo are read as already changed
+// when that coarse block comes earlier in the list and its decision (made by the
+// launch for its level, which runs first) says so.
+template <class T>
+__global__ void __launch_bounds__(64) amr_wetdry_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+                                                        int stage, int level)
+{
+    const TimeState ts = m.time[parity];
+    if (!step_live(ts)) return;
+    const int ib = m.active[blockIdx.x];
+    if (m.level[ib] != level) return;
+    const int nbm = m.nblkmem;
+    const int s = threadIdx.x >> 4, j = threadIdx.x & 15;
+    int pb, px, py;
+    if (!parent_cell(m.nbr, nbm, m.level, ib, s, j, pb, px, py)) return;
+    const T* H = a.W[stage][0];
+    const T eps = p.eps;
+    const bool earlier = a.rank[pb] < a.rank[ib];
+    auto hval = [&](int x, int y) -> T {
+        const T v = H[(size_t)pb * 324 + hi18(x, y)];
+        if (!earlier) return v;
+        int hs, hj;
+        if (x < 0) { hs = 0; hj = y; }
+        else if (x >= BW) { hs = 1; hj = y; }
+        else if (y < 0) { hs = 2; hj = x; }
+        else if (y >= BW) { hs = 3; hj = x; }
+        else return v;
+        int qb, qx, qy;
+        if (!parent_cell(m.nbr, nbm, m.level, pb, hs, hj, qb, qx, qy)) return v;
+        if (!a.pflag[(size_t)pb * 64 + hs * 16 + hj]) return v;
+        return H[(size_t)qb * 324 + hi18(qx, qy)];
+    };
+    const bool dry = !(hval(px, py) > eps && hval(px - 1, py) > eps && hval(px + 1, py) > eps &&
+                       hval(px, py + 1) > eps && hval(px, py - 1) > eps);
+    a.pflag[(size_t)ib * 64 + s * 16 + j] = dry ? 1 : 0;
+}
+
+// The prolongation decisions applied, then RecalculateZs (src/Halo.cu:72-107) on
+// the halo cells next to coarser blocks.
+template <class T>
+__global__ void __launch_bounds__(64) amr_apply_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+                                                       int stage)
+{
+    const TimeState ts = m.time[parity];
+    if (!step_live(ts)) return;
+    const int ib = m.active[blockIdx.x];
+    const int s = threadIdx.x >> 4, j = threadIdx.x & 15;
+    int pb, px, py;
+    if (!parent_cell(m.nbr, m.nblkmem, m.level, ib, s, j, pb, px, py)) return;
+    int hx, hy;
+    halo_xy(s, j, hx, hy);
+    const size_t o = (size_t)ib * 324 + hi18(hx, hy);
+    const size_t po = (size_t)pb * 324 + hi18(px, py);
+    T* H = a.W[stage][0];
+    if (a.wetdryfix && a.pflag[(size_t)ib * 64 + s * 16 + j]) {
+        H[o] = H[po];
+        a.zb[o] = a.zb[po];
+    }
+    a.W[stage][1][o] = a.zb[o] + H[o];
+}
+
+template <class T, int ENGINE>
+__global__ void __launch_bounds__(NTHREADS, 3) amr_flux_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+                                                               int stage)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
+    __shared__ SubFaces<T> sub;
+    const TimeState ts = m.time[parity];
+    if (!step_live(ts)) return;
+    const int tid = threadIdx.x;
+    const int ib = m.active[blockIdx.x];
+    const int nbm = m.nblkmem;
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    T* const* W = a.W[stage];
+    const size_t base = (size_t)ib * 324;
+
+    load_bed<T, ENGINE>(s, m, ib, tid);
+    {
+        // interior and ring 1 (the block's halo, corners excluded)
+        const int x = tid & 15, y = tid >> 4;
+        const int c18 = hi18(x, y), c = ti(x, y);
+#pragma unroll
+        for (int v = 0; v < 4; v++) s.t[v][c] = W[v][base + c18];
+    }
+    if (tid < 64) {
+        const int sd = tid >> 4, t = tid & 15;
+        int hx, hy;
+        halo_xy(sd, t, hx, hy);
+        const int c18 = hi18(hx, hy), c = ti(hx, hy);
+#pragma unroll
+        for (int v = 0; v < 4; v++) s.t[v][c] = W[v][base + c18];
+        // coarse/fine source substitution for the faces on this side
+        int pb, px, py;
+        const bool coarse = parent_cell(m.nbr, nbm, m.level, ib, sd, t, pb, px, py);
+        if (t == 0) sub.on[sd] = coarse ? 1 : 0;
+        if (coarse) {
+            sub.h[sd][t] = W[0][(size_t)pb * 324 + hi18(px, py)];
+            sub.z[sd][t] = a.zb[(size_t)pb * 324 + hi18(px, py)];
+        }
+    } else if (tid < 128) {
+        // ring 2: the outer stencil values of the halo gradients
+        const int k = tid - 64;
+        const int sd = k >> 4, t = k & 15;
+        const CellRule<T> r = outer_rule<T>(m.nbr, nbm, m.level, ib, sd, t);
+        int x, y;
+        halo_xy(sd, t, x, y);
+        if (sd == 0) x = -2;
+        else if (sd == 1) x = BW + 1;
+        else if (sd == 2) y = -2;
+        else y = BW + 1;
+        const int c = ti(x, y);
+#pragma unroll
+        for (int v = 0; v < 4; v++) s.t[v][c] = rule_eval(r, Acc324<T>{W[v]});
+    }
+    __syncthreads();
+    const T celldt = tile_fluxes<T, ENGINE, true>(s, p, delta, tid, &sub);
+    __syncthreads();
+    if (stage == 0) {
+        T v = celldt;
+        for (int o = 16; o > 0; o >>= 1) {
+            T w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w < v ? w : v;
+        }
+        if ((tid & 31) == 0) s.red[tid >> 5] = v;
+    }
+    // faces to the stage face arrays
+    const size_t fb = (size_t)ib * NFX;
+    for (int k = tid; k < NFX; k += NTHREADS) {
+        a.F[0][fb + k] = s.Fhu[k];
+        a.F[1][fb + k] = s.Fqux[k];
+        a.F[2][fb + k] = s.Su[k];
+        a.F[3][fb + k] = s.Fqvx[k];
+        a.F[4][fb + k] = s.Fhv[k];
+        a.F[5][fb + k] = s.Fqvy[k];
+        a.F[6][fb + k] = s.Sv[k];
+        a.F[7][fb + k] = s.Fquy[k];
+    }
+    if (stage == 0) {
+        __syncthreads();
+        if (tid == 0) {
+            T b = s.red[0];
+            for (int k = 1; k < NTHREADS / 32; k++) b = s.red[k] < b ? s.red[k] : b;
+            atomicMin(&m.dtmin[parity], dt_bits(b));
+        }
+    }
+}
+
+template <class T, int ENGINE>
+__global__ void __launch_bounds__(NTHREADS, 3) amr_update_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+                                                                 int stage)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
+    const TimeState ts = m.time[parity];
+    const int tid = threadIdx.x;
+    if (!step_live(ts)) {
+        if (stage == 1 && blockIdx.x == 0 && tid == 0) {
+            TimeState nt = ts;
+            nt.done = 1;
+            m.time[parity ^ 1] = nt;
+        }
+        return;
+    }
+    const int ib = m.active[blockIdx.x];
+    const int nbm = m.nblkmem;
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    const T dt = step_dt<T>(ts, m.dtmin[parity]);
+    const double dtd = (double)dt;
+    const size_t base = (size_t)ib * 324;
+    const size_t fb = (size_t)ib * NFX;
+    for (int k = tid; k < NFX; k += NTHREADS) {
+        s.Fhu[k] = a.F[0][fb + k];
+        s.Fqux[k] = a.F[1][fb + k];
+        s.Su[k] = a.F[2][fb + k];
+        s.Fqvx[k] = a.F[3][fb + k];
+        s.Fhv[k] = a.F[4][fb + k];
+        s.Fqvy[k] = a.F[5][fb + k];
+        s.Sv[k] = a.F[6][fb + k];
+        s.Fquy[k] = a.F[7][fb + k];
+    }
+    // state n on the 18x18 tile (boundary segments, full-step advance) and the bed
+    for (int k = tid; k < 324; k += NTHREADS) {
+        s.zb[k] = a.zb[base + k];
+        s.h0[k] = a.W[0][0][base + k];
+        s.u0[k] = a.W[0][2][base + k];
+        s.v0[k] = a.W[0][3][base + k];
+    }
+    __syncthreads();
+    // HaloFluxCPULR / HaloFluxCPUBT (src/Halo.cu:1441-1540, 1766-1850): the faces of
+    // a side with finer neighbours take the mean of the two fine faces
+    if (tid < 64) {
+        const int sd = tid >> 4, j = tid & 15;
+        const int nbh = m.nbr[(2 * sd + (j >= BW / 2 ? 1 : 0)) * nbm + ib];
+        if (m.level[nbh] > m.level[ib]) {
+            const int jj = j < BW / 2 ? 2 * j : (j - BW / 2) * 2;
+            const size_t nf = (size_t)nbh * NFX;
+            int own, f0, f1, a0;
+            if (sd == 0) { own = fxi(0, j); f0 = fxi(BW, jj); f1 = fxi(BW, jj + 1); a0 = 0; }
+            else if (sd == 1) { own = fxi(BW, j); f0 = fxi(0, jj); f1 = fxi(0, jj + 1); a0 = 0; }
+            else if (sd == 2) { own = fyi(j, 0); f0 = fyi(jj, BW); f1 = fyi(jj + 1, BW); a0 = 4; }
+            else { own = fyi(j, BW); f0 = fyi(jj, 0); f1 = fyi(jj + 1, 0); a0 = 4; }
+            T* dst[4];
+            if (a0 == 0) { dst[0] = s.Fhu; dst[1] = s.Fqux; dst[2] = s.Su; dst[3] = s.Fqvx; }
+            else { dst[0] = s.Fhv; dst[1] = s.Fqvy; dst[2] = s.Sv; dst[3] = s.Fquy; }
+#pragma unroll
+            for (int q = 0; q < 4; q++) dst[q][own] = (T)0.5 * (a.F[a0 + q][nf + f0] + a.F[a0 + q][nf + f1]);
+        }
+    }
+    __syncthreads();
+    apply_boundaries<T>(s, m, p, ib, stage == 0 ? ts.totaltime + ts.dt * 0.5 : ts.totaltime + dtd, tid);
+    __syncthreads();
+    const int x = tid & 15, y = tid >> 4;
+    const int c18 = hi18(x, y);
+    const T hs = a.W[stage][0][base + c18], us = a.W[stage][2][base + c18], vs = a.W[stage][3][base + c18];
+    T dh, dhu, dhv;
+    flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, hs, us, vs, dh, dhu, dhv);
+    const T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];
+    const size_t g = (size_t)ib * 256 + tid;
+    T ho, uo, vo;
+    if (stage == 0) {
+        // predictor: half step from state n into the scratch arrays (read back by the corrector's halo fill)
+        advance<T>(dt * (T)0.5, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+        m.dh[g] = ho;
+        m.dhu[g] = uo;
+        m.dhv[g] = vo;
+        return;
+    }
+    advance<T>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+    const T cfv = p.has_cf ? m.cf[g] : p.cf;
+    bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);
+    if (p.has_rain) {
+        // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580), uniform rain at the
+        // start of the step
+        const double rnow = series_at(m.rain_t, m.rain_r, p.rain_n, ts.totaltime);
+        T Rainhh = (T)rnow;
+        const T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
+        Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
+        const T hi = ho;
+        const T qvol = hi / (hi + Rainhh);
+        ho = hi + Rainhh;
+        if ((double)hi > p.eps_d) {
+            uo = uo * qvol;
+            vo = vo * qvol;
+        }
+    }
+    const int nxt = ts.cur ^ 1;
+    m.h[nxt][g] = ho;
+    m.u[nxt][g] = uo;
+    m.v[nxt][g] = vo;
+    if (blockIdx.x == 0 && tid == 0) m.time[parity ^ 1] = next_time_state<T>(ts, p, dtd, nxt, m.dtmin, parity);
+}
+
+// ---------------------------------------------------------------- bed preparation
+
+// fillHaloC on the bed (src/Halo.cu:16-51): halo from the neighbours' interiors.
+template <class T> __global__ void __launch_bounds__(64) bed_halo_kernel(DevModel<T> m, T* zb)
+{
+    const int ib = m.active[blockIdx.x];
+    const int s = threadIdx.x >> 4, j = threadIdx.x & 15;
+    const CellRule<T> r = halo_rule<T>(m.nbr, m.nblkmem, m.level, ib, s, j);
+    int hx, hy;
+    halo_xy(s, j, hx, hy);
+    zb[(size_t)ib * 324 + hi18(hx, hy)] = rule_eval(r, Acc324<T>{zb});
+}
+
+// gradientC on the bed (src/Gradients.cu:921-957)
+template <class T>
+__global__ void __launch_bounds__(NTHREADS) bed_grad_kernel(DevModel<T> m, StepParams<T> p, const T* zb, T* gx, T* gy)
+{
+    const int ib = m.active[blockIdx.x];
+    const int tid = threadIdx.x, x = tid & 15, y = tid >> 4;
+    const size_t i = (size_t)ib * 324 + hi18(x, y);
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    const T rdelta = (T)1.0 / delta;
+    gx[i] = div_by(minmod2(p.theta, zb[i - 1], zb[i], zb[i + 1]), delta, rdelta);
+    gy[i] = div_by(minmod2(p.theta, zb[i - 18], zb[i], zb[i + 18]), delta, rdelta);
+}
+
+// gradientHalo on the bed (src/Gradients.cu:2584-2605, 2713-3290)
+template <class T>
+__global__ void __launch_bounds__(64) bed_grad_halo_kernel(DevModel<T> m, StepParams<T> p, const T* zb, T* gx, T* gy)
+{
+    const int ib = m.active[blockIdx.x];
+    const int s = threadIdx.x >> 4, t = threadIdx.x & 15;
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    const T rdelta = (T)1.0 / delta;
+    const T outer = rule_eval(outer_rule<T>(m.nbr, m.nblkmem, m.level, ib, s, t), Acc324<T>{zb});
+    const Acc324<T> z{zb};
+    int hx, hy;
+    halo_xy(s, t, hx, hy);
+    const size_t i = (size_t)ib * 324 + hi18(hx, hy);
+    if (s == 0) gx[i] = div_by(minmod2(p.theta, outer, zb[i], z(ib, 0, t)), delta, rdelta);
+    else if (s == 1) gx[i] = div_by(minmod2(p.theta, z(ib, BW - 1, t), zb[i], outer), delta, rdelta);
+    else if (s == 2) gy[i] = div_by(minmod2(p.theta, outer, zb[i], z(ib, t, 0)), delta, rdelta);
+    else gy[i] = div_by(minmod2(p.theta, z(ib, t, BW - 1), zb[i], outer), delta, rdelta);
+}
+
+// refine_linear on the bed (src/Halo.cu:1044-1394)
+template <class T>
+__global__ void __launch_bounds__(64) bed_refine_kernel(DevModel<T> m, StepParams<T> p, T* zb, const T* gx, const T* gy)
+{
+    const int ib = m.active[blockIdx.x];
+    const int s = threadIdx.x >> 4, j = threadIdx.x & 15;
+    int pb, px, py;
+    if (!parent_cell(m.nbr, m.nblkmem, m.level, ib, s, j, pb, px, py)) return;
+    int hx, hy;
+    halo_xy(s, j, hx, hy);
+    zb[(size_t)ib * 324 + hi18(hx, hy)] = refine_value<T>(Acc324<T>{zb}, Acc324<T>{gx}, Acc324<T>{gy}, s, j, pb, px, py,
+                                                           m.level[ib], p.delta0, p.delta0_d);
+}
+
+// ---------------------------------------------------------------- launchers
+
+template <class T> static size_t amr_smem() { return sizeof(Smem<T>); }
+
+template <class T, int ENGINE> static cudaError_t amr_configure_engine()
+{
+    cudaError_t e = cudaFuncSetAttribute(amr_flux_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)amr_smem<T>());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(amr_update_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)amr_smem<T>());
+}
+
+template <class T> cudaError_t configure_amr_kernels()
+{
+    cudaError_t e = amr_configure_engine<T, 1>();
+    if (e != cudaSuccess) return e;
+    return amr_configure_engine<T, 2>();
+}
+
+template <class T>
+int launch_amr_stage(const DevModel<T>& m, const AmrDev<T>& a, const StepParams<T>& p, int engine, int parity, int stage,
+                     int minlev, int maxlev, cudaStream_t st)
+{
+    const int n = m.nblk;
+    int launches = 0;
+    amr_halo_kernel<T><<<n, NTHREADS, 0, st>>>(m, a, p, parity, stage);
+    amr_refine_kernel<T><<<n, 64, 0, st>>>(m, a, p, parity, stage);
+    launches += 2;
+    if (a.wetdryfix) {
+        for (int l = minlev + 1; l <= maxlev; l++) {
+            amr_wetdry_kernel<T><<<n, 64, 0, st>>>(m, a, p, parity, stage, l);
+            launches++;
+        }
+    }
+    amr_apply_kernel<T><<<n, 64, 0, st>>>(m, a, p, parity, stage);
+    if (engine == 1) {
+        amr_flux_kernel<T, 1><<<n, NTHREADS, amr_smem<T>(), st>>>(m, a, p, parity, stage);
+        amr_update_kernel<T, 1><<<n, NTHREADS, amr_smem<T>(), st>>>(m, a, p, parity, stage);
+    } else {
+        amr_flux_kernel<T, 2><<<n, NTHREADS, amr_smem<T>(), st>>>(m, a, p, parity, stage);
+        amr_update_kernel<T, 2><<<n, NTHREADS, amr_smem<T>(), st>>>(m, a, p, parity, stage);
+    }
+    return launches + 3;
+}
+
+template <class T>
+int launch_bed_init(const DevModel<T>& m, const StepParams<T>& p, T* zb, T* gx, T* gy, cudaStream_t st)
+{
+    const int n = m.nblk;
+    bed_halo_kernel<T><<<n, 64, 0, st>>>(m, zb);
+    bed_grad_kernel<T><<<n, NTHREADS, 0, st>>>(m, p, zb, gx, gy);
+    bed_grad_halo_kernel<T><<<n, 64, 0, st>>>(m, p, zb, gx, gy);
+    bed_refine_kernel<T><<<n, 64, 0, st>>>(m, p, zb, gx, gy);
+    bed_grad_halo_kernel<T><<<n, 64, 0, st>>>(m, p, zb, gx, gy);
+    return 5;
+}
+
+template cudaError_t configure_amr_kernels<float>();
+template cudaError_t configure_amr_kernels<double>();
+template int launch_amr_stage<float>(const DevModel<float>&, const AmrDev<float>&, const StepParams<float>&, int, int,
+                                     int, int, int, cudaStream_t);
+template int launch_amr_stage<double>(const DevModel<double>&, const AmrDev<double>&, const StepParams<double>&, int,
+                                      int, int, int, int, cudaStream_t);
+template int launch_bed_init<float>(const DevModel<float>&, const StepParams<float>&, float*, float*, float*,
+                                    cudaStream_t);
+template int launch_bed_init<double>(const DevModel<double>&, const StepParams<double>&, double*, double*, double*,
+                                     cudaStream_t);
+
+}  // namespace BGF_VARIANT
+}  // namespace bgf

@@ -13,7 +13,7 @@
 #include <vector>
 
 #include "../../include/bg_flood_b200.h"
-#include "bgf_flow.cuh"
+#include "bgf_amr.cuh"
 #include "bgf_internal.h"
 
 using namespace bgf;
@@ -80,6 +80,16 @@ struct bgf_handle {
     // pinned staging buffer for host <-> device copies of BUQ fields
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // multi-level meshes: stage tiles with halos, pre-prolongation gradients, face
+    // arrays, wet/dry prolongation decisions and the active-list rank of each block
+    bool amr = false;
+    int minlev = 0, maxlev = 0;
+    int steps_launches = 2;  // kernel launches per step
+    void* d_W[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
+    void* d_G0[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    void* d_F[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    uint8_t* d_pflag = nullptr;
+    int* d_rank = nullptr;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -118,6 +128,22 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     return m;
 }
 
+template <class T> static AmrDev<T> amr_dev(bgf_handle* h)
+{
+    AmrDev<T> a;
+    for (int s = 0; s < 2; s++)
+        for (int k = 0; k < 4; k++) a.W[s][k] = (T*)h->d_W[s][k];
+    for (int k = 0; k < 6; k++) a.G0[k] = (T*)h->d_G0[k];
+    for (int k = 0; k < 8; k++) a.F[k] = (T*)h->d_F[k];
+    a.zb = (T*)h->d_zb;
+    a.dzbdx = (T*)h->d_dzbdx;
+    a.dzbdy = (T*)h->d_dzbdy;
+    a.pflag = h->d_pflag;
+    a.rank = h->d_rank;
+    a.wetdryfix = h->P.wetdryfix ? 1 : 0;
+    return a;
+}
+
 template <class T> static StepParams<T> step_params(const bgf_handle* h)
 {
     const bgf_param& P = h->P;
@@ -127,6 +153,7 @@ template <class T> static StepParams<T> step_params(const bgf_handle* h)
     p.CFL = (T)P.CFL;
     p.theta = (T)P.theta;
     p.delta0 = (T)P.delta;
+    p.delta0_d = P.delta;
     p.epsi = std::nextafter((T)1.0, (T)2.0) - (T)1.0;
     p.epsface = (T)P.eps + p.epsi;
     // Coriolis factor of updateEVCPU (src/Advection.cu:187) for a Cartesian grid
@@ -294,6 +321,9 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
     h->fast = p->fastmath ? 1 : 0;
     cudaError_t e = h->dbl ? (h->fast ? fa::configure_kernels<double>() : ex::configure_kernels<double>())
                            : (h->fast ? fa::configure_kernels<float>() : ex::configure_kernels<float>());
+    if (e == cudaSuccess)
+        e = h->dbl ? (h->fast ? fa::configure_amr_kernels<double>() : ex::configure_amr_kernels<double>())
+                   : (h->fast ? fa::configure_amr_kernels<float>() : ex::configure_amr_kernels<float>());
     if (e != cudaSuccess) {
         g_last_error = std::string("configure kernels: ") + cudaGetErrorString(e);
         delete h;
@@ -344,6 +374,18 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
     return BGF_OK;
 }
 
+static void free_amr(bgf_handle* h)
+{
+    for (auto& st : h->d_W)
+        for (void*& p : st) { if (p) cudaFree(p); p = nullptr; }
+    for (void*& p : h->d_G0) { if (p) cudaFree(p); p = nullptr; }
+    for (void*& p : h->d_F) { if (p) cudaFree(p); p = nullptr; }
+    if (h->d_pflag) cudaFree(h->d_pflag);
+    if (h->d_rank) cudaFree(h->d_rank);
+    h->d_pflag = nullptr;
+    h->d_rank = nullptr;
+}
+
 int bgf_destroy(bgf_handle* h)
 {
     if (!h) return BGF_EINVAL;
@@ -356,6 +398,7 @@ int bgf_destroy(bgf_handle* h)
                     h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    free_amr(h);
     if (h->h_time) cudaFreeHost(h->h_time);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -368,6 +411,28 @@ int bgf_destroy(bgf_handle* h)
 }
 
 static int rebuild_segments(bgf_handle* h);
+
+// Buffers of the multi-level path, allocated the first time a mesh with more than
+// one level is set.
+static int alloc_amr(bgf_handle* h)
+{
+    if (h->d_rank) return BGF_OK;
+    const size_t nb = (size_t)h->nblkmem, es = h->esz;
+    bool ok = true;
+    for (auto& st : h->d_W)
+        for (void*& p : st) ok = ok && cudaMalloc(&p, nb * 324 * es) == cudaSuccess;
+    for (void*& p : h->d_G0) ok = ok && cudaMalloc(&p, nb * 324 * es) == cudaSuccess;
+    for (void*& p : h->d_F) ok = ok && cudaMalloc(&p, nb * NFX * es) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&h->d_pflag, nb * 64) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&h->d_rank, nb * sizeof(int)) == cudaSuccess;
+    if (!ok) {
+        free_amr(h);
+        g_last_error = "cudaMalloc failed (multi-level buffers)";
+        return BGF_ENOMEM;
+    }
+    BGF_CUDA(cudaMemsetAsync(h->d_pflag, 0, nb * 64, h->stream));
+    return BGF_OK;
+}
 
 int bgf_set_blocks(bgf_handle* h, const bgf_blockp* b)
 {
@@ -395,6 +460,23 @@ int bgf_set_blocks(bgf_handle* h, const bgf_blockp* b)
     BGF_CUDA(cudaMemcpyAsync(h->d_active, h->active.data(), sizeof(int) * b->nblk, cudaMemcpyHostToDevice, h->stream));
     BGF_CUDA(cudaMemcpyAsync(h->d_level, h->level.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, h->stream));
     BGF_CUDA(cudaMemcpyAsync(h->d_nbr, h->nbr.data(), sizeof(int) * 8 * nb, cudaMemcpyHostToDevice, h->stream));
+    // a mesh is multi-level when some active block has a neighbour on another level
+    h->amr = false;
+    h->minlev = h->maxlev = h->level[h->active[0]];
+    for (int ibl = 0; ibl < b->nblk; ibl++) {
+        int ib = h->active[ibl];
+        h->minlev = std::min(h->minlev, h->level[ib]);
+        h->maxlev = std::max(h->maxlev, h->level[ib]);
+        for (int k = 0; k < 8; k++) h->amr = h->amr || h->level[h->nbr[(size_t)k * nb + ib]] != h->level[ib];
+    }
+    if (h->amr) {
+        rc = alloc_amr(h);
+        if (rc) return rc;
+        std::vector<int> rank(nb, 0);
+        for (int ibl = 0; ibl < b->nblk; ibl++) rank[h->active[ibl]] = ibl;
+        BGF_CUDA(cudaMemcpyAsync(h->d_rank, rank.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, h->stream));
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
+    }
     BGF_CUDA(cudaStreamSynchronize(h->stream));
     h->has_blocks = true;
     free_graphs(h);
@@ -406,21 +488,29 @@ static int set_bed_t(bgf_handle* h, const void* zb, const void* dzbdx, const voi
                      const int* activeCell)
 {
     size_t nb = h->nblkmem;
-    std::vector<T> z, gx, gy;
+    std::vector<T> z;
     buq_to<T>(zb, h->dbl, nb * 324, z);
+    BGF_CUDA(cudaMemcpy(h->d_zb, z.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
     if (dzbdx && dzbdy) {
+        // the caller's bed halo and gradients are taken as they are
+        std::vector<T> gx, gy;
         buq_to<T>(dzbdx, h->dbl, nb * 324, gx);
         buq_to<T>(dzbdy, h->dbl, nb * 324, gy);
+        BGF_CUDA(cudaMemcpy(h->d_dzbdx, gx.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
+        BGF_CUDA(cudaMemcpy(h->d_dzbdy, gy.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
     } else {
-        gx.assign(nb * 324, (T)0);
-        gy.assign(nb * 324, (T)0);
-        int rc = host_bed_gradients<T>(h->nblk, h->active.data(), h->level.data(), h->nbr.data(), h->nblkmem,
-                                       h->P.delta, h->P.theta, z.data(), gx.data(), gy.data());
-        if (rc) return rc;
+        // bed halo and bed gradients from the interior, as the reference prepares
+        // them at initialisation (src/InitialConditions.cu:140-144)
+        BGF_CUDA(cudaMemset(h->d_dzbdx, 0, nb * 324 * sizeof(T)));
+        BGF_CUDA(cudaMemset(h->d_dzbdy, 0, nb * 324 * sizeof(T)));
+        DevModel<T> m = dev_model<T>(h);
+        StepParams<T> p = step_params<T>(h);
+        int n = h->fast ? fa::launch_bed_init<T>(m, p, (T*)h->d_zb, (T*)h->d_dzbdx, (T*)h->d_dzbdy, h->stream)
+                        : ex::launch_bed_init<T>(m, p, (T*)h->d_zb, (T*)h->d_dzbdx, (T*)h->d_dzbdy, h->stream);
+        h->launches += n;
+        BGF_CUDA(cudaGetLastError());
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
     }
-    BGF_CUDA(cudaMemcpy(h->d_zb, z.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
-    BGF_CUDA(cudaMemcpy(h->d_dzbdx, gx.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
-    BGF_CUDA(cudaMemcpy(h->d_dzbdy, gy.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
     h->has_cf = cf != nullptr;
     if (cf) {
         std::vector<T> c(nb * 256);
@@ -670,22 +760,37 @@ int bgf_init_dt(bgf_handle* h, bgf_loop* loop)
     return h->dbl ? init_dt_t<double>(h, loop) : init_dt_t<float>(h, loop);
 }
 
-template <class T> static void enqueue_flux(bgf_handle* h, int parity)
+// First and second half of a step: the fused predictor / corrector kernels, or
+// the predictor / corrector stages of the multi-level chain.  Return the number
+// of kernels launched.
+template <class T> static int enqueue_flux(bgf_handle* h, int parity)
 {
+    if (h->amr)
+        return h->fast ? fa::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
+                                                 0, h->minlev, h->maxlev, h->stream)
+                       : ex::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
+                                                 0, h->minlev, h->maxlev, h->stream);
     if (h->fast) fa::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
     else ex::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
+    return 1;
 }
 
-template <class T> static void enqueue_update(bgf_handle* h, int parity)
+template <class T> static int enqueue_update(bgf_handle* h, int parity)
 {
+    if (h->amr)
+        return h->fast ? fa::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
+                                                 1, h->minlev, h->maxlev, h->stream)
+                       : ex::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
+                                                 1, h->minlev, h->maxlev, h->stream);
     if (h->fast) fa::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
     else ex::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
+    return 1;
 }
 
-template <class T> static void enqueue_step(bgf_handle* h, int parity)
+template <class T> static int enqueue_step(bgf_handle* h, int parity)
 {
-    enqueue_flux<T>(h, parity);
-    enqueue_update<T>(h, parity);
+    int n = enqueue_flux<T>(h, parity);
+    return n + enqueue_update<T>(h, parity);
 }
 
 static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep, long long maxsteps)
@@ -719,24 +824,25 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
     if (!loop) return BGF_EINVAL;
     rc = write_time_slot(h, loop, INFINITY, 0.0, 1);
     if (rc) return rc;
+    int n = 0;
     if (h->profiling) {
         BGF_CUDA(cudaEventRecord(h->pev[0], h->stream));
         if (h->dbl) {
-            enqueue_flux<double>(h, h->parity);
+            n += enqueue_flux<double>(h, h->parity);
             BGF_CUDA(cudaEventRecord(h->pev[1], h->stream));
-            enqueue_update<double>(h, h->parity);
+            n += enqueue_update<double>(h, h->parity);
         } else {
-            enqueue_flux<float>(h, h->parity);
+            n += enqueue_flux<float>(h, h->parity);
             BGF_CUDA(cudaEventRecord(h->pev[1], h->stream));
-            enqueue_update<float>(h, h->parity);
+            n += enqueue_update<float>(h, h->parity);
         }
         BGF_CUDA(cudaEventRecord(h->pev[2], h->stream));
     } else if (h->dbl) {
-        enqueue_step<double>(h, h->parity);
+        n = enqueue_step<double>(h, h->parity);
     } else {
-        enqueue_step<float>(h, h->parity);
+        n = enqueue_step<float>(h, h->parity);
     }
-    h->launches += 2;
+    h->launches += n;
     BGF_CUDA(cudaGetLastError());
     BGF_CUDA(cudaMemcpyAsync(&h->h_time[1], h->d_time + (h->parity ^ 1), sizeof(TimeState), cudaMemcpyDeviceToHost,
                              h->stream));
@@ -765,10 +871,9 @@ static int build_graphs(bgf_handle* h)
     for (int p0 = 0; p0 < 2; p0++) {
         cudaGraph_t g;
         BGF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < 2; k++) {
-            if (h->dbl) enqueue_step<double>(h, p0 ^ k);
-            else enqueue_step<float>(h, p0 ^ k);
-        }
+        int n = 0;
+        for (int k = 0; k < 2; k++) n += h->dbl ? enqueue_step<double>(h, p0 ^ k) : enqueue_step<float>(h, p0 ^ k);
+        h->steps_launches = n / 2;
         cudaError_t e = cudaStreamEndCapture(h->stream, &g);
         if (e != cudaSuccess) {
             g_last_error = std::string("graph capture: ") + cudaGetErrorString(e);
@@ -810,7 +915,7 @@ int bgf_run(bgf_handle* h, bgf_loop* loop, double endtime, double outputtimestep
         BGF_CUDA(cudaEventRecord(h->ev0, h->stream));
         for (int b = 0; b < batch; b++) BGF_CUDA(cudaGraphLaunch(h->graph[p0], h->stream));
         BGF_CUDA(cudaEventRecord(h->ev1, h->stream));
-        launched += 4LL * batch;
+        launched += 2LL * h->steps_launches * batch;
         // after whole graphs the latest time state is in slot p0
         BGF_CUDA(cudaMemcpyAsync(&h->h_time[1], h->d_time + p0, sizeof(TimeState), cudaMemcpyDeviceToHost, h->stream));
         BGF_CUDA(cudaStreamSynchronize(h->stream));

@@ -58,6 +58,7 @@ struct SegDev {
 template <class T> struct StepParams {
     T g, eps, CFL, theta, delta0, epsi, epsface, fc;
     double eps_d, dtparam, bndfiltertime, bndrelaxtime, bndtaper, inittime, zsinit, zsoffset, dtmin;
+    double delta0_d;  // level-0 spacing in double (refine_linear left/top offsets)
     T cf;        // uniform friction coefficient
     int frictionmodel, forcemass, has_cf, has_rain, nseg, rain_n;
 };
@@ -197,9 +198,20 @@ template <> __device__ __forceinline__ double div_by<double>(double x, double d,
 }
 #endif
 
+// Source-term substitution at coarse/fine faces (src/Kurganov.cu:602-616,
+// src/Reimann.cu:350-365): on a side whose neighbour is coarser, the depth and bed
+// of the coarse neighbour's cell next to the face replace those of the halo cell.
+// Sides 0..3 = left, right, bottom, top; entry t along the side.
+template <class T> struct SubFaces {
+    T h[4][BW];
+    T z[4][BW];
+    int on[4];
+};
+
 // One X (isx) or Y face of the tile, written to the face arrays of s.
-template <class T, int ENGINE>
-__device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p, T delta, bool isx, int x, int y)
+template <class T, int ENGINE, bool SUB = false>
+__device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p, T delta, bool isx, int x, int y,
+                                             const SubFaces<T>* sub = nullptr)
 {
     FaceIn<T, ENGINE> f;
     int ci = ti(x, y), cn = isx ? ti(x - 1, y) : ti(x, y - 1);
@@ -227,6 +239,15 @@ __device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p,
         f.zsrci = f.zsi - f.hi;
         f.zsrcn = f.zsn - f.hn;
     }
+    if (SUB) {
+        if (isx) {
+            if (x == BW && sub->on[1]) { f.hsi = sub->h[1][y]; f.zsrci = sub->z[1][y]; }
+            if (x == 0 && sub->on[0]) { f.hsn = sub->h[0][y]; f.zsrcn = sub->z[0][y]; }
+        } else {
+            if (y == BW && sub->on[3]) { f.hsi = sub->h[3][x]; f.zsrci = sub->z[3][x]; }
+            if (y == 0 && sub->on[2]) { f.hsn = sub->h[2][x]; f.zsrcn = sub->z[2][x]; }
+        }
+    }
     Face<T> r = face_flux<T, ENGINE>(f, p.g, p.CFL, p.epsi, p.epsface, delta);
     if (isx) {
         int fi = fxi(x, y);
@@ -242,8 +263,9 @@ __device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p,
 // Restates gradientCPU (src/Gradients.cu:971-1054) on a single-level tile, then
 // the engine's X and Y sweeps.  Returns this thread's cell dtmax (the value the
 // reference leaves in dtmax[i] after both sweeps).
-template <class T, int ENGINE>
-__device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T delta, int tid)
+template <class T, int ENGINE, bool SUB = false>
+__device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T delta, int tid,
+                                         const SubFaces<T>* sub = nullptr)
 {
     const T theta = p.theta;
     const T rdelta = (T)1.0 / delta;
@@ -296,12 +318,12 @@ __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T d
     // Thread (tx,ty) owns the left (X) and bottom (Y) faces of its cell; threads
     // 0..15 also take X face x=16 and threads 16..31 Y face y=16 (the faces the
     // reference computes in the right / top halo column).
-    Face<T> fx = tile_face<T, ENGINE>(s, p, delta, true, tx, ty);
+    Face<T> fx = tile_face<T, ENGINE, SUB>(s, p, delta, true, tx, ty, sub);
     T celldt = fx.dt;  // dtmax after the X sweep (hugeposval exceeds any finite dt)
-    Face<T> fy = tile_face<T, ENGINE>(s, p, delta, false, tx, ty);
+    Face<T> fy = tile_face<T, ENGINE, SUB>(s, p, delta, false, tx, ty, sub);
     celldt = fy.wet ? (fy.dt < celldt ? fy.dt : celldt) : fy.dt;
-    if (tid < 16) tile_face<T, ENGINE>(s, p, delta, true, BW, tid);
-    else if (tid < 32) tile_face<T, ENGINE>(s, p, delta, false, tid - 16, BW);
+    if (tid < 16) tile_face<T, ENGINE, SUB>(s, p, delta, true, BW, tid, sub);
+    else if (tid < 32) tile_face<T, ENGINE, SUB>(s, p, delta, false, tid - 16, BW, sub);
     return celldt;
 }
 

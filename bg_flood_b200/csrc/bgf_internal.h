@@ -12,8 +12,9 @@ struct TimeState;
 struct SegDev;
 template <class T> struct DevModel;
 template <class T> struct StepParams;
+template <class T> struct AmrDev;
 
-// Kernel launchers, built twice (bgf_flow.cu): "exact" reproduces the reference
+// Kernel launchers, built twice (bgf_flow.cu, bgf_amr.cu): "exact" reproduces the reference
 // CPU arithmetic bit for bit, "fast" trades the last bits for speed.
 #define BGF_DECLARE_LAUNCHERS                                                                                   \
     template <class T> cudaError_t configure_kernels();                                                        \
@@ -24,7 +25,13 @@ template <class T> struct StepParams;
     template <class T>                                                                                         \
     void launch_initdt(const DevModel<T>& m, const StepParams<T>& p, int cur, unsigned long long* out,         \
                        cudaStream_t st);                                                                       \
-    template <class T> void launch_volume(const DevModel<T>& m, T delta0, int cur, double* out, cudaStream_t st);
+    template <class T> void launch_volume(const DevModel<T>& m, T delta0, int cur, double* out, cudaStream_t st); \
+    template <class T> cudaError_t configure_amr_kernels();                                                    \
+    template <class T>                                                                                         \
+    int launch_amr_stage(const DevModel<T>& m, const AmrDev<T>& a, const StepParams<T>& p, int engine,         \
+                         int parity, int stage, int minlev, int maxlev, cudaStream_t st);                      \
+    template <class T> int launch_bed_init(const DevModel<T>& m, const StepParams<T>& p, T* zb, T* gx, T* gy,  \
+                                           cudaStream_t st);
 namespace exact {
 BGF_DECLARE_LAUNCHERS
 }
@@ -35,11 +42,5 @@ BGF_DECLARE_LAUNCHERS
 // Records the text returned by bgf_last_error() for this thread.
 void set_last_error(const std::string& msg);
 
-// Host restatement of the bed preparation the reference performs once at
-// initialisation (src/InitialConditions.cu:140-144): bed halo fill and bed
-// gradients including halo cells, on BUQ tiles.
-template <class T>
-int host_bed_gradients(int nblk, const int* active, const int* level, const int* nbr8soa, int nblkmem, double delta,
-                       double theta, const T* zb, T* dzbdx, T* dzbdy);
 
 }  // namespace bgf

@@ -114,6 +114,7 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     p.CFL = (T)P->CFL;
     p.theta = (T)P->theta;
     p.delta0 = (T)P->delta;
+    p.delta0_d = P->delta;
     p.epsi = std::nextafter((T)1.0, (T)2.0) - (T)1.0;
     p.epsface = (T)P->eps + p.epsi;
     p.fc = (T)((double)std::sin((T)(P->lat * 3.14159265 / 180.0)) * 3.14159265 / (double)(T)21600.0);

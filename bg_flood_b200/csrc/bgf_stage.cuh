@@ -1,0 +1,171 @@
+// Device helpers shared by the fused single-level kernels (bgf_flow.cu) and the
+// multi-level kernels (bgf_amr.cu): bed tile loads, boundary-segment fluxes, the
+// flux divergence, and the step / dt bookkeeping of the device time loop.
+//
+// Included inside namespace bgf::BGF_VARIANT by each kernel file, so that every
+// arithmetic variant (exact, fast) gets its own copy compiled with its own flags.
+#pragma once
+
+// Loads the bed halo tile and (engine 1) the bed-gradient rows/columns.
+template <class T, int ENGINE>
+__device__ __forceinline__ void load_bed(Smem<T>& s, const DevModel<T>& m, int ib, int tid)
+{
+    const T* zbt = m.zb + (size_t)ib * 324;
+    for (int k = tid; k < 324; k += NTHREADS) s.zb[k] = zbt[k];
+    if (ENGINE == 1) {
+        const T* gx = m.dzbdx + (size_t)ib * 324;
+        const T* gy = m.dzbdy + (size_t)ib * 324;
+        for (int k = tid; k < 18 * 16; k += NTHREADS) {
+            int x = k % 18 - 1, y = k / 18;
+            s.dzbx[k] = gx[hi18(x, y)];
+            int xx = k % 16, yy = k / 16 - 1;
+            s.dzby[k] = gy[hi18(xx, yy)];
+        }
+    }
+}
+
+// interptime (src/Util_CPU.cu:107-110) over a uniform series, stepping as
+// FlowbndFlux does (src/Boundary.cu:130-143).
+__device__ __forceinline__ double series_at(const double* t, const double* v, int n, double time)
+{
+    int st = 1;
+    while (st < n - 1 && t[st] - time < 0.0) st++;
+    return v[st - 1] + (time - t[st - 1]) / (t[st] - t[st - 1]) * (v[st] - v[st - 1]);
+}
+
+// bndFluxGPUSideCPU (src/Boundary.cu:587-745) for the four sides of one block.
+// Face arrays in s are modified in place; state n comes from s.h0/u0/v0 and the
+// bed tile (zs = zb + h, as RecalculateZs leaves it).
+template <class T>
+__device__ __forceinline__ void apply_boundaries(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
+                                                 double tbnd, int tid)
+{
+    if (tid >= 64) return;
+    int side = tid >> 4, t = tid & 15;
+    int k = m.bndseg[ib * 4 + side];
+    if (k < 0) return;
+    SegDev sg = m.segs[k];
+    if (sg.type == 1) return;
+    double zsbnd = 0.0;
+    if (!isnan(p.zsinit)) zsbnd = p.zsinit;
+    T taper = (T)1.0;
+    if (sg.n > 0) {
+        if (p.bndtaper > 0.0) taper = (T)fmin((tbnd - p.inittime) / p.bndtaper, 1.0);
+        zsbnd = series_at(m.seg_t + sg.off, m.seg_wl + sg.off, sg.n, tbnd);
+    }
+    int isright = side == 0 ? -1 : side == 1 ? 1 : 0;
+    int istop = side == 2 ? 1 : side == 3 ? -1 : 0;
+    int ix, iy, inx, iny;
+    if (isright == 0) { ix = t; iy = istop < 0 ? 0 : BW; }
+    else { iy = t; ix = isright < 0 ? 0 : BW; }
+    if (isright < 0) { inx = ix + 1; iny = iy; }
+    else if (isright > 0) { inx = ix - 1; iny = iy; }
+    else if (istop < 0) { inx = ix; iny = iy + 1; }
+    else { inx = ix; iny = iy - 1; }
+    T sign = (T)isright + (T)istop;
+    float zsb = (float)zsbnd;
+    zsb = (float)((double)zsb + p.zsoffset);
+    int ci = hi18(ix, iy), cin = hi18(inx, iny);
+    T zsi = s.zb[ci] + s.h0[ci];
+    T zsinside = s.zb[cin] + s.h0[cin];
+    T hinside = s.h0[cin];
+    T uninside = isright != 0 ? s.u0[cin] : s.v0[cin];
+    T hface = s.h0[ci];
+    T zsX = (T)(((double)((T)zsb + (T)0.0) - 0.5 * (double)(zsi + zsinside)) * (double)taper + 0.5 * (double)(zsi + zsinside));
+    float* qm = m.qmean + ib * 64 + side * 16 + t;
+    T qmean = (T)*qm;
+    T *Fh, *Fq, *Ss;
+    int fi, fin;
+    if (isright != 0) {
+        Fh = s.Fhu; Fq = s.Fqux; Ss = s.Su;
+        fi = fxi(ix, iy); fin = fxi(inx, iny);
+    } else {
+        Fh = s.Fhv; Fq = s.Fqvy; Ss = s.Sv;
+        fi = fyi(ix, iy); fin = fyi(inx, iny);
+    }
+    T F, G, S;
+    bool lowside = isright < 0 || istop < 0;
+    if (lowside) { F = Fh[fi]; G = Fq[fi]; S = Ss[fin]; }
+    else { F = Fh[fi]; G = Ss[fi]; S = Fq[fin]; }
+    T factime = M<T>::fmin_((T)(p.dtparam / p.bndfiltertime), (T)1.0);
+    T facrel = (T)1.0 - M<T>::fmin_((T)(p.dtparam / p.bndrelaxtime), (T)1.0);
+    if (sg.type == 0) {
+        F = (T)0.0;
+        S = G;
+    } else if (sg.type == 3) {
+        if ((double)hface > p.eps_d || zsX > zsi) {
+            abs1dq<T>(p.g, sign, factime, facrel, zsi, zsX, hface, qmean, F);
+        } else {
+            F = (T)0.0; S = G; qmean = (T)0.0;
+        }
+        *qm = (float)qmean;
+    } else if (sg.type == 2) {
+        if ((double)hface > p.eps_d || zsX > zsi) {
+            dirichlet1q<T>(p.g, sign, zsX, zsinside, hinside, uninside, F);
+        } else {
+            F = (T)0.0; S = G; qmean = (T)0.0;
+        }
+        *qm = (float)qmean;
+    }
+    if (lowside) { Fh[fi] = F; Fq[fi] = G; Ss[fin] = S; }
+    else { Fh[fi] = F; Ss[fi] = G; Fq[fin] = S; }
+}
+
+// updateEVCPU (src/Advection.cu:160-254), Cartesian.  Returns dh, dhu, dhv of the
+// thread's cell from the face arrays.
+template <class T>
+__device__ __forceinline__ void flux_divergence(const Smem<T>& s, const StepParams<T>& p, T cmdinv, int x, int y, T hi,
+                                                T uui, T vvi, T& dh, T& dhu, T& dhv)
+{
+    // Cartesian grid: the metric terms dmdl, dmdt and fG of the reference are zero
+    // and their products only add signed zeros.
+    int fi = fxi(x, y), fr = fi + 1;
+    int gi = fyi(x, y), gt = gi + 16;
+    dh = (T)-1.0 * (s.Fhu[fr] - s.Fhu[fi] + s.Fhv[gt] - s.Fhv[gi]) * cmdinv;
+    dhu = (s.Fqux[fi] + s.Fquy[gi] - s.Su[fr] - s.Fquy[gt]) * cmdinv + p.fc * hi * vvi;
+    dhv = (s.Fqvy[gi] + s.Fqvx[fi] - s.Sv[gt] - s.Fqvx[fr]) * cmdinv - p.fc * hi * uui;
+}
+
+// Whether this step runs (the reference loop condition totaltime < endtime plus
+// the step budget); identical in both kernels of a step.
+__device__ __forceinline__ bool step_live(const TimeState& ts)
+{
+    return !ts.done && ts.totaltime < ts.endtime && ts.nstep < ts.maxsteps;
+}
+
+// dt of the step from the reduced minimum (CalctimestepGPU, src/Advection.cu:549-620
+// and CalctimestepCPU, :511-535): clamp to 1.5 * the previous dt, then split the
+// time to the next output into an integer number of equal steps.
+template <class T> __device__ __forceinline__ T step_dt(const TimeState& ts, unsigned long long minbits)
+{
+    T dt = dt_from_bits<T>(minbits);
+    if ((double)dt > (1.5 * ts.dtmax)) dt = (T)(1.5 * ts.dtmax);
+    if (ceil((ts.nextoutputtime - ts.totaltime) / (double)dt) > 0.0)
+        dt = (T)((ts.nextoutputtime - ts.totaltime) / ceil((ts.nextoutputtime - ts.totaltime) / (double)dt));
+    return dt;
+}
+
+
+// Time slot of the next step (the Mainloop bookkeeping, src/Mainloop.cu:43-86 and
+// the crash check :648-719), written by one thread once dt is known; re-arms the
+// running dt minimum of the slot the next step reduces into.
+template <class T>
+__device__ __forceinline__ TimeState next_time_state(const TimeState& ts, const StepParams<T>& p, double dtd, int nxt,
+                                                     unsigned long long* dtmin, int parity)
+{
+    TimeState nt = ts;
+    nt.dt = dtd;
+    nt.dtmax = dtd;
+    nt.totaltime = ts.totaltime + dtd;
+    nt.nstep = ts.nstep + 1;
+    nt.cur = nxt;
+    if (dtd < p.dtmin && nt.totaltime < ts.endtime) {
+        nt.status = 4;  // BGF_EDT_UNDERFLOW
+        nt.done = 1;
+    }
+    if (ts.outputtimestep > 0.0 && nt.nextoutputtime - nt.totaltime <= dtd * 0.00001) {
+        nt.nextoutputtime = fmin(nt.nextoutputtime + ts.outputtimestep, ts.endtime);
+    }
+    dtmin[parity ^ 1] = dt_bits(inv_epsi<T>());
+    return nt;
+}

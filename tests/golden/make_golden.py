@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path[:0] = [ROOT, os.path.join(ROOT, "tests")]
 
 import cases  # noqa: E402
-from runners import interior, make_reference  # noqa: E402
+from runners import interior, make_amr_pair, make_reference  # noqa: E402
 
 GOLDEN_CASES = {
     "gauss48_e1_b3": (lambda: cases.gauss(48, 1, 3), 40),
@@ -28,6 +28,28 @@ GOLDEN_CASES = {
     "dam48_e1": (lambda: cases.dam_break(48, 1), 40),
     "rain48_e1": (lambda: cases.rain_on_terrain(48, 1), 30),
 }
+
+# Meshes refined by the reference's own InitialAdaptation(): the block tables in
+# active order are stored with the reference's dt sequence and fields, so the
+# oracle and the GPU library can be run on the same tables without the reference.
+AMR_GOLDEN_CASES = {
+    "amrhump64_e1_l1": (lambda: cases.amr_hump(64, 1, 1, 0.3), 30),
+    "amrhump64_e2_l2": (lambda: cases.amr_hump(64, 2, 2, 0.3), 30),
+    "amrdam64_e1_l2": (lambda: cases.amr_dambreak(64, 1, 2), 40),
+    "amrdam64_e2_l2": (lambda: cases.amr_dambreak(64, 2, 2), 40),
+    "amrdam64_e1_l3": (lambda: cases.amr_dambreak(64, 1, 3), 40),
+}
+
+
+def main_amr():
+    for name, (mk, nsteps) in AMR_GOLDEN_CASES.items():
+        case = mk()
+        ref, _, (lev, nbr, xo, yo) = make_amr_pair(case)
+        dts = ref.step(nsteps)
+        out = {k: interior(ref.get(k)).astype(np.float32) for k in ("h", "u", "v")}
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), dts=dts, nsteps=nsteps, level=lev, nbr=nbr, xo=xo,
+                            yo=yo, **out)
+        print(name, nsteps, np.bincount(lev), dts[:3])
 
 
 def main():
@@ -42,3 +64,4 @@ def main():
 
 if __name__ == "__main__":
     main()
+    main_amr()

@@ -82,6 +82,57 @@ def _sample(fn, level, xo, yo, case, zb=None):
     return out.astype(np.float32).astype(np.float64)
 
 
+def amr_fields(case, lev, xo, yo):
+    """Bed and depth of an AMR case sampled at the cell centres of the given blocks."""
+    zb = _sample(case.zb_fn, lev, xo, yo, case)
+    h = _sample(lambda X, Y, Z: np.maximum(case.eta_fn(X, Y) - Z, 0.0), lev, xo, yo, case, zb=zb)
+    return zb, h
+
+
+def amr_mesh(case, lev, nbr, xo, yo):
+    from bg_flood_b200.mesh import Mesh
+    n = len(lev)
+    return Mesh(case.n0 // 16, case.n0 // 16, case.dx, n, np.asarray(lev, np.int32), np.asarray(nbr, np.int32),
+                np.asarray(xo), np.asarray(yo), np.zeros(n, np.int32), np.zeros(n, np.int32))
+
+
+def make_oracle_amr(case, tables, use_double: bool = False):
+    """The oracle on given block tables (level, nbr (n, 8), xo, yo) of an AMR case."""
+    lev, nbr, xo, yo = tables
+    zb, h = amr_fields(case, lev, xo, yo)
+    zero = np.zeros_like(zb)
+    o = Oracle(case.param, len(lev), use_double)
+    o.set_blocks(lev, nbr, xo, yo)
+    for name, a in (("zb", zb), ("h", h), ("u", zero), ("v", zero)):
+        o.set(name, a)
+    o.set("zs", (zb + h).astype(np.float32))
+    m = amr_mesh(case, lev, nbr, xo, yo)
+    for typ, times, levels, sides in boundary_segments(m, case.param.segments, case.param.aoibnd, case.xo, case.yo):
+        o.add_segment(typ, times, levels, sides)
+    o.init_bed()
+    o.init_loop(0.0, case.nextoutputtime)
+    return o
+
+
+def make_gpu_amr(case, tables):
+    """The GPU library on given block tables of an AMR case; returns (FlowB200, Loop)."""
+    from bg_flood_b200.flow import FlowB200, Loop
+    lev, nbr, xo, yo = tables
+    zb, h = amr_fields(case, lev, xo, yo)
+    zero = np.zeros_like(zb)
+    n = len(lev)
+    f = FlowB200(case.param, n)
+    f.set_blocks(np.arange(n, dtype=np.int32), lev, nbr, xo, yo)
+    f.set_bed(zb)
+    m = amr_mesh(case, lev, nbr, xo, yo)
+    for typ, times, levels, sides in boundary_segments(m, case.param.segments, case.param.aoibnd, case.xo, case.yo):
+        f.add_segment(typ, times, levels, sides)
+    f.set_state(h, zero, zero)
+    loop = Loop(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=case.nextoutputtime)
+    f.init_dt(loop)
+    return f, loop
+
+
 def make_amr_pair(case):
     """The reference adapts the mesh; the oracle gets the same tables and fields.
     Returns (reference, oracle, (level, nbr, xo, yo))."""
@@ -94,24 +145,11 @@ def make_amr_pair(case):
     z0 = np.zeros_like(zb0)
     r = Reference(case.paramtext, n0, n0, case.dx, case.xo, case.yo, zb0, h0, z0, z0, None, case.nextoutputtime)
     r.adapt()
-    lev, nbr, xo, yo = r.mesh_active_order()
-    zb = _sample(case.zb_fn, lev, xo, yo, case)
-    h = _sample(lambda X, Y, Z: np.maximum(case.eta_fn(X, Y) - Z, 0.0), lev, xo, yo, case, zb=zb)
+    tables = r.mesh_active_order()
+    lev, nbr, xo, yo = tables
+    zb, h = amr_fields(case, lev, xo, yo)
     zero = np.zeros_like(zb)
     for name, a in (("zb", zb), ("h", h), ("u", zero), ("v", zero)):
         r.set(name, a)
     r.reinit(case.nextoutputtime)
-    o = Oracle(case.param, len(lev))
-    o.set_blocks(lev, nbr, xo, yo)
-    for name, a in (("zb", zb), ("h", h), ("u", zero), ("v", zero)):
-        o.set(name, a)
-    o.set("zs", (zb + h).astype(np.float32))
-    from bg_flood_b200.mesh import Mesh
-    from bg_flood_b200.mesh import boundary_segments
-    m = Mesh(n0 // 16, n0 // 16, case.dx, len(lev), lev, nbr, xo, yo, np.zeros(len(lev), np.int32),
-             np.zeros(len(lev), np.int32))
-    for typ, times, levels, sides in boundary_segments(m, case.param.segments, case.param.aoibnd, case.xo, case.yo):
-        o.add_segment(typ, times, levels, sides)
-    o.init_bed()
-    o.init_loop(0.0, case.nextoutputtime)
-    return r, o, (lev, nbr, xo, yo)
+    return r, make_oracle_amr(case, tables), tables

@@ -129,9 +129,12 @@ int bgf_destroy(bgf_handle* h);
 int bgf_set_blocks(bgf_handle* h, const bgf_blockp* blocks);
 
 /* Bed elevation and per-cell inputs in BUQ layout (nblkmem tiles).
- * zb: bed with its halo already filled (as after fillHaloC on zb,
- *     src/Testing.cu:583).  dzbdx/dzbdy: bed gradients incl. halo cells
- *     (src/InitialConditions.cu:140-144); NULL to let the library compute them.
+ * zb, dzbdx, dzbdy: with dzbdx/dzbdy NULL, only the interior of zb is read and
+ *     the library prepares the bed on the device as the reference does at
+ *     initialisation (src/Testing.cu:583-588, src/InitialConditions.cu:140-144):
+ *     halo fill across levels, gradients, halo gradients, linear refinement of
+ *     the halos next to coarser blocks, halo gradients again.  With both given,
+ *     zb's halo and the gradients (incl. halo cells) are used as they are.
  * cf: friction coefficient per cell, NULL for the uniform Param.cf.
  * activeCell: rain mask per cell (int), NULL for all ones. */
 int bgf_set_bed(bgf_handle* h, const void* zb, const void* dzbdx, const void* dzbdy, const void* cf,

@@ -44,6 +44,10 @@ SIGNATURES = {
     "bgf_flow_step_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "bgf_mesh_uniform": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, c_void_p, c_int_p, c_int_p,
                                         c_int_p, c_double_p, c_double_p]),
+    "bgf_refine_sanity": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_int_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, c_void_p, c_void_p]),
+    "bgf_refine_tables": (ctypes.c_int, [c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_int, c_void_p, c_int_p]),
 }
 
 

@@ -31,6 +31,7 @@ SOURCES = [
     ("bgf_capi.cu", "bgf_capi.o", ["--fmad=false"]),
     ("bgf_noalloc.cu", "bgf_noalloc.o", ["--fmad=false"]),
     ("bgf_host.cpp", "bgf_host.o", ["-x", "cu", "--fmad=false"]),
+    ("bgf_adapt_host.cpp", "bgf_adapt_host.o", ["-x", "cu", "--fmad=false"]),
 ]
 
 

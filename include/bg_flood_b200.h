@@ -243,6 +243,28 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* args, bgf_
 int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* present, int* nblk, int* level,
                      int* nbr8, double* xo, double* yo);
 
+/* ------------------------------------------------------------ refinement pass */
+/* Host-only table work of the reference's adaptation (no device memory involved).
+ * Arrays are indexed by block id and sized nblkmem; nbr8 is [nblkmem][8] in the
+ * order LeftBot, LeftTop, RightBot, RightTop, BotLeft, BotRight, TopLeft, TopRight.
+ *
+ * refinesanitycheck (src/Adaptation.cu:157-296): refine/coarsen flags (one byte
+ * per block id) corrected in place -- no refinement at maxlevel, coarsening
+ * cancelled (as the reference does), coarser first neighbours of a refining block
+ * forced to refine until the mesh stays 2:1 balanced. */
+int bgf_refine_sanity(int nblk, const int* active, const int* level, const int* nbr8, int nblkmem, int minlevel,
+                      int maxlevel, uint8_t* refine, uint8_t* coarsen);
+/* CalcAvailblk + refine + Adaptationcleanup (src/Adaptation.cu:535-596,
+ * 1017-1876) on the tables: every flagged block becomes four; it keeps its id as
+ * the bottom-left child and the k-th flagged block of the active list takes the
+ * free ids 3k..3k+2 (ascending) for its bottom-right, top-left and top-right
+ * children (children[3*ib..3*ib+2]), which are appended to the active list.
+ * Levels, origins (rounded to float unless doubleprecision) and all neighbour
+ * tables are updated; *nblk is updated.  BGF_ENOMEM when fewer than 3 free block
+ * slots per flagged block exist below nblkmem. */
+int bgf_refine_tables(int* nblk, int* active, int* level, int* nbr8, double* xo, double* yo, int nblkmem, double dx,
+                      int doubleprecision, const uint8_t* refine, int* children);
+
 #ifdef __cplusplus
 }
 #endif

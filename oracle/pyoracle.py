@@ -84,6 +84,11 @@ def ref_lib():
         l.ref_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, D]
         l.ref_reinit.argtypes = [ctypes.c_void_p, ctypes.c_double]
         l.ref_get_active.argtypes = [ctypes.c_void_p, I]
+        l.ref_adaptation.argtypes = [ctypes.c_void_p]
+        l.ref_flags.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ubyte), ctypes.POINTER(ctypes.c_ubyte)]
+        l.ref_set_bathy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, D]
+        l.ref_nblkmem.argtypes = [ctypes.c_void_p]
         _rlib = l
     return _rlib
 
@@ -231,6 +236,31 @@ class Reference:
         """Runs the reference's own Adaptation() with the "Adaptation" key of paramtext."""
         self.nblk = self.lib.ref_adapt(self.h)
         return self.nblk
+
+    def adaptation(self) -> int:
+        """The reference's Adaptation() alone (no InitialConditions afterwards)."""
+        self.nblk = self.lib.ref_adaptation(self.h)
+        return self.nblk
+
+    def flags(self):
+        """(refine, coarsen) per active block of one AdaptCriteria + refinesanitycheck
+        pass; the model is refined by that one iteration of Adaptation()."""
+        r = np.zeros(self.nblk, np.uint8)
+        c = np.zeros(self.nblk, np.uint8)
+        self.lib.ref_flags(self.h, r.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                           c.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)))
+        self.nblk = self.lib.ref_nblk(self.h)
+        return r, c
+
+    def set_bathy(self, xo: float, yo: float, dx: float, val: np.ndarray):
+        """Bathymetry forcing grid (ny, nx) with node (0, 0) at (xo, yo)."""
+        v = np.ascontiguousarray(val, np.float64)
+        ny, nx = v.shape
+        self.lib.ref_set_bathy(self.h, nx, ny, xo, yo, dx, _dp(v))
+
+    @property
+    def nblkmem(self) -> int:
+        return self.lib.ref_nblkmem(self.h)
 
     def active(self) -> np.ndarray:
         a = np.zeros(self.nblk, np.int32)

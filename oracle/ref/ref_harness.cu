@@ -20,11 +20,13 @@
 #include "Setup_GPU.h"
 #include "Mainloop.h"
 #include "Adaptation.h"
+#include "AdaptCriteria.h"
 #include "Updateforcing.h"
 #include "Gradients.h"
 #include "Halo.h"
 
 #include <memory>
+#include <vector>
 #include <sstream>
 
 namespace {
@@ -38,6 +40,9 @@ struct RefBase {
     virtual int set(const char* name, const double* buq) = 0;
     virtual int reinit(double nextout) = 0;
     virtual int get_active(int* out) = 0;
+    virtual int adaptation() = 0;
+    virtual int flags(unsigned char* refine, unsigned char* coarsen) = 0;
+    virtual int set_bathy(int nx, int ny, double xo, double yo, double dx, const double* val) = 0;
     Param P;
     Forcing<float> F;
     double totaltime = 0.0, nextoutputtime = 0.0, dtmax = 0.0;
@@ -277,6 +282,59 @@ template <class T> struct RefModel : RefBase {
         for (int ibl = 0; ibl < P.nblk; ibl++) out[ibl] = M.blocks.active[ibl];
         return P.nblk;
     }
+
+    // The reference's Adaptation() alone (src/Adaptation.cu:17-121), as a time loop
+    // would call it between steps: criteria, sanity pass, refinement, bed
+    // re-interpolation from the bathymetry forcing, wet/dry fix-up, state copy.
+    int adaptation() override
+    {
+        CopyArrayBUQ(P, M.blocks, M.evolv, M.evolv_o);
+        Adaptation(P, F, M);
+        return P.nblk;
+    }
+
+    // Refine / coarsen flags of one pass of AdaptCriteria + refinesanitycheck, read
+    // off one iteration of Adaptation (refinesanitycheck is not exported by the
+    // reference build): a block was flagged for refinement when its level rose, for
+    // coarsening when it left the active list or its level fell.  Written per block
+    // of the active list before the pass; the model is adapted by one iteration.
+    int flags(unsigned char* refine, unsigned char* coarsen) override
+    {
+        const int n0 = P.nblk;
+        std::vector<int> act(M.blocks.active, M.blocks.active + n0), lev(n0);
+        for (int k = 0; k < n0; k++) lev[k] = M.blocks.level[act[k]];
+        const int saved = P.adaptmaxiteration;
+        P.adaptmaxiteration = 1;
+        CopyArrayBUQ(P, M.blocks, M.evolv, M.evolv_o);
+        Adaptation(P, F, M);
+        P.adaptmaxiteration = saved;
+        std::vector<char> still(P.nblkmem, 0);
+        for (int ibl = 0; ibl < P.nblk; ibl++) still[M.blocks.active[ibl]] = 1;
+        for (int k = 0; k < n0; k++) {
+            const int ib = act[k];
+            refine[k] = still[ib] && M.blocks.level[ib] > lev[k];
+            coarsen[k] = !still[ib] || M.blocks.level[ib] < lev[k];
+        }
+        return n0;
+    }
+
+    // Replaces the bathymetry forcing (Forcing.Bathy[0], a regular grid of nx*ny
+    // nodes from (xo, yo) with spacing dx) used when Adaptation re-interpolates zb.
+    int set_bathy(int nx, int ny, double xo, double yo, double dx, const double* val) override
+    {
+        StaticForcingP<float>& b = F.Bathy[0];
+        b.nx = nx;
+        b.ny = ny;
+        b.xo = xo;
+        b.yo = yo;
+        b.dx = dx;
+        b.dy = dx;
+        b.xmax = xo + (nx - 1) * dx;
+        b.ymax = yo + (ny - 1) * dx;
+        AllocateCPU(nx, ny, b.val);
+        for (int k = 0; k < nx * ny; k++) b.val[k] = (float)val[k];
+        return 0;
+    }
 };
 
 }  // namespace
@@ -318,6 +376,14 @@ int ref_set_segment_series(void* hdl, int iseg, int n, const double* t, const do
     s.uniform = true;
     return 0;
 }
+
+int ref_adaptation(void* hdl) { return ((RefBase*)hdl)->adaptation(); }
+int ref_flags(void* hdl, unsigned char* refine, unsigned char* coarsen) { return ((RefBase*)hdl)->flags(refine, coarsen); }
+int ref_set_bathy(void* hdl, int nx, int ny, double xo, double yo, double dx, const double* val)
+{
+    return ((RefBase*)hdl)->set_bathy(nx, ny, xo, yo, dx, val);
+}
+int ref_nblkmem(void* hdl) { return ((RefBase*)hdl)->P.nblkmem; }
 
 int ref_set_rain_series(void* hdl, int n, const double* t, const double* r)
 {

@@ -52,6 +52,32 @@ def main_amr():
         print(name, nsteps, np.bincount(lev), dts[:3])
 
 
+def main_adapt_tables():
+    """Iterations of the reference's Adaptation() with the pre-sanity criterion flags
+    and the tables before and after each iteration (tests/test_adapt_tables.py)."""
+    from adapt_cases import ADAPT_CASES, criterion_of, id_tables, reference_with_bathy
+    out = {}
+    for name in ("island64_e1_l2", "hump64_e1_l2", "dam64_e1_l3"):
+        case = ADAPT_CASES[name]()
+        crit = criterion_of(case)
+        r = reference_with_bathy(case)
+        for it in range(8):
+            act, level, nbr, xo, yo = id_tables(r)
+            stem = f"{name}_it{it}"
+            out[f"{stem}_pre"] = crit.flags(r.get(crit.var)[:, 1:17, 1:17])
+            out[f"{stem}_act"], out[f"{stem}_level"], out[f"{stem}_nbr"] = act, level, nbr
+            out[f"{stem}_xo"], out[f"{stem}_yo"] = xo, yo
+            rf, _ = r.flags()
+            out[f"{stem}_refine"] = rf
+            act_r, level_r, nbr_r, xo_r, yo_r = id_tables(r)
+            out[f"{stem}_act_out"], out[f"{stem}_level_out"], out[f"{stem}_nbr_out"] = act_r, level_r[act_r], nbr_r[act_r]
+            out[f"{stem}_xo_out"], out[f"{stem}_yo_out"] = xo_r[act_r], yo_r[act_r]
+            print(stem, len(act), "->", len(act_r))
+            if len(act_r) == len(act):
+                break
+    np.savez_compressed(os.path.join(HERE, "adapt_tables.npz"), **out)
+
+
 def main():
     for name, (mk, nsteps) in GOLDEN_CASES.items():
         case = mk()
@@ -65,3 +91,4 @@ def main():
 if __name__ == "__main__":
     main()
     main_amr()
+    main_adapt_tables()

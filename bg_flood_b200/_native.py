@@ -43,7 +43,13 @@ SIGNATURES = {
     "bgf_run_timing": (ctypes.c_int, [c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64)]),
     "bgf_flow_step_noalloc": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "bgf_mesh_uniform": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, c_void_p, c_int_p, c_int_p,
-                                        c_int_p, c_double_p, c_double_p]),
+                                        c_int_p, c_double_p, c_double_p, ctypes.c_int]),
+    "bgf_set_bathy": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, c_void_p]),
+    "bgf_adapt_flags": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "bgf_adapt": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_int_p]),
+    "bgf_get_blocks": (ctypes.c_int, [c_void_p, c_int_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "bgf_get_bed": (ctypes.c_int, [c_void_p, c_void_p]),
     "bgf_refine_sanity": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_int_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, c_void_p, c_void_p]),
     "bgf_refine_tables": (ctypes.c_int, [c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, ctypes.c_int,

@@ -28,6 +28,7 @@ SOURCES = [
     ("bgf_amr.cu", "bgf_amr_exact.o", ["-DBGF_VARIANT=exact", "--fmad=false"]),
     ("bgf_amr.cu", "bgf_amr_fast.o", ["-DBGF_VARIANT=fast", "-DBGF_FAST=1", "--fmad=true", "-prec-div=false", "-prec-sqrt=false",
                                       "-ftz=true"]),
+    ("bgf_adapt.cu", "bgf_adapt.o", ["--fmad=false"]),
     ("bgf_capi.cu", "bgf_capi.o", ["--fmad=false"]),
     ("bgf_noalloc.cu", "bgf_noalloc.o", ["--fmad=false"]),
     ("bgf_host.cpp", "bgf_host.o", ["-x", "cu", "--fmad=false"]),

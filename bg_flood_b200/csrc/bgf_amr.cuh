@@ -307,4 +307,18 @@ __device__ __forceinline__ T refine_value(const A& z, const A& gx, const A& gy, 
     return zi + (faclr * dx + facbt * dy) * ilevdx;
 }
 
+namespace adapt {
+
+// Device view of the refinement pass (bgf_adapt.cu).
+template <class T> struct AdaptDev {
+    T* W[4];            // h, zs, u, v on 18x18 tiles of the old mesh
+    T* zs;              // zs of the state, 256 per block
+    const float* dem;   // bathymetry grid, dnx * dny nodes
+    int dnx, dny;
+    double dxo, dyo, ddx, dxmax, dymax;
+    const int* child;   // [nblkmem][3]: bottom-right, top-left, top-right children, or -1
+    uint8_t* flags;     // one byte per block id
+};
+
+}  // namespace adapt
 }  // namespace bgf

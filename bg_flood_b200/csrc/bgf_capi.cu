@@ -47,6 +47,7 @@ struct bgf_handle {
     bool own_stream = false;
     // host copies of the tables
     std::vector<int> active, level, nbr;  // nbr as [8][nblkmem]
+    std::vector<double> bxo, byo;         // block origins (values of the state precision)
     std::vector<HostSeg> segs;
     std::vector<double> rain_t, rain_r;
     // device buffers
@@ -90,6 +91,13 @@ struct bgf_handle {
     void* d_F[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     uint8_t* d_pflag = nullptr;
     int* d_rank = nullptr;
+    // refinement pass: bathymetry grid, block origins, flags, children
+    float* d_dem = nullptr;
+    int dem_nx = 0, dem_ny = 0;
+    double dem_xo = 0, dem_yo = 0, dem_dx = 0;
+    double *d_bxo = nullptr, *d_byo = nullptr;
+    uint8_t* d_flags = nullptr;
+    int* d_child = nullptr;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -349,6 +357,8 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         {&h->d_dhu, nb * 256 * es},                      {&h->d_dhv, nb * 256 * es},
         {(void**)&h->d_time, 2 * sizeof(TimeState)},     {(void**)&h->d_dtmin, 2 * sizeof(unsigned long long)},
         {(void**)&h->d_scratch, 8 * sizeof(double)},
+        {(void**)&h->d_bxo, nb * sizeof(double)},        {(void**)&h->d_byo, nb * sizeof(double)},
+        {(void**)&h->d_flags, nb},                       {(void**)&h->d_child, 3 * nb * sizeof(int)},
     };
     for (auto& a : allocs) {
         if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
@@ -395,7 +405,8 @@ int bgf_destroy(bgf_handle* h)
     void* ptrs[] = {h->d_active, h->d_level, h->d_nbr, h->d_bndseg, h->d_err, h->d_zb, h->d_dzbdx, h->d_dzbdy,
                     h->d_cf, h->d_rainmask, h->d_qmean, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t,
                     h->d_rain_r, h->d_h[0], h->d_h[1], h->d_u[0], h->d_u[1], h->d_v[0], h->d_v[1], h->d_dh,
-                    h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch};
+                    h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch, h->d_bxo, h->d_byo,
+                    h->d_flags, h->d_child, h->d_dem};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     free_amr(h);
@@ -434,36 +445,22 @@ static int alloc_amr(bgf_handle* h)
     return BGF_OK;
 }
 
-int bgf_set_blocks(bgf_handle* h, const bgf_blockp* b)
+// Uploads the host tables (active, level, neighbours, origins), classifies the
+// mesh as single- or multi-level and prepares the multi-level buffers.
+static int upload_tables(bgf_handle* h)
 {
-    if (!h || !b || b->nblk <= 0 || b->nblk > h->nblkmem || !b->active || !b->level) return BGF_EINVAL;
-    const int* tabs[8] = {b->LeftBot, b->LeftTop, b->RightBot, b->RightTop, b->BotLeft, b->BotRight, b->TopLeft, b->TopRight};
-    for (int k = 0; k < 8; k++)
-        if (!tabs[k]) return BGF_EINVAL;
-    int nb = h->nblkmem;
-    h->nblk = b->nblk;
-    h->active.assign(b->active, b->active + b->nblk);
-    h->level.assign(b->level, b->level + nb);
-    h->nbr.assign((size_t)8 * nb, 0);
-    for (int k = 0; k < 8; k++)
-        for (int ib = 0; ib < nb; ib++) h->nbr[(size_t)k * nb + ib] = tabs[k][ib];
-    for (int ibl = 0; ibl < b->nblk; ibl++) {
-        int ib = b->active[ibl];
-        if (ib < 0 || ib >= nb) return BGF_EINVAL;
-        for (int k = 0; k < 8; k++) {
-            int q = tabs[k][ib];
-            if (q < 0 || q >= nb) return BGF_EINVAL;
-        }
-    }
+    const int nb = h->nblkmem;
     int rc = set_device(h);
     if (rc) return rc;
-    BGF_CUDA(cudaMemcpyAsync(h->d_active, h->active.data(), sizeof(int) * b->nblk, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_active, h->active.data(), sizeof(int) * h->nblk, cudaMemcpyHostToDevice, h->stream));
     BGF_CUDA(cudaMemcpyAsync(h->d_level, h->level.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, h->stream));
     BGF_CUDA(cudaMemcpyAsync(h->d_nbr, h->nbr.data(), sizeof(int) * 8 * nb, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_bxo, h->bxo.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_byo, h->byo.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, h->stream));
     // a mesh is multi-level when some active block has a neighbour on another level
     h->amr = false;
     h->minlev = h->maxlev = h->level[h->active[0]];
-    for (int ibl = 0; ibl < b->nblk; ibl++) {
+    for (int ibl = 0; ibl < h->nblk; ibl++) {
         int ib = h->active[ibl];
         h->minlev = std::min(h->minlev, h->level[ib]);
         h->maxlev = std::max(h->maxlev, h->level[ib]);
@@ -473,13 +470,45 @@ int bgf_set_blocks(bgf_handle* h, const bgf_blockp* b)
         rc = alloc_amr(h);
         if (rc) return rc;
         std::vector<int> rank(nb, 0);
-        for (int ibl = 0; ibl < b->nblk; ibl++) rank[h->active[ibl]] = ibl;
+        for (int ibl = 0; ibl < h->nblk; ibl++) rank[h->active[ibl]] = ibl;
         BGF_CUDA(cudaMemcpyAsync(h->d_rank, rank.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, h->stream));
-        BGF_CUDA(cudaStreamSynchronize(h->stream));
     }
     BGF_CUDA(cudaStreamSynchronize(h->stream));
     h->has_blocks = true;
     free_graphs(h);
+    return BGF_OK;
+}
+
+int bgf_set_blocks(bgf_handle* h, const bgf_blockp* b)
+{
+    if (!h || !b || b->nblk <= 0 || b->nblk > h->nblkmem || !b->active || !b->level) return BGF_EINVAL;
+    const int* tabs[8] = {b->LeftBot, b->LeftTop, b->RightBot, b->RightTop, b->BotLeft, b->BotRight, b->TopLeft, b->TopRight};
+    for (int k = 0; k < 8; k++)
+        if (!tabs[k]) return BGF_EINVAL;
+    int nb = h->nblkmem;
+    for (int ibl = 0; ibl < b->nblk; ibl++) {
+        int ib = b->active[ibl];
+        if (ib < 0 || ib >= nb) return BGF_EINVAL;
+        for (int k = 0; k < 8; k++) {
+            int q = tabs[k][ib];
+            if (q < 0 || q >= nb) return BGF_EINVAL;
+        }
+    }
+    h->nblk = b->nblk;
+    h->active.assign(b->active, b->active + b->nblk);
+    h->level.assign(b->level, b->level + nb);
+    h->nbr.assign((size_t)8 * nb, 0);
+    for (int k = 0; k < 8; k++)
+        for (int ib = 0; ib < nb; ib++) h->nbr[(size_t)k * nb + ib] = tabs[k][ib];
+    h->bxo.assign(nb, 0.0);
+    h->byo.assign(nb, 0.0);
+    if (b->xo && b->yo)
+        for (int ib = 0; ib < nb; ib++) {
+            h->bxo[ib] = h->dbl ? ((const double*)b->xo)[ib] : (double)((const float*)b->xo)[ib];
+            h->byo[ib] = h->dbl ? ((const double*)b->yo)[ib] : (double)((const float*)b->yo)[ib];
+        }
+    int rc = upload_tables(h);
+    if (rc) return rc;
     return rebuild_segments(h);
 }
 
@@ -982,5 +1011,243 @@ int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches)
     if (!h) return BGF_EINVAL;
     if (gpu_ms) *gpu_ms = h->last_run_ms;
     if (launches) *launches = h->last_run_launches;
+    return BGF_OK;
+}
+
+// ---------------------------------------------------------------- refinement pass
+
+int bgf_set_bathy(bgf_handle* h, int nx, int ny, double xo, double yo, double dx, const float* val)
+{
+    if (!h || nx < 2 || ny < 2 || !(dx > 0.0) || !val) return BGF_EINVAL;
+    int rc = set_device(h);
+    if (rc) return rc;
+    if (h->d_dem) cudaFree(h->d_dem);
+    h->d_dem = nullptr;
+    BGF_CUDA(cudaMalloc((void**)&h->d_dem, sizeof(float) * (size_t)nx * ny));
+    BGF_CUDA(cudaMemcpy(h->d_dem, val, sizeof(float) * (size_t)nx * ny, cudaMemcpyHostToDevice));
+    h->dem_nx = nx;
+    h->dem_ny = ny;
+    h->dem_xo = xo;
+    h->dem_yo = yo;
+    h->dem_dx = dx;
+    return BGF_OK;
+}
+
+int bgf_get_blocks(bgf_handle* h, int* nblk, int* active, int* level, int* nbr8, double* xo, double* yo)
+{
+    if (!h || !nblk) return BGF_EINVAL;
+    if (!h->has_blocks) return BGF_ESTATE;
+    const int nb = h->nblkmem;
+    *nblk = h->nblk;
+    if (active) memcpy(active, h->active.data(), sizeof(int) * h->nblk);
+    if (level) memcpy(level, h->level.data(), sizeof(int) * nb);
+    if (nbr8)
+        for (int ib = 0; ib < nb; ib++)
+            for (int k = 0; k < 8; k++) nbr8[8 * ib + k] = h->nbr[(size_t)k * nb + ib];
+    if (xo) memcpy(xo, h->bxo.data(), sizeof(double) * nb);
+    if (yo) memcpy(yo, h->byo.data(), sizeof(double) * nb);
+    return BGF_OK;
+}
+
+template <class T> static adapt::AdaptDev<T> adapt_dev(bgf_handle* h)
+{
+    adapt::AdaptDev<T> a;
+    for (int k = 0; k < 4; k++) a.W[k] = (T*)h->d_W[0][k];
+    a.zs = (T*)h->d_dh;  // the flow step's scratch is free between steps
+    a.dem = h->d_dem;
+    a.dnx = h->dem_nx;
+    a.dny = h->dem_ny;
+    a.dxo = h->dem_xo;
+    a.dyo = h->dem_yo;
+    a.ddx = h->dem_dx;
+    a.dxmax = h->dem_xo + (h->dem_nx - 1) * h->dem_dx;
+    a.dymax = h->dem_yo + (h->dem_ny - 1) * h->dem_dx;
+    a.child = h->d_child;
+    a.flags = h->d_flags;
+    return a;
+}
+
+// AdaptCriteria (src/AdaptCriteria.cu:20-130) on the device, then the host sanity
+// pass.  refine/coarsen are indexed by block id (nblkmem bytes each).
+template <class T> static int adapt_flags_t(bgf_handle* h, const bgf_adapt_param* ap, std::vector<uint8_t>& refine,
+                                            std::vector<uint8_t>& coarsen)
+{
+    const int nb = h->nblkmem;
+    DevModel<T> m = dev_model<T>(h);
+    const T* z = nullptr;
+    int stride324 = 0;
+    switch (ap->var) {
+    case BGF_VAR_H: z = (const T*)h->d_h[h->cur]; break;
+    case BGF_VAR_ZS: z = (const T*)h->d_dh; break;
+    case BGF_VAR_U: z = (const T*)h->d_u[h->cur]; break;
+    case BGF_VAR_V: z = (const T*)h->d_v[h->cur]; break;
+    case BGF_VAR_ZB: z = (const T*)h->d_zb; stride324 = 1; break;
+    default: return BGF_EINVAL;
+    }
+    adapt::launch_criteria<T>(m, z, stride324, ap->criterion, (T)ap->arg1, (T)ap->arg2, h->d_flags, h->stream);
+    h->launches++;
+    BGF_CUDA(cudaGetLastError());
+    refine.assign(nb, 0);
+    coarsen.assign(nb, 0);
+    BGF_CUDA(cudaMemcpyAsync(refine.data(), h->d_flags, nb, cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<uint8_t> mask(nb, 0);
+    for (int ibl = 0; ibl < h->nblk; ibl++) mask[h->active[ibl]] = 1;
+    for (int ib = 0; ib < nb; ib++) {
+        refine[ib] = mask[ib] ? refine[ib] : 0;
+        coarsen[ib] = mask[ib] ? !refine[ib] : 0;  // Thresholdcriteria: coarsen = !refine
+    }
+    std::vector<int> nbr8((size_t)8 * nb);
+    for (int ib = 0; ib < nb; ib++)
+        for (int k = 0; k < 8; k++) nbr8[8 * ib + k] = h->nbr[(size_t)k * nb + ib];
+    return bgf_refine_sanity(h->nblk, h->active.data(), h->level.data(), nbr8.data(), nb, h->P.minlevel, h->P.maxlevel,
+                             refine.data(), coarsen.data());
+}
+
+static int check_adapt_param(const bgf_adapt_param* ap)
+{
+    if (!ap) return BGF_EINVAL;
+    if (ap->criterion != BGF_ADAPT_THRESHOLD && ap->criterion != BGF_ADAPT_INRANGE) return BGF_EINVAL;
+    if (ap->var < BGF_VAR_H || ap->var > BGF_VAR_ZB) return BGF_EINVAL;
+    return BGF_OK;
+}
+
+template <class T> static void zs_from_state(bgf_handle* h)
+{
+    adapt::launch_zs<T>(dev_model<T>(h), (T*)h->d_dh, h->cur, h->stream);
+    h->launches++;
+}
+
+int bgf_adapt_flags(bgf_handle* h, const bgf_adapt_param* ap, uint8_t* refine, uint8_t* coarsen)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if ((rc = check_adapt_param(ap))) return rc;
+    std::vector<uint8_t> r, c;
+    if (h->dbl) {
+        zs_from_state<double>(h);
+        rc = adapt_flags_t<double>(h, ap, r, c);
+    } else {
+        zs_from_state<float>(h);
+        rc = adapt_flags_t<float>(h, ap, r, c);
+    }
+    if (rc) return rc;
+    for (int ibl = 0; ibl < h->nblk; ibl++) {
+        if (refine) refine[ibl] = r[h->active[ibl]];
+        if (coarsen) coarsen[ibl] = c[h->active[ibl]];
+    }
+    return BGF_OK;
+}
+
+// Adaptation (src/Adaptation.cu:17-121): repeats {criteria, sanity pass, refine,
+// bed re-interpolation, wet/dry fix-up} until the block count stops changing or
+// maxiteration passes ran, then prepares the bed halo and gradients of the new
+// mesh and carries the boundary segments over to the children of refined blocks.
+template <class T> static int adapt_t(bgf_handle* h, const bgf_adapt_param* ap, int* niter)
+{
+    const int nb = h->nblkmem;
+    int rc = alloc_amr(h);  // stage tiles double as the old-mesh halo tiles
+    if (rc) return rc;
+    zs_from_state<T>(h);
+    const int maxit = ap->maxiteration > 0 ? ap->maxiteration : 20;
+    int it = 0;
+    bool changed_any = false;
+    while (it < maxit) {
+        it++;
+        const int oldn = h->nblk;
+        std::vector<uint8_t> refine, coarsen;
+        if ((rc = adapt_flags_t<T>(h, ap, refine, coarsen))) return rc;
+        std::vector<int> act(nb, -1), lev = h->level, nbr8((size_t)8 * nb), child((size_t)3 * nb, -1);
+        std::copy(h->active.begin(), h->active.end(), act.begin());
+        for (int ib = 0; ib < nb; ib++)
+            for (int k = 0; k < 8; k++) nbr8[8 * ib + k] = h->nbr[(size_t)k * nb + ib];
+        std::vector<double> xo = h->bxo, yo = h->byo;
+        int n = h->nblk;
+        rc = bgf_refine_tables(&n, act.data(), lev.data(), nbr8.data(), xo.data(), yo.data(), nb, h->P.dx, h->dbl,
+                               refine.data(), child.data());
+        if (rc) {
+            if (rc == BGF_ENOMEM) g_last_error = "refinement needs more block slots than nblkmem";
+            return rc;
+        }
+        adapt::AdaptDev<T> a = adapt_dev<T>(h);
+        DevModel<T> m = dev_model<T>(h);
+        if (n != oldn) {
+            // children from the old mesh (old tables still on the device)
+            BGF_CUDA(cudaMemcpyAsync(h->d_child, child.data(), sizeof(int) * 3 * nb, cudaMemcpyHostToDevice, h->stream));
+            adapt::launch_children<T>(m, a, h->cur, h->has_cf ? (T*)h->d_cf : nullptr,
+                                      h->has_rainmask ? h->d_rainmask : nullptr, h->stream);
+            h->launches += 4;
+            BGF_CUDA(cudaGetLastError());
+            // segments: the children on a listed side inherit it
+            const int kids_side[4][2] = {{0, 2}, {1, 3}, {2, 3}, {0, 1}};  // left, right, top, bot: child slots
+            for (HostSeg& sg : h->segs)
+                for (int sidx = 0; sidx < 4; sidx++) {
+                    std::vector<int> out;
+                    for (int ib : sg.blk[sidx]) {
+                        if (ib >= 0 && ib < nb && child[3 * ib] >= 0) {
+                            const int kids[4] = {ib, child[3 * ib], child[3 * ib + 1], child[3 * ib + 2]};
+                            out.push_back(kids[kids_side[sidx][0]]);
+                            out.push_back(kids[kids_side[sidx][1]]);
+                        } else {
+                            out.push_back(ib);
+                        }
+                    }
+                    sg.blk[sidx] = out;
+                }
+            changed_any = true;
+        }
+        h->nblk = n;
+        h->active.assign(act.begin(), act.begin() + n);
+        h->level = lev;
+        for (int ib = 0; ib < nb; ib++)
+            for (int k = 0; k < 8; k++) h->nbr[(size_t)k * nb + ib] = nbr8[8 * ib + k];
+        h->bxo = xo;
+        h->byo = yo;
+        if ((rc = upload_tables(h))) return rc;
+        m = dev_model<T>(h);
+        adapt::launch_bed<T>(m, a, step_params<T>(h), h->cur, (T*)h->d_zb, std::isnan(h->P.xo) ? 0.0 : h->P.xo,
+                             std::isnan(h->P.yo) ? 0.0 : h->P.yo, h->d_bxo, h->d_byo, h->P.mask,
+                             h->has_rainmask ? h->d_rainmask : nullptr, h->stream);
+        h->launches++;
+        BGF_CUDA(cudaGetLastError());
+        if (n == oldn) break;
+    }
+    // bed halo and gradients of the new mesh
+    BGF_CUDA(cudaMemsetAsync(h->d_dzbdx, 0, (size_t)nb * 324 * sizeof(T), h->stream));
+    BGF_CUDA(cudaMemsetAsync(h->d_dzbdy, 0, (size_t)nb * 324 * sizeof(T), h->stream));
+    DevModel<T> m = dev_model<T>(h);
+    int nl = h->fast ? fa::launch_bed_init<T>(m, step_params<T>(h), (T*)h->d_zb, (T*)h->d_dzbdx, (T*)h->d_dzbdy, h->stream)
+                     : ex::launch_bed_init<T>(m, step_params<T>(h), (T*)h->d_zb, (T*)h->d_dzbdx, (T*)h->d_dzbdy, h->stream);
+    h->launches += nl;
+    BGF_CUDA(cudaGetLastError());
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if (changed_any && (rc = rebuild_segments(h))) return rc;
+    free_graphs(h);
+    if (niter) *niter = it;
+    return BGF_OK;
+}
+
+int bgf_adapt(bgf_handle* h, const bgf_adapt_param* ap, int* nblk, int* niter)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if ((rc = check_adapt_param(ap))) return rc;
+    if (!h->d_dem) {
+        g_last_error = "bgf_adapt needs the bathymetry grid (bgf_set_bathy)";
+        return BGF_ESTATE;
+    }
+    rc = h->dbl ? adapt_t<double>(h, ap, niter) : adapt_t<float>(h, ap, niter);
+    if (nblk) *nblk = h->nblk;
+    return rc;
+}
+
+int bgf_get_bed(bgf_handle* h, void* zb)
+{
+    if (!h || !zb) return BGF_EINVAL;
+    if (!h->has_bed) return BGF_ESTATE;
+    int rc = set_device(h);
+    if (rc) return rc;
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    BGF_CUDA(cudaMemcpy(zb, h->d_zb, (size_t)h->nblkmem * 324 * h->esz, cudaMemcpyDeviceToHost));
     return BGF_OK;
 }

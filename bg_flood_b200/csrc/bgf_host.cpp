@@ -10,7 +10,7 @@
 
 
 extern "C" int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* present, int* nblk, int* level,
-                                int* nbr8, double* xo, double* yo)
+                                int* nbr8, double* xo, double* yo, int doubleprecision)
 {
     if (nbx <= 0 || nby <= 0 || !nblk || !level || !nbr8) return BGF_EINVAL;
     // InitBlockxoyo (src/Mesh.cu:257-347): row-major candidate blocks, masked ones skipped.
@@ -22,8 +22,15 @@ extern "C" int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* p
             if (present && !present[k]) continue;
             id[k] = n;
             level[n] = 0;
-            if (xo) xo[n] = bx * 16.0 * levdx + 0.5 * levdx;
-            if (yo) yo[n] = by * 16.0 * levdx + 0.5 * levdx;
+            // nblkx * blkwidth * levdx + levdx / 2, evaluated in the state precision
+            if (doubleprecision) {
+                if (xo) xo[n] = bx * 16.0 * levdx + 0.5 * levdx;
+                if (yo) yo[n] = by * 16.0 * levdx + 0.5 * levdx;
+            } else {
+                const float l = (float)levdx;
+                if (xo) xo[n] = (double)(bx * 16.0f * l + 0.5f * l);
+                if (yo) yo[n] = (double)(by * 16.0f * l + 0.5f * l);
+            }
             n++;
         }
     // InitBlockneighbours (src/Mesh.cu:351-433): neighbours by position, self at edges.

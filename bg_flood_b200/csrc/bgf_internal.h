@@ -39,6 +39,19 @@ namespace fast {
 BGF_DECLARE_LAUNCHERS
 }
 
+// Refinement-pass kernels (bgf_adapt.cu), built once without FMA contraction.
+namespace adapt {
+template <class T> struct AdaptDev;
+template <class T> void launch_criteria(const DevModel<T>& m, const T* z, int stride324, int kind, T a1, T a2,
+                                        uint8_t* flags, cudaStream_t st);
+template <class T> void launch_zs(const DevModel<T>& m, T* zs, int cur, cudaStream_t st);
+template <class T> void launch_children(const DevModel<T>& m, const AdaptDev<T>& a, int cur, T* cf, uint8_t* rainmask,
+                                        cudaStream_t st);
+template <class T> void launch_bed(const DevModel<T>& m, const AdaptDev<T>& a, const StepParams<T>& p, int cur, T* zb,
+                                   double xo0, double yo0, const double* bxo, const double* byo, double mask,
+                                   uint8_t* rainmask, cudaStream_t st);
+}  // namespace adapt
+
 // Records the text returned by bgf_last_error() for this thread.
 void set_last_error(const std::string& msg);
 

@@ -41,6 +41,11 @@ class CBlockP(ctypes.Structure):
                                         "RightBot", "RightTop", "xo", "yo")]
 
 
+class CAdaptParam(ctypes.Structure):
+    _fields_ = [("criterion", ctypes.c_int), ("var", ctypes.c_int), ("arg1", ctypes.c_double),
+                ("arg2", ctypes.c_double), ("maxiteration", ctypes.c_int)]
+
+
 class CEvolving(ctypes.Structure):
     _fields_ = [("zs", ctypes.c_void_p), ("h", ctypes.c_void_p), ("u", ctypes.c_void_p), ("v", ctypes.c_void_p)]
 
@@ -153,6 +158,52 @@ class FlowB200:
         _check(lib().bgf_get_state(self.handle, ctypes.byref(ev)), "bgf_get_state")
         return tuple(out)
 
+    def get_bed(self) -> np.ndarray:
+        """zb on (nblkmem, 18, 18) tiles, halo included."""
+        out = np.zeros((self.nblkmem, 18, 18), self.dtype)
+        _check(lib().bgf_get_bed(self.handle, _ptr(out)), "bgf_get_bed")
+        return out
+
+    # -- refinement pass ---------------------------------------------------------------
+    def set_bathy(self, xo: float, yo: float, dx: float, grid: np.ndarray) -> None:
+        """Bathymetry grid (ny, nx) of nodes from (xo, yo) with spacing dx."""
+        g = np.ascontiguousarray(grid, np.float32)
+        ny, nx = g.shape
+        _check(lib().bgf_set_bathy(self.handle, nx, ny, float(xo), float(yo), float(dx), _ptr(g)), "bgf_set_bathy")
+
+    def _adapt_param(self, crit, maxiteration: int):
+        from .adapt import VARS
+        return CAdaptParam(crit.kind, VARS[crit.var], float(crit.arg1), float(crit.arg2), int(maxiteration))
+
+    def adapt_flags(self, crit):
+        """(refine, coarsen) per active block of one criterion + sanity pass."""
+        n = ctypes.c_int(0)
+        _check(lib().bgf_get_blocks(self.handle, ctypes.byref(n), None, None, None, None, None), "bgf_get_blocks")
+        r = np.zeros(n.value, np.uint8)
+        c = np.zeros(n.value, np.uint8)
+        p = self._adapt_param(crit, 1)
+        _check(lib().bgf_adapt_flags(self.handle, ctypes.byref(p), _ptr(r), _ptr(c)), "bgf_adapt_flags")
+        return r, c
+
+    def adapt(self, crit, maxiteration: int = 20):
+        """Adaptation of the mesh and state; returns (nblk, passes)."""
+        p = self._adapt_param(crit, maxiteration)
+        n, it = ctypes.c_int(0), ctypes.c_int(0)
+        _check(lib().bgf_adapt(self.handle, ctypes.byref(p), ctypes.byref(n), ctypes.byref(it)), "bgf_adapt")
+        return n.value, it.value
+
+    def get_blocks(self):
+        """(active, level, nbr (nblkmem, 8), xo, yo) host copies of the tables."""
+        n = ctypes.c_int(0)
+        act = np.zeros(self.nblkmem, np.int32)
+        lev = np.zeros(self.nblkmem, np.int32)
+        nb = np.zeros((self.nblkmem, 8), np.int32)
+        xo = np.zeros(self.nblkmem)
+        yo = np.zeros(self.nblkmem)
+        _check(lib().bgf_get_blocks(self.handle, ctypes.byref(n), _ptr(act), _ptr(lev), _ptr(nb), _ptr(xo), _ptr(yo)),
+               "bgf_get_blocks")
+        return act[: n.value], lev, nb, xo, yo
+
     # -- time stepping --------------------------------------------------------------
     def init_dt(self, loop: Loop) -> float:
         c = loop.to_c()
@@ -210,7 +261,7 @@ def build_model(param: Param, zb: np.ndarray, h: np.ndarray, u: np.ndarray | Non
     segments plus the remainder of type ``aoibnd``), optional per-cell cf and a
     uniform rain series (times, mm/h).  Returns (FlowB200, Mesh)."""
     ny, nx = zb.shape
-    mesh = mesh or uniform_mesh(nx, ny, param.dx)
+    mesh = mesh or uniform_mesh(nx, ny, param.dx, doubleprecision=bool(param.doubleprecision))
     dt = np.float64 if param.doubleprecision else np.float32
     f = FlowB200(param, mesh.nblk)
     f.set_blocks(mesh.active, mesh.level, mesh.nbr, mesh.xo, mesh.yo)

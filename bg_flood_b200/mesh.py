@@ -39,7 +39,7 @@ class Mesh:
         return np.arange(self.nblk, dtype=np.int32)
 
 
-def uniform_mesh(nx: int, ny: int, dx: float, present: np.ndarray | None = None) -> Mesh:
+def uniform_mesh(nx: int, ny: int, dx: float, present: np.ndarray | None = None, doubleprecision: bool = False) -> Mesh:
     """Uniform level-0 mesh of nx*ny cells (multiples of 16), as InitBlockxoyo and
     InitBlockneighbours build it (src/Mesh.cu:257-433).  ``present`` (nby, nbx) masks
     out blocks (the reference drops blocks whose cells are all above ``mask``)."""
@@ -59,7 +59,7 @@ def uniform_mesh(nx: int, ny: int, dx: float, present: np.ndarray | None = None)
                                 ctypes.byref(nblk), level.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                                 nbr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                                 xo.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                                yo.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+                                yo.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1 if doubleprecision else 0)
     if rc != 0:
         raise RuntimeError(f"bgf_mesh_uniform failed ({rc})")
     n = nblk.value

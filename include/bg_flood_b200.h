@@ -239,11 +239,55 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* args, bgf_
  * whose present[] entry is 0 are skipped (masked), ids are assigned in order,
  * neighbours are matched by position and default to the block itself at the
  * domain edge.  Outputs are sized nbx*nby; returns the block count in *nblk.
- * xo/yo (double) are the block origins relative to the domain origin. */
+ * xo/yo (double) are the block origins (first cell centre) relative to the
+ * domain origin, evaluated in the state precision as the reference stores them
+ * (float unless doubleprecision). */
 int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* present, int* nblk, int* level,
-                     int* nbr8, double* xo, double* yo);
+                     int* nbr8, double* xo, double* yo, int doubleprecision);
 
 /* ------------------------------------------------------------ refinement pass */
+/* Criterion of the reference's "Adaptation" key (src/AdaptCriteria.cu:20-130):
+ * a block is flagged for refinement when any of its cells has var > arg1
+ * (Threshold) or arg1 <= var <= arg2 (Inrange), compared in the state precision. */
+enum { BGF_ADAPT_THRESHOLD = 1, BGF_ADAPT_INRANGE = 2 };
+enum { BGF_VAR_H = 0, BGF_VAR_ZS = 1, BGF_VAR_U = 2, BGF_VAR_V = 3, BGF_VAR_ZB = 4 };
+typedef struct bgf_adapt_param {
+    int criterion;     /* BGF_ADAPT_THRESHOLD or BGF_ADAPT_INRANGE            */
+    int var;           /* BGF_VAR_*                                          */
+    double arg1, arg2; /* threshold, or zmin and zmax                         */
+    int maxiteration;  /* adaptmaxiteration, 20 when <= 0                     */
+} bgf_adapt_param;
+
+/* Bathymetry forcing (the reference's Forcing.Bathy[0]): nx*ny float nodes,
+ * row-major, node (0, 0) at (xo, yo), spacing dx in x and y.  bgf_adapt
+ * re-interpolates the bed of every block from it, as the reference does
+ * (interp2BUQ + setedges, src/GridManip.cu:222-575). */
+int bgf_set_bathy(bgf_handle* h, int nx, int ny, double xo, double yo, double dx, const float* val);
+
+/* Refine / coarsen flags of one criterion + sanity pass on the current mesh and
+ * state, one byte per active block (active order); the mesh is not changed. */
+int bgf_adapt_flags(bgf_handle* h, const bgf_adapt_param* a, uint8_t* refine, uint8_t* coarsen);
+
+/* Adaptation (src/Adaptation.cu:17-121) of the handle's mesh and state: up to
+ * maxiteration passes of {criterion, sanity pass, refinement with bilinear
+ * interpolation of h, zs, u, v into the children, bed re-interpolation from the
+ * bathymetry grid, wet/dry fix-up}, stopping when a pass adds no block.  The
+ * new blocks take free block slots below nblkmem (BGF_ENOMEM when there are not
+ * enough).  Afterwards the bed halo and gradients are prepared for the new mesh
+ * and every boundary segment lists the children of its refined blocks on the
+ * same side.  Per-cell friction and rain-mask inputs are carried to the children
+ * from the covering parent cell.  Writes the new block count and the number of
+ * passes. */
+int bgf_adapt(bgf_handle* h, const bgf_adapt_param* a, int* nblk, int* niter);
+
+/* Host copies of the current block tables: active (nblk entries), level and
+ * origins per block slot, neighbours as [nblkmem][8] (LB, LT, RB, RT, BL, BR, TL,
+ * TR).  Any output pointer may be NULL. */
+int bgf_get_blocks(bgf_handle* h, int* nblk, int* active, int* level, int* nbr8, double* xo, double* yo);
+/* The bed on 18x18 tiles of every block slot (nblkmem * 324 values of the state
+ * precision), halo included. */
+int bgf_get_bed(bgf_handle* h, void* zb);
+
 /* Host-only table work of the reference's adaptation (no device memory involved).
  * Arrays are indexed by block id and sized nblkmem; nbr8 is [nblkmem][8] in the
  * order LeftBot, LeftTop, RightBot, RightTop, BotLeft, BotRight, TopLeft, TopRight.

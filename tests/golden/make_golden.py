@@ -78,6 +78,21 @@ def main_adapt_tables():
     np.savez_compressed(os.path.join(HERE, "adapt_tables.npz"), **out)
 
 
+def main_adapt_full():
+    """The reference's whole Adaptation() from a uniform level-0 mesh: final tables
+    and interior h, zs, u, v, zb in active order (tests/test_gpu_adapt.py)."""
+    from adapt_cases import ADAPT_CASES, id_tables, reference_with_bathy
+    for name in ("island64_e1_l2", "hump64_e1_l2", "dam64_e1_l3"):
+        case = ADAPT_CASES[name]()
+        r = reference_with_bathy(case)
+        r.adaptation()
+        act, level, nbr, xo, yo = id_tables(r)
+        out = {k: interior(r.get(k)).astype(np.float32) for k in ("h", "zs", "u", "v", "zb")}
+        np.savez_compressed(os.path.join(HERE, f"adapt_{name}.npz"), act=act, level=level[act], nbr=nbr[act],
+                            xo=xo[act], yo=yo[act], **out)
+        print("adapt", name, len(act))
+
+
 def main():
     for name, (mk, nsteps) in GOLDEN_CASES.items():
         case = mk()
@@ -92,3 +107,4 @@ if __name__ == "__main__":
     main()
     main_amr()
     main_adapt_tables()
+    main_adapt_full()

@@ -16,7 +16,7 @@ def interior(a: np.ndarray) -> np.ndarray:
 
 
 def make_oracle(case: Case, use_double: bool = False, mesh=None):
-    mesh = mesh or uniform_mesh(case.nx, case.ny, case.dx)
+    mesh = mesh or uniform_mesh(case.nx, case.ny, case.dx, doubleprecision=use_double)
     o = Oracle(case.param, mesh.nblk, use_double)
     o.set_blocks(mesh.level, mesh.nbr, mesh.xo, mesh.yo)
     o.set("zb", grid_to_buq(case.zb, mesh))

@@ -54,7 +54,7 @@ def test_invalid_arguments_are_rejected():
     l = lib()
     h = ctypes.c_void_p()
     assert l.bgf_create(None, 4, None, ctypes.byref(h)) == 1
-    assert l.bgf_mesh_uniform(0, 3, 1.0, None, None, None, None, None, None) == 1
+    assert l.bgf_mesh_uniform(0, 3, 1.0, None, None, None, None, None, None, 0) == 1
 
 
 def test_uniform_mesh_tables():

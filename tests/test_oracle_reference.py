@@ -31,7 +31,8 @@ def test_oracle_matches_reference_bitwise(have_reference, mk, nsteps):
     # neighbour tables and levels of the product mesh builder == the reference InitMesh
     assert np.array_equal(lev, mesh.level)
     assert np.array_equal(nbr, mesh.nbr)
-    assert np.allclose(xo, mesh.xo.astype(np.float32)) and np.allclose(yo, mesh.yo.astype(np.float32))
+    assert np.array_equal(xo.astype(np.float32), mesh.xo.astype(np.float32))
+    assert np.array_equal(yo.astype(np.float32), mesh.yo.astype(np.float32))
     # bed, bed halo and bed gradients (corner halo cells are never written by either)
     # (x-gradients exist on the interior and the left/right halo columns, y-gradients
     # on the interior and the bottom/top halo rows; the other halo cells are never written)

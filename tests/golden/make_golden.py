@@ -91,6 +91,17 @@ def main_adapt_full():
         np.savez_compressed(os.path.join(HERE, f"adapt_{name}.npz"), act=act, level=level[act], nbr=nbr[act],
                             xo=xo[act], yo=yo[act], **out)
         print("adapt", name, len(act))
+    # adaptation in the middle of a run: 20 flow steps first, so u and v are not zero
+    for name in ("hump64_e1_l2", "island64_e1_l2"):
+        case = ADAPT_CASES[name]()
+        r = reference_with_bathy(case)
+        r.step(20)
+        r.adaptation()
+        act, level, nbr, xo, yo = id_tables(r)
+        out = {k: interior(r.get(k)).astype(np.float32) for k in ("h", "zs", "u", "v", "zb")}
+        np.savez_compressed(os.path.join(HERE, f"adapt_{name}_t20.npz"), act=act, level=level[act], nbr=nbr[act],
+                            xo=xo[act], yo=yo[act], **out)
+        print("adapt after 20 steps", name, len(act))
 
 
 def main():

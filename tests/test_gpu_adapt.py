@@ -19,7 +19,7 @@ from runners import interior
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.dirname(os.path.abspath(__file__)) + "/golden"
-UV_TOL = 1e-6  # m/s (velocities start at zero in these cases)
+UV_TOL = 1e-5  # m/s
 
 
 def _pad(a, n):
@@ -28,7 +28,7 @@ def _pad(a, n):
     return out
 
 
-def adapted_model(name):
+def adapted_model(name, steps=0):
     case = ADAPT_CASES[name]()
     zb0, h0 = level0_grids(case)
     mesh = uniform_mesh(case.n0, case.n0, case.dx)
@@ -40,16 +40,24 @@ def adapted_model(name):
     z = np.zeros_like(h0)
     f.set_state(*(_pad(grid_to_buq(a, mesh), MEM) for a in (h0, z, z)))
     f.set_bathy(case.xo + 0.5 * case.dx, case.yo + 0.5 * case.dx, case.dx, zb0)
+    if steps:
+        loop = Loop(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=case.nextoutputtime)
+        f.init_dt(loop)
+        for _ in range(steps):
+            loop.totaltime += f.flow_step(loop)
     n, it = f.adapt(criterion_of(case))
     return case, f, n, it
 
 
-@pytest.mark.parametrize("name", ["island64_e1_l2", "hump64_e1_l2", "dam64_e1_l3"])
-def test_adaptation_matches_reference(name):
-    g = np.load(os.path.join(GOLDEN, f"adapt_{name}.npz"))
-    case, f, n, it = adapted_model(name)
+@pytest.mark.parametrize("name,steps", [("island64_e1_l2", 0), ("hump64_e1_l2", 0), ("dam64_e1_l3", 0),
+                                        ("hump64_e1_l2", 20), ("island64_e1_l2", 20)])
+def test_adaptation_matches_reference(name, steps):
+    """steps > 0: adaptation in the middle of a run (the flow steps before it are
+    bit-exact with the reference, so both adapt the same state)."""
+    g = np.load(os.path.join(GOLDEN, f"adapt_{name}{'_t%d' % steps if steps else ''}.npz"))
+    case, f, n, it = adapted_model(name, steps)
     act, lev, nb, xo, yo = f.get_blocks()
-    assert n == len(g["act"]) and it >= 2
+    assert n == len(g["act"]) and it >= 1
     assert np.array_equal(act, g["act"])
     assert np.array_equal(lev[act], g["level"])
     assert np.array_equal(nb[act], g["nbr"])

@@ -50,6 +50,17 @@ SIGNATURES = {
     "bgf_adapt": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_int_p]),
     "bgf_get_blocks": (ctypes.c_int, [c_void_p, c_int_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "bgf_get_bed": (ctypes.c_int, [c_void_p, c_void_p]),
+    "bgf_pool_create": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p,
+                                       ctypes.POINTER(c_void_p)]),
+    "bgf_pool_destroy": (ctypes.c_int, [c_void_p]),
+    "bgf_pool_admit": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                      c_int_p]),
+    "bgf_pool_retire": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_int_p]),
+    "bgf_pool_run": (ctypes.c_int, [c_void_p, ctypes.c_int, c_int_p]),
+    "bgf_pool_query": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_int_p, ctypes.POINTER(ctypes.c_int64)]),
+    "bgf_pool_get_depth": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p]),
+    "bgf_pool_timing": (ctypes.c_int, [c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64), c_int_p]),
+    "bgf_pool_set_grid": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "bgf_refine_sanity": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_int_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, c_void_p, c_void_p]),
     "bgf_refine_tables": (ctypes.c_int, [c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, ctypes.c_int,

@@ -86,6 +86,7 @@ struct bgf_handle {
     bool amr = false;
     int minlev = 0, maxlev = 0;
     int steps_launches = 2;  // kernel launches per step
+    int grid = 0;            // CTAs of the fused kernels (0: one per block)
     void* d_W[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
     void* d_G0[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     void* d_F[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -133,6 +134,10 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.time = h->d_time;
     m.dtmin = h->d_dtmin;
     m.err = h->d_err;
+    m.scen = nullptr;
+    m.sparams = nullptr;
+    m.lead = nullptr;
+    m.hmax = nullptr;
     return m;
 }
 
@@ -182,6 +187,7 @@ template <class T> static StepParams<T> step_params(const bgf_handle* h)
     p.has_rain = h->rain_n_dev > 0 ? 1 : 0;
     p.nseg = h->nseg_dev;
     p.rain_n = h->rain_n_dev;
+    p.rain_off = 0;
     return p;
 }
 
@@ -649,6 +655,8 @@ int bgf_set_rain_series(bgf_handle* h, int n, const double* t, const double* r)
     if (h->d_rain_t) { cudaFree(h->d_rain_t); h->d_rain_t = nullptr; }
     if (h->d_rain_r) { cudaFree(h->d_rain_r); h->d_rain_r = nullptr; }
     h->rain_n_dev = n;
+    h->rain_t.assign(t, t + n);
+    h->rain_r.assign(r, r + n);
     if (n > 0) {
         BGF_CUDA(cudaMalloc((void**)&h->d_rain_t, n * sizeof(double)));
         BGF_CUDA(cudaMalloc((void**)&h->d_rain_r, n * sizeof(double)));
@@ -799,8 +807,8 @@ template <class T> static int enqueue_flux(bgf_handle* h, int parity)
                                                  0, h->minlev, h->maxlev, h->stream)
                        : ex::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
                                                  0, h->minlev, h->maxlev, h->stream);
-    if (h->fast) fa::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
-    else ex::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
+    if (h->fast) fa::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream, h->grid);
+    else ex::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream, h->grid);
     return 1;
 }
 
@@ -811,8 +819,8 @@ template <class T> static int enqueue_update(bgf_handle* h, int parity)
                                                  1, h->minlev, h->maxlev, h->stream)
                        : ex::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
                                                  1, h->minlev, h->maxlev, h->stream);
-    if (h->fast) fa::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
-    else ex::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream);
+    if (h->fast) fa::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream, h->grid);
+    else ex::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream, h->grid);
     return 1;
 }
 
@@ -1251,3 +1259,7 @@ int bgf_get_bed(bgf_handle* h, void* zb)
     BGF_CUDA(cudaMemcpy(zb, h->d_zb, (size_t)h->nblkmem * 324 * h->esz, cudaMemcpyDeviceToHost));
     return BGF_OK;
 }
+
+// ---------------------------------------------------------------- batched pools
+
+#include "bgf_pool.inc"

@@ -105,119 +105,139 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
 
 // ---------------------------------------------------------------- kernels
 
+// Both kernels walk the active list with a grid-stride loop: a launch of one CTA
+// per block and a persistent launch of a few CTAs per SM give the same result.
+// In a batched pool every block belongs to a scenario with its own parameters,
+// time slot and dt minimum (the segmented CFL reduction).
+
 template <class T, int ENGINE>
-__global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepParams<T> p, int parity)
+__global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
-    const TimeState ts = m.time[parity];
-    if (!step_live(ts)) return;
     const int tid = threadIdx.x;
-    const int ib = m.active[blockIdx.x];
-    const T delta = calcres<T>(p.delta0, m.level[ib]);
-    const int cur = ts.cur;
+    for (int w = blockIdx.x; w < m.nblk; w += gridDim.x) {
+        const int ib = m.active[w];
+        const int sc = scen_of(m, ib);
+        const TimeState ts = m.time[2 * sc + parity];
+        if (!step_live(ts)) continue;
+        const StepParams<T> p = params_of(m, p0, sc);
+        const T delta = calcres<T>(p.delta0, m.level[ib]);
+        const int cur = ts.cur;
 
-    load_bed<T, ENGINE>(s, m, ib, tid);
-    __syncthreads();
-    load_state_tile<T>(s, m, ib, cur, tid);
-    __syncthreads();
-    T celldt = tile_fluxes<T, ENGINE>(s, p, delta, tid);
-    __syncthreads();
-    // CFL minimum: the interior dtmax values reduced with the warp shuffle, then one
-    // atomic per block on the float bit pattern (dt > 0, so integer order == float order).
-    T v = celldt;
-    for (int o = 16; o > 0; o >>= 1) {
-        T w = __shfl_xor_sync(0xffffffffu, v, o);
-        v = w < v ? w : v;
+        load_bed<T, ENGINE>(s, m, ib, tid);
+        __syncthreads();
+        load_state_tile<T>(s, m, ib, cur, tid);
+        __syncthreads();
+        T celldt = tile_fluxes<T, ENGINE>(s, p, delta, tid);
+        __syncthreads();
+        // CFL minimum: the interior dtmax values reduced with the warp shuffle, then one
+        // atomic per block on the float bit pattern (dt > 0, so integer order == float order).
+        T v = celldt;
+        for (int o = 16; o > 0; o >>= 1) {
+            T q = __shfl_xor_sync(0xffffffffu, v, o);
+            v = q < v ? q : v;
+        }
+        if ((tid & 31) == 0) s.red[tid >> 5] = v;
+        // Boundary segments (FlowbndFlux) after the dt, at t + dt_prev/2 as FlowCPU does.
+        apply_boundaries<T>(s, m, p, ib, ts.totaltime + ts.dt * 0.5, tid);
+        __syncthreads();
+        if (tid == 0) {
+            T b = s.red[0];
+            for (int k = 1; k < NTHREADS / 32; k++) b = s.red[k] < b ? s.red[k] : b;
+            atomicMin(&m.dtmin[2 * sc + parity], dt_bits(b));
+        }
+        const int x = tid & 15, y = tid >> 4;
+        const int c = ti(x, y);
+        T dh, dhu, dhv;
+        flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, s.t[VH][c], s.t[VU][c], s.t[VV][c], dh, dhu, dhv);
+        size_t g = (size_t)ib * 256 + tid;
+        m.dh[g] = dh;
+        m.dhu[g] = dhu;
+        m.dhv[g] = dhv;
+        __syncthreads();  // the tile is reused by the next block
     }
-    if ((tid & 31) == 0) s.red[tid >> 5] = v;
-    // Boundary segments (FlowbndFlux) after the dt, at t + dt_prev/2 as FlowCPU does.
-    apply_boundaries<T>(s, m, p, ib, ts.totaltime + ts.dt * 0.5, tid);
-    __syncthreads();
-    if (tid == 0) {
-        T b = s.red[0];
-        for (int k = 1; k < NTHREADS / 32; k++) b = s.red[k] < b ? s.red[k] : b;
-        atomicMin(&m.dtmin[parity], dt_bits(b));
-    }
-    const int x = tid & 15, y = tid >> 4;
-    const int c = ti(x, y);
-    T dh, dhu, dhv;
-    flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, s.t[VH][c], s.t[VU][c], s.t[VV][c], dh, dhu, dhv);
-    size_t g = (size_t)ib * 256 + tid;
-    m.dh[g] = dh;
-    m.dhu[g] = dhu;
-    m.dhv[g] = dhv;
 }
 
 template <class T, int ENGINE>
-__global__ void __launch_bounds__(NTHREADS, 4) update_kernel(DevModel<T> m, StepParams<T> p, int parity)
+__global__ void __launch_bounds__(NTHREADS, 4) update_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
-    const TimeState ts = m.time[parity];
     const int tid = threadIdx.x;
-    if (!step_live(ts)) {
-        if (blockIdx.x == 0 && tid == 0) {
-            TimeState nt = ts;
-            nt.done = 1;
-            m.time[parity ^ 1] = nt;
+    for (int w = blockIdx.x; w < m.nblk; w += gridDim.x) {
+        const int ib = m.active[w];
+        const int sc = scen_of(m, ib);
+        const TimeState ts = m.time[2 * sc + parity];
+        const bool lead = lead_of(m, ib, w);
+        if (!step_live(ts)) {
+            if (lead && tid == 0) {
+                TimeState nt = ts;
+                nt.done = 1;
+                m.time[2 * sc + (parity ^ 1)] = nt;
+            }
+            continue;
         }
-        return;
-    }
-    const int ib = m.active[blockIdx.x];
-    const T delta = calcres<T>(p.delta0, m.level[ib]);
-    const int cur = ts.cur;
-    const T dt = step_dt<T>(ts, m.dtmin[parity]);
-    const double dtd = (double)dt;
+        const StepParams<T> p = params_of(m, p0, sc);
+        const T delta = calcres<T>(p.delta0, m.level[ib]);
+        const int cur = ts.cur;
+        const T dt = step_dt<T>(ts, m.dtmin[2 * sc + parity]);
+        const double dtd = (double)dt;
 
-    load_bed<T, ENGINE>(s, m, ib, tid);
-    __syncthreads();
-    load_half_tile<T>(s, m, p, ib, cur, dt * (T)0.5, tid);
-    __syncthreads();
-    (void)tile_fluxes<T, ENGINE>(s, p, delta, tid);
-    __syncthreads();
-    apply_boundaries<T>(s, m, p, ib, ts.totaltime + dtd, tid);
-    __syncthreads();
-    const int x = tid & 15, y = tid >> 4;
-    const int c = ti(x, y);
-    T dh, dhu, dhv;
-    flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, s.t[VH][c], s.t[VU][c], s.t[VV][c], dh, dhu, dhv);
-    // full step from state n (AdvkernelCPU with evolv), then friction on the result
-    const int c18 = hi18(x, y);
-    T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];
-    T ho, uo, vo;
-    advance<T>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
-    size_t g = (size_t)ib * 256 + tid;
-    T cfv = p.has_cf ? m.cf[g] : p.cf;
-    bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);
-    if (p.has_rain) {
-        // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): uniform rain rate
-        // interpolated at the start of the step (updateforcing)
-        double rnow = series_at(m.rain_t, m.rain_r, p.rain_n, ts.totaltime);
-        T Rainhh = (T)rnow;
-        T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
-        Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
-        T hi = ho;
-        T qvol = hi / (hi + Rainhh);
-        ho = hi + Rainhh;
-        if ((double)hi > p.eps_d) {
-            uo = uo * qvol;
-            vo = vo * qvol;
+        load_bed<T, ENGINE>(s, m, ib, tid);
+        __syncthreads();
+        load_half_tile<T>(s, m, p, ib, cur, dt * (T)0.5, tid);
+        __syncthreads();
+        (void)tile_fluxes<T, ENGINE>(s, p, delta, tid);
+        __syncthreads();
+        apply_boundaries<T>(s, m, p, ib, ts.totaltime + dtd, tid);
+        __syncthreads();
+        const int x = tid & 15, y = tid >> 4;
+        const int c = ti(x, y);
+        T dh, dhu, dhv;
+        flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, s.t[VH][c], s.t[VU][c], s.t[VV][c], dh, dhu, dhv);
+        // full step from state n (AdvkernelCPU with evolv), then friction on the result
+        const int c18 = hi18(x, y);
+        T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];
+        T ho, uo, vo;
+        advance<T>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+        size_t g = (size_t)ib * 256 + tid;
+        T cfv = p.has_cf ? m.cf[g] : p.cf;
+        bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);
+        if (p.has_rain) {
+            // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): uniform rain rate
+            // interpolated at the start of the step (updateforcing)
+            double rnow = series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime);
+            T Rainhh = (T)rnow;
+            T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
+            Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
+            T hi = ho;
+            T qvol = hi / (hi + Rainhh);
+            ho = hi + Rainhh;
+            if ((double)hi > p.eps_d) {
+                uo = uo * qvol;
+                vo = vo * qvol;
+            }
         }
+        const int nxt = cur ^ 1;
+        m.h[nxt][g] = ho;
+        m.u[nxt][g] = uo;
+        m.v[nxt][g] = vo;
+        if (m.hmax) m.hmax[g] = ho > m.hmax[g] ? ho : m.hmax[g];
+        if (lead && tid == 0)
+            m.time[2 * sc + (parity ^ 1)] = next_time_state<T>(ts, p, dtd, nxt, m.dtmin + 2 * sc, parity);
+        __syncthreads();  // the tile is reused by the next block
     }
-    const int nxt = cur ^ 1;
-    m.h[nxt][g] = ho;
-    m.u[nxt][g] = uo;
-    m.v[nxt][g] = vo;
-    if (blockIdx.x == 0 && tid == 0) m.time[parity ^ 1] = next_time_state<T>(ts, p, dtd, nxt, m.dtmin, parity);
 }
 
 // initdt (src/Mainloop.cu:515-554): CalcInitdtCPU per cell, block minimum, atomic.
-template <class T> __global__ void initdt_kernel(DevModel<T> m, StepParams<T> p, int cur, unsigned long long* out)
+template <class T> __global__ void initdt_kernel(DevModel<T> m, StepParams<T> p0, int cur, unsigned long long* out)
 {
     __shared__ T red[NTHREADS / 32];
     const int tid = threadIdx.x;
     const int ib = m.active[blockIdx.x];
+    const int sc = scen_of(m, ib);
+    const StepParams<T> p = params_of(m, p0, sc);
     const T delta = calcres<T>(p.delta0, m.level[ib]);
     T hv = m.h[cur][(size_t)ib * 256 + tid];
     T epsT = (T)p.eps_d;
@@ -232,7 +252,7 @@ template <class T> __global__ void initdt_kernel(DevModel<T> m, StepParams<T> p,
     if (tid == 0) {
         T b = red[0];
         for (int k = 1; k < NTHREADS / 32; k++) b = red[k] < b ? red[k] : b;
-        atomicMin(out, dt_bits(b));
+        atomicMin(out + sc, dt_bits(b));
     }
 }
 
@@ -242,6 +262,7 @@ template <class T> __global__ void volume_kernel(DevModel<T> m, T delta0, int cu
     __shared__ double red[NTHREADS / 32];
     const int tid = threadIdx.x;
     const int ib = m.active[blockIdx.x];
+    const int sc = scen_of(m, ib);
     double d = (double)calcres<T>(delta0, m.level[ib]);
     double v = (double)m.h[cur][(size_t)ib * 256 + tid] * d * d;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -250,7 +271,7 @@ template <class T> __global__ void volume_kernel(DevModel<T> m, T delta0, int cu
     if (tid == 0) {
         double b = 0;
         for (int k = 0; k < NTHREADS / 32; k++) b += red[k];
-        atomicAdd(out, b);
+        atomicAdd(out + sc, b);
     }
 }
 
@@ -274,18 +295,21 @@ template <class T> cudaError_t configure_kernels()
     return configure_engine<T, 2>();
 }
 
+// grid: CTAs of the launch (0: one per active block); fewer CTAs loop over the blocks
 template <class T>
-void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st)
+void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st, int grid)
 {
-    if (engine == 1) flux_kernel<T, 1><<<m.nblk, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
-    else flux_kernel<T, 2><<<m.nblk, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+    const int g = grid > 0 && grid < m.nblk ? grid : m.nblk;
+    if (engine == 1) flux_kernel<T, 1><<<g, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+    else flux_kernel<T, 2><<<g, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
 }
 
 template <class T>
-void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st)
+void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st, int grid)
 {
-    if (engine == 1) update_kernel<T, 1><<<m.nblk, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
-    else update_kernel<T, 2><<<m.nblk, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+    const int g = grid > 0 && grid < m.nblk ? grid : m.nblk;
+    if (engine == 1) update_kernel<T, 1><<<g, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+    else update_kernel<T, 2><<<g, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
 }
 
 template <class T>
@@ -301,10 +325,10 @@ template <class T> void launch_volume(const DevModel<T>& m, T delta0, int cur, d
 
 template cudaError_t configure_kernels<float>();
 template cudaError_t configure_kernels<double>();
-template void launch_flux<float>(const DevModel<float>&, const StepParams<float>&, int, int, cudaStream_t);
-template void launch_flux<double>(const DevModel<double>&, const StepParams<double>&, int, int, cudaStream_t);
-template void launch_update<float>(const DevModel<float>&, const StepParams<float>&, int, int, cudaStream_t);
-template void launch_update<double>(const DevModel<double>&, const StepParams<double>&, int, int, cudaStream_t);
+template void launch_flux<float>(const DevModel<float>&, const StepParams<float>&, int, int, cudaStream_t, int);
+template void launch_flux<double>(const DevModel<double>&, const StepParams<double>&, int, int, cudaStream_t, int);
+template void launch_update<float>(const DevModel<float>&, const StepParams<float>&, int, int, cudaStream_t, int);
+template void launch_update<double>(const DevModel<double>&, const StepParams<double>&, int, int, cudaStream_t, int);
 template void launch_initdt<float>(const DevModel<float>&, const StepParams<float>&, int, unsigned long long*, cudaStream_t);
 template void launch_initdt<double>(const DevModel<double>&, const StepParams<double>&, int, unsigned long long*, cudaStream_t);
 template void launch_volume<float>(const DevModel<float>&, float, int, double*, cudaStream_t);

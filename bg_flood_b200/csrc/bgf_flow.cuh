@@ -60,7 +60,7 @@ template <class T> struct StepParams {
     double eps_d, dtparam, bndfiltertime, bndrelaxtime, bndtaper, inittime, zsinit, zsoffset, dtmin;
     double delta0_d;  // level-0 spacing in double (refine_linear left/top offsets)
     T cf;        // uniform friction coefficient
-    int frictionmodel, forcemass, has_cf, has_rain, nseg, rain_n;
+    int frictionmodel, forcemass, has_cf, has_rain, nseg, rain_n, rain_off;
 };
 
 template <class T> struct DevModel {
@@ -86,9 +86,14 @@ template <class T> struct DevModel {
     T* dh;
     T* dhu;
     T* dhv;
-    TimeState* time;       // [2]
-    unsigned long long* dtmin;  // [2] bit patterns of the running minimum (dt > 0: integer order)
+    TimeState* time;       // [nscen][2]
+    unsigned long long* dtmin;  // [nscen][2] bit patterns of the running minimum (dt > 0: integer order)
     int* err;              // device error word (0 ok)
+    // batched pools (all null for a single scenario)
+    const int* scen;                  // per block slot: scenario index
+    const StepParams<T>* sparams;     // per scenario
+    const uint8_t* lead;              // per block slot: 1 for the first block of its scenario
+    T* hmax;                          // per cell (256 per block): running maximum depth, or null
 };
 
 // Positive floating-point values order like their bit patterns.

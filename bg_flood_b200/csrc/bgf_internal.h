@@ -19,9 +19,11 @@ template <class T> struct AmrDev;
 #define BGF_DECLARE_LAUNCHERS                                                                                   \
     template <class T> cudaError_t configure_kernels();                                                        \
     template <class T>                                                                                         \
-    void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st);   \
+    void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st,    \
+                     int grid);                                                                                \
     template <class T>                                                                                         \
-    void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st); \
+    void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st,  \
+                       int grid);                                                                              \
     template <class T>                                                                                         \
     void launch_initdt(const DevModel<T>& m, const StepParams<T>& p, int cur, unsigned long long* out,         \
                        cudaStream_t st);                                                                       \

@@ -107,6 +107,10 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     m.time = (TimeState*)(sc + kOffTime);
     m.dtmin = (unsigned long long*)(sc + kOffDt);
     m.err = (int*)(sc + kOffErr);
+    m.scen = nullptr;
+    m.sparams = nullptr;
+    m.lead = nullptr;
+    m.hmax = nullptr;
 
     StepParams<T> p;
     p.g = (T)P->g;
@@ -134,6 +138,7 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     p.has_rain = 0;
     p.nseg = 4;
     p.rain_n = 0;
+    p.rain_off = 0;
 
     // per-call state: time slot 0 from the caller's loop, the dt minimum, the error
     // word and the absorbing-boundary running means start from zero
@@ -156,11 +161,11 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
         return BGF_ECUDA;
     }
     if (P->fastmath) {
-        fast::launch_flux<T>(m, p, P->engine, 0, st);
-        fast::launch_update<T>(m, p, P->engine, 0, st);
+        fast::launch_flux<T>(m, p, P->engine, 0, st, 0);
+        fast::launch_update<T>(m, p, P->engine, 0, st, 0);
     } else {
-        exact::launch_flux<T>(m, p, P->engine, 0, st);
-        exact::launch_update<T>(m, p, P->engine, 0, st);
+        exact::launch_flux<T>(m, p, P->engine, 0, st, 0);
+        exact::launch_update<T>(m, p, P->engine, 0, st, 0);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) {
         bgf::set_last_error(std::string("launch: ") + cudaGetErrorString(e));

@@ -126,6 +126,20 @@ __device__ __forceinline__ void flux_divergence(const Smem<T>& s, const StepPara
     dhv = (s.Fqvy[gi] + s.Fqvx[fi] - s.Sv[gt] - s.Fqvx[fr]) * cmdinv - p.fc * hi * uui;
 }
 
+// Scenario of block slot ib (0 unless the model is a batched pool), its
+// parameters, and whether the block writes its scenario's next time slot (the
+// first block of the scenario in the active list).
+template <class T> __device__ __forceinline__ int scen_of(const DevModel<T>& m, int ib) { return m.scen ? m.scen[ib] : 0; }
+template <class T>
+__device__ __forceinline__ StepParams<T> params_of(const DevModel<T>& m, const StepParams<T>& p, int sc)
+{
+    return m.sparams ? m.sparams[sc] : p;
+}
+template <class T> __device__ __forceinline__ bool lead_of(const DevModel<T>& m, int ib, int w)
+{
+    return m.lead ? m.lead[ib] != 0 : w == 0;
+}
+
 // Whether this step runs (the reference loop condition totaltime < endtime plus
 // the step budget); identical in both kernels of a step.
 __device__ __forceinline__ bool step_live(const TimeState& ts)

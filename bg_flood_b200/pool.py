@@ -1,0 +1,109 @@
+"""Batched scenario pool: many independent scenarios advanced together on one GPU
+(the C ABI's bgf_pool_*).  No counterpart in the reference, which runs one
+scenario per process.
+
+A scenario is prepared in its own ``FlowB200`` handle (tables, bed, state,
+boundaries, rain), then admitted into the pool's block slots; every pool step is
+one launch pair over all admitted scenarios, each with its own dt and clock.
+Retiring copies the state back into the scenario's handle."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._native import lib
+from .flow import BGFError, FlowB200, Loop, _check
+
+__all__ = ["ScenarioPool"]
+
+
+class ScenarioPool:
+    def __init__(self, param, nblk_pool: int, max_scenarios: int, track_hmax: bool = False, stream: int | None = None):
+        self.param = param
+        self.dtype = np.float64 if param.doubleprecision else np.float32
+        self._cparam = param.to_c()
+        h = ctypes.c_void_p()
+        _check(lib().bgf_pool_create(ctypes.byref(self._cparam), int(nblk_pool), int(max_scenarios),
+                                     1 if track_hmax else 0, ctypes.c_void_p(stream) if stream else None,
+                                     ctypes.byref(h)), "bgf_pool_create")
+        self.handle = h
+        self.nblk_pool = int(nblk_pool)
+        self.members: dict[int, FlowB200] = {}
+
+    def close(self):
+        if self.handle:
+            lib().bgf_pool_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def admit(self, f: FlowB200, loop: Loop, endtime: float, outputtimestep: float = 0.0,
+              maxsteps: int = 2**31 - 1) -> int:
+        c = loop.to_c()
+        slot = ctypes.c_int(-1)
+        _check(lib().bgf_pool_admit(self.handle, f.handle, ctypes.byref(c), float(endtime), float(outputtimestep),
+                                    int(maxsteps), ctypes.byref(slot)), "bgf_pool_admit")
+        self.members[slot.value] = f
+        return slot.value
+
+    def try_admit(self, f: FlowB200, loop: Loop, endtime: float, **kw) -> int | None:
+        """admit, or None when the pool has no room (BGF_EBUDGET)."""
+        try:
+            return self.admit(f, loop, endtime, **kw)
+        except BGFError as e:
+            if e.status == 7:
+                return None
+            raise
+
+    def run(self, maxsteps: int) -> int:
+        """Pool steps until all scenarios finished or maxsteps ran; returns the number still running."""
+        n = ctypes.c_int(0)
+        _check(lib().bgf_pool_run(self.handle, int(maxsteps), ctypes.byref(n)), "bgf_pool_run")
+        return n.value
+
+    def query(self, slot: int):
+        """(Loop, status, nsteps); status 0 running, 1 finished, 2 dt underflow."""
+        c = Loop().to_c()
+        st = ctypes.c_int(0)
+        n = ctypes.c_int64(0)
+        _check(lib().bgf_pool_query(self.handle, int(slot), ctypes.byref(c), ctypes.byref(st), ctypes.byref(n)),
+               "bgf_pool_query")
+        loop = Loop()
+        loop.from_c(c)
+        return loop, st.value, n.value
+
+    def retire(self, slot: int):
+        """Copies the scenario back into its handle; returns (FlowB200, Loop, nsteps)."""
+        c = Loop().to_c()
+        n = ctypes.c_int(0)
+        _check(lib().bgf_pool_retire(self.handle, int(slot), ctypes.byref(c), ctypes.byref(n)), "bgf_pool_retire")
+        loop = Loop()
+        loop.from_c(c)
+        return self.members.pop(slot), loop, n.value
+
+    def depth(self, slot: int, nblk: int, with_max: bool = False):
+        """Interior depth (nblk, 16, 16) of a scenario in its active order, and its
+        running maximum when the pool tracks it."""
+        h = np.zeros((nblk, 16, 16), self.dtype)
+        hm = np.zeros((nblk, 16, 16), self.dtype) if with_max else None
+        _check(lib().bgf_pool_get_depth(self.handle, int(slot), h.ctypes.data_as(ctypes.c_void_p),
+                                        None if hm is None else hm.ctypes.data_as(ctypes.c_void_p)),
+               "bgf_pool_get_depth")
+        return (h, hm) if with_max else h
+
+    def timing(self):
+        """(gpu_ms, steps) of the last run() and the free block slots."""
+        ms = ctypes.c_double(0)
+        st = ctypes.c_int64(0)
+        fb = ctypes.c_int(0)
+        _check(lib().bgf_pool_timing(self.handle, ctypes.byref(ms), ctypes.byref(st), ctypes.byref(fb)),
+               "bgf_pool_timing")
+        return ms.value, st.value, fb.value
+
+    def set_grid(self, grid: int) -> None:
+        _check(lib().bgf_pool_set_grid(self.handle, int(grid)), "bgf_pool_set_grid")

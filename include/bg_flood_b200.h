@@ -245,6 +245,41 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* args, bgf_
 int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* present, int* nblk, int* level,
                      int* nbr8, double* xo, double* yo, int doubleprecision);
 
+/* ------------------------------------------------------------ batched scenario pool */
+/* No counterpart in the reference, which runs one scenario per process.  A pool
+ * holds device memory for nblk_pool block slots shared by up to max_scenarios
+ * independent scenarios (same engine, precision and kernel variant; single-level
+ * meshes).  Every pool step is one launch pair over all admitted scenarios; each
+ * scenario keeps its own parameters, dt (a per-scenario CFL minimum), time,
+ * output times, end time and step budget, so its results are those it has when
+ * run alone.  Steps run in CUDA graphs. */
+typedef struct bgf_pool bgf_pool;
+/* track_hmax: keep the running maximum depth of every cell. */
+int bgf_pool_create(const bgf_param* p, int nblk_pool, int max_scenarios, int track_hmax, void* stream,
+                    bgf_pool** out);
+int bgf_pool_destroy(bgf_pool* pool);
+/* Copies the scenario prepared in handle h (blocks, bed, state, segments, rain,
+ * parameters) into free block slots; loop is its time-loop state (after
+ * bgf_init_dt).  BGF_EBUDGET when the pool has too few free block or scenario
+ * slots.  *slot identifies the scenario in the pool. */
+int bgf_pool_admit(bgf_pool* pool, bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep,
+                   int maxsteps, int* slot);
+/* Copies the scenario's state back into its handle, writes its loop state and
+ * step count, and frees its slots. */
+int bgf_pool_retire(bgf_pool* pool, int slot, bgf_loop* loop, int* nsteps);
+/* Runs pool steps until every admitted scenario has finished or maxsteps steps
+ * ran; *nlive receives the number still running. */
+int bgf_pool_run(bgf_pool* pool, int maxsteps, int* nlive);
+/* status: 0 running, 1 finished (end time or step budget), 2 dt underflow. */
+int bgf_pool_query(bgf_pool* pool, int slot, bgf_loop* loop, int* status, int64_t* nsteps);
+/* Interior depth (and running maximum depth, if tracked) of a scenario's blocks
+ * in its active order, 256 values per block. */
+int bgf_pool_get_depth(bgf_pool* pool, int slot, void* h, void* hmax);
+/* Device time (ms) and pool steps of the last bgf_pool_run; free block slots. */
+int bgf_pool_timing(bgf_pool* pool, double* gpu_ms, int64_t* steps, int* free_blocks);
+/* CTAs of the fused kernels (0: one per block; fewer CTAs loop over the blocks). */
+int bgf_pool_set_grid(bgf_pool* pool, int grid);
+
 /* ------------------------------------------------------------ refinement pass */
 /* Criterion of the reference's "Adaptation" key (src/AdaptCriteria.cu:20-130):
  * a block is flagged for refinement when any of its cells has var > arg1

@@ -1,0 +1,89 @@
+"""Batched pool: scenarios of different sizes, forcings and boundaries advanced
+together give bit for bit the results they give alone (same kernels, own dt per
+scenario), including scenarios admitted while others are running."""
+import numpy as np
+import pytest
+
+import cases
+from bg_flood_b200.pool import ScenarioPool
+from runners import interior, make_gpu
+
+pytestmark = pytest.mark.gpu
+
+MIX = [
+    lambda: cases.gauss(48, 1, 3),
+    lambda: cases.dam_break(48, 1),
+    lambda: cases.conical_island(64, 1),
+    lambda: cases.rain_on_terrain(48, 1),
+    lambda: cases.hump_walls(32, 1),
+]
+ENDTIME = 1e30
+BUDGET = [40, 55, 70, 85, 100]   # steps per scenario: they finish at different pool steps
+
+
+def alone(mk, maxsteps):
+    f, mesh, loop = make_gpu(mk())
+    n = f.run(loop, endtime=ENDTIME, maxsteps=maxsteps)
+    return f.get_state(), loop, n
+
+
+def test_pool_results_equal_alone():
+    ref = [alone(mk, n) for mk, n in zip(MIX, BUDGET)]
+    case0 = MIX[0]()
+    pool = ScenarioPool(case0.param, 4096, 8)
+    slots = []
+    for mk, n in zip(MIX, BUDGET):
+        f, mesh, loop = make_gpu(mk())
+        slots.append(pool.admit(f, loop, ENDTIME, maxsteps=n))
+    left = pool.run(100000)
+    assert left == 0
+    for s, (st, loop_a, n_a) in zip(slots, ref):
+        f, loop, n = pool.retire(s)
+        assert n == n_a and loop.totaltime == loop_a.totaltime and loop.dt == loop_a.dt
+        for a, b in zip(f.get_state()[1:], st[1:]):
+            assert np.array_equal(interior(a), interior(b))
+
+
+def test_pool_admission_while_running():
+    """Continuous batching: B joins after A has run 30 steps; C replaces A when A ends."""
+    mkA, mkB, mkC = MIX[1], MIX[2], MIX[4]
+    budget = {"A": 80, "B": 120, "C": 60}
+    ref = {k: alone(mk, budget[k]) for k, mk in (("A", mkA), ("B", mkB), ("C", mkC))}
+    pool = ScenarioPool(mkA().param, 1200, 2)
+    fA, _, lA = make_gpu(mkA())
+    sA = pool.admit(fA, lA, ENDTIME, maxsteps=budget["A"])
+    pool.run(30)
+    fB, _, lB = make_gpu(mkB())
+    sB = pool.admit(fB, lB, ENDTIME, maxsteps=budget["B"])
+    fC, _, lC = make_gpu(mkC())
+    assert pool.try_admit(fC, lC, ENDTIME, maxsteps=budget["C"]) is None  # two scenario slots only
+    names = {sA: "A", sB: "B"}
+    pending = [("C", fC, lC)]
+    done = {}
+    while len(done) < 3:
+        pool.run(64)
+        for s in list(names):
+            loop, status, n = pool.query(s)
+            if status:
+                f, loop, n = pool.retire(s)
+                done[names.pop(s)] = (f.get_state(), loop, n)
+                if pending:
+                    k, f2, l2 = pending.pop()
+                    names[pool.admit(f2, l2, ENDTIME, maxsteps=budget[k])] = k
+    for k, (st, loop, n) in done.items():
+        st_a, loop_a, n_a = ref[k]
+        assert n == n_a and loop.totaltime == loop_a.totaltime, k
+        for a, b in zip(st[1:], st_a[1:]):
+            assert np.array_equal(interior(a), interior(b)), k
+
+
+def test_pool_tracks_maximum_depth():
+    mk = MIX[1]
+    pool = ScenarioPool(mk().param, 512, 1, track_hmax=True)
+    f, mesh, loop = make_gpu(mk())
+    h0 = interior(f.get_state()[1])
+    s = pool.admit(f, loop, ENDTIME, maxsteps=60)
+    pool.run(100000)
+    h, hmax = pool.depth(s, mesh.nblk, with_max=True)
+    assert np.all(hmax >= h) and np.all(hmax >= h0)
+    assert float((hmax - h).max()) > 0.0

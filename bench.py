@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--engine", type=int, default=1)
     ap.add_argument("--fastmath", type=int, default=1, help="1: fast-math kernels, 0: bit-exact kernels")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--ensemble", type=int, default=64, help="members of the batched-ensemble measurement (0: skip)")
+    ap.add_argument("--ens-max-blocks", type=int, default=16384)
+    ap.add_argument("--serve", type=int, default=48, help="requests of the serving measurement (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     return ap.parse_args()
 
 
@@ -167,6 +171,100 @@ def cpu_reference_sample(steps: int, warmup: int, engine: int):
     o.step(steps)
     dt = time.perf_counter() - t0
     return ncell * steps / dt, "port", dt
+
+
+def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, steps: int, dev: int, fastmath: int):
+    """Batched ensemble against the plain one-scenario-at-a-time loop on the same
+    seeded members (block counts log-uniform in [min_blocks, max_blocks], rain on
+    fractal terrain and deep-water tsunamis), each member advanced by `steps`
+    steps.  Device time of the steps (CUDA events around the graphs) and wall
+    clock including the host set-up of every member."""
+    import cases
+    from bg_flood_b200.pool import ScenarioPool
+    from runners import make_gpu
+    members = [cases.ensemble_member(k, seed, min_blocks, max_blocks) for k in range(nscen)]
+    for c in members:
+        c.param.GPUDEVICE = dev
+        c.param.fastmath = fastmath
+    blocks = [(c.nx // 16) * (c.ny // 16) for c in members]
+    # warm-up of both paths on the smallest member
+    small = members[int(np.argmin(blocks))]
+    f, _, lp = make_gpu(small)
+    f.run(lp, endtime=1e30, maxsteps=4)
+    del f
+    plain_ms, t0 = 0.0, time.perf_counter()
+    for c in members:
+        f, _, lp = make_gpu(c)
+        f.run(lp, endtime=1e30, maxsteps=steps)
+        plain_ms += f.last_run_timing()[0]
+        del f
+    plain_wall = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    pool = ScenarioPool(members[0].param, sum(blocks), nscen)
+    t1 = time.perf_counter()
+    built = [make_gpu(c) for c in members]
+    t2 = time.perf_counter()
+    for f, _, lp in built:
+        pool.admit(f, lp, 1e30, maxsteps=steps)
+    t3 = time.perf_counter()
+    left = pool.run(steps + 2)
+    batched_ms = pool.timing()[0]
+    batched_wall = time.perf_counter() - t0
+    phases = {"pool_create_s": t1 - t0, "build_s": t2 - t1, "admit_s": t3 - t2, "run_s": time.perf_counter() - t3}
+    assert left == 0
+    return {"scenarios": nscen, "blocks_total": int(sum(blocks)), "blocks_min": int(min(blocks)),
+            "blocks_max": int(max(blocks)), "steps_per_scenario": steps,
+            "plain_device_ms": plain_ms, "batched_device_ms": batched_ms,
+            "plain_scenarios_per_s": nscen / (plain_ms / 1e3), "batched_scenarios_per_s": nscen / (batched_ms / 1e3),
+            "speedup_device": plain_ms / batched_ms,
+            "plain_wall_s": plain_wall, "batched_wall_s": batched_wall,
+            "speedup_wall": plain_wall / batched_wall, "batched_phases": phases,
+            "cell_updates_per_s_batched": sum(blocks) * 256 * steps / (batched_ms / 1e3)}
+
+
+def serving_bench(nreq: int, seed: int, rate: float, dev: int, fastmath: int, budget_gb: float = 150.0):
+    """Poisson stream of flood scenarios (blocks log-uniform in [16, 2048], 100-400
+    steps each) served by the continuous-batching server under an HBM budget, and by
+    the plain loop (one at a time, arrival order).  Time-to-solution percentiles and
+    completed scenarios per second of wall clock."""
+    import cases
+    from bg_flood_b200.serve import FloodServer, Request, serve_sequential
+    from runners import make_gpu
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    reqs = []
+    for k in range(nreq):
+        case = cases.ensemble_member(k, seed, 16, 2048)
+        case.param.GPUDEVICE = dev
+        case.param.fastmath = fastmath
+
+        def build(case=case):
+            f, mesh, loop = make_gpu(case)
+            return f, loop
+        reqs.append(Request(k, float(arrivals[k]), (case.nx // 16) * (case.ny // 16), build,
+                            maxsteps=int(rng.integers(100, 400))))
+    param = cases.ensemble_member(0, seed, 16, 2048).param
+    param.GPUDEVICE = dev
+    param.fastmath = fastmath
+    out = {}
+    for name, fn in (("served", None), ("plain", serve_sequential)):
+        t0 = time.perf_counter()
+        if fn is None:
+            srv = FloodServer(param, budget_gb * 1e9, max_scenarios=64, chunk_steps=32, keep_fields=True)
+            res = srv.serve(reqs, realtime=True)
+        else:
+            res = fn(reqs, realtime=True)
+        wall = time.perf_counter() - t0
+        tts = np.array([r.time_to_solution for r in res])
+        out[name] = {"p50_s": float(np.percentile(tts, 50)), "p99_s": float(np.percentile(tts, 99)),
+                     "scenarios_per_s": nreq / wall, "wall_s": wall}
+        if fn is None:
+            out[name]["host_s"] = srv.host_s
+            out[name]["gpu_ms"] = srv.gpu_ms
+            out[name]["pool_blocks"] = srv.nblk_pool
+    out["rate_per_s"] = rate
+    out["requests"] = nreq
+    return out
 
 
 def run_reference_arm(args, rank, world):
@@ -292,6 +390,11 @@ def main():
         msb, _ = fb.last_run_timing()
         extra["device_loop_4096x4096"] = {"value": mb.nblk * 256 * 100 / (msb / 1e3), "steps": 100, "ms": msb}
         del fb
+        if args.ensemble > 0:
+            extra["ensemble"] = ensemble_bench(args.ensemble, 2024, 64, args.ens_max_blocks, 100, local,
+                                               args.fastmath)
+        if args.serve > 0:
+            extra["serving"] = serving_bench(args.serve, 7, args.serve_rate, local, args.fastmath)
 
     cpu = None
     if rank == 0 and world == 1:

@@ -87,6 +87,8 @@ struct bgf_handle {
     int minlev = 0, maxlev = 0;
     int steps_launches = 2;  // kernel launches per step
     int grid = 0;            // CTAs of the fused kernels (0: one per block)
+    int ntab = 0;            // table entries uploaded (highest active block id + 1)
+    size_t seg_cap = 0, ser_cap = 0;  // capacities of the segment buffers
     void* d_W[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
     void* d_G0[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     void* d_F[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -458,11 +460,17 @@ static int upload_tables(bgf_handle* h)
     const int nb = h->nblkmem;
     int rc = set_device(h);
     if (rc) return rc;
+    // only the slots up to the highest active id are uploaded (pools hand out low ids first)
+    int nt = 0;
+    for (int ibl = 0; ibl < h->nblk; ibl++) nt = std::max(nt, h->active[ibl] + 1);
+    h->ntab = nt;
     BGF_CUDA(cudaMemcpyAsync(h->d_active, h->active.data(), sizeof(int) * h->nblk, cudaMemcpyHostToDevice, h->stream));
-    BGF_CUDA(cudaMemcpyAsync(h->d_level, h->level.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, h->stream));
-    BGF_CUDA(cudaMemcpyAsync(h->d_nbr, h->nbr.data(), sizeof(int) * 8 * nb, cudaMemcpyHostToDevice, h->stream));
-    BGF_CUDA(cudaMemcpyAsync(h->d_bxo, h->bxo.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, h->stream));
-    BGF_CUDA(cudaMemcpyAsync(h->d_byo, h->byo.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_level, h->level.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, h->stream));
+    for (int k = 0; k < 8; k++)
+        BGF_CUDA(cudaMemcpyAsync(h->d_nbr + (size_t)k * nb, h->nbr.data() + (size_t)k * nb, sizeof(int) * nt,
+                                 cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_bxo, h->bxo.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_byo, h->byo.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, h->stream));
     // a mesh is multi-level when some active block has a neighbour on another level
     h->amr = false;
     h->minlev = h->maxlev = h->level[h->active[0]];
@@ -475,9 +483,10 @@ static int upload_tables(bgf_handle* h)
     if (h->amr) {
         rc = alloc_amr(h);
         if (rc) return rc;
-        std::vector<int> rank(nb, 0);
+        std::vector<int> rank(nt, 0);
         for (int ibl = 0; ibl < h->nblk; ibl++) rank[h->active[ibl]] = ibl;
-        BGF_CUDA(cudaMemcpyAsync(h->d_rank, rank.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, h->stream));
+        BGF_CUDA(cudaMemcpyAsync(h->d_rank, rank.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, h->stream));
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
     }
     BGF_CUDA(cudaStreamSynchronize(h->stream));
     h->has_blocks = true;
@@ -587,7 +596,8 @@ int bgf_set_bed(bgf_handle* h, const void* zb, const void* dzbdx, const void* dz
 static int rebuild_segments(bgf_handle* h)
 {
     int nb = h->nblkmem;
-    std::vector<int> side(4 * (size_t)nb, -1);
+    const int nt = h->ntab > 0 ? h->ntab : nb;
+    std::vector<int> side(4 * (size_t)nt, -1);
     std::vector<SegDev> sd;
     std::vector<double> st, swl;
     for (size_t k = 0; k < h->segs.size(); k++) {
@@ -603,19 +613,26 @@ static int rebuild_segments(bgf_handle* h)
         for (int sidx = 0; sidx < 4; sidx++)
             for (int ib : s.blk[sidx]) {
                 if (ib < 0 || ib >= nb) return BGF_EINVAL;
-                side[(size_t)ib * 4 + sidx] = (int)k;
+                if (ib < nt) side[(size_t)ib * 4 + sidx] = (int)k;
             }
     }
     int rc = set_device(h);
     if (rc) return rc;
     BGF_CUDA(cudaStreamSynchronize(h->stream));
-    if (h->d_segs) { cudaFree(h->d_segs); h->d_segs = nullptr; }
-    if (h->d_seg_t) { cudaFree(h->d_seg_t); h->d_seg_t = nullptr; }
-    if (h->d_seg_wl) { cudaFree(h->d_seg_wl); h->d_seg_wl = nullptr; }
-    size_t ns = std::max<size_t>(1, sd.size()), nt = std::max<size_t>(1, st.size());
-    BGF_CUDA(cudaMalloc((void**)&h->d_segs, ns * sizeof(SegDev)));
-    BGF_CUDA(cudaMalloc((void**)&h->d_seg_t, nt * sizeof(double)));
-    BGF_CUDA(cudaMalloc((void**)&h->d_seg_wl, nt * sizeof(double)));
+    // segment buffers only grow (pools rebuild them on every admission)
+    size_t ns = std::max<size_t>(1, sd.size()), nser = std::max<size_t>(1, st.size());
+    if (ns > h->seg_cap || !h->d_segs) {
+        if (h->d_segs) cudaFree(h->d_segs);
+        h->seg_cap = std::max(ns, 2 * h->seg_cap);
+        BGF_CUDA(cudaMalloc((void**)&h->d_segs, h->seg_cap * sizeof(SegDev)));
+    }
+    if (nser > h->ser_cap || !h->d_seg_t) {
+        if (h->d_seg_t) cudaFree(h->d_seg_t);
+        if (h->d_seg_wl) cudaFree(h->d_seg_wl);
+        h->ser_cap = std::max(nser, 2 * h->ser_cap);
+        BGF_CUDA(cudaMalloc((void**)&h->d_seg_t, h->ser_cap * sizeof(double)));
+        BGF_CUDA(cudaMalloc((void**)&h->d_seg_wl, h->ser_cap * sizeof(double)));
+    }
     if (!sd.empty()) BGF_CUDA(cudaMemcpy(h->d_segs, sd.data(), sd.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
     if (!st.empty()) {
         BGF_CUDA(cudaMemcpy(h->d_seg_t, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));

@@ -1,0 +1,178 @@
+"""Serving loop: flood scenarios arrive over time and are run together on one GPU
+(continuous batching over the scenario pool).  No counterpart in the reference.
+
+A request carries a builder that prepares the scenario in its own handle (host
+set-up and upload), its block count and its run length.  The server admits
+requests in arrival order while the pool's block slots -- sized from an HBM
+budget -- and scenario slots allow, keeps admitted scenarios resident, advances
+all of them together in chunks of pool steps, and retires each one as soon as it
+finishes, copying its final depth and maximum-depth map back to the host.  Its
+gauge readings are sampled at every chunk boundary.  Time-to-solution is measured
+from arrival to retirement."""
+from __future__ import annotations
+
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .flow import FlowB200, Loop
+from .pool import ScenarioPool
+
+__all__ = ["Request", "Result", "FloodServer", "bytes_per_block_slot", "serve_sequential"]
+
+
+def bytes_per_block_slot(doubleprecision: bool = False, track_hmax: bool = True) -> int:
+    """Device bytes one block slot of a pool holds: state (two buffers of h, u, v),
+    step scratch, bed and bed gradients with halos, friction, rain mask, boundary
+    means, maximum depth and the block tables."""
+    e = 8 if doubleprecision else 4
+    cells = 256 * (6 + 3 + 1 + (1 if track_hmax else 0)) * e + 324 * 3 * e
+    return cells + 256 + 64 * 4 + 128
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float             # seconds after the start of the stream
+    nblk: int
+    build: object              # () -> (FlowB200, Loop)
+    endtime: float = 1e30
+    maxsteps: int = 2**31 - 1
+    gauges: list = field(default_factory=list)  # (block index in active order, cell j*16+i)
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    nsteps: int
+    totaltime: float
+    h: np.ndarray | None = None
+    hmax: np.ndarray | None = None
+    gauge_series: list = field(default_factory=list)  # (wall time, [h at each gauge])
+
+    @property
+    def time_to_solution(self) -> float:
+        return self.finished - self.arrival
+
+
+class FloodServer:
+    def __init__(self, param, hbm_budget_bytes: float, max_scenarios: int = 64, chunk_steps: int = 64,
+                 track_hmax: bool = True, keep_fields: bool = True):
+        per = bytes_per_block_slot(bool(param.doubleprecision), track_hmax)
+        self.nblk_pool = max(1, int(hbm_budget_bytes // per))
+        self.pool = ScenarioPool(param, self.nblk_pool, max_scenarios, track_hmax=track_hmax)
+        self.chunk = int(chunk_steps)
+        self.track_hmax = track_hmax
+        self.keep_fields = keep_fields
+        self.gpu_ms = 0.0
+        self.host_s = {"admit": 0.0, "run": 0.0, "query": 0.0, "retire": 0.0, "fields": 0.0}
+
+    def serve(self, requests: list[Request], realtime: bool = True, prefetch: int = 8) -> list[Result]:
+        """Runs the stream to completion.  With realtime, a request becomes visible at
+        its arrival time on the wall clock; otherwise all are queued at t = 0.
+        Arrived requests are prepared (host set-up and upload into their own handle)
+        by a background thread while the pool computes, at most `prefetch` ahead."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        ready: list[tuple[Request, object]] = []   # (request, (FlowB200, Loop)) in arrival order
+        lock = threading.Condition()
+        stop = [False]
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0
+
+        def builder():
+            for r in pending:
+                with lock:
+                    while len(ready) >= prefetch and not stop[0]:
+                        lock.wait(0.01)
+                    if stop[0]:
+                        return
+                if realtime and r.arrival > now():
+                    time.sleep(r.arrival - now())
+                if r.nblk > self.nblk_pool:
+                    raise ValueError(f"request {r.rid} needs {r.nblk} blocks, the pool holds {self.nblk_pool}")
+                built = r.build()
+                with lock:
+                    ready.append((r, built))
+                    lock.notify_all()
+
+        th = threading.Thread(target=builder, daemon=True)
+        th.start()
+        live: dict[int, tuple[Request, FlowB200, float, list]] = {}
+        out: list[Result] = []
+        nreq = len(pending)
+        try:
+            while len(out) < nreq:
+                # admission in arrival order while block and scenario slots allow
+                with lock:
+                    while ready:
+                        r, (f, loop) = ready[0]
+                        ta = time.perf_counter()
+                        slot = self.pool.try_admit(f, loop, r.endtime, maxsteps=r.maxsteps)
+                        self.host_s["admit"] += time.perf_counter() - ta
+                        if slot is None:
+                            break
+                        ready.pop(0)
+                        live[slot] = (r, f, now(), [])
+                        lock.notify_all()
+                    if not live:
+                        if not th.is_alive() and not ready:
+                            raise RuntimeError("request preparation stopped before the stream ended")
+                        lock.wait(0.01)
+                        continue
+                ta = time.perf_counter()
+                self.pool.run(self.chunk)
+                self.host_s["run"] += time.perf_counter() - ta
+                self.gpu_ms += self.pool.timing()[0]
+                for slot in list(live):
+                    r, f, t_adm, series = live[slot]
+                    ta = time.perf_counter()
+                    loop, status, n = self.pool.query(slot)
+                    self.host_s["query"] += time.perf_counter() - ta
+                    if r.gauges:
+                        h = self.pool.depth(slot, r.nblk)
+                        series.append((now(), [float(h[b].reshape(-1)[c]) for b, c in r.gauges]))
+                    if status == 0:
+                        continue
+                    h = hmax = None
+                    ta = time.perf_counter()
+                    if self.keep_fields:
+                        if self.track_hmax:
+                            h, hmax = self.pool.depth(slot, r.nblk, with_max=True)
+                        else:
+                            h = self.pool.depth(slot, r.nblk)
+                    tb = time.perf_counter()
+                    self.host_s["fields"] += tb - ta
+                    f, loop, n = self.pool.retire(slot)
+                    f.close()
+                    self.host_s["retire"] += time.perf_counter() - tb
+                    del live[slot]
+                    out.append(Result(r.rid, r.arrival, t_adm, now(), n, loop.totaltime, h, hmax, series))
+        finally:
+            with lock:
+                stop[0] = True
+                lock.notify_all()
+            th.join(timeout=10)
+        return sorted(out, key=lambda x: x.rid)
+
+
+def serve_sequential(requests: list[Request], realtime: bool = True) -> list[Result]:
+    """The plain loop: one scenario at a time in arrival order, each run alone to
+    completion with the device-resident loop (bgf_run)."""
+    out = []
+    t0 = time.perf_counter()
+    now = lambda: time.perf_counter() - t0
+    for r in sorted(requests, key=lambda r: r.arrival):
+        if realtime and r.arrival > now():
+            time.sleep(r.arrival - now())
+        t_adm = now()
+        f, loop = r.build()
+        n = f.run(loop, endtime=r.endtime, maxsteps=r.maxsteps)
+        zs, h, u, v = f.get_state()
+        f.close()
+        out.append(Result(r.rid, r.arrival, t_adm, now(), n, loop.totaltime, None, None))
+    return out

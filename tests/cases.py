@@ -234,3 +234,43 @@ def amr_dambreak(n0: int = 64, engine: int = 1, maxlevel: int = 2, seed: int = 5
     crit = lambda x, y: np.where(x < 0.33 * L, 2.0, -10.0)
     return AMRCase(f"amrdam{n0}_e{engine}_l{maxlevel}", p, _amr_text(p, "Threshold,0.5,zs", maxlevel), n0, dx, 0.0,
                    0.0, zb, eta, adapt_eta_fn=crit)
+
+
+# ---------------------------------------------------------------- ensembles
+
+def _blocks_grid(nblocks: int, rng) -> tuple[int, int]:
+    """Block columns and rows of a near-square grid with about nblocks blocks."""
+    nbx = max(1, int(round(math.sqrt(nblocks) * rng.uniform(0.8, 1.25))))
+    nby = max(1, int(round(nblocks / nbx)))
+    return nbx, nby
+
+
+def ensemble_member(k: int, seed: int, min_blocks: int = 64, max_blocks: int = 16384, engine: int = 1) -> Case:
+    """Member k of a seeded ensemble: block count log-uniform in [min_blocks,
+    max_blocks]; three in four members are rain on fractal terrain (0-300 m relief,
+    rain 10-100 mm/h, Manning n in [0.02, 0.06], dx = 10 m), one in four a tsunami
+    (bed -4000..-200 m with a seamount ridge, initial Gaussian surface hump of
+    0.01-1 m, dx = 500 m, no friction).  Walls on all sides."""
+    rng = np.random.default_rng([seed, k])
+    nblocks = int(round(math.exp(rng.uniform(math.log(min_blocks), math.log(max_blocks)))))
+    nbx, nby = _blocks_grid(nblocks, rng)
+    nx, ny = 16 * nbx, 16 * nby
+    z = np.zeros((ny, nx), np.float32)
+    if k % 4 != 3:
+        m = max(nx, ny)
+        zb = fractal_terrain(m, int(rng.integers(1 << 30)))[:ny, :nx].copy()
+        rain_mmh = float(rng.uniform(10.0, 100.0))
+        manning = float(rng.uniform(0.02, 0.06))
+        p = Param(dx=10.0, xo=0.0, yo=0.0, engine=engine, aoibnd=0, cf=manning, frictionmodel=-1)
+        rain = ([0.0, 3600.0, 3601.0, 1e9], [rain_mmh, rain_mmh, 0.0, 0.0])
+        return Case(f"ens{seed}_{k}_rain_{nbx}x{nby}", p, _param_text(p), 10.0, 0.0, 0.0, zb,
+                    np.zeros((ny, nx), np.float32), z, z.copy(), rain=rain)
+    dx = 500.0
+    X, Y = _cell_centres(nx, ny, dx, 0.0, 0.0)
+    L = nx * dx
+    zb = (-4000.0 + 3800.0 * np.exp(-((X - 0.7 * L) / (0.08 * L)) ** 2)).astype(np.float32)
+    amp = float(rng.uniform(0.01, 1.0))
+    eta = amp * np.exp(-((X - 0.3 * L) ** 2 + (Y - 0.5 * ny * dx) ** 2) / (2 * (0.05 * L) ** 2))
+    h = np.maximum(eta - zb, 0.0).astype(np.float32)
+    p = Param(dx=dx, xo=0.0, yo=0.0, engine=engine, aoibnd=0, cf=0.0, frictionmodel=0)
+    return Case(f"ens{seed}_{k}_tsunami_{nbx}x{nby}", p, _param_text(p), dx, 0.0, 0.0, zb, h, z, z.copy())

@@ -42,6 +42,10 @@ struct HostSeg {
 struct bgf_handle {
     bgf_param P;
     int nblkmem = 0, nblk = 0, dbl = 0, dev = 0, fast = 0;
+    int split = 0;           // split precision: FP32 deviations from per-block datums
+    int iodbl = 0;           // field pointers at the boundary are double* (doubleprecision or split)
+    std::vector<double> datum, zbd;  // split: datum per block slot, bed as given (double)
+    void* d_datum = nullptr;
     size_t esz = 4;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -140,6 +144,7 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.sparams = nullptr;
     m.lead = nullptr;
     m.hmax = nullptr;
+    m.datum = h->split ? (const T*)h->d_datum : nullptr;
     return m;
 }
 
@@ -286,6 +291,7 @@ void bgf_param_default(bgf_param* p)
     p->rainbnd = 0;
     p->GPUDEVICE = 0;
     p->fastmath = 0;
+    p->splitprecision = 0;
 }
 
 const char* bgf_strerror(int s)
@@ -326,6 +332,8 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
     h->nblkmem = nblkmem;
     h->dbl = p->doubleprecision ? 1 : 0;
     h->esz = h->dbl ? 8 : 4;
+    h->split = (p->splitprecision && !h->dbl) ? 1 : 0;
+    h->iodbl = (h->dbl || h->split) ? 1 : 0;
     h->dev = p->GPUDEVICE;
     int rc;
     if ((rc = set_device(h)) != BGF_OK) { delete h; return rc; }
@@ -367,6 +375,7 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         {(void**)&h->d_scratch, 8 * sizeof(double)},
         {(void**)&h->d_bxo, nb * sizeof(double)},        {(void**)&h->d_byo, nb * sizeof(double)},
         {(void**)&h->d_flags, nb},                       {(void**)&h->d_child, 3 * nb * sizeof(int)},
+        {&h->d_datum, nb * es},
     };
     for (auto& a : allocs) {
         if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
@@ -381,6 +390,7 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
     cudaMemsetAsync(h->d_dh, 0, nb * 256 * es, h->stream);
     cudaMemsetAsync(h->d_dhu, 0, nb * 256 * es, h->stream);
     cudaMemsetAsync(h->d_dhv, 0, nb * 256 * es, h->stream);
+    cudaMemsetAsync(h->d_datum, 0, nb * es, h->stream);
     if (cudaMallocHost((void**)&h->h_time, 2 * sizeof(TimeState)) != cudaSuccess) {
         bgf_destroy(h);
         return BGF_ENOMEM;
@@ -414,7 +424,7 @@ int bgf_destroy(bgf_handle* h)
                     h->d_cf, h->d_rainmask, h->d_qmean, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t,
                     h->d_rain_r, h->d_h[0], h->d_h[1], h->d_u[0], h->d_u[1], h->d_v[0], h->d_v[1], h->d_dh,
                     h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch, h->d_bxo, h->d_byo,
-                    h->d_flags, h->d_child, h->d_dem};
+                    h->d_flags, h->d_child, h->d_dem, h->d_datum};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     free_amr(h);
@@ -480,6 +490,10 @@ static int upload_tables(bgf_handle* h)
         h->maxlev = std::max(h->maxlev, h->level[ib]);
         for (int k = 0; k < 8; k++) h->amr = h->amr || h->level[h->nbr[(size_t)k * nb + ib]] != h->level[ib];
     }
+    if (h->amr && h->split) {
+        g_last_error = "split precision supports single-level meshes only";
+        return BGF_EINVAL;
+    }
     if (h->amr) {
         rc = alloc_amr(h);
         if (rc) return rc;
@@ -519,8 +533,8 @@ int bgf_set_blocks(bgf_handle* h, const bgf_blockp* b)
     h->byo.assign(nb, 0.0);
     if (b->xo && b->yo)
         for (int ib = 0; ib < nb; ib++) {
-            h->bxo[ib] = h->dbl ? ((const double*)b->xo)[ib] : (double)((const float*)b->xo)[ib];
-            h->byo[ib] = h->dbl ? ((const double*)b->yo)[ib] : (double)((const float*)b->yo)[ib];
+            h->bxo[ib] = h->iodbl ? ((const double*)b->xo)[ib] : (double)((const float*)b->xo)[ib];
+            h->byo[ib] = h->iodbl ? ((const double*)b->yo)[ib] : (double)((const float*)b->yo)[ib];
         }
     int rc = upload_tables(h);
     if (rc) return rc;
@@ -533,13 +547,28 @@ static int set_bed_t(bgf_handle* h, const void* zb, const void* dzbdx, const voi
 {
     size_t nb = h->nblkmem;
     std::vector<T> z;
-    buq_to<T>(zb, h->dbl, nb * 324, z);
+    buq_to<T>(zb, h->iodbl, nb * 324, z);
+    if (h->split) {
+        // datum per block: the mean depth below zero of its interior, in whole metres
+        h->zbd.assign((const double*)zb, (const double*)zb + nb * 324);
+        h->datum.assign(nb, 0.0);
+        std::vector<T> dt(nb, (T)0);
+        for (int ibl = 0; ibl < h->nblk; ibl++) {
+            const size_t ib = h->active[ibl];
+            double sum = 0.0;
+            for (int j = 0; j < 16; j++)
+                for (int i = 0; i < 16; i++) sum += h->zbd[ib * 324 + (i + 1) + (j + 1) * 18];
+            h->datum[ib] = std::max(0.0, std::round(-sum / 256.0));
+            dt[ib] = (T)h->datum[ib];
+        }
+        BGF_CUDA(cudaMemcpy(h->d_datum, dt.data(), nb * sizeof(T), cudaMemcpyHostToDevice));
+    }
     BGF_CUDA(cudaMemcpy(h->d_zb, z.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
     if (dzbdx && dzbdy) {
         // the caller's bed halo and gradients are taken as they are
         std::vector<T> gx, gy;
-        buq_to<T>(dzbdx, h->dbl, nb * 324, gx);
-        buq_to<T>(dzbdy, h->dbl, nb * 324, gy);
+        buq_to<T>(dzbdx, h->iodbl, nb * 324, gx);
+        buq_to<T>(dzbdy, h->iodbl, nb * 324, gy);
         BGF_CUDA(cudaMemcpy(h->d_dzbdx, gx.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
         BGF_CUDA(cudaMemcpy(h->d_dzbdy, gy.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
     } else {
@@ -562,7 +591,7 @@ static int set_bed_t(bgf_handle* h, const void* zb, const void* dzbdx, const voi
             for (int j = 0; j < 16; j++)
                 for (int i = 0; i < 16; i++) {
                     size_t s = ib * 324 + (i + 1) + (j + 1) * 18;
-                    c[ib * 256 + j * 16 + i] = h->dbl ? (T)((const double*)cf)[s] : (T)((const float*)cf)[s];
+                    c[ib * 256 + j * 16 + i] = h->iodbl ? (T)((const double*)cf)[s] : (T)((const float*)cf)[s];
                 }
         BGF_CUDA(cudaMemcpy(h->d_cf, c.data(), nb * 256 * sizeof(T), cudaMemcpyHostToDevice));
     }
@@ -697,7 +726,18 @@ template <class T> static int set_state_t(bgf_handle* h, const bgf_evolving* ev)
             for (int j = 0; j < 16; j++)
                 for (int i = 0; i < 16; i++) {
                     size_t s = ib * 324 + (i + 1) + (j + 1) * 18;
-                    o[ib * 256 + j * 16 + i] = h->dbl ? (T)((const double*)src[f])[s] : (T)((const float*)src[f])[s];
+                    const size_t q = ib * 256 + j * 16 + i;
+                    if (h->split && f == 0) {
+                        // deviation from the datum, chosen so that the model surface
+                        // zb (as stored) + datum + deviation is the given zb + h
+                        const double hv = ((const double*)src[0])[s];
+                        const double D = h->datum[ib];
+                        const double zf = (double)(T)h->zbd[s];
+                        double dev = hv > 0.0 ? (h->zbd[s] + hv) - zf - D : -D;
+                        o[q] = (T)std::max(dev, -D);
+                        continue;
+                    }
+                    o[q] = h->iodbl ? (T)((const double*)src[f])[s] : (T)((const float*)src[f])[s];
                 }
         BGF_CUDA(cudaMemcpyAsync(dst[f], o, nb * 256 * sizeof(T), cudaMemcpyHostToDevice, h->stream));
     }
@@ -712,6 +752,7 @@ int bgf_set_state(bgf_handle* h, const bgf_evolving* ev)
     int rc = set_device(h);
     if (rc) return rc;
     BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->split && h->datum.empty()) return BGF_ESTATE;  // split mode: bed (and datums) first
     return h->dbl ? set_state_t<double>(h, ev) : set_state_t<float>(h, ev);
 }
 
@@ -732,7 +773,14 @@ template <class T> static int get_state_t(bgf_handle* h, bgf_evolving* ev)
             for (int i = 0; i < 16; i++) {
                 size_t d = ib * 324 + (i + 1) + (j + 1) * 18, s = ib * 256 + j * 16 + i;
                 T z = zb[d] + hh[s];
-                if (h->dbl) {
+                if (h->split) {
+                    // full depth and surface in double from the datum and the deviation
+                    const double D = h->datum[ib];
+                    if (ev->h) ((double*)ev->h)[d] = D + (double)hh[s];
+                    if (ev->u) ((double*)ev->u)[d] = (double)uu[s];
+                    if (ev->v) ((double*)ev->v)[d] = (double)vv[s];
+                    if (ev->zs) ((double*)ev->zs)[d] = (double)zb[d] + D + (double)hh[s];
+                } else if (h->dbl) {
                     if (ev->h) ((double*)ev->h)[d] = (double)hh[s];
                     if (ev->u) ((double*)ev->u)[d] = (double)uu[s];
                     if (ev->v) ((double*)ev->v)[d] = (double)vv[s];
@@ -1261,6 +1309,10 @@ int bgf_adapt(bgf_handle* h, const bgf_adapt_param* ap, int* nblk, int* niter)
         g_last_error = "bgf_adapt needs the bathymetry grid (bgf_set_bathy)";
         return BGF_ESTATE;
     }
+    if (h->split) {
+        g_last_error = "bgf_adapt does not support split precision";
+        return BGF_EINVAL;
+    }
     rc = h->dbl ? adapt_t<double>(h, ap, niter) : adapt_t<float>(h, ap, niter);
     if (nblk) *nblk = h->nblk;
     return rc;
@@ -1280,3 +1332,11 @@ int bgf_get_bed(bgf_handle* h, void* zb)
 // ---------------------------------------------------------------- batched pools
 
 #include "bgf_pool.inc"
+
+int bgf_set_grid(bgf_handle* h, int grid)
+{
+    if (!h || grid < 0) return BGF_EINVAL;
+    h->grid = grid;
+    free_graphs(h);
+    return BGF_OK;
+}

@@ -23,18 +23,29 @@ namespace BGF_VARIANT {
 
 // zs of a tile cell: ring 1 and the interior use the block's own bed tile
 // (RecalculateZs, src/Halo.cu:72-107); ring 2 uses the bed under its source cell,
-// as the neighbour's own RecalculateZs does before gradientHalo reads it.
-template <class T>
-__device__ __forceinline__ T tile_zb(const Smem<T>& s, const DevModel<T>& m, int x, int y, int sb, int sx, int sy)
+// as the neighbour's own RecalculateZs does before gradientHalo reads it.  In split
+// mode beds are deviations zb + D of the tile block's datum D.
+template <class T, bool SPLIT>
+__device__ __forceinline__ T tile_zb(const Smem<T>& s, const DevModel<T>& m, int x, int y, int sb, int sx, int sy, T D)
 {
     bool ring2 = x < -1 || x > BW || y < -1 || y > BW;
     if (!ring2) return s.zb[hi18(x, y)];
-    return m.zb[(size_t)sb * 324 + hi18(sx, sy)];
+    const T z = m.zb[(size_t)sb * 324 + hi18(sx, sy)];
+    return SPLIT ? z + D : z;
+}
+
+// Depth of a source cell in the tile block's frame: split mode converts the source
+// block's deviation to the tile block's datum (datums are whole metres, so the
+// difference is exact).
+template <class T, bool SPLIT>
+__device__ __forceinline__ T to_tile_datum(const DevModel<T>& m, T hv, int sb, int ib, T D)
+{
+    return SPLIT && sb != ib ? hv + (m.datum[sb] - D) : hv;
 }
 
 // Predictor tile: state n of the block and its two-cell ring.
-template <class T>
-__device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m, int ib, int cur, int tid)
+template <class T, bool SPLIT>
+__device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m, int ib, int cur, int tid, T D)
 {
     const T* H = m.h[cur];
     const T* U = m.u[cur];
@@ -57,10 +68,10 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
             sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
         }
         size_t g = (size_t)sb * 256 + sy * 16 + sx;
-        T hv = H[g], uv = U[g], vv = V[g];
+        T hv = to_tile_datum<T, SPLIT>(m, H[g], sb, ib, D), uv = U[g], vv = V[g];
         int c = ti(x, y);
         s.t[VH][c] = hv; s.t[VU][c] = uv; s.t[VV][c] = vv;
-        s.t[VZS][c] = tile_zb(s, m, x, y, sb, sx, sy) + hv;
+        s.t[VZS][c] = tile_zb<T, SPLIT>(s, m, x, y, sb, sx, sy, D) + hv;
         if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
             int c18 = hi18(x, y);
             s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
@@ -71,9 +82,9 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
 // Corrector tile: half-step state h* = Advance(state n, adv, dt/2) at every tile
 // cell, evaluated from the source cell's state and flux divergence; state n is kept
 // on the 18x18 tile for the boundary fluxes and the full-step advance.
-template <class T>
+template <class T, bool SPLIT>
 __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
-                                               int cur, T halfdt, int tid)
+                                               int cur, T halfdt, int tid, T D)
 {
     const T* H = m.h[cur];
     const T* U = m.u[cur];
@@ -92,10 +103,17 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
         size_t g = (size_t)sb * 256 + sy * 16 + sx;
         T hv = H[g], uv = U[g], vv = V[g];
         T ho, uo, vo;
-        advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, m.dh[g], m.dhu[g], m.dhv[g], ho, uo, vo);
+        if (SPLIT) {
+            const T Ds = sb == ib ? D : m.datum[sb];
+            advance_split<T>(halfdt, p.eps, p.forcemass != 0, Ds, hv, uv, vv, m.dh[g], m.dhu[g], m.dhv[g], ho, uo, vo);
+            hv = to_tile_datum<T, SPLIT>(m, hv, sb, ib, D);
+            ho = to_tile_datum<T, SPLIT>(m, ho, sb, ib, D);
+        } else {
+            advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, m.dh[g], m.dhu[g], m.dhv[g], ho, uo, vo);
+        }
         int c = ti(x, y);
         s.t[VH][c] = ho; s.t[VU][c] = uo; s.t[VV][c] = vo;
-        s.t[VZS][c] = tile_zb(s, m, x, y, sb, sx, sy) + ho;
+        s.t[VZS][c] = tile_zb<T, SPLIT>(s, m, x, y, sb, sx, sy, D) + ho;
         if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
             int c18 = hi18(x, y);
             s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
@@ -110,7 +128,7 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
 // In a batched pool every block belongs to a scenario with its own parameters,
 // time slot and dt minimum (the segmented CFL reduction).
 
-template <class T, int ENGINE>
+template <class T, int ENGINE, bool SPLIT>
 __global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -124,12 +142,13 @@ __global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepPa
         const StepParams<T> p = params_of(m, p0, sc);
         const T delta = calcres<T>(p.delta0, m.level[ib]);
         const int cur = ts.cur;
+        const T D = SPLIT ? m.datum[ib] : (T)0;
 
-        load_bed<T, ENGINE>(s, m, ib, tid);
+        load_bed<T, ENGINE, SPLIT>(s, m, ib, tid, D);
         __syncthreads();
-        load_state_tile<T>(s, m, ib, cur, tid);
+        load_state_tile<T, SPLIT>(s, m, ib, cur, tid, D);
         __syncthreads();
-        T celldt = tile_fluxes<T, ENGINE>(s, p, delta, tid);
+        T celldt = tile_fluxes<T, ENGINE, false, SPLIT>(s, p, delta, tid, nullptr, D);
         __syncthreads();
         // CFL minimum: the interior dtmax values reduced with the warp shuffle, then one
         // atomic per block on the float bit pattern (dt > 0, so integer order == float order).
@@ -140,7 +159,7 @@ __global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepPa
         }
         if ((tid & 31) == 0) s.red[tid >> 5] = v;
         // Boundary segments (FlowbndFlux) after the dt, at t + dt_prev/2 as FlowCPU does.
-        apply_boundaries<T>(s, m, p, ib, ts.totaltime + ts.dt * 0.5, tid);
+        apply_boundaries<T, SPLIT>(s, m, p, ib, ts.totaltime + ts.dt * 0.5, tid, D);
         __syncthreads();
         if (tid == 0) {
             T b = s.red[0];
@@ -150,7 +169,8 @@ __global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepPa
         const int x = tid & 15, y = tid >> 4;
         const int c = ti(x, y);
         T dh, dhu, dhv;
-        flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, s.t[VH][c], s.t[VU][c], s.t[VV][c], dh, dhu, dhv);
+        flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, SPLIT ? D + s.t[VH][c] : s.t[VH][c], s.t[VU][c],
+                           s.t[VV][c], dh, dhu, dhv);
         size_t g = (size_t)ib * 256 + tid;
         m.dh[g] = dh;
         m.dhu[g] = dhu;
@@ -159,7 +179,7 @@ __global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepPa
     }
 }
 
-template <class T, int ENGINE>
+template <class T, int ENGINE, bool SPLIT>
 __global__ void __launch_bounds__(NTHREADS, 4) update_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -183,27 +203,35 @@ __global__ void __launch_bounds__(NTHREADS, 4) update_kernel(DevModel<T> m, Step
         const int cur = ts.cur;
         const T dt = step_dt<T>(ts, m.dtmin[2 * sc + parity]);
         const double dtd = (double)dt;
+        const T D = SPLIT ? m.datum[ib] : (T)0;
 
-        load_bed<T, ENGINE>(s, m, ib, tid);
+        load_bed<T, ENGINE, SPLIT>(s, m, ib, tid, D);
         __syncthreads();
-        load_half_tile<T>(s, m, p, ib, cur, dt * (T)0.5, tid);
+        load_half_tile<T, SPLIT>(s, m, p, ib, cur, dt * (T)0.5, tid, D);
         __syncthreads();
-        (void)tile_fluxes<T, ENGINE>(s, p, delta, tid);
+        (void)tile_fluxes<T, ENGINE, false, SPLIT>(s, p, delta, tid, nullptr, D);
         __syncthreads();
-        apply_boundaries<T>(s, m, p, ib, ts.totaltime + dtd, tid);
+        apply_boundaries<T, SPLIT>(s, m, p, ib, ts.totaltime + dtd, tid, D);
         __syncthreads();
         const int x = tid & 15, y = tid >> 4;
         const int c = ti(x, y);
         T dh, dhu, dhv;
-        flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, s.t[VH][c], s.t[VU][c], s.t[VV][c], dh, dhu, dhv);
+        flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, SPLIT ? D + s.t[VH][c] : s.t[VH][c], s.t[VU][c],
+                           s.t[VV][c], dh, dhu, dhv);
         // full step from state n (AdvkernelCPU with evolv), then friction on the result
         const int c18 = hi18(x, y);
         T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];
         T ho, uo, vo;
-        advance<T>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+        if (SPLIT) advance_split<T>(dt, p.eps, p.forcemass != 0, D, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+        else advance<T>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
         size_t g = (size_t)ib * 256 + tid;
         T cfv = p.has_cf ? m.cf[g] : p.cf;
-        bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);
+        if (SPLIT) {
+            // friction on the full depth; the deviation is not changed by it
+            bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, D + ho, uo, vo);
+        } else {
+            bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);
+        }
         if (p.has_rain) {
             // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): uniform rain rate
             // interpolated at the start of the step (updateforcing)
@@ -211,9 +239,9 @@ __global__ void __launch_bounds__(NTHREADS, 4) update_kernel(DevModel<T> m, Step
             T Rainhh = (T)rnow;
             T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
             Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
-            T hi = ho;
+            T hi = SPLIT ? D + ho : ho;
             T qvol = hi / (hi + Rainhh);
-            ho = hi + Rainhh;
+            ho = ho + Rainhh;
             if ((double)hi > p.eps_d) {
                 uo = uo * qvol;
                 vo = vo * qvol;
@@ -223,7 +251,10 @@ __global__ void __launch_bounds__(NTHREADS, 4) update_kernel(DevModel<T> m, Step
         m.h[nxt][g] = ho;
         m.u[nxt][g] = uo;
         m.v[nxt][g] = vo;
-        if (m.hmax) m.hmax[g] = ho > m.hmax[g] ? ho : m.hmax[g];
+        if (m.hmax) {
+            const T hf = SPLIT ? D + ho : ho;
+            m.hmax[g] = hf > m.hmax[g] ? hf : m.hmax[g];
+        }
         if (lead && tid == 0)
             m.time[2 * sc + (parity ^ 1)] = next_time_state<T>(ts, p, dtd, nxt, m.dtmin + 2 * sc, parity);
         __syncthreads();  // the tile is reused by the next block
@@ -240,6 +271,7 @@ template <class T> __global__ void initdt_kernel(DevModel<T> m, StepParams<T> p0
     const StepParams<T> p = params_of(m, p0, sc);
     const T delta = calcres<T>(p.delta0, m.level[ib]);
     T hv = m.h[cur][(size_t)ib * 256 + tid];
+    if (m.datum) hv = m.datum[ib] + hv;
     T epsT = (T)p.eps_d;
     T hm = hv < epsT ? epsT : hv;
     T v = delta / M<T>::sqrt_(p.g * hm);
@@ -264,7 +296,7 @@ template <class T> __global__ void volume_kernel(DevModel<T> m, T delta0, int cu
     const int ib = m.active[blockIdx.x];
     const int sc = scen_of(m, ib);
     double d = (double)calcres<T>(delta0, m.level[ib]);
-    double v = (double)m.h[cur][(size_t)ib * 256 + tid] * d * d;
+    double v = ((double)m.h[cur][(size_t)ib * 256 + tid] + (m.datum ? (double)m.datum[ib] : 0.0)) * d * d;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((tid & 31) == 0) red[tid >> 5] = v;
     __syncthreads();
@@ -281,11 +313,15 @@ template <class T> size_t smem_bytes() { return sizeof(Smem<T>); }
 
 template <class T, int ENGINE> cudaError_t configure_engine()
 {
-    cudaError_t e = cudaFuncSetAttribute(flux_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_bytes<T>());
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(update_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_bytes<T>());
+    const int sm = (int)smem_bytes<T>();
+    cudaError_t e = cudaFuncSetAttribute(flux_kernel<T, ENGINE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(update_kernel<T, ENGINE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(flux_kernel<T, ENGINE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(update_kernel<T, ENGINE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return e;
 }
 
 template <class T> cudaError_t configure_kernels()
@@ -300,16 +336,24 @@ template <class T>
 void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st, int grid)
 {
     const int g = grid > 0 && grid < m.nblk ? grid : m.nblk;
-    if (engine == 1) flux_kernel<T, 1><<<g, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
-    else flux_kernel<T, 2><<<g, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+    const size_t sm = smem_bytes<T>();
+    if (m.datum) {
+        if (engine == 1) flux_kernel<T, 1, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
+        else flux_kernel<T, 2, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
+    } else if (engine == 1) flux_kernel<T, 1, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
+    else flux_kernel<T, 2, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
 }
 
 template <class T>
 void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st, int grid)
 {
     const int g = grid > 0 && grid < m.nblk ? grid : m.nblk;
-    if (engine == 1) update_kernel<T, 1><<<g, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
-    else update_kernel<T, 2><<<g, NTHREADS, smem_bytes<T>(), st>>>(m, p, parity);
+    const size_t sm = smem_bytes<T>();
+    if (m.datum) {
+        if (engine == 1) update_kernel<T, 1, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
+        else update_kernel<T, 2, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
+    } else if (engine == 1) update_kernel<T, 1, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
+    else update_kernel<T, 2, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
 }
 
 template <class T>

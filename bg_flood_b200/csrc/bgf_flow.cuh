@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include "bgf_numerics.cuh"
+#include "bgf_split.cuh"
 
 namespace bgf {
 
@@ -94,6 +95,7 @@ template <class T> struct DevModel {
     const StepParams<T>* sparams;     // per scenario
     const uint8_t* lead;              // per block slot: 1 for the first block of its scenario
     T* hmax;                          // per cell (256 per block): running maximum depth, or null
+    const T* datum;                   // per block slot: datum depth of split mode, or null
 };
 
 // Positive floating-point values order like their bit patterns.
@@ -214,9 +216,9 @@ template <class T> struct SubFaces {
 };
 
 // One X (isx) or Y face of the tile, written to the face arrays of s.
-template <class T, int ENGINE, bool SUB = false>
+template <class T, int ENGINE, bool SUB = false, bool SPLIT = false>
 __device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p, T delta, bool isx, int x, int y,
-                                             const SubFaces<T>* sub = nullptr)
+                                             const SubFaces<T>* sub = nullptr, T D = (T)0)
 {
     FaceIn<T, ENGINE> f;
     int ci = ti(x, y), cn = isx ? ti(x - 1, y) : ti(x, y - 1);
@@ -253,7 +255,9 @@ __device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p,
             if (y == 0 && sub->on[2]) { f.hsn = sub->h[2][x]; f.zsrcn = sub->z[2][x]; }
         }
     }
-    Face<T> r = face_flux<T, ENGINE>(f, p.g, p.CFL, p.epsi, p.epsface, delta);
+    Face<T> r;
+    if (SPLIT) r = face_flux_split<T, ENGINE>(f, D, p.g, p.CFL, p.epsi, p.epsface, delta);
+    else r = face_flux<T, ENGINE>(f, p.g, p.CFL, p.epsi, p.epsface, delta);
     if (isx) {
         int fi = fxi(x, y);
         s.Fhu[fi] = r.Fh; s.Fqux[fi] = r.Fq; s.Su[fi] = r.S; s.Fqvx[fi] = r.Ft;
@@ -268,9 +272,9 @@ __device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p,
 // Restates gradientCPU (src/Gradients.cu:971-1054) on a single-level tile, then
 // the engine's X and Y sweeps.  Returns this thread's cell dtmax (the value the
 // reference leaves in dtmax[i] after both sweeps).
-template <class T, int ENGINE, bool SUB = false>
+template <class T, int ENGINE, bool SUB = false, bool SPLIT = false>
 __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T delta, int tid,
-                                         const SubFaces<T>* sub = nullptr)
+                                         const SubFaces<T>* sub = nullptr, T D = (T)0)
 {
     const T theta = p.theta;
     const T rdelta = (T)1.0 / delta;
@@ -305,17 +309,20 @@ __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T d
         const T* hh = s.t[VH];
         {
             const int c = ti(tx, ty), gi = gxi(tx, ty), gj = gyi(tx, ty);
-            s.gx[VZS][gi] = wetslope(delta, zs[c], hh[c], zs[c - 1], zs[c + 1], s.gx[VZS][gi], s.gx[VH][gi], s.dzbx[gi]);
-            s.gy[VZS][gj] = wetslope(delta, zs[c], hh[c], zs[c - TW], zs[c - TW], s.gy[VZS][gj], s.gy[VH][gj], s.dzby[gj]);
+            const T hc = SPLIT ? D + hh[c] : hh[c];
+            s.gx[VZS][gi] = wetslope(delta, zs[c], hc, zs[c - 1], zs[c + 1], s.gx[VZS][gi], s.gx[VH][gi], s.dzbx[gi]);
+            s.gy[VZS][gj] = wetslope(delta, zs[c], hc, zs[c - TW], zs[c - TW], s.gy[VZS][gj], s.gy[VH][gj], s.dzby[gj]);
         }
         if (tid < 64) {
             const int side = tid >> 4, q = tid & 15;
             if (side < 2) {
                 const int x = side == 0 ? -1 : BW, c = ti(x, q), g = gxi(x, q);
-                s.gx[VZS][g] = wetslope(delta, zs[c], hh[c], zs[c - 1], zs[c + 1], s.gx[VZS][g], s.gx[VH][g], s.dzbx[g]);
+                const T hc = SPLIT ? D + hh[c] : hh[c];
+                s.gx[VZS][g] = wetslope(delta, zs[c], hc, zs[c - 1], zs[c + 1], s.gx[VZS][g], s.gx[VH][g], s.dzbx[g]);
             } else {
                 const int y = side == 2 ? -1 : BW, c = ti(q, y), g = gyi(q, y);
-                s.gy[VZS][g] = wetslope(delta, zs[c], hh[c], zs[c - TW], zs[c + TW], s.gy[VZS][g], s.gy[VH][g], s.dzby[g]);
+                const T hc = SPLIT ? D + hh[c] : hh[c];
+                s.gy[VZS][g] = wetslope(delta, zs[c], hc, zs[c - TW], zs[c + TW], s.gy[VZS][g], s.gy[VH][g], s.dzby[g]);
             }
         }
         __syncthreads();
@@ -323,12 +330,12 @@ __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T d
     // Thread (tx,ty) owns the left (X) and bottom (Y) faces of its cell; threads
     // 0..15 also take X face x=16 and threads 16..31 Y face y=16 (the faces the
     // reference computes in the right / top halo column).
-    Face<T> fx = tile_face<T, ENGINE, SUB>(s, p, delta, true, tx, ty, sub);
+    Face<T> fx = tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, true, tx, ty, sub, D);
     T celldt = fx.dt;  // dtmax after the X sweep (hugeposval exceeds any finite dt)
-    Face<T> fy = tile_face<T, ENGINE, SUB>(s, p, delta, false, tx, ty, sub);
+    Face<T> fy = tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, false, tx, ty, sub, D);
     celldt = fy.wet ? (fy.dt < celldt ? fy.dt : celldt) : fy.dt;
-    if (tid < 16) tile_face<T, ENGINE, SUB>(s, p, delta, true, BW, tid, sub);
-    else if (tid < 32) tile_face<T, ENGINE, SUB>(s, p, delta, false, tid - 16, BW, sub);
+    if (tid < 16) tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, true, BW, tid, sub, D);
+    else if (tid < 32) tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, false, tid - 16, BW, sub, D);
     return celldt;
 }
 

@@ -7,11 +7,12 @@
 #pragma once
 
 // Loads the bed halo tile and (engine 1) the bed-gradient rows/columns.
-template <class T, int ENGINE>
-__device__ __forceinline__ void load_bed(Smem<T>& s, const DevModel<T>& m, int ib, int tid)
+// Split mode stores the tile's bed as the deviation zb + D of the block's datum.
+template <class T, int ENGINE, bool SPLIT = false>
+__device__ __forceinline__ void load_bed(Smem<T>& s, const DevModel<T>& m, int ib, int tid, T D = (T)0)
 {
     const T* zbt = m.zb + (size_t)ib * 324;
-    for (int k = tid; k < 324; k += NTHREADS) s.zb[k] = zbt[k];
+    for (int k = tid; k < 324; k += NTHREADS) s.zb[k] = SPLIT ? zbt[k] + D : zbt[k];
     if (ENGINE == 1) {
         const T* gx = m.dzbdx + (size_t)ib * 324;
         const T* gy = m.dzbdy + (size_t)ib * 324;
@@ -36,9 +37,9 @@ __device__ __forceinline__ double series_at(const double* t, const double* v, in
 // bndFluxGPUSideCPU (src/Boundary.cu:587-745) for the four sides of one block.
 // Face arrays in s are modified in place; state n comes from s.h0/u0/v0 and the
 // bed tile (zs = zb + h, as RecalculateZs leaves it).
-template <class T>
+template <class T, bool SPLIT = false>
 __device__ __forceinline__ void apply_boundaries(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
-                                                 double tbnd, int tid)
+                                                 double tbnd, int tid, T D = (T)0)
 {
     if (tid >= 64) return;
     int side = tid >> 4, t = tid & 15;
@@ -68,9 +69,10 @@ __device__ __forceinline__ void apply_boundaries(Smem<T>& s, const DevModel<T>& 
     int ci = hi18(ix, iy), cin = hi18(inx, iny);
     T zsi = s.zb[ci] + s.h0[ci];
     T zsinside = s.zb[cin] + s.h0[cin];
-    T hinside = s.h0[cin];
+    // (split mode: the tile holds deviations; zs = zb' + h' is the surface either way)
+    T hinside = SPLIT ? D + s.h0[cin] : s.h0[cin];
     T uninside = isright != 0 ? s.u0[cin] : s.v0[cin];
-    T hface = s.h0[ci];
+    T hface = SPLIT ? D + s.h0[ci] : s.h0[ci];
     T zsX = (T)(((double)((T)zsb + (T)0.0) - 0.5 * (double)(zsi + zsinside)) * (double)taper + 0.5 * (double)(zsi + zsinside));
     float* qm = m.qmean + ib * 64 + side * 16 + t;
     T qmean = (T)*qm;

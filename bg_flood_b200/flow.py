@@ -79,7 +79,9 @@ class FlowB200:
 
     def __init__(self, param: Param, nblkmem: int, stream: int | None = None):
         self.param = param
-        self.dtype = np.float64 if param.doubleprecision else np.float32
+        # field arrays at the C boundary: double with doubleprecision or split precision
+        self.dtype = np.float64 if (param.doubleprecision or getattr(param, "splitprecision", 0)) else np.float32
+        self.dev_dtype = np.float64 if param.doubleprecision else np.float32
         self.nblkmem = int(nblkmem)
         self._cparam = param.to_c()
         h = ctypes.c_void_p()
@@ -158,9 +160,13 @@ class FlowB200:
         _check(lib().bgf_get_state(self.handle, ctypes.byref(ev)), "bgf_get_state")
         return tuple(out)
 
+    def set_grid(self, grid: int) -> None:
+        """CTAs of the fused kernels (0: one per block; fewer: persistent launch)."""
+        _check(lib().bgf_set_grid(self.handle, int(grid)), "bgf_set_grid")
+
     def get_bed(self) -> np.ndarray:
         """zb on (nblkmem, 18, 18) tiles, halo included."""
-        out = np.zeros((self.nblkmem, 18, 18), self.dtype)
+        out = np.zeros((self.nblkmem, 18, 18), self.dev_dtype)
         _check(lib().bgf_get_bed(self.handle, _ptr(out)), "bgf_get_bed")
         return out
 
@@ -262,7 +268,7 @@ def build_model(param: Param, zb: np.ndarray, h: np.ndarray, u: np.ndarray | Non
     uniform rain series (times, mm/h).  Returns (FlowB200, Mesh)."""
     ny, nx = zb.shape
     mesh = mesh or uniform_mesh(nx, ny, param.dx, doubleprecision=bool(param.doubleprecision))
-    dt = np.float64 if param.doubleprecision else np.float32
+    dt = np.float64 if (param.doubleprecision or param.splitprecision) else np.float32
     f = FlowB200(param, mesh.nblk)
     f.set_blocks(mesh.active, mesh.level, mesh.nbr, mesh.xo, mesh.yo)
     zbb = fill_halo(grid_to_buq(np.asarray(zb, np.float64).astype(dt).astype(np.float64), mesh), mesh)

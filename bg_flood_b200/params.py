@@ -23,7 +23,8 @@ class CParam(ctypes.Structure):
         "bndtaper", "bndrelaxtime", "bndfiltertime", "inittime", "dtmin", "dtinit", "mask")] + \
         [(n, ctypes.c_int) for n in (
             "engine", "frictionmodel", "ForceMassConserve", "wetdryfix", "conserveElevation",
-            "doubleprecision", "minlevel", "maxlevel", "initlevel", "aoibnd", "rainbnd", "GPUDEVICE", "fastmath")]
+            "doubleprecision", "minlevel", "maxlevel", "initlevel", "aoibnd", "rainbnd", "GPUDEVICE", "fastmath",
+            "splitprecision")]
 
 
 @dataclass
@@ -55,6 +56,7 @@ class Param:
     GPUDEVICE: int = 0
     doubleprecision: int = 0
     fastmath: int = 0  # library option, not a reference key: 1 selects the fast-math kernels
+    splitprecision: int = 0  # library option: FP32 depths as deviations from per-block datums (deep water)
     engine: int = 1
     dx: float = math.nan
     xo: float = math.nan

@@ -21,7 +21,7 @@ __all__ = ["ScenarioPool"]
 class ScenarioPool:
     def __init__(self, param, nblk_pool: int, max_scenarios: int, track_hmax: bool = False, stream: int | None = None):
         self.param = param
-        self.dtype = np.float64 if param.doubleprecision else np.float32
+        self.dtype = np.float64 if param.doubleprecision else np.float32  # device precision
         self._cparam = param.to_c()
         h = ctypes.c_void_p()
         _check(lib().bgf_pool_create(ctypes.byref(self._cparam), int(nblk_pool), int(max_scenarios),

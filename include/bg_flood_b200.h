@@ -82,6 +82,11 @@ typedef struct bgf_param {
                              square root); 1: FMA contraction and approximate
                              division / square root (results within the
                              tolerances of the parity tests)                   */
+    int splitprecision;   /* 1 (with doubleprecision 0, single-level meshes):
+                             FP32 state stored as deviations from a per-block
+                             datum depth (whole metres, FP64 on the host), for
+                             deep water; field pointers at this boundary are
+                             then double*.  No counterpart in the reference.  */
 } bgf_param;
 
 /* Reference Loop<T> members the step reads and writes (src/Arrays.h:359-404). */
@@ -192,6 +197,10 @@ int64_t bgf_kernel_launches(bgf_handle* h);
  * accumulate their device times; turning it on resets the totals. */
 int bgf_set_profiling(bgf_handle* h, int on);
 int bgf_kernel_timing(bgf_handle* h, double* flux_ms, double* update_ms, int64_t* steps);
+/* CTAs of the two fused single-level kernels: 0 (default) launches one per
+ * active block; a smaller count makes each CTA loop over blocks (a persistent
+ * launch).  Results do not depend on it. */
+int bgf_set_grid(bgf_handle* h, int grid);
 /* Device time (ms) and kernel launches of the last bgf_run (events around its graphs). */
 int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches);
 

@@ -1,0 +1,61 @@
+"""Split precision (FP32 deviations from per-block datums) against the FP64 build
+on deep-water cases: the surface error stays below 1e-3 m where plain FP32 does
+not, a deep lake at rest stays at rest, and shallow cases keep the accuracy of
+plain FP32."""
+import numpy as np
+import pytest
+
+import cases
+from runners import interior, make_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def run_to(case, endtime, mode):
+    """mode: 'fp32', 'split' or 'fp64'; returns (zs, hu) interior arrays in double."""
+    case.param.doubleprecision = 1 if mode == "fp64" else 0
+    case.param.splitprecision = 1 if mode == "split" else 0
+    case.nextoutputtime = endtime
+    f, mesh, loop = make_gpu(case)
+    f.run(loop, endtime=endtime)
+    assert loop.totaltime == endtime
+    zs, h, u, v = f.get_state()
+    zs, h, u = (interior(a).astype(np.float64) for a in (zs, h, u))
+    return zs, h * u
+
+
+@pytest.mark.parametrize("k", [3, 7])
+def test_tsunami_surface_error_below_1mm(k):
+    T = 300.0
+    ref = run_to(cases.ensemble_member(k, 2024, 64, 512), T, "fp64")
+    sp = run_to(cases.ensemble_member(k, 2024, 64, 512), T, "split")
+    f32 = run_to(cases.ensemble_member(k, 2024, 64, 512), T, "fp32")
+    e_split = float(np.abs(sp[0] - ref[0]).max())
+    e_f32 = float(np.abs(f32[0] - ref[0]).max())
+    assert e_split <= 1e-3, e_split
+    assert e_split < 0.5 * e_f32, (e_split, e_f32)
+
+
+def test_deep_lake_at_rest():
+    """A flat surface over the 4000 m basin with its 3800 m ridge stays flat: split
+    precision keeps the drift at the resolution of the deviations of the ridge's
+    blocks (whose beds span the whole depth range), far below plain FP32."""
+    def lake():
+        case = cases.ensemble_member(3, 2024, 64, 512)
+        case.h = np.maximum(0.0 - case.zb, 0.0).astype(np.float32)   # flat surface at 0
+        return case
+    zs_s, hu_s = run_to(lake(), 200.0, "split")
+    zs_f, hu_f = run_to(lake(), 200.0, "fp32")
+    e_s, e_f = float(np.abs(zs_s).max()), float(np.abs(zs_f).max())
+    assert e_s <= 2.5e-4 and e_s < 0.25 * e_f, (e_s, e_f)
+
+
+def test_shallow_cases_keep_fp32_accuracy():
+    T = 2.0
+    for mk in (lambda: cases.dam_break(48, 1), lambda: cases.conical_island(64, 2)):
+        ref = run_to(mk(), T, "fp64")
+        sp = run_to(mk(), T, "split")
+        f32 = run_to(mk(), T, "fp32")
+        e_split = float(np.abs(sp[0] - ref[0]).max())
+        e_f32 = float(np.abs(f32[0] - ref[0]).max())
+        assert e_split <= max(2.0 * e_f32, 1e-5), (e_split, e_f32)

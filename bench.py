@@ -186,6 +186,7 @@ def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, step
     for c in members:
         c.param.GPUDEVICE = dev
         c.param.fastmath = fastmath
+        c.param.splitprecision = 1   # FP32 bulk, deviations from FP64 block datums
     blocks = [(c.nx // 16) * (c.ny // 16) for c in members]
     # warm-up of both paths on the smallest member
     small = members[int(np.argmin(blocks))]
@@ -212,7 +213,33 @@ def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, step
     batched_wall = time.perf_counter() - t0
     phases = {"pool_create_s": t1 - t0, "build_s": t2 - t1, "admit_s": t3 - t2, "run_s": time.perf_counter() - t3}
     assert left == 0
-    return {"scenarios": nscen, "blocks_total": int(sum(blocks)), "blocks_min": int(min(blocks)),
+    del pool, built
+    # accuracy: split-precision FP32 against the FP64 build at the same simulated time
+    acc = {}
+    for k in range(min(nscen, 8)):
+        if len(acc) >= 4:
+            break
+        kind = "tsunami" if k % 4 == 3 else "rain"
+        if kind == "rain" and sum(1 for v in acc.values() if v["kind"] == "rain") >= 2:
+            continue
+        res = {}
+        for mode in ("split", "fp64"):
+            c = cases.ensemble_member(k, seed, min_blocks, min(max_blocks, 1024))
+            c.param.GPUDEVICE = dev
+            c.param.fastmath = fastmath
+            c.param.splitprecision = 1 if mode == "split" else 0
+            c.param.doubleprecision = 1 if mode == "fp64" else 0
+            c.nextoutputtime = 300.0
+            f, _, lp = make_gpu(c)
+            f.run(lp, endtime=300.0)
+            zs, h, u, v = f.get_state()
+            res[mode] = (zs[:, 1:17, 1:17].astype(np.float64), (h * u)[:, 1:17, 1:17].astype(np.float64))
+            del f
+        acc[c.name] = {"kind": kind, "max_eta_err_m": float(np.abs(res["split"][0] - res["fp64"][0]).max()),
+                       "max_hu_err_m2s": float(np.abs(res["split"][1] - res["fp64"][1]).max()),
+                       "simulated_s": 300.0}
+    return {"scenarios": nscen, "precision": "FP32 split (deviations from FP64 block datums)",
+            "accuracy_vs_fp64": acc, "blocks_total": int(sum(blocks)), "blocks_min": int(min(blocks)),
             "blocks_max": int(max(blocks)), "steps_per_scenario": steps,
             "plain_device_ms": plain_ms, "batched_device_ms": batched_ms,
             "plain_scenarios_per_s": nscen / (plain_ms / 1e3), "batched_scenarios_per_s": nscen / (batched_ms / 1e3),

@@ -123,13 +123,26 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
 
 // ---------------------------------------------------------------- kernels
 
+// Minimum resident CTAs per SM the register allocation must allow (launch
+// bounds): the fast build trades a few spilled registers for occupancy, which
+// hides the tile loads; FP64 instantiations keep more registers.
+#if BGF_FAST
+template <class T> struct Occ {
+    static constexpr int flux = sizeof(T) == 4 ? 6 : 3, update = sizeof(T) == 4 ? 5 : 3;
+};
+#else
+template <class T> struct Occ {
+    static constexpr int flux = sizeof(T) == 4 ? 4 : 3, update = sizeof(T) == 4 ? 4 : 3;
+};
+#endif
+
 // Both kernels walk the active list with a grid-stride loop: a launch of one CTA
 // per block and a persistent launch of a few CTAs per SM give the same result.
 // In a batched pool every block belongs to a scenario with its own parameters,
 // time slot and dt minimum (the segmented CFL reduction).
 
 template <class T, int ENGINE, bool SPLIT>
-__global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepParams<T> p0, int parity)
+__global__ void __launch_bounds__(NTHREADS, Occ<T>::flux) flux_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
@@ -180,7 +193,7 @@ __global__ void __launch_bounds__(NTHREADS, 4) flux_kernel(DevModel<T> m, StepPa
 }
 
 template <class T, int ENGINE, bool SPLIT>
-__global__ void __launch_bounds__(NTHREADS, 4) update_kernel(DevModel<T> m, StepParams<T> p0, int parity)
+__global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);

@@ -227,7 +227,12 @@ template <class T>
 __device__ __forceinline__ void advance(T dt, T eps, double eps_d, bool forcemass, T hold, T uold, T vold, T dhi,
                                         T dhui, T dhvi, T& ho, T& uo, T& vo)
 {
+#if BGF_FAST
+    // fast build: the limiter in the state precision
+    T edt = forcemass ? dt : dhi >= (T)0.0 ? dt : M<T>::fmin_(dt, M<T>::fmax_(hold, (T)eps_d) / M<T>::fabs_(dhi));
+#else
     T edt = forcemass ? dt : dhi >= (T)0.0 ? dt : (T)fmin((double)dt, fmax((double)hold, eps_d) / (double)M<T>::fabs_(dhi));
+#endif
     ho = hold + edt * dhi;
     if (ho > eps) {
         uo = (hold * uold + edt * dhui) / ho;

@@ -144,6 +144,7 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.sparams = nullptr;
     m.lead = nullptr;
     m.hmax = nullptr;
+    m.checklev = 0;
     m.datum = h->split ? (const T*)h->d_datum : nullptr;
     return m;
 }

@@ -63,7 +63,7 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
     if (tid < 128) {
         int x, y, sb, sx, sy;
         ring_pos(tid, x, y);
-        if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy)) {
+        if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy, m.checklev != 0)) {
             atomicOr(m.err, 1);
             sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
         }
@@ -95,7 +95,7 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
             x = k & 15; y = k >> 4; sx = x; sy = y;
         } else {
             ring_pos(k - 256, x, y);
-            if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy)) {
+            if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy, m.checklev != 0)) {
                 atomicOr(m.err, 1);
                 sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
             }
@@ -141,7 +141,7 @@ template <class T> struct Occ {
 // In a batched pool every block belongs to a scenario with its own parameters,
 // time slot and dt minimum (the segmented CFL reduction).
 
-template <class T, int ENGINE, bool SPLIT>
+template <class T, int ENGINE, bool SPLIT, bool POOL>
 __global__ void __launch_bounds__(NTHREADS, Occ<T>::flux) flux_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -149,10 +149,10 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::flux) flux_kernel(DevModel<T
     const int tid = threadIdx.x;
     for (int w = blockIdx.x; w < m.nblk; w += gridDim.x) {
         const int ib = m.active[w];
-        const int sc = scen_of(m, ib);
+        const int sc = POOL ? m.scen[ib] : 0;
         const TimeState ts = m.time[2 * sc + parity];
         if (!step_live(ts)) continue;
-        const StepParams<T> p = params_of(m, p0, sc);
+        const StepParams<T>& p = params_ref<POOL>(m, p0, sc);
         const T delta = calcres<T>(p.delta0, m.level[ib]);
         const int cur = ts.cur;
         const T D = SPLIT ? m.datum[ib] : (T)0;
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::flux) flux_kernel(DevModel<T
     }
 }
 
-template <class T, int ENGINE, bool SPLIT>
+template <class T, int ENGINE, bool SPLIT, bool POOL>
 __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -200,9 +200,9 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
     const int tid = threadIdx.x;
     for (int w = blockIdx.x; w < m.nblk; w += gridDim.x) {
         const int ib = m.active[w];
-        const int sc = scen_of(m, ib);
+        const int sc = POOL ? m.scen[ib] : 0;
         const TimeState ts = m.time[2 * sc + parity];
-        const bool lead = lead_of(m, ib, w);
+        const bool lead = POOL ? m.lead[ib] != 0 : w == 0;
         if (!step_live(ts)) {
             if (lead && tid == 0) {
                 TimeState nt = ts;
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
             }
             continue;
         }
-        const StepParams<T> p = params_of(m, p0, sc);
+        const StepParams<T>& p = params_ref<POOL>(m, p0, sc);
         const T delta = calcres<T>(p.delta0, m.level[ib]);
         const int cur = ts.cur;
         const T dt = step_dt<T>(ts, m.dtmin[2 * sc + parity]);
@@ -324,16 +324,23 @@ template <class T> __global__ void volume_kernel(DevModel<T> m, T delta0, int cu
 
 template <class T> size_t smem_bytes() { return sizeof(Smem<T>); }
 
-template <class T, int ENGINE> cudaError_t configure_engine()
+template <class T, int ENGINE, bool SPLIT, bool POOL> cudaError_t configure_one()
 {
     const int sm = (int)smem_bytes<T>();
-    cudaError_t e = cudaFuncSetAttribute(flux_kernel<T, ENGINE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(update_kernel<T, ENGINE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(flux_kernel<T, ENGINE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(update_kernel<T, ENGINE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaError_t e = cudaFuncSetAttribute(flux_kernel<T, ENGINE, SPLIT, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(update_kernel<T, ENGINE, SPLIT, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+template <class T, int ENGINE> cudaError_t configure_engine()
+{
+    cudaError_t e = configure_one<T, ENGINE, false, false>();
+    if (e == cudaSuccess) e = configure_one<T, ENGINE, false, true>();
+    if constexpr (sizeof(T) == 4) {
+        // split precision is an FP32 mode
+        if (e == cudaSuccess) e = configure_one<T, ENGINE, true, false>();
+        if (e == cudaSuccess) e = configure_one<T, ENGINE, true, true>();
+    }
     return e;
 }
 
@@ -345,28 +352,50 @@ template <class T> cudaError_t configure_kernels()
 }
 
 // grid: CTAs of the launch (0: one per active block); fewer CTAs loop over the blocks
+template <class T, bool FLUX, int ENGINE>
+static void launch_step_kernel(const DevModel<T>& m, const StepParams<T>& p, int parity, cudaStream_t st, int g)
+{
+    const size_t sm = smem_bytes<T>();
+    const bool pool = m.scen != nullptr;
+    bool split = false;
+    if constexpr (sizeof(T) == 4) split = m.datum != nullptr;
+    if constexpr (FLUX) {
+        if constexpr (sizeof(T) == 4) {
+            if (split) {
+                if (pool) flux_kernel<T, ENGINE, true, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
+                else flux_kernel<T, ENGINE, true, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
+                return;
+            }
+        }
+        if (pool) flux_kernel<T, ENGINE, false, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
+        else flux_kernel<T, ENGINE, false, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
+    } else {
+        if constexpr (sizeof(T) == 4) {
+            if (split) {
+                if (pool) update_kernel<T, ENGINE, true, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
+                else update_kernel<T, ENGINE, true, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
+                return;
+            }
+        }
+        if (pool) update_kernel<T, ENGINE, false, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
+        else update_kernel<T, ENGINE, false, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
+    }
+}
+
 template <class T>
 void launch_flux(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st, int grid)
 {
     const int g = grid > 0 && grid < m.nblk ? grid : m.nblk;
-    const size_t sm = smem_bytes<T>();
-    if (m.datum) {
-        if (engine == 1) flux_kernel<T, 1, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
-        else flux_kernel<T, 2, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
-    } else if (engine == 1) flux_kernel<T, 1, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
-    else flux_kernel<T, 2, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
+    if (engine == 1) launch_step_kernel<T, true, 1>(m, p, parity, st, g);
+    else launch_step_kernel<T, true, 2>(m, p, parity, st, g);
 }
 
 template <class T>
 void launch_update(const DevModel<T>& m, const StepParams<T>& p, int engine, int parity, cudaStream_t st, int grid)
 {
     const int g = grid > 0 && grid < m.nblk ? grid : m.nblk;
-    const size_t sm = smem_bytes<T>();
-    if (m.datum) {
-        if (engine == 1) update_kernel<T, 1, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
-        else update_kernel<T, 2, true><<<g, NTHREADS, sm, st>>>(m, p, parity);
-    } else if (engine == 1) update_kernel<T, 1, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
-    else update_kernel<T, 2, false><<<g, NTHREADS, sm, st>>>(m, p, parity);
+    if (engine == 1) launch_step_kernel<T, false, 1>(m, p, parity, st, g);
+    else launch_step_kernel<T, false, 2>(m, p, parity, st, g);
 }
 
 template <class T>

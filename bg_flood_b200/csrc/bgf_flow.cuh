@@ -96,6 +96,7 @@ template <class T> struct DevModel {
     const uint8_t* lead;              // per block slot: 1 for the first block of its scenario
     T* hmax;                          // per cell (256 per block): running maximum depth, or null
     const T* datum;                   // per block slot: datum depth of split mode, or null
+    int checklev;                     // fused kernels: verify that neighbours share the block's level
 };
 
 // Positive floating-point values order like their bit patterns.
@@ -117,8 +118,11 @@ __device__ __forceinline__ int fyi(int x, int y) { return y * 16 + x; }         
 // and whose value gradientHalo uses as the outer stencil point for ring 2
 // (src/Gradients.cu:2713-3290).  At a domain edge (neighbour == self) both rings
 // take the block's own edge cell.  Returns false for cross-level sides.
+// checklev: also verify that the neighbour is on the block's level (callers that
+// cannot know the mesh is single-level); the handle path knows it and skips the
+// dependent level loads.
 __device__ __forceinline__ bool tile_source(const int* nbr, int nblkmem, const int* level, int ib, int x, int y,
-                                            int& sb, int& sx, int& sy)
+                                            int& sb, int& sx, int& sy, bool checklev = true)
 {
     sb = ib;
     sx = x;
@@ -126,22 +130,22 @@ __device__ __forceinline__ bool tile_source(const int* nbr, int nblkmem, const i
     if (x < 0) {
         int nb = nbr[0 * nblkmem + ib];
         if (nb == ib) { sx = 0; return nbr[1 * nblkmem + ib] == ib; }
-        if (level[nb] != level[ib]) return false;
+        if (checklev && level[nb] != level[ib]) return false;
         sb = nb; sx = BW + x;
     } else if (x >= BW) {
         int nb = nbr[2 * nblkmem + ib];
         if (nb == ib) { sx = BW - 1; return nbr[3 * nblkmem + ib] == ib; }
-        if (level[nb] != level[ib]) return false;
+        if (checklev && level[nb] != level[ib]) return false;
         sb = nb; sx = x - BW;
     } else if (y < 0) {
         int nb = nbr[4 * nblkmem + ib];
         if (nb == ib) { sy = 0; return nbr[5 * nblkmem + ib] == ib; }
-        if (level[nb] != level[ib]) return false;
+        if (checklev && level[nb] != level[ib]) return false;
         sb = nb; sy = BW + y;
     } else if (y >= BW) {
         int nb = nbr[6 * nblkmem + ib];
         if (nb == ib) { sy = BW - 1; return nbr[7 * nblkmem + ib] == ib; }
-        if (level[nb] != level[ib]) return false;
+        if (checklev && level[nb] != level[ib]) return false;
         sb = nb; sy = y - BW;
     }
     return true;

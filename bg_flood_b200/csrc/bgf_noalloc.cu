@@ -111,6 +111,8 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     m.sparams = nullptr;
     m.lead = nullptr;
     m.hmax = nullptr;
+    m.checklev = 1;
+    m.datum = nullptr;
 
     StepParams<T> p;
     p.g = (T)P->g;

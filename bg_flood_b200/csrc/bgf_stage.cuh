@@ -141,6 +141,14 @@ template <class T> __device__ __forceinline__ bool lead_of(const DevModel<T>& m,
 {
     return m.lead ? m.lead[ib] != 0 : w == 0;
 }
+// The step parameters of a block: the kernel argument for a single scenario, the
+// scenario's entry of the pool's table otherwise (global memory, cached).
+template <bool POOL, class T>
+__device__ __forceinline__ const StepParams<T>& params_ref(const DevModel<T>& m, const StepParams<T>& p0, int sc)
+{
+    if constexpr (POOL) return m.sparams[sc];
+    else return p0;
+}
 
 // Whether this step runs (the reference loop condition totaltime < endtime plus
 // the step budget); identical in both kernels of a step.

@@ -88,14 +88,16 @@ __device__ __forceinline__ T wetdry_restrict(const Acc256<T>& h, const Acc324<T>
 // ---------------------------------------------------------------- stage kernels
 
 template <class T>
-__global__ void __launch_bounds__(NTHREADS) amr_halo_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+__global__ void __launch_bounds__(NTHREADS) amr_halo_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
                                                              int stage)
 {
     __shared__ T th[3][324];
-    const TimeState ts = m.time[parity];
-    if (!step_live(ts)) return;
     const int tid = threadIdx.x;
     const int ib = m.active[blockIdx.x];
+    const int sc = scen_of(m, ib);
+    const TimeState ts = m.time[2 * sc + parity];
+    if (!step_live(ts)) return;
+    const StepParams<T>& p = m.sparams ? m.sparams[sc] : p0;
     const int nbm = m.nblkmem;
     const T* src[3] = {stage == 0 ? m.h[ts.cur] : m.dh, stage == 0 ? m.u[ts.cur] : m.dhu,
                        stage == 0 ? m.v[ts.cur] : m.dhv};
@@ -146,12 +148,14 @@ __global__ void __launch_bounds__(NTHREADS) amr_halo_kernel(DevModel<T> m, AmrDe
 }
 
 template <class T>
-__global__ void __launch_bounds__(64) amr_refine_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+__global__ void __launch_bounds__(64) amr_refine_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
                                                         int stage)
 {
-    const TimeState ts = m.time[parity];
-    if (!step_live(ts)) return;
     const int ib = m.active[blockIdx.x];
+    const int sc = scen_of(m, ib);
+    const TimeState ts = m.time[2 * sc + parity];
+    if (!step_live(ts)) return;
+    const StepParams<T>& p = m.sparams ? m.sparams[sc] : p0;
     const int s = threadIdx.x >> 4, j = threadIdx.x & 15;
     int pb, px, py;
     if (!parent_cell(m.nbr, m.nblkmem, m.level, ib, s, j, pb, px, py)) return;
@@ -175,19 +179,19 @@ __global__ void __launch_bounds__(64) amr_refine_kernel(DevModel<T> m, AmrDev<T>
 // when that coarse block comes earlier in the list and its decision (made by the
 // launch for its level, which runs first) says so.
 template <class T>
-__global__ void __launch_bounds__(64) amr_wetdry_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+__global__ void __launch_bounds__(64) amr_wetdry_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
                                                         int stage, int level)
 {
-    const TimeState ts = m.time[parity];
-    if (!step_live(ts)) return;
     const int ib = m.active[blockIdx.x];
+    const TimeState ts = m.time[2 * scen_of(m, ib) + parity];
+    if (!step_live(ts)) return;
     if (m.level[ib] != level) return;
     const int nbm = m.nblkmem;
     const int s = threadIdx.x >> 4, j = threadIdx.x & 15;
     int pb, px, py;
     if (!parent_cell(m.nbr, nbm, m.level, ib, s, j, pb, px, py)) return;
     const T* H = a.W[stage][0];
-    const T eps = p.eps;
+    const T eps = (m.sparams ? m.sparams[scen_of(m, ib)] : p0).eps;
     const bool earlier = a.rank[pb] < a.rank[ib];
     auto hval = [&](int x, int y) -> T {
         const T v = H[(size_t)pb * 324 + hi18(x, y)];
@@ -214,9 +218,9 @@ template <class T>
 __global__ void __launch_bounds__(64) amr_apply_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
                                                        int stage)
 {
-    const TimeState ts = m.time[parity];
-    if (!step_live(ts)) return;
     const int ib = m.active[blockIdx.x];
+    const TimeState ts = m.time[2 * scen_of(m, ib) + parity];
+    if (!step_live(ts)) return;
     const int s = threadIdx.x >> 4, j = threadIdx.x & 15;
     int pb, px, py;
     if (!parent_cell(m.nbr, m.nblkmem, m.level, ib, s, j, pb, px, py)) return;
@@ -233,16 +237,18 @@ __global__ void __launch_bounds__(64) amr_apply_kernel(DevModel<T> m, AmrDev<T> 
 }
 
 template <class T, int ENGINE>
-__global__ void __launch_bounds__(NTHREADS, 3) amr_flux_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+__global__ void __launch_bounds__(NTHREADS, 3) amr_flux_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
                                                                int stage)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
     __shared__ SubFaces<T> sub;
-    const TimeState ts = m.time[parity];
-    if (!step_live(ts)) return;
     const int tid = threadIdx.x;
     const int ib = m.active[blockIdx.x];
+    const int sc = scen_of(m, ib);
+    const TimeState ts = m.time[2 * sc + parity];
+    if (!step_live(ts)) return;
+    const StepParams<T>& p = m.sparams ? m.sparams[sc] : p0;
     const int nbm = m.nblkmem;
     const T delta = calcres<T>(p.delta0, m.level[ib]);
     T* const* W = a.W[stage];
@@ -314,31 +320,34 @@ __global__ void __launch_bounds__(NTHREADS, 3) amr_flux_kernel(DevModel<T> m, Am
         if (tid == 0) {
             T b = s.red[0];
             for (int k = 1; k < NTHREADS / 32; k++) b = s.red[k] < b ? s.red[k] : b;
-            atomicMin(&m.dtmin[parity], dt_bits(b));
+            atomicMin(&m.dtmin[2 * sc + parity], dt_bits(b));
         }
     }
 }
 
 template <class T, int ENGINE>
-__global__ void __launch_bounds__(NTHREADS, 3) amr_update_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p, int parity,
+__global__ void __launch_bounds__(NTHREADS, 3) amr_update_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
                                                                  int stage)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
-    const TimeState ts = m.time[parity];
     const int tid = threadIdx.x;
+    const int ib = m.active[blockIdx.x];
+    const int sc = scen_of(m, ib);
+    const bool lead = lead_of(m, ib, blockIdx.x);
+    const TimeState ts = m.time[2 * sc + parity];
     if (!step_live(ts)) {
-        if (stage == 1 && blockIdx.x == 0 && tid == 0) {
+        if (stage == 1 && lead && tid == 0) {
             TimeState nt = ts;
             nt.done = 1;
-            m.time[parity ^ 1] = nt;
+            m.time[2 * sc + (parity ^ 1)] = nt;
         }
         return;
     }
-    const int ib = m.active[blockIdx.x];
+    const StepParams<T>& p = m.sparams ? m.sparams[sc] : p0;
     const int nbm = m.nblkmem;
     const T delta = calcres<T>(p.delta0, m.level[ib]);
-    const T dt = step_dt<T>(ts, m.dtmin[parity]);
+    const T dt = step_dt<T>(ts, m.dtmin[2 * sc + parity]);
     const double dtd = (double)dt;
     const size_t base = (size_t)ib * 324;
     const size_t fb = (size_t)ib * NFX;
@@ -405,7 +414,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) amr_update_kernel(DevModel<T> m, 
     if (p.has_rain) {
         // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580), uniform rain at the
         // start of the step
-        const double rnow = series_at(m.rain_t, m.rain_r, p.rain_n, ts.totaltime);
+        const double rnow = series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime);
         T Rainhh = (T)rnow;
         const T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
         Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
@@ -421,7 +430,8 @@ __global__ void __launch_bounds__(NTHREADS, 3) amr_update_kernel(DevModel<T> m, 
     m.h[nxt][g] = ho;
     m.u[nxt][g] = uo;
     m.v[nxt][g] = vo;
-    if (blockIdx.x == 0 && tid == 0) m.time[parity ^ 1] = next_time_state<T>(ts, p, dtd, nxt, m.dtmin, parity);
+    if (m.hmax) m.hmax[g] = ho > m.hmax[g] ? ho : m.hmax[g];
+    if (lead && tid == 0) m.time[2 * sc + (parity ^ 1)] = next_time_state<T>(ts, p, dtd, nxt, m.dtmin + 2 * sc, parity);
 }
 
 // ---------------------------------------------------------------- bed preparation

@@ -87,3 +87,44 @@ def test_pool_tracks_maximum_depth():
     h, hmax = pool.depth(s, mesh.nblk, with_max=True)
     assert np.all(hmax >= h) and np.all(hmax >= h0)
     assert float((hmax - h).max()) > 0.0
+
+
+def test_pool_with_multilevel_scenarios():
+    """Adapted (2- and 3-level) and single-level scenarios in one pool: the pool takes
+    the multi-level chain, and every result still equals the one run alone."""
+    import os
+    from runners import make_gpu_amr
+    golden = os.path.join(os.path.dirname(__file__), "golden")
+
+    def amr(name, mk):
+        g = np.load(os.path.join(golden, f"{name}.npz"))
+        return lambda: make_gpu_amr(mk(), (g["level"], g["nbr"], g["xo"], g["yo"]))
+
+    def single(mk):
+        def b():
+            f, mesh, loop = make_gpu(mk())
+            return f, loop
+        return b
+
+    members = [
+        (amr("amrhump64_e1_l1", lambda: cases.amr_hump(64, 1, 1, 0.3)), 45),
+        (amr("amrdam64_e1_l2", lambda: cases.amr_dambreak(64, 1, 2)), 30),
+        (single(lambda: cases.dam_break(48, 1)), 50),
+        (single(lambda: cases.gauss(32, 1, 0)), 35),
+    ]
+    ref = []
+    for build, n in members:
+        f, loop = build()
+        assert f.run(loop, endtime=ENDTIME, maxsteps=n) == n
+        ref.append((f.get_state(), loop))
+    pool = ScenarioPool(cases.dam_break(48, 1).param, 4096, 4)
+    slots = []
+    for build, n in members:
+        f, loop = build()
+        slots.append(pool.admit(f, loop, ENDTIME, maxsteps=n))
+    assert pool.run(100000) == 0
+    for s, (st, loop_a), (_, n) in zip(slots, ref, members):
+        f, loop, nn = pool.retire(s)
+        assert nn == n and loop.totaltime == loop_a.totaltime and loop.dt == loop_a.dt
+        for a, b in zip(f.get_state()[1:], st[1:]):
+            assert np.array_equal(interior(a), interior(b))

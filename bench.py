@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--engine", type=int, default=1)
     ap.add_argument("--fastmath", type=int, default=1, help="1: fast-math kernels, 0: bit-exact kernels")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--amr", type=int, default=1024, help="level-0 cells per side of the AMR measurement (0: skip)")
     ap.add_argument("--ensemble", type=int, default=64, help="members of the batched-ensemble measurement (0: skip)")
     ap.add_argument("--ens-max-blocks", type=int, default=16384)
     ap.add_argument("--serve", type=int, default=48, help="requests of the serving measurement (0: skip)")
@@ -249,6 +250,46 @@ def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, step
             "cell_updates_per_s_batched": sum(blocks) * 256 * steps / (batched_ms / 1e3)}
 
 
+def amr_bench(n0: int, maxlevel: int, steps: int, dev: int, fastmath: int):
+    """Quadtree rain-on-grid: seeded fractal terrain (0-300 m relief) on an n0 x n0
+    level-0 grid (dx = 10 m), refined by the library's own adaptation pass up to
+    maxlevel where the bed lies in the lowest 60 m (Inrange criterion), rain of 50
+    mm/h, Manning n = 0.035; the device loop's cell-updates/s over all levels."""
+    import cases
+    from bg_flood_b200.adapt import Criterion, INRANGE
+    from bg_flood_b200.flow import FlowB200, Loop
+    from bg_flood_b200.mesh import boundary_segments, grid_to_buq, uniform_mesh
+    case = cases.rain_on_terrain(n0, engine=1, dx=10.0, seed=11)
+    case.param.GPUDEVICE = dev
+    case.param.fastmath = fastmath
+    case.param.maxlevel, case.param.minlevel, case.param.initlevel = maxlevel, 0, 0
+    mesh = uniform_mesh(n0, n0, case.dx)
+    mem = mesh.nblk * (4 ** maxlevel)
+    f = FlowB200(case.param, mem)
+    f.set_blocks(mesh.active, mesh.level, mesh.nbr, mesh.xo, mesh.yo)
+    pad = lambda a: np.concatenate([a, np.zeros((mem - len(a), 18, 18), a.dtype)])
+    f.set_bed(pad(grid_to_buq(case.zb, mesh)))
+    for typ, times, levels, sides in boundary_segments(mesh, case.param.segments, case.param.aoibnd, 0.0, 0.0):
+        f.add_segment(typ, times, levels, sides)
+    f.set_rain(*case.rain)
+    z = np.zeros_like(case.zb)
+    f.set_state(*(pad(grid_to_buq(a, mesh)) for a in (case.h, z, z)))
+    f.set_bathy(0.5 * case.dx, 0.5 * case.dx, case.dx, case.zb)
+    t0 = time.perf_counter()
+    nblk, it = f.adapt(Criterion(INRANGE, "zb", 0.0, 60.0), maxiteration=maxlevel + 1)
+    adapt_s = time.perf_counter() - t0
+    act, lev, _, _, _ = f.get_blocks()
+    hist = np.bincount(lev[act], minlength=maxlevel + 1).tolist()
+    loop = Loop(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=1e30)
+    f.init_dt(loop)
+    f.run(loop, endtime=1e30, maxsteps=10)
+    f.run(loop, endtime=1e30, maxsteps=steps)
+    ms, launches = f.last_run_timing()
+    return {"level0_cells": n0 * n0, "blocks": int(nblk), "blocks_per_level": hist, "adapt_passes": it,
+            "adapt_s": adapt_s, "steps": steps, "ms": ms, "launches_per_step": launches / steps,
+            "cell_updates_per_s": nblk * 256 * steps / (ms / 1e3)}
+
+
 def serving_bench(nreq: int, seed: int, rate: float, dev: int, fastmath: int, budget_gb: float = 150.0):
     """Poisson stream of flood scenarios (blocks log-uniform in [16, 2048], 100-400
     steps each) served by the continuous-batching server under an HBM budget, and by
@@ -417,6 +458,8 @@ def main():
         msb, _ = fb.last_run_timing()
         extra["device_loop_4096x4096"] = {"value": mb.nblk * 256 * 100 / (msb / 1e3), "steps": 100, "ms": msb}
         del fb
+        if args.amr > 0:
+            extra["amr_rain_on_grid"] = amr_bench(args.amr, 2, 100, local, args.fastmath)
         if args.ensemble > 0:
             extra["ensemble"] = ensemble_bench(args.ensemble, 2024, 64, args.ens_max_blocks, 100, local,
                                                args.fastmath)

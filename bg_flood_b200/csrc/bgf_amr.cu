@@ -363,10 +363,11 @@ __global__ void __launch_bounds__(NTHREADS, 3) amr_update_kernel(DevModel<T> m, 
     }
     // state n on the 18x18 tile (boundary segments, full-step advance) and the bed
     for (int k = tid; k < 324; k += NTHREADS) {
-        s.zb[k] = a.zb[base + k];
-        s.h0[k] = a.W[0][0][base + k];
-        s.u0[k] = a.W[0][2][base + k];
-        s.v0[k] = a.W[0][3][base + k];
+        const int q = si(k % 18 - 1, k / 18 - 1);
+        s.zb[q] = a.zb[base + k];
+        s.h0[q] = a.W[0][0][base + k];
+        s.u0[q] = a.W[0][2][base + k];
+        s.v0[q] = a.W[0][3][base + k];
     }
     __syncthreads();
     // HaloFluxCPULR / HaloFluxCPUBT (src/Halo.cu:1441-1540, 1766-1850): the faces of
@@ -393,11 +394,11 @@ __global__ void __launch_bounds__(NTHREADS, 3) amr_update_kernel(DevModel<T> m, 
     apply_boundaries<T>(s, m, p, ib, stage == 0 ? ts.totaltime + ts.dt * 0.5 : ts.totaltime + dtd, tid);
     __syncthreads();
     const int x = tid & 15, y = tid >> 4;
-    const int c18 = hi18(x, y);
+    const int c18 = hi18(x, y), q18 = si(x, y);
     const T hs = a.W[stage][0][base + c18], us = a.W[stage][2][base + c18], vs = a.W[stage][3][base + c18];
     T dh, dhu, dhv;
     flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, hs, us, vs, dh, dhu, dhv);
-    const T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];
+    const T hold = s.h0[q18], uold = s.u0[q18], vold = s.v0[q18];
     const size_t g = (size_t)ib * 256 + tid;
     T ho, uo, vo;
     if (stage == 0) {

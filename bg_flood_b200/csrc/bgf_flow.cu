@@ -29,7 +29,7 @@ template <class T, bool SPLIT>
 __device__ __forceinline__ T tile_zb(const Smem<T>& s, const DevModel<T>& m, int x, int y, int sb, int sx, int sy, T D)
 {
     bool ring2 = x < -1 || x > BW || y < -1 || y > BW;
-    if (!ring2) return s.zb[hi18(x, y)];
+    if (!ring2) return s.zb[si(x, y)];
     const T z = m.zb[(size_t)sb * 324 + hi18(sx, sy)];
     return SPLIT ? z + D : z;
 }
@@ -56,8 +56,8 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
         T hv = H[g], uv = U[g], vv = V[g];
         int c = ti(x, y);
         s.t[VH][c] = hv; s.t[VU][c] = uv; s.t[VV][c] = vv;
-        s.t[VZS][c] = s.zb[hi18(x, y)] + hv;
-        int c18 = hi18(x, y);
+        s.t[VZS][c] = s.zb[si(x, y)] + hv;
+        int c18 = si(x, y);
         s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
     }
     if (tid < 128) {
@@ -73,7 +73,7 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
         s.t[VH][c] = hv; s.t[VU][c] = uv; s.t[VV][c] = vv;
         s.t[VZS][c] = tile_zb<T, SPLIT>(s, m, x, y, sb, sx, sy, D) + hv;
         if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
-            int c18 = hi18(x, y);
+            int c18 = si(x, y);
             s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
         }
     }
@@ -115,7 +115,7 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
         s.t[VH][c] = ho; s.t[VU][c] = uo; s.t[VV][c] = vo;
         s.t[VZS][c] = tile_zb<T, SPLIT>(s, m, x, y, sb, sx, sy, D) + ho;
         if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
-            int c18 = hi18(x, y);
+            int c18 = si(x, y);
             s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
         }
     }
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
         flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, SPLIT ? D + s.t[VH][c] : s.t[VH][c], s.t[VU][c],
                            s.t[VV][c], dh, dhu, dhv);
         // full step from state n (AdvkernelCPU with evolv), then friction on the result
-        const int c18 = hi18(x, y);
+        const int c18 = si(x, y);
         T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];
         T ho, uo, vo;
         if (SPLIT) advance_split<T>(dt, p.eps, p.forcemass != 0, D, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);

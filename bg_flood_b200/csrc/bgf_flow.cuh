@@ -106,12 +106,31 @@ template <class T> __device__ __forceinline__ T dt_from_bits(unsigned long long 
 template <> __device__ __forceinline__ float dt_from_bits<float>(unsigned long long b) { return __uint_as_float((unsigned int)b); }
 template <> __device__ __forceinline__ double dt_from_bits<double>(unsigned long long b) { return __longlong_as_double((long long)b); }
 
-__device__ __forceinline__ int ti(int x, int y) { return (y + 2) * TW + (x + 2); }
-__device__ __forceinline__ int hi18(int x, int y) { return (y + 1) * 18 + (x + 1); }  // memloc within a tile
-__device__ __forceinline__ int gxi(int x, int y) { return y * 18 + (x + 1); }          // x-gradients, x=-1..16
-__device__ __forceinline__ int gyi(int x, int y) { return (y + 1) * 16 + x; }          // y-gradients, y=-1..16
-__device__ __forceinline__ int fxi(int x, int y) { return y * 17 + x; }                // X faces x=0..16
-__device__ __forceinline__ int fyi(int x, int y) { return y * 16 + x; }                // Y faces y=0..16
+// Global BUQ tile index (memloc within a block).
+__device__ __forceinline__ int hi18(int x, int y) { return (y + 1) * 18 + (x + 1); }
+
+// Shared-memory layouts.  A warp covers two rows of 16 cells (tx, ty), so a row
+// pair is free of bank conflicts when the two rows start 16 words apart modulo 32
+// words; interior rows are therefore stored with stride 16 (or in even/odd halves
+// for the 20-wide tile) and edge columns apart.
+constexpr int TODD = 336;   // first odd row of the 20x20 tile (16 modulo 32 words)
+constexpr int TSIZE = 656;  // words of one 20x20 tile variable
+__device__ __forceinline__ int ti(int x, int y)  // 20x20 tile, x, y = -2..17
+{
+    const int Y = y + 2;
+    return ((Y & 1) ? TODD : 0) + (Y >> 1) * 32 + (x + 2);
+}
+__device__ __forceinline__ int si(int x, int y)  // 18x18 tile, x, y = -1..16
+{
+    return (x >= 0 && x < BW) ? (y + 1) * 16 + x : (x < 0 ? 288 : 306) + (y + 1);
+}
+__device__ __forceinline__ int gxi(int x, int y)  // x-gradients, x = -1..16, y = 0..15
+{
+    return (x >= 0 && x < BW) ? y * 16 + x : (x < 0 ? 256 : 272) + y;
+}
+__device__ __forceinline__ int gyi(int x, int y) { return (y + 1) * 16 + x; }  // y-gradients, y = -1..16
+__device__ __forceinline__ int fxi(int x, int y) { return x < BW ? y * 16 + x : 256 + y; }  // X faces x = 0..16
+__device__ __forceinline__ int fyi(int x, int y) { return y * 16 + x; }                     // Y faces y = 0..16
 
 // Source cell of tile position (x, y) for a single-level neighbourhood: the
 // interior cell whose value fillHalo copies into ring 1 (src/Halo.cu:2083-2286)
@@ -165,8 +184,8 @@ __device__ __forceinline__ void ring_pos(int k, int& x, int& y)
 enum { VH = 0, VZS = 1, VU = 2, VV = 3 };
 
 template <class T> struct Smem {
-    T t[4][TW * TW];           // h, zs, u, v on the 20x20 tile
-    T zb[18 * 18];
+    T t[4][TSIZE];             // h, zs, u, v on the 20x20 tile (layout ti)
+    T zb[18 * 18];             // layout si
     T gx[4][18 * 16];          // x-gradients at x=-1..16, rows 0..15
     T gy[4][16 * 18];          // y-gradients at y=-1..16, cols 0..15
     T dzbx[18 * 16], dzby[16 * 18];
@@ -229,7 +248,7 @@ __device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p,
     f.hi = s.t[VH][ci]; f.hn = s.t[VH][cn];
     f.zsi = s.t[VZS][ci]; f.zsn = s.t[VZS][cn];
     if (isx) {
-        int gi = gxi(x, y), gn = gi - 1;
+        int gi = gxi(x, y), gn = gxi(x - 1, y);
         f.uni = s.t[VU][ci]; f.unn = s.t[VU][cn]; f.uti = s.t[VV][ci]; f.utn = s.t[VV][cn];
         f.dhi = s.gx[VH][gi]; f.dhn = s.gx[VH][gn]; f.dzsi = s.gx[VZS][gi]; f.dzsn = s.gx[VZS][gn];
         f.duni = s.gx[VU][gi]; f.dunn = s.gx[VU][gn]; f.duti = s.gx[VV][gi]; f.dutn = s.gx[VV][gn];
@@ -242,8 +261,8 @@ __device__ __forceinline__ Face<T> tile_face(Smem<T>& s, const StepParams<T>& p,
     f.hsi = f.hi;
     f.hsn = f.hn;
     if (ENGINE == 1) {
-        f.zbi = s.zb[hi18(x, y)];
-        f.zbn = isx ? s.zb[hi18(x - 1, y)] : s.zb[hi18(x, y - 1)];
+        f.zbi = s.zb[si(x, y)];
+        f.zbn = isx ? s.zb[si(x - 1, y)] : s.zb[si(x, y - 1)];
         f.zsrci = f.zbi;
         f.zsrcn = f.zbn;
     } else {
@@ -290,20 +309,19 @@ __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T d
         for (int k = 0; k < 4; k++) {
             const T* a = s.t[k];
             s.gx[k][gi] = div_by(minmod2(theta, a[c - 1], a[c], a[c + 1]), delta, rdelta);
-            s.gy[k][gj] = div_by(minmod2(theta, a[c - TW], a[c], a[c + TW]), delta, rdelta);
+            s.gy[k][gj] = div_by(minmod2(theta, a[ti(tx, ty - 1)], a[c], a[ti(tx, ty + 1)]), delta, rdelta);
         }
         // one ring gradient per thread: ring cell r = tid/4 (64 cells), variable tid%4;
         // x-gradients on the left/right ring columns, y-gradients on the bottom/top rows
         const int r = tid >> 2, k = tid & 3, side = r >> 4, q = r & 15;
         const T* a = s.t[k];
-        int cr, st, o;
+        int cm, cr, cp;
         T* out;
-        if (side == 0) { cr = ti(-1, q); st = 1; out = &s.gx[k][gxi(-1, q)]; }
-        else if (side == 1) { cr = ti(BW, q); st = 1; out = &s.gx[k][gxi(BW, q)]; }
-        else if (side == 2) { cr = ti(q, -1); st = TW; out = &s.gy[k][gyi(q, -1)]; }
-        else { cr = ti(q, BW); st = TW; out = &s.gy[k][gyi(q, BW)]; }
-        (void)o;
-        *out = div_by(minmod2(theta, a[cr - st], a[cr], a[cr + st]), delta, rdelta);
+        if (side == 0) { cm = ti(-2, q); cr = ti(-1, q); cp = ti(0, q); out = &s.gx[k][gxi(-1, q)]; }
+        else if (side == 1) { cm = ti(BW - 1, q); cr = ti(BW, q); cp = ti(BW + 1, q); out = &s.gx[k][gxi(BW, q)]; }
+        else if (side == 2) { cm = ti(q, -2); cr = ti(q, -1); cp = ti(q, 0); out = &s.gy[k][gyi(q, -1)]; }
+        else { cm = ti(q, BW - 1); cr = ti(q, BW); cp = ti(q, BW + 1); out = &s.gy[k][gyi(q, BW)]; }
+        *out = div_by(minmod2(theta, a[cm], a[cr], a[cp]), delta, rdelta);
     }
     __syncthreads();
     if (ENGINE == 1) {
@@ -314,8 +332,9 @@ __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T d
         {
             const int c = ti(tx, ty), gi = gxi(tx, ty), gj = gyi(tx, ty);
             const T hc = SPLIT ? D + hh[c] : hh[c];
+            const T zsm = zs[ti(tx, ty - 1)];
             s.gx[VZS][gi] = wetslope(delta, zs[c], hc, zs[c - 1], zs[c + 1], s.gx[VZS][gi], s.gx[VH][gi], s.dzbx[gi]);
-            s.gy[VZS][gj] = wetslope(delta, zs[c], hc, zs[c - TW], zs[c - TW], s.gy[VZS][gj], s.gy[VH][gj], s.dzby[gj]);
+            s.gy[VZS][gj] = wetslope(delta, zs[c], hc, zsm, zsm, s.gy[VZS][gj], s.gy[VH][gj], s.dzby[gj]);
         }
         if (tid < 64) {
             const int side = tid >> 4, q = tid & 15;
@@ -326,7 +345,8 @@ __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T d
             } else {
                 const int y = side == 2 ? -1 : BW, c = ti(q, y), g = gyi(q, y);
                 const T hc = SPLIT ? D + hh[c] : hh[c];
-                s.gy[VZS][g] = wetslope(delta, zs[c], hc, zs[c - TW], zs[c + TW], s.gy[VZS][g], s.gy[VH][g], s.dzby[g]);
+                s.gy[VZS][g] = wetslope(delta, zs[c], hc, zs[ti(q, y - 1)], zs[ti(q, y + 1)], s.gy[VZS][g], s.gy[VH][g],
+                                        s.dzby[g]);
             }
         }
         __syncthreads();

@@ -12,13 +12,16 @@ template <class T, int ENGINE, bool SPLIT = false>
 __device__ __forceinline__ void load_bed(Smem<T>& s, const DevModel<T>& m, int ib, int tid, T D = (T)0)
 {
     const T* zbt = m.zb + (size_t)ib * 324;
-    for (int k = tid; k < 324; k += NTHREADS) s.zb[k] = SPLIT ? zbt[k] + D : zbt[k];
+    for (int k = tid; k < 324; k += NTHREADS) {
+        const int x = k % 18 - 1, y = k / 18 - 1;
+        s.zb[si(x, y)] = SPLIT ? zbt[k] + D : zbt[k];
+    }
     if (ENGINE == 1) {
         const T* gx = m.dzbdx + (size_t)ib * 324;
         const T* gy = m.dzbdy + (size_t)ib * 324;
         for (int k = tid; k < 18 * 16; k += NTHREADS) {
             int x = k % 18 - 1, y = k / 18;
-            s.dzbx[k] = gx[hi18(x, y)];
+            s.dzbx[gxi(x, y)] = gx[hi18(x, y)];
             int xx = k % 16, yy = k / 16 - 1;
             s.dzby[k] = gy[hi18(xx, yy)];
         }
@@ -66,7 +69,7 @@ __device__ __forceinline__ void apply_boundaries(Smem<T>& s, const DevModel<T>& 
     T sign = (T)isright + (T)istop;
     float zsb = (float)zsbnd;
     zsb = (float)((double)zsb + p.zsoffset);
-    int ci = hi18(ix, iy), cin = hi18(inx, iny);
+    int ci = si(ix, iy), cin = si(inx, iny);
     T zsi = s.zb[ci] + s.h0[ci];
     T zsinside = s.zb[cin] + s.h0[cin];
     // (split mode: the tile holds deviations; zs = zb' + h' is the surface either way)
@@ -121,7 +124,7 @@ __device__ __forceinline__ void flux_divergence(const Smem<T>& s, const StepPara
 {
     // Cartesian grid: the metric terms dmdl, dmdt and fG of the reference are zero
     // and their products only add signed zeros.
-    int fi = fxi(x, y), fr = fi + 1;
+    int fi = fxi(x, y), fr = fxi(x + 1, y);
     int gi = fyi(x, y), gt = gi + 16;
     dh = (T)-1.0 * (s.Fhu[fr] - s.Fhu[fi] + s.Fhv[gt] - s.Fhv[gi]) * cmdinv;
     dhu = (s.Fqux[fi] + s.Fquy[gi] - s.Su[fr] - s.Fquy[gt]) * cmdinv + p.fc * hi * vvi;

@@ -394,11 +394,9 @@ def main():
     launches = f.kernel_launches() - launches0
     f.set_profiling(False)
     step_ms = (flux_ms + update_ms) / max(nprof, 1)
-    tot_ms = torch.tensor([flux_ms + update_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(tot_ms, op=dist.ReduceOp.MAX)
-    tmax_s = float(tot_ms.item()) / 1e3
-    value = world * ncell * args.steps / tmax_s
+    from bg_flood_b200.replicas import replica_throughput
+    value, tmax_ms = replica_throughput(ncell * args.steps, flux_ms + update_ms, dist if world > 1 else None,
+                                        device=f"cuda:{local}")
 
     # dominant kernel roofline
     peak, peak_kind = measured_peak_hbm()

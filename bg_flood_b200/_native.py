@@ -62,6 +62,13 @@ SIGNATURES = {
     "bgf_pool_get_depth": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p]),
     "bgf_pool_timing": (ctypes.c_int, [c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64), c_int_p]),
     "bgf_pool_set_grid": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "bgf_read_asc_head": (ctypes.c_int, [ctypes.c_char_p, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p,
+                                         c_double_p]),
+    "bgf_read_asc": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, c_void_p]),
+    "bgf_mask_blocks": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_double, c_void_p, c_int_p]),
+    "bgf_interp_bathy": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, c_void_p]),
     "bgf_refine_sanity": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_int_p, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, c_void_p, c_void_p]),
     "bgf_refine_tables": (ctypes.c_int, [c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, ctypes.c_int,

@@ -33,6 +33,7 @@ SOURCES = [
     ("bgf_noalloc.cu", "bgf_noalloc.o", ["--fmad=false"]),
     ("bgf_host.cpp", "bgf_host.o", ["-x", "cu", "--fmad=false"]),
     ("bgf_adapt_host.cpp", "bgf_adapt_host.o", ["-x", "cu", "--fmad=false"]),
+    ("bgf_io.cpp", "bgf_io.o", ["-x", "cu", "--fmad=false"]),
 ]
 
 

@@ -36,6 +36,7 @@ class BndSegmentSpec:
     type: int
     times: list = field(default_factory=list)
     levels: list = field(default_factory=list)
+    file: str = ""  # uniform water-level series file ("time value" lines)
 
 
 @dataclass
@@ -87,9 +88,13 @@ class Param:
     adaptmaxiteration: int = 20
     AdaptCrit: str = ""
     Adapt_args: list = field(default_factory=list)
+    posdown: int = 0
+    grdalpha: float = math.nan
+    reftime: str = ""
     # forcing-side keys the path uses (reference Forcing class)
     segments: list = field(default_factory=list)
     rain: str = ""
+    bathy: list = field(default_factory=list)  # bathymetry files, first one the base grid
 
     @property
     def delta(self) -> float:
@@ -153,7 +158,13 @@ _KEYS = [
     ("ForceMassConserve", bool, ["ForceMassConserve", "MassConservation", "MassCon", "forcemassconservation",
                                   "forcevolumeconservation", "Volumeconservation", "VolumeCon", "ForceVolConserve"]),
     ("adaptmaxiteration", int, ["adaptmaxiteration", "maxiterationadapt"]),
+    ("posdown", int, ["posdown"]),
+    ("grdalpha", float, ["grdalpha"]),
+    ("reftime", str, ["reftime", "referencetime", "timeref"]),
 ]
+
+# bathymetry file keys (readparamstr for Forcing, src/ReadInput.cu:899-906)
+_BATHY_KEYS = ("bathy", "bathyfile", "bathymetry", "depfile", "depthfile", "topofile", "topo", "dem")
 
 
 def _split_line(line: str):
@@ -195,12 +206,19 @@ def read_param_text(text: str, param: Param | None = None) -> Param:
         if k in ("left", "leftbndfile", "leftbnd", "right", "rightbndfile", "rightbnd", "top", "topbndfile",
                  "topbnd", "bot", "botbndfile", "botbnd", "bottom"):
             side = {"l": "left", "r": "right", "t": "top", "b": "bot"}[k[0]]
-            items = [s.strip() for s in val.split(",")]
+            # readbndlineside (src/ReadInput.cu:1952-2005): "type" or "type,file" / "file,type"
+            items = [s.strip() for s in val.split(",") if s.strip()]
             if len(items) == 1:
                 p.segments.append(BndSegmentSpec(side, int(items[0])))
             else:
-                typ = int(items[1]) if items[1][:1].isdigit() else int(items[0])
-                p.segments.append(BndSegmentSpec(side, typ))
+                if items[1][:1].isdigit():
+                    typ, fname = int(items[1]), items[0]
+                else:
+                    typ, fname = int(items[0]), items[1]
+                p.segments.append(BndSegmentSpec(side, typ, file=fname))
+            continue
+        if k in _BATHY_KEYS:
+            p.bathy.append(val)
             continue
         if k in ("adaptation", "adapt"):
             items = [s.strip() for s in val.split(",")]

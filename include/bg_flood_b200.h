@@ -254,6 +254,46 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* args, bgf_
 int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* present, int* nblk, int* level,
                      int* nbr8, double* xo, double* yo, int doubleprecision);
 
+/* ------------------------------------------------------------ input files and set-up */
+/* A regular grid of nx*ny nodes from (xo, yo) with spacings dx, dy, values
+ * row-major with row 0 at yo: the reference's StaticForcingP<float>
+ * (src/Forcing.h), as the bathymetry is held after reading. */
+typedef struct bgf_grid {
+    int nx, ny;
+    double xo, yo, dx, dy, xmax, ymax;
+    const float* val;
+} bgf_grid;
+
+/* Header of an ESRI ASCII grid, as readbathyASCHead (src/ReadForcing.cu:2067-2176)
+ * reads it: the first six non-empty lines, "key value" split on blanks (or tabs),
+ * keys ncols, nrows, cellsize, xllcenter, yllcenter, xllcorner, yllcorner
+ * (case-sensitive).  When yllcenter or xllcorner is present both origins move
+ * by half a cell, as in the reference.  Errors (file missing, header short or
+ * unreadable, ncols/nrows/cellsize absent) return BGF_EINVAL with the reason in
+ * bgf_last_error; the reference exits or loops there instead. */
+int bgf_read_asc_head(const char* path, int* nx, int* ny, double* dx, double* xo, double* yo, double* grdalpha);
+/* Values of an ESRI ASCII grid, as readbathyASCzb (src/ReadForcing.cu:2186-2220):
+ * six raw lines skipped, then nx*ny numbers, the first file row stored as the
+ * last (northern) row of val.  NODATA values are kept as numbers, as in the
+ * reference.  Too few values or a non-number return BGF_EINVAL. */
+int bgf_read_asc(const char* path, int nx, int ny, float* val);
+/* Presence of the nbx*nby candidate blocks of a uniform level mesh with cell
+ * size levdx from (xo, yo), as CalcInitnblk / InitBlockxoyo (src/Mesh.cu:36-120,
+ * 257-347) decide it: a block is dropped when all its cell centres have a
+ * bilinear bed value >= mask.  present is row-major (by, bx); *nblk counts kept. */
+int bgf_mask_blocks(const bgf_grid* g, int nbx, int nby, double xo, double yo, double levdx, double mask,
+                    uint8_t* present, int* nblk);
+/* Bed of every block interpolated from the grid (interp2BUQ,
+ * src/GridManip.cu:380-575: bilinear when the block's cells are not coarser than
+ * the grid, else the mean of the grid nodes in the cell), then the domain-edge
+ * cells set from their inner neighbours (setedges, src/GridManip.cu:222-330).
+ * Tables as bgf_set_blocks takes them (blocks 0..nblk-1, nbr8 per block, xo/yo
+ * relative to the domain origin (xo, yo)); dx is the level-0 cell size.  The
+ * arithmetic follows the model precision (float unless doubleprecision).  zb is
+ * nblk*324 doubles: interior cells are written, halo cells are left as given. */
+int bgf_interp_bathy(const bgf_grid* g, int nblk, const int* level, const int* nbr8, const double* bxo,
+                     const double* byo, double xo, double yo, double dx, int doubleprecision, double* zb);
+
 /* ------------------------------------------------------------ batched scenario pool */
 /* No counterpart in the reference, which runs one scenario per process.  A pool
  * holds device memory for nblk_pool block slots shared by up to max_scenarios

@@ -89,6 +89,14 @@ def ref_lib():
         l.ref_set_bathy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, D]
         l.ref_nblkmem.argtypes = [ctypes.c_void_p]
+        l.ref_create_from_file.restype = ctypes.c_void_p
+        l.ref_create_from_file.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        l.ref_read_asc_head.argtypes = [ctypes.c_char_p, I, I, D, D, D, D]
+        l.ref_read_asc.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+        l.ref_param.argtypes = [ctypes.c_void_p, D]
+        l.ref_rain.argtypes = [ctypes.c_void_p, D, D]
+        l.ref_segment.argtypes = [ctypes.c_void_p, ctypes.c_int, I, D, D]
+        l.ref_get_active_cell.argtypes = [ctypes.c_void_p, I]
         _rlib = l
     return _rlib
 
@@ -184,6 +192,25 @@ class Oracle:
         return oracle_lib().ora_totaltime(self.h)
 
 
+def ref_read_asc(path: str):
+    """The reference's readbathyASCHead + readbathyASCzb<float> on a file:
+    ((nx, ny, dx, xo, yo, grdalpha), values (ny, nx) float32)."""
+    nx, ny = ctypes.c_int(0), ctypes.c_int(0)
+    dx, xo, yo, ga = (ctypes.c_double(0.0) for _ in range(4))
+    l = ref_lib()
+    l.ref_read_asc_head(path.encode(), ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(dx), ctypes.byref(xo),
+                        ctypes.byref(yo), ctypes.byref(ga))
+    val = np.zeros((ny.value, nx.value), np.float32)
+    l.ref_read_asc(path.encode(), nx.value, ny.value, val.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+    return (nx.value, ny.value, dx.value, xo.value, yo.value, ga.value), val
+
+
+# names of the scalars ref_param returns, in order
+REF_PARAM_NAMES = ("xo", "yo", "xmax", "ymax", "dx", "delta", "nx", "ny", "nblk", "nblkmem", "doubleprecision",
+                   "zsinit", "zsoffset", "endtime", "totaltime", "nextoutputtime", "dtmax", "CFL", "engine", "mask",
+                   "initlevel", "minlevel", "maxlevel", "nrain", "nseg")
+
+
 class Reference:
     """The reference BG_Flood flow step (FlowCPU, or FlowGPU with gpudevice >= 0)."""
 
@@ -195,6 +222,39 @@ class Reference:
         self.h = self.lib.ref_create(paramtext.encode(), 1 if use_double else 0, nx, ny, dx, xo, yo,
                                      *[_dp(a) for a in arrs], None if cfa is None else _dp(cfa), nextoutputtime)
         self.nblk = self.lib.ref_nblk(self.h)
+
+    @classmethod
+    def from_file(cls, paramfile: str, fix_asc_dy: bool = True) -> "Reference":
+        """The reference's own start-up from a BG_param.txt (paths in it relative to
+        the working directory), on the CPU."""
+        self = cls.__new__(cls)
+        self.lib = ref_lib()
+        self.h = self.lib.ref_create_from_file(paramfile.encode(), 1 if fix_asc_dy else 0)
+        self.nblk = self.lib.ref_nblk(self.h)
+        return self
+
+    def params(self) -> dict:
+        out = np.zeros(64)
+        n = self.lib.ref_param(self.h, _dp(out))
+        return dict(zip(REF_PARAM_NAMES, out[:n].tolist()))
+
+    def rain(self):
+        n = int(self.params()["nrain"])
+        t, r = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+        self.lib.ref_rain(self.h, _dp(t), _dp(r))
+        return t[:n], r[:n]
+
+    def segment(self, iseg: int):
+        typ = ctypes.c_int(0)
+        cap = 4096
+        t, w = np.zeros(cap), np.zeros(cap)
+        n = self.lib.ref_segment(self.h, iseg, ctypes.byref(typ), _dp(t), _dp(w))
+        return typ.value, t[:n], w[:n]
+
+    def active_cell(self) -> np.ndarray:
+        a = np.zeros(self.nblk * 324, np.int32)
+        self.lib.ref_get_active_cell(self.h, a.ctypes.data_as(I))
+        return a.reshape(self.nblk, 18, 18)
 
     def __del__(self):
         if getattr(self, "h", None):

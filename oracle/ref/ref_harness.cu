@@ -24,6 +24,7 @@
 #include "Updateforcing.h"
 #include "Gradients.h"
 #include "Halo.h"
+#include "ReadForcing.h"
 
 #include <memory>
 #include <vector>
@@ -43,6 +44,10 @@ struct RefBase {
     virtual int adaptation() = 0;
     virtual int flags(unsigned char* refine, unsigned char* coarsen) = 0;
     virtual int set_bathy(int nx, int ny, double xo, double yo, double dx, const double* val) = 0;
+    virtual int setup_loaded() = 0;
+    virtual double loop_nextoutputtime() = 0;
+    virtual int get_active_cell(int* out) = 0;
+    virtual double loop_dtmax() = 0;
     Param P;
     Forcing<float> F;
     double totaltime = 0.0, nextoutputtime = 0.0, dtmax = 0.0;
@@ -149,6 +154,39 @@ template <class T> struct RefModel : RefBase {
         }
         return 0;
     }
+
+    // The reference's own start-up after Readparamfile, readforcing and
+    // checkparamsanity (src/BG_Flood.cu:132-152): InitMesh, InitialConditions,
+    // InitialAdaptation, then the loop as InitLoop (src/Mainloop.cu:207-240) and
+    // the first mapoutput (src/Mainloop.cu:323-340) leave it.  CPU only.
+    int setup_loaded() override
+    {
+        gpu = -1;
+        InitMesh(P, F, M);
+        InitialConditions(P, F, M);
+        InitialAdaptation(P, F, M);
+        L.hugeposval = std::numeric_limits<T>::max();
+        L.hugenegval = T(-1.0) * L.hugeposval;
+        L.epsilon = std::numeric_limits<T>::epsilon();
+        L.totaltime = P.totaltime;
+        L.nextoutputtime = M.OutputT.empty() ? P.endtime : M.OutputT[0];
+        L.dtmax = initdt(P, L, M);
+        if (M.OutputT.size() > 1) L.nextoutputtime = std::min(M.OutputT[1], P.endtime);
+        return 0;
+    }
+
+    // activeCell (rain mask) tiles in active-block order, 18x18 per block.
+    int get_active_cell(int* out) override
+    {
+        for (int ibl = 0; ibl < P.nblk; ibl++) {
+            int ib = M.blocks.active[ibl];
+            for (int k = 0; k < P.blksize; k++) out[(size_t)ibl * P.blksize + k] = M.blocks.activeCell[(size_t)ib * P.blksize + k];
+        }
+        return P.nblk;
+    }
+
+    double loop_nextoutputtime() override { return gpu >= 0 ? Lg.nextoutputtime : L.nextoutputtime; }
+    double loop_dtmax() override { return gpu >= 0 ? Lg.dtmax : L.dtmax; }
 
     int step(int nsteps, double* dts) override
     {
@@ -399,6 +437,87 @@ int ref_set_rain_series(void* hdl, int n, const double* t, const double* r)
     }
     return 0;
 }
+
+// A model set up by the reference's own start-up from a BG_param.txt file (paths
+// in it relative to the working directory), on the CPU.  The reference leaves the
+// y spacing (dy) of an .asc bathymetry at 0, which its bilinear interp2BUQ
+// divides by; with fix_asc_dy the harness sets dy = dx after reading, as the
+// reference's .md reader does.
+void* ref_create_from_file(const char* paramfile, int fix_asc_dy)
+{
+    Param P;
+    Forcing<float> F;
+    Readparamfile(P, F, std::string(paramfile));
+    P.GPUDEVICE = -1;
+    readforcing(P, F);
+    if (fix_asc_dy)
+        for (auto& b : F.Bathy)
+            if (b.dy == 0.0) b.dy = b.dx;
+    checkparamsanity(P, F);
+    RefBase* m;
+    if (P.doubleprecision) m = new RefModel<double>();
+    else m = new RefModel<float>();
+    m->P = P;
+    m->F = F;
+    m->setup_loaded();
+    return m;
+}
+
+// readbathyASCHead / readbathyASCzb (src/ReadForcing.cu:2067-2220) as they are.
+int ref_read_asc_head(const char* path, int* nx, int* ny, double* dx, double* xo, double* yo, double* grdalpha)
+{
+    readbathyASCHead(std::string(path), *nx, *ny, *dx, *xo, *yo, *grdalpha);
+    return 0;
+}
+int ref_read_asc(const char* path, int nx, int ny, float* val)
+{
+    readbathyASCzb<float>(std::string(path), nx, ny, val);
+    return 0;
+}
+
+// Scalars of the set-up model: xo, yo, xmax, ymax, dx, delta, nx, ny, nblk, nblkmem,
+// doubleprecision, zsinit, zsoffset, endtime, totaltime, loop nextoutputtime,
+// loop dtmax, CFL, engine, mask, initlevel, minlevel, maxlevel, rain samples, segments.
+int ref_param(void* hdl, double* out)
+{
+    RefBase* m = (RefBase*)hdl;
+    const Param& P = m->P;
+    double v[] = {P.xo, P.yo, P.xmax, P.ymax, P.dx, P.delta, (double)P.nx, (double)P.ny, (double)P.nblk,
+                  (double)P.nblkmem, (double)P.doubleprecision, P.zsinit, P.zsoffset, P.endtime, P.totaltime,
+                  m->loop_nextoutputtime(), m->loop_dtmax(), P.CFL, (double)P.engine, P.mask, (double)P.initlevel,
+                  (double)P.minlevel, (double)P.maxlevel, (double)m->F.Rain.unidata.size(), (double)m->F.bndseg.size()};
+    const int n = (int)(sizeof(v) / sizeof(v[0]));
+    for (int k = 0; k < n; k++) out[k] = v[k];
+    return n;
+}
+
+// Uniform rain series (time, mm/h) as the reference read it.
+int ref_rain(void* hdl, double* t, double* r)
+{
+    RefBase* m = (RefBase*)hdl;
+    const auto& d = m->F.Rain.unidata;
+    for (size_t k = 0; k < d.size(); k++) {
+        t[k] = d[k].time;
+        r[k] = d[k].wspeed;
+    }
+    return (int)d.size();
+}
+
+// Segment iseg: type, number of samples; times and levels of a uniform series.
+int ref_segment(void* hdl, int iseg, int* type, double* t, double* wl)
+{
+    RefBase* m = (RefBase*)hdl;
+    if (iseg < 0 || iseg >= (int)m->F.bndseg.size()) return -1;
+    const bndsegment& s = m->F.bndseg[iseg];
+    *type = s.type;
+    for (size_t k = 0; k < s.data.size(); k++) {
+        if (t) t[k] = s.data[k].time;
+        if (wl) wl[k] = s.data[k].wspeed;
+    }
+    return (int)s.data.size();
+}
+
+int ref_get_active_cell(void* hdl, int* out) { return ((RefBase*)hdl)->get_active_cell(out); }
 
 int ref_step(void* hdl, int nsteps, double* dts) { return ((RefBase*)hdl)->step(nsteps, dts); }
 int ref_adapt(void* hdl) { return ((RefBase*)hdl)->adapt(); }

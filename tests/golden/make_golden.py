@@ -114,7 +114,61 @@ def main():
         print(name, nsteps, dts[:3])
 
 
+SETUP_STEPS = 20
+
+
+def main_setup():
+    """Scenarios set up by the reference's own start-up from BG_param.txt files
+    (tests/setup_cases.py; ref_create_from_file, with dy = dx for the .asc grid):
+    scalars, tables in active order, interior bed and initial state, rain mask,
+    series; then, with the initial zs set to zb + h, SETUP_STEPS steps of its
+    FlowCPU (cases of RUN_CASES).  Also the reference's .asc reader on the reader
+    variants.  Written to setup_<case>.npz and asc_variants.npz."""
+    import tempfile
+
+    from oracle.pyoracle import REF_PARAM_NAMES, Reference, ref_read_asc
+    from runners import normalise_reference_surface
+    from setup_cases import ASC_VARIANTS, CASES, RUN_CASES, write_asc_variant, write_case
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        for name in CASES:
+            d = os.path.join(tmp, name)
+            write_case(name, d)
+            os.chdir(d)
+            try:
+                r = Reference.from_file("BG_param.txt")
+                prm = r.params()
+                lev, nbr, xo, yo = r.mesh_active_order()
+                out = dict(params=np.array([prm[k] for k in REF_PARAM_NAMES]), level=lev, nbr=nbr, xo=xo, yo=yo)
+                for k in ("zb", "h", "zs", "u", "v"):
+                    out[k] = interior(r.get(k))
+                out["active_cell"] = interior(r.active_cell()).astype(np.int8)
+                out["rain_t"], out["rain_r"] = r.rain()
+                for s in range(int(prm["nseg"])):
+                    typ, t, w = r.segment(s)
+                    out[f"seg{s}_type"], out[f"seg{s}_t"], out[f"seg{s}_w"] = np.int32(typ), t, w
+                if name in RUN_CASES:
+                    normalise_reference_surface(r, bool(prm["doubleprecision"]))
+                    out["dts"] = r.step(SETUP_STEPS)
+                    for k in ("h", "zs", "u", "v"):
+                        out[f"run_{k}"] = interior(r.get(k))
+                np.savez_compressed(os.path.join(HERE, f"setup_{name}.npz"), **out)
+                print("setup", name, r.nblk, prm["doubleprecision"])
+            finally:
+                os.chdir(cwd)
+        out = {}
+        for name, _ in ASC_VARIANTS:
+            path = write_asc_variant(name, tmp)
+            head, val = ref_read_asc(path)
+            out[f"{name}_head"] = np.array(head, np.float64)
+            out[f"{name}_val"] = val
+        np.savez_compressed(os.path.join(HERE, "asc_variants.npz"), **out)
+
+
 if __name__ == "__main__":
+    if sys.argv[1:] == ["setup"]:
+        main_setup()
+        sys.exit(0)
     main()
     main_amr()
     main_adapt_tables()

@@ -153,3 +153,39 @@ def make_amr_pair(case):
         r.set(name, a)
     r.reinit(case.nextoutputtime)
     return r, make_oracle_amr(case, tables), tables
+
+
+def make_oracle_inputs(inp):
+    """The oracle on a scenario set up from its input files (bg_flood_b200.model_setup
+    ModelInputs): same tables, bed, state (zs = zb + h), segments, rain and mask,
+    the loop as InitLoop and the first map output leave it."""
+    p = inp.param
+    m = inp.mesh
+    dbl = bool(p.doubleprecision)
+    o = Oracle(p, m.nblk, dbl)
+    o.set_blocks(m.level, m.nbr, m.xo, m.yo)
+    T = np.float64 if dbl else np.float32
+    zb = inp.zb.astype(T)
+    h = inp.h.astype(T)
+    for name, a in (("zb", zb), ("h", h), ("u", inp.u), ("v", inp.v)):
+        o.set(name, a)
+    o.set("zs", (zb + h).astype(T))
+    if inp.active_cell is not None:
+        o.set("activeCell", inp.active_cell)
+    for typ, times, levels, sides in inp.segments:
+        o.add_segment(typ, times, levels, sides)
+    if inp.rain is not None:
+        o.set_rain(inp.rain[0], inp.rain[1])
+    o.init_bed()
+    dtmax = o.init_loop(inp.totaltime, inp.output_times[0])
+    o.set_loop(inp.totaltime, inp.nextoutputtime, dtmax)
+    return o
+
+
+def normalise_reference_surface(ref, dbl: bool) -> None:
+    """Sets the reference's initial zs to zb + h (in the model precision), the
+    surface this library's state implies, before stepping it."""
+    T = np.float64 if dbl else np.float32
+    zb, h, zs = ref.get("zb"), ref.get("h"), ref.get("zs")
+    zs[:, 1:17, 1:17] = (zb[:, 1:17, 1:17].astype(T) + h[:, 1:17, 1:17].astype(T)).astype(np.float64)
+    ref.set("zs", zs)

@@ -398,6 +398,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) amr_update_kernel(DevModel<T> m, 
     const T hs = a.W[stage][0][base + c18], us = a.W[stage][2][base + c18], vs = a.W[stage][3][base + c18];
     T dh, dhu, dhv;
     flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, hs, us, vs, dh, dhu, dhv);
+    dh = add_rivers<T>(m, p, ib, x, y, dh, ts.totaltime);
     const T hold = s.h0[q18], uold = s.u0[q18], vold = s.v0[q18];
     const size_t g = (size_t)ib * 256 + tid;
     T ho, uo, vo;

@@ -54,6 +54,10 @@ struct bgf_handle {
     std::vector<double> bxo, byo;         // block origins (values of the state precision)
     std::vector<HostSeg> segs;
     std::vector<double> rain_t, rain_r;
+    std::vector<RiverDev> rivers;          // rivers with a non-zero discharge area
+    std::vector<double> riv_t, riv_q;     // their discharge series, one after the other
+    RiverDev* d_rivers = nullptr;
+    double *d_riv_t = nullptr, *d_riv_q = nullptr;
     // device buffers
     int *d_active = nullptr, *d_level = nullptr, *d_nbr = nullptr, *d_bndseg = nullptr, *d_err = nullptr;
     void *d_zb = nullptr, *d_dzbdx = nullptr, *d_dzbdy = nullptr, *d_cf = nullptr;
@@ -129,6 +133,11 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.seg_wl = h->d_seg_wl;
     m.rain_t = h->d_rain_t;
     m.rain_r = h->d_rain_r;
+    m.rivers = h->d_rivers;
+    m.riv_t = h->d_riv_t;
+    m.riv_q = h->d_riv_q;
+    m.bxo = h->d_bxo;
+    m.byo = h->d_byo;
     for (int k = 0; k < 2; k++) {
         m.h[k] = (T*)h->d_h[k];
         m.u[k] = (T*)h->d_u[k];
@@ -196,6 +205,10 @@ template <class T> static StepParams<T> step_params(const bgf_handle* h)
     p.nseg = h->nseg_dev;
     p.rain_n = h->rain_n_dev;
     p.rain_off = 0;
+    p.xo_d = std::isnan(P.xo) ? 0.0 : P.xo;
+    p.yo_d = std::isnan(P.yo) ? 0.0 : P.yo;
+    p.nriver = (int)h->rivers.size();
+    p.riv_first = 0;
     return p;
 }
 
@@ -425,7 +438,7 @@ int bgf_destroy(bgf_handle* h)
                     h->d_cf, h->d_rainmask, h->d_qmean, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t,
                     h->d_rain_r, h->d_h[0], h->d_h[1], h->d_u[0], h->d_u[1], h->d_v[0], h->d_v[1], h->d_dh,
                     h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch, h->d_bxo, h->d_byo,
-                    h->d_flags, h->d_child, h->d_dem, h->d_datum};
+                    h->d_flags, h->d_child, h->d_dem, h->d_datum, h->d_rivers, h->d_riv_t, h->d_riv_q};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     free_amr(h);
@@ -710,6 +723,59 @@ int bgf_set_rain_series(bgf_handle* h, int n, const double* t, const double* r)
         BGF_CUDA(cudaMemcpy(h->d_rain_t, t, n * sizeof(double), cudaMemcpyHostToDevice));
         BGF_CUDA(cudaMemcpy(h->d_rain_r, r, n * sizeof(double), cudaMemcpyHostToDevice));
     }
+    free_graphs(h);
+    return BGF_OK;
+}
+
+// Rivers: InitRivers (src/InitialConditions.cu:336-420) for the discharge area,
+// with the handle's current blocks; the series go to the device with the others.
+int bgf_add_river(bgf_handle* h, double xstart, double xend, double ystart, double yend, int n, const double* t,
+                  const double* q, double* area)
+{
+    if (!h || n < 2 || !t || !q) return BGF_EINVAL;
+    if (!h->has_blocks) return BGF_ESTATE;
+    if ((int)h->rivers.size() >= BGF_MAX_RIVERS) return BGF_EINVAL;
+    for (int k = 1; k < n; k++)
+        if (!(t[k] > t[k - 1])) return BGF_EINVAL;
+    int rc = set_device(h);
+    if (rc) return rc;
+    const bgf_param& P = h->P;
+    const double xo = std::isnan(P.xo) ? 0.0 : P.xo, yo = std::isnan(P.yo) ? 0.0 : P.yo;
+    double a = 0.0;
+    for (int ibl = 0; ibl < h->nblk; ibl++) {
+        const int ib = h->active[ibl];
+        const int lev = h->level[ib];
+        const double levdx = lev < 0 ? P.dx * (1 << -lev) : P.dx / (1 << lev);
+        const double levdelta = lev < 0 ? P.delta * (1 << -lev) : P.delta / (1 << lev);
+        for (int j = 0; j < 16; j++)
+            for (int i = 0; i < 16; i++) {
+                const double xi = xo + h->bxo[ib] + i * levdx, yi = yo + h->byo[ib] + j * levdx;
+                const double xl = xi - 0.5 * levdx, yb = yi - 0.5 * levdx, xr = xi + 0.5 * levdx, yt = yi + 0.5 * levdx;
+                if (xstart <= xr && xend >= xl && ystart <= yt && yend >= yb) a = a + levdelta * levdelta;
+            }
+    }
+    if (area) *area = a;
+    if (a == 0.0) return BGF_OK;  // outside the model: the reference drops such a river
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    RiverDev r;
+    r.xs = xstart;
+    r.xe = xend;
+    r.ys = ystart;
+    r.ye = yend;
+    r.area = a;
+    r.off = (int)h->riv_t.size();
+    r.n = n;
+    h->rivers.push_back(r);
+    h->riv_t.insert(h->riv_t.end(), t, t + n);
+    h->riv_q.insert(h->riv_q.end(), q, q + n);
+    for (void** d : {(void**)&h->d_rivers, (void**)&h->d_riv_t, (void**)&h->d_riv_q})
+        if (*d) { cudaFree(*d); *d = nullptr; }
+    BGF_CUDA(cudaMalloc((void**)&h->d_rivers, h->rivers.size() * sizeof(RiverDev)));
+    BGF_CUDA(cudaMalloc((void**)&h->d_riv_t, h->riv_t.size() * sizeof(double)));
+    BGF_CUDA(cudaMalloc((void**)&h->d_riv_q, h->riv_q.size() * sizeof(double)));
+    BGF_CUDA(cudaMemcpy(h->d_rivers, h->rivers.data(), h->rivers.size() * sizeof(RiverDev), cudaMemcpyHostToDevice));
+    BGF_CUDA(cudaMemcpy(h->d_riv_t, h->riv_t.data(), h->riv_t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    BGF_CUDA(cudaMemcpy(h->d_riv_q, h->riv_q.data(), h->riv_q.size() * sizeof(double), cudaMemcpyHostToDevice));
     free_graphs(h);
     return BGF_OK;
 }

@@ -84,7 +84,7 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
 // on the 18x18 tile for the boundary fluxes and the full-step advance.
 template <class T, bool SPLIT>
 __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
-                                               int cur, T halfdt, int tid, T D)
+                                               int cur, T halfdt, int tid, T D, double time)
 {
     const T* H = m.h[cur];
     const T* U = m.u[cur];
@@ -102,14 +102,16 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
         }
         size_t g = (size_t)sb * 256 + sy * 16 + sx;
         T hv = H[g], uv = U[g], vv = V[g];
+        // the predictor's river source (AddRiverForcing after updateEV) of the source cell
+        const T dhs = add_rivers<T>(m, p, sb, sx, sy, m.dh[g], time);
         T ho, uo, vo;
         if (SPLIT) {
             const T Ds = sb == ib ? D : m.datum[sb];
-            advance_split<T>(halfdt, p.eps, p.forcemass != 0, Ds, hv, uv, vv, m.dh[g], m.dhu[g], m.dhv[g], ho, uo, vo);
+            advance_split<T>(halfdt, p.eps, p.forcemass != 0, Ds, hv, uv, vv, dhs, m.dhu[g], m.dhv[g], ho, uo, vo);
             hv = to_tile_datum<T, SPLIT>(m, hv, sb, ib, D);
             ho = to_tile_datum<T, SPLIT>(m, ho, sb, ib, D);
         } else {
-            advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, m.dh[g], m.dhu[g], m.dhv[g], ho, uo, vo);
+            advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, dhs, m.dhu[g], m.dhv[g], ho, uo, vo);
         }
         int c = ti(x, y);
         s.t[VH][c] = ho; s.t[VU][c] = uo; s.t[VV][c] = vo;
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
 
         load_bed<T, ENGINE, SPLIT>(s, m, ib, tid, D);
         __syncthreads();
-        load_half_tile<T, SPLIT>(s, m, p, ib, cur, dt * (T)0.5, tid, D);
+        load_half_tile<T, SPLIT>(s, m, p, ib, cur, dt * (T)0.5, tid, D, ts.totaltime);
         __syncthreads();
         (void)tile_fluxes<T, ENGINE, false, SPLIT>(s, p, delta, tid, nullptr, D);
         __syncthreads();
@@ -231,6 +233,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
         T dh, dhu, dhv;
         flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, SPLIT ? D + s.t[VH][c] : s.t[VH][c], s.t[VU][c],
                            s.t[VV][c], dh, dhu, dhv);
+        dh = add_rivers<T>(m, p, ib, x, y, dh, ts.totaltime);
         // full step from state n (AdvkernelCPU with evolv), then friction on the result
         const int c18 = si(x, y);
         T hold = s.h0[c18], uold = s.u0[c18], vold = s.v0[c18];

@@ -60,8 +60,18 @@ template <class T> struct StepParams {
     T g, eps, CFL, theta, delta0, epsi, epsface, fc;
     double eps_d, dtparam, bndfiltertime, bndrelaxtime, bndtaper, inittime, zsinit, zsoffset, dtmin;
     double delta0_d;  // level-0 spacing in double (refine_linear left/top offsets)
+    double xo_d, yo_d;  // domain origin (river boxes)
     T cf;        // uniform friction coefficient
     int frictionmodel, forcemass, has_cf, has_rain, nseg, rain_n, rain_off;
+    int nriver, riv_first;  // rivers of this scenario: entries riv_first .. riv_first + nriver - 1
+};
+
+// A river (the reference's River / RiverInfo): discharge box, discharge area (sum
+// of the cell areas the box overlaps, InitRivers) and its discharge series at
+// riv_t / riv_q [off, off + n).
+struct RiverDev {
+    double xs, xe, ys, ye, area;
+    int off, n;
 };
 
 template <class T> struct DevModel {
@@ -81,6 +91,11 @@ template <class T> struct DevModel {
     const double* seg_wl;
     const double* rain_t;
     const double* rain_r;
+    const RiverDev* rivers;
+    const double* riv_t;
+    const double* riv_q;
+    const double* bxo;  // block origins relative to the domain origin (values of the state precision)
+    const double* byo;
     T* h[2];
     T* u[2];
     T* v[2];

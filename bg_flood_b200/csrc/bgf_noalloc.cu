@@ -113,6 +113,11 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     m.hmax = nullptr;
     m.checklev = 1;
     m.datum = nullptr;
+    m.rivers = nullptr;
+    m.riv_t = nullptr;
+    m.riv_q = nullptr;
+    m.bxo = nullptr;
+    m.byo = nullptr;
 
     StepParams<T> p;
     p.g = (T)P->g;
@@ -141,6 +146,10 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     p.nseg = 4;
     p.rain_n = 0;
     p.rain_off = 0;
+    p.xo_d = 0.0;
+    p.yo_d = 0.0;
+    p.nriver = 0;
+    p.riv_first = 0;
 
     // per-call state: time slot 0 from the caller's loop, the dt minimum, the error
     // word and the absorbing-boundary running means start from zero

@@ -37,6 +37,50 @@ __device__ __forceinline__ double series_at(const double* t, const double* v, in
     return v[st - 1] + (time - t[st - 1]) / (t[st] - t[st - 1]) * (v[st] - v[st - 1]);
 }
 
+// River discharge of one river at `time` per unit area, as AddRiverForcing computes
+// it (src/Updateforcing.cu:146-170): the first sample later than `time`, the
+// interpolated discharge rounded to T, then divided by the discharge area.
+template <class T> __device__ __forceinline__ T river_rate(const RiverDev& r, const double* t, const double* q, double time)
+{
+    int st = 0;
+    while (st < r.n - 1 && t[r.off + st] - time <= 0.0) st++;
+    const int pv = st > 0 ? st - 1 : 0;
+    // before the first sample the reference divides by zero; the first value is used here
+    const double qi = st == pv ? q[r.off + st]
+                               : q[r.off + pv] + (time - t[r.off + pv]) / (t[r.off + st] - t[r.off + pv]) *
+                                                     (q[r.off + st] - q[r.off + pv]);
+    return (T)((double)(T)qi / r.area);
+}
+
+// InjectManyRiversGPU (src/Updateforcing.cu:245-300) for cell (x, y) of block ib:
+// every river whose box overlaps the cell's box (OBBdetect in T) adds its rate to
+// dh, in river order.  `time` is the start of the step (both stages).
+template <class T>
+__device__ __forceinline__ T add_rivers_cell(const RiverDev* rivers, const double* riv_t, const double* riv_q, int first,
+                                          int nriver, T levdx, double xo, double yo, int x, int y, T dh, double time)
+{
+    const T xllo = (T)xo, yllo = (T)yo;
+    const T half = (T)0.5 * levdx;
+    const T xl = xllo + (T)x * levdx - half, xr = xllo + (T)x * levdx + half;
+    const T yb = yllo + (T)y * levdx - half, yt = yllo + (T)y * levdx + half;
+    for (int k = 0; k < nriver; k++) {
+        const RiverDev r = rivers[first + k];
+        const bool ox = (T)r.xs <= xr && (T)r.xe >= xl;
+        const bool oy = (T)r.ys <= yt && (T)r.ye >= yb;
+        if (ox && oy) dh = dh + river_rate<T>(r, riv_t, riv_q, time);
+    }
+    return dh;
+}
+
+template <class T>
+__device__ __forceinline__ T add_rivers(const DevModel<T>& m, const StepParams<T>& p, int ib, int x, int y, T dh,
+                                        double time)
+{
+    if (p.nriver == 0) return dh;
+    return add_rivers_cell<T>(m.rivers, m.riv_t, m.riv_q, p.riv_first, p.nriver, calcres<T>(p.delta0, m.level[ib]),
+                              p.xo_d + m.bxo[ib], p.yo_d + m.byo[ib], x, y, dh, time);
+}
+
 // bndFluxGPUSideCPU (src/Boundary.cu:587-745) for the four sides of one block.
 // Face arrays in s are modified in place; state n comes from s.h0/u0/v0 and the
 // bed tile (zs = zb + h, as RecalculateZs leaves it).

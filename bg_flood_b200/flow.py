@@ -148,6 +148,18 @@ class FlowB200:
         _check(lib().bgf_set_rain_series(self.handle, len(t), t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                          r.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "bgf_set_rain_series")
 
+    def add_river(self, xstart: float, xend: float, ystart: float, yend: float, times, q) -> float:
+        """A river discharging q(t) (m^3/s) over the cells its box overlaps; returns
+        the discharge area (0: the box misses every cell and the river is dropped)."""
+        t = np.ascontiguousarray(times, np.float64)
+        qq = np.ascontiguousarray(q, np.float64)
+        a = ctypes.c_double(0.0)
+        _check(lib().bgf_add_river(self.handle, float(xstart), float(xend), float(ystart), float(yend), len(t),
+                                   t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                   qq.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(a)),
+               "bgf_add_river")
+        return a.value
+
     def set_state(self, h: np.ndarray, u: np.ndarray, v: np.ndarray) -> None:
         hh, uu, vv = (np.ascontiguousarray(a, self.dtype) for a in (h, u, v))
         ev = CEvolving(None, _ptr(hh), _ptr(uu), _ptr(vv))

@@ -5,8 +5,9 @@
 
 1. Readparamfile (src/ReadInput.cu:57-95): keys and aliases of params.py, the
    bathymetry, rain and boundary file keys;
-2. readforcing (src/ReadForcing.cu:38-53, 75-97, 365-381): bathymetry grid,
-   uniform boundary series, uniform rain series;
+2. readforcing (src/ReadForcing.cu:38-53, 75-97, 250-280, 365-381): bathymetry
+   grid, uniform boundary series, river discharge series (the run's end and start
+   times are fitted into each river's time range), uniform rain series;
 3. checkparamsanity (src/ReadInput.cu:1189-1480): level defaults, rain forces
    double precision, zsoffset, domain extent from the bathymetry, nx/ny rounded
    up to whole blocks, end time and output times;
@@ -15,7 +16,8 @@
 5. InitialConditions (src/InitialConditions.cu:23-120): bed by interp2BUQ and
    setedges, cold start (zs = max(zsinit + zsoffset, zb)) or, with no zsinit and
    a boundary series, the warm start from the series' mean level
-   (src/InitEvolv.cu:36-290), boundary blocks, rain mask;
+   (src/InitEvolv.cu:36-290), rivers (discharge areas, InitRivers), boundary
+   blocks, rain mask;
 6. InitialAdaptation (src/Adaptation.cu:133-146) when maxlevel != minlevel: the
    refinement pass on the device, then step 5 again on the refined mesh;
 7. InitLoop and the first map output (src/Mainloop.cu:207-240, 323-340).
@@ -25,8 +27,8 @@ with its Loop, ready for ``run``.
 
 Inputs outside this library's scope raise ValueError: netCDF or other grid
 formats, several bathymetry layers, roughness / infiltration / deformation
-maps, rivers, wind, atmospheric pressure, AOI polygons, spherical grids,
-engine 5, hot starts.
+maps, wind, atmospheric pressure, AOI polygons, spherical grids, engine 5,
+hot starts.
 """
 from __future__ import annotations
 
@@ -40,7 +42,7 @@ import numpy as np
 from ._native import lib
 from .mesh import Mesh, boundary_segments, uniform_mesh
 from .params import Param, read_param_text
-from .readforcing import BathyGrid, read_bathy, read_uniform_series
+from .readforcing import BathyGrid, read_bathy, read_flow_file, read_uniform_series
 
 __all__ = ["ModelInputs", "read_param_file", "prepare_model", "setup_model", "check_param_sanity", "inputs_on_mesh"]
 
@@ -62,6 +64,7 @@ class ModelInputs:
     active_cell: np.ndarray | None
     segments: list          # (type, times, levels, [left, right, top, bot] blocks)
     rain: tuple | None      # (times s, mm/h)
+    rivers: list            # (xstart, xend, ystart, yend, times, discharges m^3/s)
     output_times: list
     totaltime: float
     nextoutputtime: float
@@ -86,7 +89,7 @@ def read_param_file(path: str) -> Param:
 
 # keys of inputs this library does not read (readparamstr, src/ReadInput.cu:890-1180)
 _UNSUPPORTED = {
-    "aoi": "AOI polygons", "aoipoly": "AOI polygons", "river": "rivers", "cfmap": "roughness maps",
+    "aoi": "AOI polygons", "aoipoly": "AOI polygons", "cfmap": "roughness maps",
     "roughnessmap": "roughness maps", "wind": "wind forcing", "windfiles": "wind forcing", "atmp": "pressure forcing",
     "atmpfile": "pressure forcing", "deform": "deformation", "hotstartfile": "hot start", "hotstart": "hot start",
     "initiallossmap": "infiltration maps", "ilmap": "infiltration maps", "continuouslossmap": "infiltration maps",
@@ -230,6 +233,20 @@ def _boundary_series(p: Param, basedir: str, reftime: list) -> None:
             s.times, s.levels = list(t), list(w)
 
 
+def _river_series(p: Param, basedir: str, reftime: list) -> list:
+    """readforcing's river part: the discharge series, and the end and start times
+    fitted into each river's time range."""
+    out = []
+    for fname, xs, xe, ys, ye in p.rivers:
+        t, q = read_flow_file(_resolve(fname, basedir), reftime)
+        if t[-1] < p.endtime:
+            p.endtime = float(t[-1])
+        if t[0] > p.totaltime:
+            p.totaltime = float(t[0])
+        out.append((xs, xe, ys, ye, t, q))
+    return out
+
+
 def _rain_series(p: Param, basedir: str, reftime: list):
     if not p.rain:
         return None
@@ -265,6 +282,7 @@ def prepare_model(param_file: str, basedir: str | None = None, nblkmem: int | No
     reftime = [p.reftime]
     bathy = read_bathy(_resolve(p.bathy[0], basedir), p.posdown, first=True)
     _boundary_series(p, basedir, reftime)
+    rivers = _river_series(p, basedir, reftime)
     rain = _rain_series(p, basedir, reftime)
     outt = check_param_sanity(p, bathy, rain is not None)
     nx, ny, levdx = _mesh_counts(p)
@@ -285,7 +303,7 @@ def prepare_model(param_file: str, basedir: str | None = None, nblkmem: int | No
     nmem = nblkmem if nblkmem is not None else int(math.ceil(mesh.nblk * p.membuffer))
     nextout = min(outt[1], p.endtime) if len(outt) > 1 else p.endtime
     return ModelInputs(p, bathy, mesh, ic["zb"], ic["h"], ic["u"], ic["v"], ic["zs"], ic["active_cell"],
-                       ic["segments"], rain, outt, p.totaltime, nextout, max(nmem, mesh.nblk))
+                       ic["segments"], rain, rivers, outt, p.totaltime, nextout, max(nmem, mesh.nblk))
 
 
 def _load(inp: ModelInputs, nblkmem: int):
@@ -298,6 +316,8 @@ def _load(inp: ModelInputs, nblkmem: int):
         f.add_segment(typ, times, levels, sides)
     if inp.rain is not None:
         f.set_rain(inp.rain[0], inp.rain[1])
+    for xs, xe, ys, ye, t, q in inp.rivers:
+        f.add_river(xs, xe, ys, ye, t, q)
     f.set_state(_pad(inp.h, nblkmem), _pad(inp.u, nblkmem), _pad(inp.v, nblkmem))
     return f
 
@@ -318,7 +338,7 @@ def inputs_on_mesh(inp: ModelInputs, level, nbr, xo, yo) -> ModelInputs:
                 np.zeros(n, np.int32), np.zeros(n, np.int32))
     ic = _initial_conditions(inp.param, inp.bathy, mesh, mesh.level, mesh.nbr, mesh.xo, mesh.yo)
     return ModelInputs(inp.param, inp.bathy, mesh, ic["zb"], ic["h"], ic["u"], ic["v"], ic["zs"], ic["active_cell"],
-                       ic["segments"], inp.rain, inp.output_times, inp.totaltime, inp.nextoutputtime,
+                       ic["segments"], inp.rain, inp.rivers, inp.output_times, inp.totaltime, inp.nextoutputtime,
                        max(inp.nblkmem, n), adapted=True)
 
 

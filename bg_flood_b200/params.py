@@ -95,6 +95,7 @@ class Param:
     segments: list = field(default_factory=list)
     rain: str = ""
     bathy: list = field(default_factory=list)  # bathymetry files, first one the base grid
+    rivers: list = field(default_factory=list)  # (discharge file, xstart, xend, ystart, yend)
 
     @property
     def delta(self) -> float:
@@ -219,6 +220,13 @@ def read_param_text(text: str, param: Param | None = None) -> Param:
             continue
         if k in _BATHY_KEYS:
             p.bathy.append(val)
+            continue
+        if k in ("river", "rivers"):
+            # "file, xstart, xend, ystart, yend" (src/ReadInput.cu:1020-1045)
+            items = [s for s in val.split(",") if s]
+            if len(items) != 5:
+                raise ValueError(f"river needs 5 comma-separated items (file, xstart, xend, ystart, yend): {val!r}")
+            p.rivers.append((items[0].strip(), float(items[1]), float(items[2]), float(items[3]), float(items[4])))
             continue
         if k in ("adaptation", "adapt"):
             items = [s.strip() for s in val.split(",")]

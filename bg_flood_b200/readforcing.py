@@ -23,7 +23,6 @@ from __future__ import annotations
 
 import ctypes
 import datetime as _dt
-import math
 import os
 from dataclasses import dataclass
 
@@ -31,7 +30,8 @@ import numpy as np
 
 from ._native import lib
 
-__all__ = ["BathyGrid", "read_asc_header", "read_asc", "read_bathy", "read_uniform_series", "readinputtimetxt"]
+__all__ = ["BathyGrid", "read_asc_header", "read_asc", "read_bathy", "read_uniform_series", "readinputtimetxt",
+           "read_flow_file"]
 
 
 class CGrid(ctypes.Structure):
@@ -150,5 +150,26 @@ def read_uniform_series(path: str, reftime: list | None = None) -> tuple:
     return np.asarray(times, np.float64), np.asarray(vals, np.float64)
 
 
-def _isnan(v) -> bool:
-    return isinstance(v, float) and math.isnan(v)
+def read_flow_file(path: str, reftime: list | None = None) -> tuple:
+    """(times, discharges) of a river discharge file as readFlowfile reads it
+    (src/ReadForcing.cu:1277-1345): exactly two items per line, tab, blank or
+    comma separated, ``#`` lines skipped."""
+    ref = reftime if reftime is not None else [""]
+    times, q = [], []
+    with open(path, "r") as fh:
+        for line in fh:
+            line = line.rstrip("\n")
+            if not line or line.startswith("#"):
+                continue
+            el = [e for e in line.split("\t") if e]
+            if len(el) != 2:
+                el = [e for e in line.split(" ") if e]
+            if len(el) != 2:
+                el = [e for e in line.split(",") if e]
+            if len(el) != 2:
+                raise ValueError(f"{path}: flow file format error, 2 items expected per line: {line!r}")
+            times.append(readinputtimetxt(el[0], ref))
+            q.append(float(el[1]))
+    if len(times) < 2:
+        raise ValueError(f"{path}: a discharge series needs at least 2 samples")
+    return np.asarray(times, np.float64), np.asarray(q, np.float64)

@@ -254,6 +254,22 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* args, bgf_
 int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* present, int* nblk, int* level,
                      int* nbr8, double* xo, double* yo, int doubleprecision);
 
+/* ------------------------------------------------------------ rivers */
+#define BGF_MAX_RIVERS 64
+/* A river: discharge q(t) (m^3/s, n >= 2 samples, increasing times) spread over
+ * the cells whose box overlaps [xstart, xend] x [ystart, yend] (absolute
+ * coordinates, as the reference's "river = file, xstart, xend, ystart, yend").
+ * The discharge area is computed from the handle's blocks as InitRivers does
+ * (src/InitialConditions.cu:336-420) and written to *area; a river that
+ * overlaps no cell (area 0) is not added, as the reference drops it.  Each
+ * stage of a step adds q(t)/area to the depth tendency of those cells
+ * (AddRiverForcing / InjectManyRiversGPU, src/Updateforcing.cu:146-300), t
+ * being the start of the step.  Call after bgf_set_blocks; at most
+ * BGF_MAX_RIVERS rivers.  The area is kept when a refinement pass changes the
+ * mesh, as in the reference. */
+int bgf_add_river(bgf_handle* h, double xstart, double xend, double ystart, double yend, int n, const double* t,
+                  const double* q, double* area);
+
 /* ------------------------------------------------------------ input files and set-up */
 /* A regular grid of nx*ny nodes from (xo, yo) with spacings dx, dy, values
  * row-major with row 0 at yo: the reference's StaticForcingP<float>

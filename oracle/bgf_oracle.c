@@ -83,6 +83,8 @@ int ora_add_segment(void* m, int type, int n, const double* t, const double* wl,
                   api_add_segment_d(MD, type, n, t, wl, nblk_side, blk_side)); }
 int ora_set_rain(void* m, int n, const double* t, const double* r)
 { return DISPATCH(api_set_rain_f(MF, n, t, r), api_set_rain_d(MD, n, t, r)); }
+double ora_add_river(void* m, double xs, double xe, double ys, double ye, int n, const double* t, const double* q)
+{ return DISPATCH(api_add_river_f(MF, xs, xe, ys, ye, n, t, q), api_add_river_d(MD, xs, xe, ys, ye, n, t, q)); }
 int ora_init_bed(void* m) { return DISPATCH(api_init_bed_f(MF), api_init_bed_d(MD)); }
 double ora_init_loop(void* m, double totaltime, double nextoutputtime)
 { return DISPATCH(api_init_loop_f(MF, totaltime, nextoutputtime), api_init_loop_d(MD, totaltime, nextoutputtime)); }

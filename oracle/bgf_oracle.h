@@ -56,6 +56,8 @@ int ora_get_field(void* m, const char* name, double* buq);
 int ora_add_segment(void* m, int type, int n, const double* t, const double* wl,
                     const int* nblk_side, const int* const* blk_side);
 int ora_set_rain(void* m, int n, const double* t, const double* r);
+/* A river (box in absolute coordinates, discharge series); returns the discharge area. */
+double ora_add_river(void* m, double xs, double xe, double ys, double ye, int n, const double* t, const double* q);
 
 /* Bed halo + bed gradients exactly as src/Testing.cu:583-588. */
 int ora_init_bed(void* m);

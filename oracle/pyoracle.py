@@ -51,6 +51,9 @@ def oracle_lib():
         l.ora_add_segment.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D, D, I, ctypes.POINTER(I)]
         l.ora_set_rain.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         l.ora_init_bed.argtypes = [ctypes.c_void_p]
+        l.ora_add_river.restype = ctypes.c_double
+        l.ora_add_river.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, D, D]
         l.ora_init_loop.restype = ctypes.c_double
         l.ora_init_loop.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         l.ora_set_loop.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -168,6 +171,11 @@ class Oracle:
         t = np.ascontiguousarray(times, np.float64)
         r = np.ascontiguousarray(rates, np.float64)
         oracle_lib().ora_set_rain(self.h, len(t), _dp(t), _dp(r))
+
+    def add_river(self, xs, xe, ys, ye, times, q) -> float:
+        t = np.ascontiguousarray(times, np.float64)
+        qq = np.ascontiguousarray(q, np.float64)
+        return oracle_lib().ora_add_river(self.h, xs, xe, ys, ye, len(t), _dp(t), _dp(qq))
 
     def init_bed(self):
         rc = oracle_lib().ora_init_bed(self.h)

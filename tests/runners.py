@@ -176,6 +176,8 @@ def make_oracle_inputs(inp):
         o.add_segment(typ, times, levels, sides)
     if inp.rain is not None:
         o.set_rain(inp.rain[0], inp.rain[1])
+    for xs, xe, ys, ye, t, q in inp.rivers:
+        o.add_river(xs, xe, ys, ye, t, q)
     o.init_bed()
     dtmax = o.init_loop(inp.totaltime, inp.output_times[0])
     o.set_loop(inp.totaltime, inp.nextoutputtime, dtmax)

@@ -12,12 +12,12 @@ import os
 import numpy as np
 
 # name -> description; every case is built by write_case(name, dir)
-CASES = ("cold", "rain", "warm", "coarse", "offset", "adapt")
+CASES = ("cold", "rain", "warm", "coarse", "offset", "adapt", "river")
 # cases whose run the reference's CPU step can pin: with zsoffset != 0 its CPU
 # boundary loop adds the offset once per boundary cell visited, cumulatively
 # (src/Boundary.cu:646-648, zsbnd is the loop's own variable), where its GPU
 # kernel adds it once (src/Boundary.cu:460); this library follows the GPU kernel.
-RUN_CASES = ("cold", "rain", "warm", "coarse", "adapt")
+RUN_CASES = ("cold", "rain", "warm", "coarse", "adapt", "river")
 
 
 def asc_text(z: np.ndarray, cellsize: float, x0: float, y0: float, reg: str = "corner", sep: str = " ",
@@ -85,6 +85,19 @@ def write_case(name: str, d: str) -> str:
         w("bathy.asc", asc_text(z, 1.0, 0.0, 0.0, "corner"))
         w("BG_param.txt", "bathy = bathy.asc\nzsinit = 0.2\ninitlevel = 0\nmaxlevel = 1\nminlevel = 0\n"
                           "Adaptation = Threshold,0.3,h\nendtime = 30\noutputtimestep = 10\n")
+    elif name == "river":
+        # two rivers into a dry valley (one box straddling two blocks), one box
+        # outside the domain (dropped); the run's end time comes from the flow files
+        z = bed(48, 48, 7, slope=0.0, base=0.2, amp=0.1)
+        yy = np.arange(48)[:, None]
+        z = (z + 0.02 * np.abs(yy - 24)).astype(np.float32)
+        w("bathy.asc", asc_text(z, 1.0, 0.0, 0.0, "corner"))
+        w("q1.txt", "0 0.0\n10 2.5\n60 4.0\n")
+        w("q2.txt", "# t q\n0,1.0\n80,0.5\n")
+        w("q3.txt", "0 1.0\n100 1.0\n")
+        w("BG_param.txt", "bathy = bathy.asc\nzsinit = -1\nriver = q1.txt,3.2,5.9,22.1,26.8\n"
+                          "river = q2.txt,15.5,16.6,10.0,12.0\nriver = q3.txt,100,110,100,110\n"
+                          "outputtimestep = 10\nfrictionmodel = 0\ncf = 0.001\n")
     else:
         raise KeyError(name)
     return os.path.join(d, "BG_param.txt")

@@ -95,3 +95,32 @@ def test_setup_model_run_to_end(tmp_path):
         assert np.isfinite(f.volume()) and f.volume() > v0  # it rained
     finally:
         f.close()
+
+
+def test_river_scenario_in_a_pool(tmp_path):
+    # the river case batched with the cold-start case gives its results alone
+    from bg_flood_b200.pool import ScenarioPool
+    nsteps = 30
+    alone = {}
+    for name in ("river", "cold"):
+        f, inp, loop = setup_model(write_case(name, str(tmp_path / f"a_{name}")))
+        f.run(loop, endtime=1e30, maxsteps=nsteps)
+        alone[name] = (f.get_state(), inp.mesh.nblk, loop.totaltime)
+        f.close()
+    pool = None
+    slots = {}
+    handles = []
+    for name in ("river", "cold"):
+        f, inp, loop = setup_model(write_case(name, str(tmp_path / f"p_{name}")))
+        if pool is None:
+            pool = ScenarioPool(inp.param, 64, 4)
+        slots[name] = pool.admit(f, loop, 1e30, maxsteps=nsteps)
+        handles.append(f)
+    assert pool.run(100000) == 0
+    for name, s in slots.items():
+        f, loop, n = pool.retire(s)
+        st, nb, t = alone[name]
+        assert n == nsteps and loop.totaltime == t
+        for a, b in zip(f.get_state()[1:], st[1:]):
+            assert np.array_equal(a[:nb][I], b[:nb][I])
+    pool.close()

@@ -109,9 +109,14 @@ def test_param_file_keys(tmp_path):
     assert p.bathy == ["bathy.asc"] and p.zsoffset == 0.05
     assert len(p.segments) == 1 and p.segments[0].side == "bot" and p.segments[0].type == 3
     assert p.segments[0].file == "bnd.txt"
-    (tmp_path / "BG_param.txt").write_text("bathy = bathy.asc\nriver = r.txt,1,2,3,4\n")
+    (tmp_path / "BG_param.txt").write_text("bathy = bathy.asc\nwindfiles = w.txt\n")
     with pytest.raises(ValueError, match="not supported"):
         read_param_file(str(tmp_path / "BG_param.txt"))
+    (tmp_path / "BG_param.txt").write_text("bathy = bathy.asc\nriver = r.txt,1,2,3\n")
+    with pytest.raises(ValueError, match="5 comma-separated"):
+        read_param_file(str(tmp_path / "BG_param.txt"))
+    (tmp_path / "BG_param.txt").write_text("bathy = bathy.asc\nriver = r.txt, 1,2,3,4\n")
+    assert read_param_file(str(tmp_path / "BG_param.txt")).rivers == [("r.txt", 1.0, 2.0, 3.0, 4.0)]
     (tmp_path / "BG_param.txt").write_text("bathy = bathy.nc?z\n")
     with pytest.raises(ValueError, match="not supported"):
         prepare_model(str(tmp_path / "BG_param.txt"))

@@ -62,6 +62,9 @@ SIGNATURES = {
     "bgf_pool_get_depth": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p]),
     "bgf_pool_timing": (ctypes.c_int, [c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64), c_int_p]),
     "bgf_pool_set_grid": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "bgf_set_rain_map": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_double, c_void_p]),
     "bgf_add_river": (ctypes.c_int, [c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_int, c_double_p, c_double_p, c_double_p]),
     "bgf_read_asc_head": (ctypes.c_int, [ctypes.c_char_p, c_int_p, c_int_p, c_double_p, c_double_p, c_double_p,

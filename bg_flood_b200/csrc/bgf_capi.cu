@@ -57,6 +57,8 @@ struct bgf_handle {
     std::vector<RiverDev> rivers;          // rivers with a non-zero discharge area
     std::vector<double> riv_t, riv_q;     // their discharge series, one after the other
     RiverDev* d_rivers = nullptr;
+    RainMapDev rmap = {};                 // gridded rain (val: device frames), or none
+    bool has_rmap = false;
     double *d_riv_t = nullptr, *d_riv_q = nullptr;
     // device buffers
     int *d_active = nullptr, *d_level = nullptr, *d_nbr = nullptr, *d_bndseg = nullptr, *d_err = nullptr;
@@ -133,6 +135,7 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.seg_wl = h->d_seg_wl;
     m.rain_t = h->d_rain_t;
     m.rain_r = h->d_rain_r;
+    m.rmap = h->rmap;
     m.rivers = h->d_rivers;
     m.riv_t = h->d_riv_t;
     m.riv_q = h->d_riv_q;
@@ -201,7 +204,8 @@ template <class T> static StepParams<T> step_params(const bgf_handle* h)
     p.frictionmodel = P.frictionmodel;
     p.forcemass = P.ForceMassConserve;
     p.has_cf = h->has_cf ? 1 : 0;
-    p.has_rain = h->rain_n_dev > 0 ? 1 : 0;
+    p.has_rain = (h->rain_n_dev > 0 || h->has_rmap) ? 1 : 0;
+    p.rain_map = h->has_rmap ? 1 : 0;
     p.nseg = h->nseg_dev;
     p.rain_n = h->rain_n_dev;
     p.rain_off = 0;
@@ -438,7 +442,8 @@ int bgf_destroy(bgf_handle* h)
                     h->d_cf, h->d_rainmask, h->d_qmean, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t,
                     h->d_rain_r, h->d_h[0], h->d_h[1], h->d_u[0], h->d_u[1], h->d_v[0], h->d_v[1], h->d_dh,
                     h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch, h->d_bxo, h->d_byo,
-                    h->d_flags, h->d_child, h->d_dem, h->d_datum, h->d_rivers, h->d_riv_t, h->d_riv_q};
+                    h->d_flags, h->d_child, h->d_dem, h->d_datum, h->d_rivers, h->d_riv_t, h->d_riv_q,
+                    (void*)h->rmap.val};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     free_amr(h);
@@ -717,12 +722,53 @@ int bgf_set_rain_series(bgf_handle* h, int n, const double* t, const double* r)
     h->rain_n_dev = n;
     h->rain_t.assign(t, t + n);
     h->rain_r.assign(r, r + n);
+    if (h->rmap.val) cudaFree((void*)h->rmap.val);  // a uniform series replaces a gridded one
+    h->rmap = RainMapDev{};
+    h->has_rmap = false;
     if (n > 0) {
         BGF_CUDA(cudaMalloc((void**)&h->d_rain_t, n * sizeof(double)));
         BGF_CUDA(cudaMalloc((void**)&h->d_rain_r, n * sizeof(double)));
         BGF_CUDA(cudaMemcpy(h->d_rain_t, t, n * sizeof(double), cudaMemcpyHostToDevice));
         BGF_CUDA(cudaMemcpy(h->d_rain_r, r, n * sizeof(double), cudaMemcpyHostToDevice));
     }
+    free_graphs(h);
+    return BGF_OK;
+}
+
+int bgf_set_rain_map(bgf_handle* h, int nx, int ny, double xo, double yo, double dx, double dy, int nt, double to,
+                     double dt, const float* frames)
+{
+    if (!h || nx < 2 || ny < 2 || nt < 2 || !(dx > 0.0) || !(dy > 0.0) || !(dt > 0.0) || !frames) return BGF_EINVAL;
+    int rc = set_device(h);
+    if (rc) return rc;
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->rmap.val) cudaFree((void*)h->rmap.val);
+    h->rmap = RainMapDev{};
+    h->has_rmap = false;
+    // a gridded series replaces a uniform one
+    if (h->d_rain_t) { cudaFree(h->d_rain_t); h->d_rain_t = nullptr; }
+    if (h->d_rain_r) { cudaFree(h->d_rain_r); h->d_rain_r = nullptr; }
+    h->rain_n_dev = 0;
+    h->rain_t.clear();
+    h->rain_r.clear();
+    const size_t n = (size_t)nx * ny * nt;
+    float* d = nullptr;
+    BGF_CUDA(cudaMalloc((void**)&d, n * sizeof(float)));
+    BGF_CUDA(cudaMemcpy(d, frames, n * sizeof(float), cudaMemcpyHostToDevice));
+    RainMapDev& r = h->rmap;
+    r.val = d;
+    r.nx = nx;
+    r.ny = ny;
+    r.nt = nt;
+    r.xo = xo;
+    r.yo = yo;
+    r.dx = dx;
+    r.dy = dy;
+    r.xmax = xo + (nx - 1) * dx;
+    r.ymax = yo + (ny - 1) * dy;
+    r.to = to;
+    r.dt = dt;
+    h->has_rmap = true;
     free_graphs(h);
     return BGF_OK;
 }

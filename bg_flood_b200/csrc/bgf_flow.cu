@@ -249,10 +249,17 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
             bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);
         }
         if (p.has_rain) {
-            // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): uniform rain rate
-            // interpolated at the start of the step (updateforcing)
-            double rnow = series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime);
-            T Rainhh = (T)rnow;
+            // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): the rain rate at
+            // the start of the step (updateforcing), uniform or gridded
+            T Rainhh;
+            if (p.rain_map) {
+                // the cell position as AddrainforcingImplicitCPU forms it, in T
+                const T xc = (T)p.xo_d + (T)m.bxo[ib] + (T)x * delta;
+                const T yc = (T)p.yo_d + (T)m.byo[ib] + (T)y * delta;
+                Rainhh = rain_map_at<T>(m.rmap, xc, yc, ts.totaltime);
+            } else {
+                Rainhh = (T)series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime);
+            }
             T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
             Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
             T hi = SPLIT ? D + ho : ho;

@@ -64,6 +64,16 @@ template <class T> struct StepParams {
     T cf;        // uniform friction coefficient
     int frictionmodel, forcemass, has_cf, has_rain, nseg, rain_n, rain_off;
     int nriver, riv_first;  // rivers of this scenario: entries riv_first .. riv_first + nriver - 1
+    int rain_map;           // 1: the rain rate is a gridded series (m.rmap), else the uniform series
+};
+
+// A gridded rain series (the reference's DynForcingP<float> Rain read from a
+// file): nt frames of nx*ny nodes from (xo, yo) with spacings dx, dy, frame k at
+// time to + k*dt; frames row-major with row 0 at yo.
+struct RainMapDev {
+    const float* val;
+    int nx, ny, nt;
+    double xo, yo, dx, dy, xmax, ymax, to, dt;
 };
 
 // A river (the reference's River / RiverInfo): discharge box, discharge area (sum
@@ -91,6 +101,7 @@ template <class T> struct DevModel {
     const double* seg_wl;
     const double* rain_t;
     const double* rain_r;
+    RainMapDev rmap;
     const RiverDev* rivers;
     const double* riv_t;
     const double* riv_q;

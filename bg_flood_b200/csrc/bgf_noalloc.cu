@@ -113,6 +113,7 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     m.hmax = nullptr;
     m.checklev = 1;
     m.datum = nullptr;
+    m.rmap = RainMapDev{};
     m.rivers = nullptr;
     m.riv_t = nullptr;
     m.riv_q = nullptr;
@@ -149,6 +150,7 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     p.xo_d = 0.0;
     p.yo_d = 0.0;
     p.nriver = 0;
+    p.rain_map = 0;
     p.riv_first = 0;
 
     // per-call state: time slot 0 from the caller's loop, the dt minimum, the error

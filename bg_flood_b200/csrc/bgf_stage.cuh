@@ -37,6 +37,33 @@ __device__ __forceinline__ double series_at(const double* t, const double* v, in
     return v[st - 1] + (time - t[st - 1]) / (t[st] - t[st - 1]) * (v[st] - v[st - 1]);
 }
 
+// Gridded rain rate (mm/h) at (x, y) and `time`: the two frames around `time`
+// (Forcingthisstep, src/Updateforcing.cu:87-125: frame index clamped to
+// [0, nt-2]) interpolated in time at the four grid nodes around the point, each
+// rounded to float as the reference's "now" grid holds it, then the bilinear
+// interpolation of interp2BUQ (src/GridManip.cu:540-575) in double.
+template <class T> __device__ __forceinline__ T rain_map_at(const RainMapDev& r, T x, T y, double time)
+{
+    int st = (int)floor((time - r.to) / r.dt);
+    st = min(max(st, 0), r.nt - 2);
+    const double tb = r.to + r.dt * st;
+    const float* b = r.val + (size_t)st * r.nx * r.ny;
+    const float* a = b + (size_t)r.nx * r.ny;
+    const double xi = fmax(fmin((double)x, r.xmax), r.xo);
+    const double yi = fmax(fmin((double)y, r.ymax), r.yo);
+    const int cfi = min(max((int)floor((xi - r.xo) / r.dx), 0), r.nx - 2), cfip = cfi + 1;
+    const int cfj = min(max((int)floor((yi - r.yo) / r.dy), 0), r.ny - 2), cfjp = cfj + 1;
+    auto now = [&](int i, int j) -> double {
+        const size_t k = (size_t)i + (size_t)j * r.nx;
+        return (double)(float)((double)b[k] + (time - tb) * (double)(a[k] - b[k]) / r.dt);
+    };
+    const double q11 = now(cfi, cfj), q12 = now(cfi, cfjp), q21 = now(cfip, cfj), q22 = now(cfip, cfjp);
+    const double x1 = r.xo + r.dx * cfi, x2 = r.xo + r.dx * cfip;
+    const double y1 = r.yo + r.dy * cfj, y2 = r.yo + r.dy * cfjp;
+    const double x2x1 = x2 - x1, y2y1 = y2 - y1, x2x = x2 - xi, y2y = y2 - yi, yy1 = yi - y1, xx1 = xi - x1;
+    return (T)(1.0 / (x2x1 * y2y1) * (q11 * x2x * y2y + q21 * xx1 * y2y + q12 * x2x * yy1 + q22 * xx1 * yy1));
+}
+
 // River discharge of one river at `time` per unit area, as AddRiverForcing computes
 // it (src/Updateforcing.cu:146-170): the first sample later than `time`, the
 // interpolated discharge rounded to T, then divided by the discharge area.

@@ -148,6 +148,15 @@ class FlowB200:
         _check(lib().bgf_set_rain_series(self.handle, len(t), t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                          r.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "bgf_set_rain_series")
 
+    def set_rain_map(self, xo: float, yo: float, dx: float, dy: float, to: float, dt: float, frames) -> None:
+        """Gridded rain (mm/h): frames (nt, ny, nx) of nodes from (xo, yo), frame k at
+        time to + k*dt."""
+        fr = np.ascontiguousarray(frames, np.float32)
+        nt, ny, nx = fr.shape
+        _check(lib().bgf_set_rain_map(self.handle, nx, ny, float(xo), float(yo), float(dx), float(dy), nt,
+                                      float(to), float(dt), fr.ctypes.data), "bgf_set_rain_map")
+        self._rain_map = fr
+
     def add_river(self, xstart: float, xend: float, ystart: float, yend: float, times, q) -> float:
         """A river discharging q(t) (m^3/s) over the cells its box overlaps; returns
         the discharge area (0: the box misses every cell and the river is dropped)."""

@@ -254,6 +254,21 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* args, bgf_
 int bgf_mesh_uniform(int nbx, int nby, double levdx, const uint8_t* present, int* nblk, int* level,
                      int* nbr8, double* xo, double* yo, int doubleprecision);
 
+/* ------------------------------------------------------------ gridded rain */
+/* Rain rate (mm/h) as a gridded series: nt >= 2 frames of nx*ny float nodes from
+ * (xo, yo) (absolute coordinates) with spacings dx, dy, frame k at time
+ * to + k*dt, frames row-major with row 0 at yo (frames[k*nx*ny + j*nx + i]) --
+ * the reference's Rain DynForcingP read from a netCDF file, whose reader is not
+ * part of this library.  At the start of each step the two frames around the
+ * time (index clamped to [0, nt-2], Forcingthisstep, src/Updateforcing.cu:87-125)
+ * are interpolated in time at the grid nodes, then bilinearly at the cell
+ * centre as the reference's CPU rain does (interp2BUQ, AddrainforcingImplicitCPU,
+ * src/GridManip.cu:540-575, src/Updateforcing.cu:530-580); the reference's GPU
+ * path samples a texture instead.  Replaces a uniform series (and
+ * bgf_set_rain_series replaces the map).  Not supported in pools. */
+int bgf_set_rain_map(bgf_handle* h, int nx, int ny, double xo, double yo, double dx, double dy, int nt, double to,
+                     double dt, const float* frames);
+
 /* ------------------------------------------------------------ rivers */
 #define BGF_MAX_RIVERS 64
 /* A river: discharge q(t) (m^3/s, n >= 2 samples, increasing times) spread over

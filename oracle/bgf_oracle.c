@@ -83,6 +83,10 @@ int ora_add_segment(void* m, int type, int n, const double* t, const double* wl,
                   api_add_segment_d(MD, type, n, t, wl, nblk_side, blk_side)); }
 int ora_set_rain(void* m, int n, const double* t, const double* r)
 { return DISPATCH(api_set_rain_f(MF, n, t, r), api_set_rain_d(MD, n, t, r)); }
+int ora_set_rain_map(void* m, int nx, int ny, double xo, double yo, double dx, double dy, int nt, double to, double dt,
+                     const float* frames)
+{ return DISPATCH(api_set_rain_map_f(MF, nx, ny, xo, yo, dx, dy, nt, to, dt, frames),
+                  api_set_rain_map_d(MD, nx, ny, xo, yo, dx, dy, nt, to, dt, frames)); }
 double ora_add_river(void* m, double xs, double xe, double ys, double ye, int n, const double* t, const double* q)
 { return DISPATCH(api_add_river_f(MF, xs, xe, ys, ye, n, t, q), api_add_river_d(MD, xs, xe, ys, ye, n, t, q)); }
 int ora_init_bed(void* m) { return DISPATCH(api_init_bed_f(MF), api_init_bed_d(MD)); }

@@ -56,6 +56,9 @@ int ora_get_field(void* m, const char* name, double* buq);
 int ora_add_segment(void* m, int type, int n, const double* t, const double* wl,
                     const int* nblk_side, const int* const* blk_side);
 int ora_set_rain(void* m, int n, const double* t, const double* r);
+/* Gridded rain: nt frames (row-major, row 0 at yo) of nx*ny nodes, frame k at to + k*dt. */
+int ora_set_rain_map(void* m, int nx, int ny, double xo, double yo, double dx, double dy, int nt, double to, double dt,
+                     const float* frames);
 /* A river (box in absolute coordinates, discharge series); returns the discharge area. */
 double ora_add_river(void* m, double xs, double xe, double ys, double ye, int n, const double* t, const double* q);
 

@@ -51,6 +51,9 @@ def oracle_lib():
         l.ora_add_segment.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D, D, I, ctypes.POINTER(I)]
         l.ora_set_rain.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         l.ora_init_bed.argtypes = [ctypes.c_void_p]
+        l.ora_set_rain_map.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                       ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_float)]
         l.ora_add_river.restype = ctypes.c_double
         l.ora_add_river.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_int, D, D]
@@ -100,6 +103,9 @@ def ref_lib():
         l.ref_rain.argtypes = [ctypes.c_void_p, D, D]
         l.ref_segment.argtypes = [ctypes.c_void_p, ctypes.c_int, I, D, D]
         l.ref_get_active_cell.argtypes = [ctypes.c_void_p, I]
+        l.ref_set_rain_map.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         _rlib = l
     return _rlib
 
@@ -171,6 +177,13 @@ class Oracle:
         t = np.ascontiguousarray(times, np.float64)
         r = np.ascontiguousarray(rates, np.float64)
         oracle_lib().ora_set_rain(self.h, len(t), _dp(t), _dp(r))
+
+    def set_rain_map(self, xo, yo, dx, dy, to, dt, frames):
+        fr = np.ascontiguousarray(frames, np.float32)
+        nt, ny, nx = fr.shape
+        oracle_lib().ora_set_rain_map(self.h, nx, ny, xo, yo, dx, dy, nt, to, dt,
+                                      fr.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        self._rain_map = fr
 
     def add_river(self, xs, xe, ys, ye, times, q) -> float:
         t = np.ascontiguousarray(times, np.float64)
@@ -258,6 +271,13 @@ class Reference:
         t, w = np.zeros(cap), np.zeros(cap)
         n = self.lib.ref_segment(self.h, iseg, ctypes.byref(typ), _dp(t), _dp(w))
         return typ.value, t[:n], w[:n]
+
+    def set_rain_map(self, xo, yo, dx, dy, to, dt, before, after):
+        b = np.ascontiguousarray(before, np.float32)
+        a = np.ascontiguousarray(after, np.float32)
+        ny, nx = b.shape
+        F = ctypes.POINTER(ctypes.c_float)
+        self.lib.ref_set_rain_map(self.h, nx, ny, xo, yo, dx, dy, to, dt, b.ctypes.data_as(F), a.ctypes.data_as(F))
 
     def active_cell(self) -> np.ndarray:
         a = np.zeros(self.nblk * 324, np.int32)

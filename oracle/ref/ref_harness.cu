@@ -519,6 +519,44 @@ int ref_segment(void* hdl, int iseg, int* type, double* t, double* wl)
 
 int ref_get_active_cell(void* hdl, int* out) { return ((RefBase*)hdl)->get_active_cell(out); }
 
+// Gridded rain of two frames (before at time `to`, after at to + dt) installed as
+// the reference holds a netCDF rain map after its first read (DynForcingP with
+// instep = 1, so Forcingthisstep interpolates without reading a file while the
+// time stays below to + dt).  Its CPU time interpolation counts from time 0
+// (InterpstepCPU, src/GridManip.cu:602-621), so `to` must be 0.
+int ref_set_rain_map(void* hdl, int nx, int ny, double xo, double yo, double dx, double dy, double to, double dt,
+                     const float* before, const float* after)
+{
+    RefBase* m = (RefBase*)hdl;
+    DynForcingP<float>& R = m->F.Rain;
+    R.inputfile = "rain_map";
+    R.uniform = false;
+    R.nx = nx;
+    R.ny = ny;
+    R.xo = xo;
+    R.yo = yo;
+    R.dx = dx;
+    R.dy = dy;
+    R.xmax = xo + (nx - 1) * dx;
+    R.ymax = yo + (ny - 1) * dy;
+    R.nt = 2;
+    R.to = to;
+    R.dt = dt;
+    R.tmax = to + dt;
+    R.instep = 1;
+    const size_t n = (size_t)nx * ny;
+    R.before = (float*)malloc(n * sizeof(float));
+    R.after = (float*)malloc(n * sizeof(float));
+    R.val = (float*)malloc(n * sizeof(float));
+    R.now = R.val;
+    for (size_t k = 0; k < n; k++) {
+        R.before[k] = before[k];
+        R.after[k] = after[k];
+        R.val[k] = before[k];
+    }
+    return 0;
+}
+
 int ref_step(void* hdl, int nsteps, double* dts) { return ((RefBase*)hdl)->step(nsteps, dts); }
 int ref_adapt(void* hdl) { return ((RefBase*)hdl)->adapt(); }
 int ref_set(void* hdl, const char* name, const double* buq) { return ((RefBase*)hdl)->set(name, buq); }

@@ -165,9 +165,24 @@ def main_setup():
         np.savez_compressed(os.path.join(HERE, "asc_variants.npz"), **out)
 
 
+def main_rainmap():
+    """The reference's FlowCPU with a two-frame rain map (tests/rainmap_case.py)."""
+    from rainmap_case import MAP, NSTEPS, rainmap_case
+    c, before, after = rainmap_case()
+    r = make_reference(c)
+    r.set_rain_map(MAP["xo"], MAP["yo"], MAP["dx"], MAP["dy"], MAP["to"], MAP["dt"], before, after)
+    dts = r.step(NSTEPS)
+    out = {k: interior(r.get(k)).astype(np.float32) for k in ("h", "u", "v", "zs")}
+    np.savez_compressed(os.path.join(HERE, "rainmap48_e1.npz"), dts=dts, nsteps=NSTEPS, **out)
+    print("rainmap48_e1", NSTEPS, dts[:3])
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["setup"]:
         main_setup()
+        sys.exit(0)
+    if sys.argv[1:] == ["rainmap"]:
+        main_rainmap()
         sys.exit(0)
     main()
     main_amr()

@@ -9,8 +9,8 @@ A step is one full flow step (predictor + corrector) of the whole grid.
 * value:   device time of K steps (CUDA events around the two kernels on the
            library's stream), L2 flushed before every step, max over ranks.
 * e2e:     the same K steps through the C ABI with host buffers: state upload
-           from host, K bgf_flow_step calls (each returns dt to the host), state
-           download; wall clock.
+           from page-locked host arrays, K bgf_flow_step calls (each returns dt
+           to the host), state download into page-locked arrays; wall clock.
 * roofline: the dominant kernel's algorithmic bytes per launch / its mean event
            time, against the measured HBM copy bandwidth.
 * cpu_baseline: the reference BG_Flood FlowCPU (built from its sources,
@@ -413,7 +413,15 @@ def main():
                 traffic = float(ln.split(":")[1]) * ncell
 
     # end to end through the C ABI with host buffers
+    # the step inputs and results live in page-locked host buffers, allocated once as
+    # a caller that streams states would hold them
     zs, h, u, v = f.get_state()
+    keep = [torch.empty(a.shape, dtype=torch.float64 if a.dtype == np.float64 else torch.float32, pin_memory=True)
+            for a in (zs, h, u, v, h, u, v)]
+    outs = [t.numpy() for t in keep[:4]]
+    h, u, v = [t.numpy() for t in keep[4:]]
+    f.get_state(out=outs)
+    h[...], u[...], v[...] = outs[1], outs[2], outs[3]
     e2e_loop = type(loop)(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=case.nextoutputtime)
     f.init_dt(e2e_loop)
     torch.cuda.synchronize()
@@ -421,11 +429,15 @@ def main():
     f.set_state(h, u, v)
     for _ in range(args.steps):
         e2e_loop.totaltime += f.flow_step(e2e_loop)
-    zs2, h2, u2, v2 = f.get_state()
+    f.get_state(out=outs)
     e2e_s = time.perf_counter() - t0
+    # bytes that crossed the host link: whole 18x18 tiles of h, u, v up and of zs, h,
+    # u, v down (page-locked arrays go by DMA), and per step the time state up (80 B)
+    # with the dt seed (8 B), the time state (80 B) and the error word (4 B) down
     tslot = 80
-    h2d = (3 * ncell * 4 + args.steps * (tslot + 8)) / args.steps
-    d2h = ((3 * ncell + mesh.nblk * 324) * 4 + args.steps * tslot) / args.steps
+    es = outs[0].itemsize
+    h2d = (3 * f.nblkmem * 324 * es + args.steps * (tslot + 8)) / args.steps
+    d2h = (4 * f.nblkmem * 324 * es + args.steps * (tslot + 4)) / args.steps
     e2e_val = world * ncell * args.steps / e2e_s
 
     extra = {}

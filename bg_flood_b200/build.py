@@ -34,6 +34,7 @@ SOURCES = [
     ("bgf_host.cpp", "bgf_host.o", ["-x", "cu", "--fmad=false"]),
     ("bgf_adapt_host.cpp", "bgf_adapt_host.o", ["-x", "cu", "--fmad=false"]),
     ("bgf_io.cpp", "bgf_io.o", ["-x", "cu", "--fmad=false"]),
+    ("bgf_layout.cu", "bgf_layout.o", ["--fmad=false"]),
 ]
 
 

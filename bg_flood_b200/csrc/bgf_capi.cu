@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/bg_flood_b200.h"
@@ -73,6 +74,8 @@ struct bgf_handle {
     unsigned long long* d_dtmin = nullptr;
     double* d_scratch = nullptr;
     TimeState* h_time = nullptr;  // pinned
+    // pinned scalars: [0] dt-minimum seed (H2D), [1] device error word (D2H)
+    unsigned long long* h_misc = nullptr;
     int cur = 0, parity = 0;
     bool has_blocks = false, has_bed = false, has_state = false, has_cf = false, has_rainmask = false;
     int nseg_dev = 0, rain_n_dev = 0;
@@ -91,6 +94,9 @@ struct bgf_handle {
     // pinned staging buffer for host <-> device copies of BUQ fields
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // device tile scratch for the layout kernels (pinned caller arrays)
+    void* d_tiles = nullptr;
+    size_t tiles_bytes = 0;
     // multi-level meshes: stage tiles with halos, pre-prolongation gradients, face
     // arrays, wet/dry prolongation decisions and the active-list rank of each block
     bool amr = false;
@@ -269,6 +275,35 @@ static void* staging(bgf_handle* h, size_t bytes)
     return h->pinned;
 }
 
+// Device tile scratch of at least `bytes` (grown on demand, kept for the handle).
+static void* tile_scratch(bgf_handle* h, size_t bytes)
+{
+    if (h->tiles_bytes < bytes) {
+        if (h->d_tiles) cudaFree(h->d_tiles);
+        h->d_tiles = nullptr;
+        h->tiles_bytes = 0;
+        if (cudaMalloc(&h->d_tiles, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        h->tiles_bytes = bytes;
+    }
+    return h->d_tiles;
+}
+
+// True when p is page-locked host memory (cudaMallocHost / cudaHostRegister):
+// such arrays can be copied by DMA as they are.
+static bool host_pinned(const void* p)
+{
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 // ---------------------------------------------------------------- C ABI
 // (C linkage comes from the declarations in include/bg_flood_b200.h)
 
@@ -409,6 +444,10 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
     cudaMemsetAsync(h->d_dhu, 0, nb * 256 * es, h->stream);
     cudaMemsetAsync(h->d_dhv, 0, nb * 256 * es, h->stream);
     cudaMemsetAsync(h->d_datum, 0, nb * es, h->stream);
+    if (cudaMallocHost((void**)&h->h_misc, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+        bgf_destroy(h);
+        return BGF_ENOMEM;
+    }
     if (cudaMallocHost((void**)&h->h_time, 2 * sizeof(TimeState)) != cudaSuccess) {
         bgf_destroy(h);
         return BGF_ENOMEM;
@@ -443,11 +482,12 @@ int bgf_destroy(bgf_handle* h)
                     h->d_rain_r, h->d_h[0], h->d_h[1], h->d_u[0], h->d_u[1], h->d_v[0], h->d_v[1], h->d_dh,
                     h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch, h->d_bxo, h->d_byo,
                     h->d_flags, h->d_child, h->d_dem, h->d_datum, h->d_rivers, h->d_riv_t, h->d_riv_q,
-                    (void*)h->rmap.val};
+                    (void*)h->rmap.val, h->d_tiles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     free_amr(h);
     if (h->h_time) cudaFreeHost(h->h_time);
+    if (h->h_misc) cudaFreeHost(h->h_misc);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     for (int k = 0; k < 3; k++)
@@ -826,6 +866,38 @@ int bgf_add_river(bgf_handle* h, double xstart, double xend, double ystart, doub
     return BGF_OK;
 }
 
+// Runs fn(b0, b1) over the block range [0, n) in contiguous pieces on up to 8 host
+// threads when the range is large enough to pay for starting them.
+template <class F> static void parallel_blocks(size_t n, F fn)
+{
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = std::min<unsigned>(8, hw);
+    if (n < 1024 || nt <= 1) {
+        fn((size_t)0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t chunk = (n + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; t++) {
+        const size_t b0 = t * chunk, b1 = std::min(n, b0 + chunk);
+        if (b0 >= b1) break;
+        th.emplace_back(fn, b0, b1);
+    }
+    for (auto& x : th) x.join();
+}
+
+// Interior cells of BUQ tiles (324 per block, source type S) to compact blocks
+// (256 per block, type T), blocks [b0, b1).
+template <class T, class S> static void tiles_to_compact(const S* src, T* dst, size_t b0, size_t b1)
+{
+    for (size_t ib = b0; ib < b1; ib++)
+        for (int j = 0; j < 16; j++) {
+            const S* r = src + ib * 324 + (size_t)(j + 1) * 18 + 1;
+            T* w = dst + ib * 256 + (size_t)j * 16;
+            for (int i = 0; i < 16; i++) w[i] = (T)r[i];
+        }
+}
+
 template <class T> static int set_state_t(bgf_handle* h, const bgf_evolving* ev)
 {
     size_t nb = h->nblkmem;
@@ -833,27 +905,48 @@ template <class T> static int set_state_t(bgf_handle* h, const bgf_evolving* ev)
     if (!a) return BGF_ENOMEM;
     void* dst[3] = {h->d_h[h->cur], h->d_u[h->cur], h->d_v[h->cur]};
     const void* src[3] = {ev->h, ev->u, ev->v};
-    for (int f = 0; f < 3; f++) {
-        T* o = a + f * nb * 256;
-        for (size_t ib = 0; ib < nb; ib++)
-            for (int j = 0; j < 16; j++)
-                for (int i = 0; i < 16; i++) {
-                    size_t s = ib * 324 + (i + 1) + (j + 1) * 18;
-                    const size_t q = ib * 256 + j * 16 + i;
-                    if (h->split && f == 0) {
-                        // deviation from the datum, chosen so that the model surface
-                        // zb (as stored) + datum + deviation is the given zb + h
-                        const double hv = ((const double*)src[0])[s];
-                        const double D = h->datum[ib];
-                        const double zf = (double)(T)h->zbd[s];
-                        double dev = hv > 0.0 ? (h->zbd[s] + hv) - zf - D : -D;
-                        o[q] = (T)std::max(dev, -D);
-                        continue;
-                    }
-                    o[q] = h->iodbl ? (T)((const double*)src[f])[s] : (T)((const float*)src[f])[s];
-                }
-        BGF_CUDA(cudaMemcpyAsync(dst[f], o, nb * 256 * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    const bool split = h->split != 0, iodbl = h->iodbl != 0;
+    if (!split && host_pinned(src[0]) && host_pinned(src[1]) && host_pinned(src[2])) {
+        // pinned caller arrays: whole tiles by DMA, interiors picked out on the device
+        T* tiles = (T*)tile_scratch(h, 3 * nb * 324 * sizeof(T));
+        if (!tiles) return BGF_ENOMEM;
+        for (int f = 0; f < 3; f++)
+            BGF_CUDA(cudaMemcpyAsync(tiles + f * nb * 324, src[f], nb * 324 * sizeof(T), cudaMemcpyHostToDevice,
+                                     h->stream));
+        layout::launch_tiles_to_compact<T>(tiles, (T*)dst[0], (T*)dst[1], (T*)dst[2], nb, h->stream);
+        BGF_CUDA(cudaGetLastError());
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
+        h->has_state = true;
+        return BGF_OK;
     }
+    // one pass over the blocks converts the three fields
+    parallel_blocks(nb, [=](size_t b0, size_t b1) {
+        for (int f = 0; f < 3; f++) {
+            T* o = a + f * nb * 256;
+            if (split && f == 0) {
+                // deviation from the datum, chosen so that the model surface
+                // zb (as stored) + datum + deviation is the given zb + h
+                const double* hs = (const double*)src[0];
+                for (size_t ib = b0; ib < b1; ib++) {
+                    const double D = h->datum[ib];
+                    for (int j = 0; j < 16; j++)
+                        for (int i = 0; i < 16; i++) {
+                            const size_t s = ib * 324 + (i + 1) + (j + 1) * 18;
+                            const double hv = hs[s];
+                            const double zf = (double)(T)h->zbd[s];
+                            const double dev = hv > 0.0 ? (h->zbd[s] + hv) - zf - D : -D;
+                            o[ib * 256 + j * 16 + i] = (T)std::max(dev, -D);
+                        }
+                }
+            } else if (iodbl) {
+                tiles_to_compact<T, double>((const double*)src[f], o, b0, b1);
+            } else {
+                tiles_to_compact<T, float>((const float*)src[f], o, b0, b1);
+            }
+        }
+    });
+    for (int f = 0; f < 3; f++)
+        BGF_CUDA(cudaMemcpyAsync(dst[f], a + f * nb * 256, nb * 256 * sizeof(T), cudaMemcpyHostToDevice, h->stream));
     BGF_CUDA(cudaStreamSynchronize(h->stream));
     h->has_state = true;
     return BGF_OK;
@@ -869,9 +962,70 @@ int bgf_set_state(bgf_handle* h, const bgf_evolving* ev)
     return h->dbl ? set_state_t<double>(h, ev) : set_state_t<float>(h, ev);
 }
 
+// Compact blocks (type T) back into BUQ tiles (type O): the interior cells of the
+// active blocks hold the state (zs = zb + h in T; in double from the datum in split
+// mode), every other entry of the nblkmem tiles is set to 0.
+template <class T, class O> static void compact_to_tiles(const bgf_handle* h, const T* hh, const T* uu, const T* vv,
+                                                         const T* zb, bgf_evolving* ev)
+{
+    O* outs[4] = {(O*)ev->zs, (O*)ev->h, (O*)ev->u, (O*)ev->v};
+    std::vector<uint8_t> isact(h->nblkmem, 0);
+    for (int ibl = 0; ibl < h->nblk; ibl++) isact[h->active[ibl]] = 1;
+    const uint8_t* act = isact.data();
+    const bool split = h->split != 0;
+    parallel_blocks((size_t)h->nblkmem, [=](size_t b0, size_t b1) {
+        for (size_t ib = b0; ib < b1; ib++) {
+            if (!act[ib]) {
+                for (O* o : outs)
+                    if (o) memset(o + ib * 324, 0, 324 * sizeof(O));
+                continue;
+            }
+            const double D = split ? h->datum[ib] : 0.0;
+            for (O* o : outs)
+                if (o) {
+                    memset(o + ib * 324, 0, 18 * sizeof(O));
+                    memset(o + ib * 324 + 17 * 18, 0, 18 * sizeof(O));
+                }
+            for (int j = 0; j < 16; j++) {
+                const size_t d0 = ib * 324 + (size_t)(j + 1) * 18, s0 = ib * 256 + (size_t)j * 16;
+                for (O* o : outs)
+                    if (o) o[d0] = o[d0 + 17] = (O)0;
+                for (int i = 0; i < 16; i++) {
+                    const size_t d = d0 + 1 + i, s = s0 + i;
+                    if (split) {
+                        // full depth and surface in double from the datum and the deviation
+                        if (outs[1]) outs[1][d] = (O)(D + (double)hh[s]);
+                        if (outs[0]) outs[0][d] = (O)((double)zb[d] + D + (double)hh[s]);
+                    } else {
+                        if (outs[1]) outs[1][d] = (O)hh[s];
+                        if (outs[0]) outs[0][d] = (O)(T)(zb[d] + hh[s]);
+                    }
+                    if (outs[2]) outs[2][d] = (O)uu[s];
+                    if (outs[3]) outs[3][d] = (O)vv[s];
+                }
+            }
+        }
+    });
+}
+
 template <class T> static int get_state_t(bgf_handle* h, bgf_evolving* ev)
 {
     size_t nb = h->nblkmem;
+    if (!h->split && host_pinned(ev->zs) && host_pinned(ev->h) && host_pinned(ev->u) && host_pinned(ev->v)) {
+        // pinned caller arrays: tiles composed on the device, then copied by DMA
+        T* tiles = (T*)tile_scratch(h, 4 * nb * 324 * sizeof(T));
+        if (!tiles) return BGF_ENOMEM;
+        BGF_CUDA(cudaMemsetAsync(tiles, 0, 4 * nb * 324 * sizeof(T), h->stream));
+        layout::launch_compact_to_tiles<T>(h->d_active, h->nblk, (const T*)h->d_h[h->cur], (const T*)h->d_u[h->cur],
+                                           (const T*)h->d_v[h->cur], (const T*)h->d_zb, tiles, nb, h->stream);
+        BGF_CUDA(cudaGetLastError());
+        void* outs[4] = {ev->zs, ev->h, ev->u, ev->v};
+        for (int f = 0; f < 4; f++)
+            BGF_CUDA(cudaMemcpyAsync(outs[f], tiles + f * nb * 324, nb * 324 * sizeof(T), cudaMemcpyDeviceToHost,
+                                     h->stream));
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
+        return BGF_OK;
+    }
     T* a = (T*)staging(h, (3 * nb * 256 + nb * 324) * sizeof(T));
     if (!a) return BGF_ENOMEM;
     T *hh = a, *uu = a + nb * 256, *vv = a + 2 * nb * 256, *zb = a + 3 * nb * 256;
@@ -880,32 +1034,8 @@ template <class T> static int get_state_t(bgf_handle* h, bgf_evolving* ev)
     BGF_CUDA(cudaMemcpyAsync(vv, h->d_v[h->cur], nb * 256 * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
     BGF_CUDA(cudaMemcpyAsync(zb, h->d_zb, nb * 324 * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
     BGF_CUDA(cudaStreamSynchronize(h->stream));
-    for (int ibl = 0; ibl < h->nblk; ibl++) {
-        size_t ib = h->active[ibl];
-        for (int j = 0; j < 16; j++)
-            for (int i = 0; i < 16; i++) {
-                size_t d = ib * 324 + (i + 1) + (j + 1) * 18, s = ib * 256 + j * 16 + i;
-                T z = zb[d] + hh[s];
-                if (h->split) {
-                    // full depth and surface in double from the datum and the deviation
-                    const double D = h->datum[ib];
-                    if (ev->h) ((double*)ev->h)[d] = D + (double)hh[s];
-                    if (ev->u) ((double*)ev->u)[d] = (double)uu[s];
-                    if (ev->v) ((double*)ev->v)[d] = (double)vv[s];
-                    if (ev->zs) ((double*)ev->zs)[d] = (double)zb[d] + D + (double)hh[s];
-                } else if (h->dbl) {
-                    if (ev->h) ((double*)ev->h)[d] = (double)hh[s];
-                    if (ev->u) ((double*)ev->u)[d] = (double)uu[s];
-                    if (ev->v) ((double*)ev->v)[d] = (double)vv[s];
-                    if (ev->zs) ((double*)ev->zs)[d] = (double)z;
-                } else {
-                    if (ev->h) ((float*)ev->h)[d] = (float)hh[s];
-                    if (ev->u) ((float*)ev->u)[d] = (float)uu[s];
-                    if (ev->v) ((float*)ev->v)[d] = (float)vv[s];
-                    if (ev->zs) ((float*)ev->zs)[d] = (float)z;
-                }
-            }
-    }
+    if (h->split || h->dbl) compact_to_tiles<T, double>(h, hh, uu, vv, zb, ev);
+    else compact_to_tiles<T, float>(h, hh, uu, vv, zb, ev);
     return BGF_OK;
 }
 
@@ -1008,6 +1138,9 @@ template <class T> static int enqueue_step(bgf_handle* h, int parity)
     return n + enqueue_update<T>(h, parity);
 }
 
+// Writes the loop state into the device time slot of the current parity and seeds
+// the dt minimum.  Both copies read pinned slots that are not written again before
+// the caller's next stream synchronisation, so no synchronisation is needed here.
 static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep, long long maxsteps)
 {
     TimeState ts;
@@ -1024,11 +1157,10 @@ static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, 
     ts.done = 0;
     ts.status = 0;
     h->h_time[0] = ts;
-    unsigned long long init = dt_init_bits(h->dbl);
+    h->h_misc[0] = dt_init_bits(h->dbl);
     BGF_CUDA(cudaMemcpyAsync(h->d_time + h->parity, &h->h_time[0], sizeof(TimeState), cudaMemcpyHostToDevice, h->stream));
-    BGF_CUDA(cudaMemcpyAsync(h->d_dtmin + h->parity, &init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
-    // the pinned staging slot must not be reused before the copy has executed
-    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->d_dtmin + h->parity, &h->h_misc[0], sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                             h->stream));
     return BGF_OK;
 }
 
@@ -1059,8 +1191,10 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
     }
     h->launches += n;
     BGF_CUDA(cudaGetLastError());
+    // the step's time state and the device error word, read back with one synchronisation
     BGF_CUDA(cudaMemcpyAsync(&h->h_time[1], h->d_time + (h->parity ^ 1), sizeof(TimeState), cudaMemcpyDeviceToHost,
                              h->stream));
+    BGF_CUDA(cudaMemcpyAsync(&h->h_misc[1], h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     BGF_CUDA(cudaStreamSynchronize(h->stream));
     if (h->profiling) {
         float a = 0.f, b = 0.f;
@@ -1070,8 +1204,10 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
         h->update_ms += b;
         h->profiled_steps++;
     }
-    rc = check_err_word(h);
-    if (rc) return rc;
+    if (*(const int*)&h->h_misc[1]) {
+        g_last_error = "mesh has cross-level neighbours, which this build does not support yet";
+        return BGF_EINVAL;
+    }
     const TimeState& nt = h->h_time[1];
     loop->dt = nt.dt;
     loop->dtmax = nt.dtmax;

@@ -54,6 +54,14 @@ template <class T> void launch_bed(const DevModel<T>& m, const AdaptDev<T>& a, c
                                    uint8_t* rainmask, cudaStream_t st);
 }  // namespace adapt
 
+// Tile <-> compact layout kernels (bgf_layout.cu) for pinned host arrays.
+namespace layout {
+template <class T> void launch_tiles_to_compact(const T* tiles, T* h, T* u, T* v, size_t nb, cudaStream_t st);
+template <class T>
+void launch_compact_to_tiles(const int* active, int nblk, const T* h, const T* u, const T* v, const T* zb, T* tiles,
+                             size_t nb, cudaStream_t st);
+}  // namespace layout
+
 // Records the text returned by bgf_last_error() for this thread.
 void set_last_error(const std::string& msg);
 

@@ -174,9 +174,16 @@ class FlowB200:
         ev = CEvolving(None, _ptr(hh), _ptr(uu), _ptr(vv))
         _check(lib().bgf_set_state(self.handle, ctypes.byref(ev)), "bgf_set_state")
 
-    def get_state(self):
-        """Returns (zs, h, u, v) as (nblkmem, 18, 18) arrays (interior cells filled)."""
-        out = [np.zeros((self.nblkmem, 18, 18), self.dtype) for _ in range(4)]
+    def get_state(self, out=None):
+        """Returns (zs, h, u, v) as (nblkmem, 18, 18) arrays (interior cells filled).
+        ``out``: four such arrays of the handle's field type to fill instead of new ones."""
+        if out is None:
+            out = [np.zeros((self.nblkmem, 18, 18), self.dtype) for _ in range(4)]
+        else:
+            out = list(out)
+            for a in out:
+                if a.dtype != self.dtype or a.shape != (self.nblkmem, 18, 18) or not a.flags.c_contiguous:
+                    raise ValueError("get_state: out arrays must be C-contiguous (nblkmem, 18, 18) of the field type")
         ev = CEvolving(*[_ptr(a) for a in out])
         _check(lib().bgf_get_state(self.handle, ctypes.byref(ev)), "bgf_get_state")
         return tuple(out)

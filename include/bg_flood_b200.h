@@ -159,8 +159,12 @@ int bgf_set_rain_series(bgf_handle* h, int n, const double* t, const double* rai
 
 /* Uploads / downloads the evolving state (EvolvingP) in BUQ layout.  zs is
  * ignored on upload (the step recomputes zs = zb + h everywhere, as
- * RecalculateZs does, src/Halo.cu:72-107); on download only the 16x16
- * interior of each active block is written. */
+ * RecalculateZs does, src/Halo.cu:72-107).  On download the whole nblkmem
+ * tiles of each non-NULL field are written: the 16x16 interior of the active
+ * blocks holds the state, every other entry is 0.  When all arrays are
+ * page-locked (cudaMallocHost / cudaHostRegister), the tiles cross the host
+ * link by DMA and the interiors are picked out on the device; otherwise the
+ * host converts through a pinned staging buffer. */
 int bgf_set_state(bgf_handle* h, const bgf_evolving* ev);
 int bgf_get_state(bgf_handle* h, bgf_evolving* ev);
 

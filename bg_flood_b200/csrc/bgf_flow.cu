@@ -25,12 +25,13 @@ namespace BGF_VARIANT {
 // (RecalculateZs, src/Halo.cu:72-107); ring 2 uses the bed under its source cell,
 // as the neighbour's own RecalculateZs does before gradientHalo reads it.  In split
 // mode beds are deviations zb + D of the tile block's datum D.
+// Read from global memory (the block's own tile for ring 1 and the interior), so
+// that the state tile can be assembled in the same phase as the bed tile.
 template <class T, bool SPLIT>
-__device__ __forceinline__ T tile_zb(const Smem<T>& s, const DevModel<T>& m, int x, int y, int sb, int sx, int sy, T D)
+__device__ __forceinline__ T tile_zb(const DevModel<T>& m, int ib, int x, int y, int sb, int sx, int sy, T D)
 {
     bool ring2 = x < -1 || x > BW || y < -1 || y > BW;
-    if (!ring2) return s.zb[si(x, y)];
-    const T z = m.zb[(size_t)sb * 324 + hi18(sx, sy)];
+    const T z = ring2 ? m.zb[(size_t)sb * 324 + hi18(sx, sy)] : m.zb[(size_t)ib * 324 + hi18(x, y)];
     return SPLIT ? z + D : z;
 }
 
@@ -56,7 +57,8 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
         T hv = H[g], uv = U[g], vv = V[g];
         int c = ti(x, y);
         s.t[VH][c] = hv; s.t[VU][c] = uv; s.t[VV][c] = vv;
-        s.t[VZS][c] = s.zb[si(x, y)] + hv;
+        const T zbv = m.zb[(size_t)ib * 324 + hi18(x, y)];
+        s.t[VZS][c] = (SPLIT ? zbv + D : zbv) + hv;
         int c18 = si(x, y);
         s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
     }
@@ -71,7 +73,7 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
         T hv = to_tile_datum<T, SPLIT>(m, H[g], sb, ib, D), uv = U[g], vv = V[g];
         int c = ti(x, y);
         s.t[VH][c] = hv; s.t[VU][c] = uv; s.t[VV][c] = vv;
-        s.t[VZS][c] = tile_zb<T, SPLIT>(s, m, x, y, sb, sx, sy, D) + hv;
+        s.t[VZS][c] = tile_zb<T, SPLIT>(m, ib, x, y, sb, sx, sy, D) + hv;
         if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
             int c18 = si(x, y);
             s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
@@ -115,7 +117,7 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
         }
         int c = ti(x, y);
         s.t[VH][c] = ho; s.t[VU][c] = uo; s.t[VV][c] = vo;
-        s.t[VZS][c] = tile_zb<T, SPLIT>(s, m, x, y, sb, sx, sy, D) + ho;
+        s.t[VZS][c] = tile_zb<T, SPLIT>(m, ib, x, y, sb, sx, sy, D) + ho;
         if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
             int c18 = si(x, y);
             s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
@@ -159,8 +161,8 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::flux) flux_kernel(DevModel<T
         const int cur = ts.cur;
         const T D = SPLIT ? m.datum[ib] : (T)0;
 
+        // bed and state tiles in one phase (the state tile takes zs from global zb)
         load_bed<T, ENGINE, SPLIT>(s, m, ib, tid, D);
-        __syncthreads();
         load_state_tile<T, SPLIT>(s, m, ib, cur, tid, D);
         __syncthreads();
         T celldt = tile_fluxes<T, ENGINE, false, SPLIT>(s, p, delta, tid, nullptr, D);
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::flux) flux_kernel(DevModel<T
         m.dh[g] = dh;
         m.dhu[g] = dhu;
         m.dhv[g] = dhv;
-        __syncthreads();  // the tile is reused by the next block
+        if (w + (int)gridDim.x < m.nblk) __syncthreads();  // the tile is reused by the next block
     }
 }
 
@@ -220,9 +222,8 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
         const double dtd = (double)dt;
         const T D = SPLIT ? m.datum[ib] : (T)0;
 
-        load_bed<T, ENGINE, SPLIT>(s, m, ib, tid, D);
-        __syncthreads();
         load_half_tile<T, SPLIT>(s, m, p, ib, cur, dt * (T)0.5, tid, D, ts.totaltime);
+        load_bed<T, ENGINE, SPLIT>(s, m, ib, tid, D);
         __syncthreads();
         (void)tile_fluxes<T, ENGINE, false, SPLIT>(s, p, delta, tid, nullptr, D);
         __syncthreads();
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
         }
         if (lead && tid == 0)
             m.time[2 * sc + (parity ^ 1)] = next_time_state<T>(ts, p, dtd, nxt, m.dtmin + 2 * sc, parity);
-        __syncthreads();  // the tile is reused by the next block
+        if (w + (int)gridDim.x < m.nblk) __syncthreads();  // the tile is reused by the next block
     }
 }
 

@@ -348,35 +348,34 @@ __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T d
         else if (side == 2) { cm = ti(q, -2); cr = ti(q, -1); cp = ti(q, 0); out = &s.gy[k][gyi(q, -1)]; }
         else { cm = ti(q, BW - 1); cr = ti(q, BW); cp = ti(q, BW + 1); out = &s.gy[k][gyi(q, BW)]; }
         *out = div_by(minmod2(theta, a[cm], a[cr], a[cp]), delta, rdelta);
-    }
-    __syncthreads();
-    if (ENGINE == 1) {
-        // Wet-slope reset: interior cells follow WetsloperesetCPU (its y test compares
-        // both reconstructions with zs[yminus]); ring-1 cells follow the halo variants.
-        const T* zs = s.t[VZS];
-        const T* hh = s.t[VH];
-        {
-            const int c = ti(tx, ty), gi = gxi(tx, ty), gj = gyi(tx, ty);
-            const T hc = SPLIT ? D + hh[c] : hh[c];
-            const T zsm = zs[ti(tx, ty - 1)];
-            s.gx[VZS][gi] = wetslope(delta, zs[c], hc, zs[c - 1], zs[c + 1], s.gx[VZS][gi], s.gx[VH][gi], s.dzbx[gi]);
-            s.gy[VZS][gj] = wetslope(delta, zs[c], hc, zsm, zsm, s.gy[VZS][gj], s.gy[VH][gj], s.dzby[gj]);
-        }
-        if (tid < 64) {
-            const int side = tid >> 4, q = tid & 15;
-            if (side < 2) {
-                const int x = side == 0 ? -1 : BW, c = ti(x, q), g = gxi(x, q);
+        if (ENGINE == 1) {
+            // Wet-slope reset, in the same phase: each thread resets the zs gradients of its
+            // own interior cell (WetsloperesetCPU; its y test compares both reconstructions
+            // with zs[yminus]); the lane holding a ring cell's zs gradient reads that cell's
+            // h gradient, written by the previous lane of the same warp (halo variants).
+            const T* zs = s.t[VZS];
+            const T* hh = s.t[VH];
+            {
+                const int c = ti(tx, ty), gi = gxi(tx, ty), gj = gyi(tx, ty);
                 const T hc = SPLIT ? D + hh[c] : hh[c];
-                s.gx[VZS][g] = wetslope(delta, zs[c], hc, zs[c - 1], zs[c + 1], s.gx[VZS][g], s.gx[VH][g], s.dzbx[g]);
-            } else {
-                const int y = side == 2 ? -1 : BW, c = ti(q, y), g = gyi(q, y);
-                const T hc = SPLIT ? D + hh[c] : hh[c];
-                s.gy[VZS][g] = wetslope(delta, zs[c], hc, zs[ti(q, y - 1)], zs[ti(q, y + 1)], s.gy[VZS][g], s.gy[VH][g],
-                                        s.dzby[g]);
+                const T zsm = zs[ti(tx, ty - 1)];
+                s.gx[VZS][gi] = wetslope(delta, zs[c], hc, zs[c - 1], zs[c + 1], s.gx[VZS][gi], s.gx[VH][gi], s.dzbx[gi]);
+                s.gy[VZS][gj] = wetslope(delta, zs[c], hc, zsm, zsm, s.gy[VZS][gj], s.gy[VH][gj], s.dzby[gj]);
+            }
+            __syncwarp();
+            if (k == VZS) {
+                const T hc = SPLIT ? D + hh[cr] : hh[cr];
+                if (side < 2) {
+                    const int g = side == 0 ? gxi(-1, q) : gxi(BW, q);
+                    s.gx[VZS][g] = wetslope(delta, zs[cr], hc, zs[cr - 1], zs[cr + 1], s.gx[VZS][g], s.gx[VH][g], s.dzbx[g]);
+                } else {
+                    const int g = side == 2 ? gyi(q, -1) : gyi(q, BW);
+                    s.gy[VZS][g] = wetslope(delta, zs[cr], hc, zs[cm], zs[cp], s.gy[VZS][g], s.gy[VH][g], s.dzby[g]);
+                }
             }
         }
-        __syncthreads();
     }
+    __syncthreads();
     // Thread (tx,ty) owns the left (X) and bottom (Y) faces of its cell; threads
     // 0..15 also take X face x=16 and threads 16..31 Y face y=16 (the faces the
     // reference computes in the right / top halo column).

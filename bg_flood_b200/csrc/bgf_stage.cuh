@@ -41,8 +41,10 @@ __device__ __forceinline__ double series_at(const double* t, const double* v, in
 // (Forcingthisstep, src/Updateforcing.cu:87-125: frame index clamped to
 // [0, nt-2]) interpolated in time at the four grid nodes around the point, each
 // rounded to float as the reference's "now" grid holds it, then the bilinear
-// interpolation of interp2BUQ (src/GridManip.cu:540-575) in double.
-template <class T> __device__ __forceinline__ T rain_map_at(const RainMapDev& r, T x, T y, double time)
+// interpolation of interp2BUQ (src/GridManip.cu:540-575) in double.  Kept out of
+// line: inlined, its live values push the update kernels into register spills even
+// when no scenario has a rain map.
+template <class T> __device__ __noinline__ T rain_map_at(const RainMapDev r, T x, T y, double time)
 {
     int st = (int)floor((time - r.to) / r.dt);
     st = min(max(st, 0), r.nt - 2);

@@ -83,6 +83,9 @@ struct bgf_handle {
     // graph of two consecutive steps (parities p, p^1)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graph_valid = false;
+    // graph of one bgf_flow_step per parity: time-slot upload, the step, result download
+    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+    int step_graph_launches[2] = {0, 0};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_run_ms = 0.0;
     int64_t last_run_launches = 0;
@@ -246,11 +249,16 @@ static unsigned long long dt_init_bits(int dbl)
 
 static void free_graphs(bgf_handle* h)
 {
-    for (int k = 0; k < 2; k++)
+    for (int k = 0; k < 2; k++) {
         if (h->graph[k]) {
             cudaGraphExecDestroy(h->graph[k]);
             h->graph[k] = nullptr;
         }
+        if (h->step_graph[k]) {
+            cudaGraphExecDestroy(h->step_graph[k]);
+            h->step_graph[k] = nullptr;
+        }
+    }
     h->graph_valid = false;
 }
 
@@ -1138,10 +1146,9 @@ template <class T> static int enqueue_step(bgf_handle* h, int parity)
     return n + enqueue_update<T>(h, parity);
 }
 
-// Writes the loop state into the device time slot of the current parity and seeds
-// the dt minimum.  Both copies read pinned slots that are not written again before
-// the caller's next stream synchronisation, so no synchronisation is needed here.
-static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep, long long maxsteps)
+// The host side of write_time_slot: fills the pinned time slot and dt seed.
+static void set_time_slot_host(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep,
+                               long long maxsteps)
 {
     TimeState ts;
     memset(&ts, 0, sizeof(ts));
@@ -1158,9 +1165,59 @@ static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, 
     ts.status = 0;
     h->h_time[0] = ts;
     h->h_misc[0] = dt_init_bits(h->dbl);
+}
+
+// Writes the loop state into the device time slot of the current parity and seeds
+// the dt minimum.  Both copies read pinned slots that are not written again before
+// the caller's next stream synchronisation, so no synchronisation is needed here.
+static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep, long long maxsteps)
+{
+    set_time_slot_host(h, loop, endtime, outputtimestep, maxsteps);
     BGF_CUDA(cudaMemcpyAsync(h->d_time + h->parity, &h->h_time[0], sizeof(TimeState), cudaMemcpyHostToDevice, h->stream));
     BGF_CUDA(cudaMemcpyAsync(h->d_dtmin + h->parity, &h->h_misc[0], sizeof(unsigned long long), cudaMemcpyHostToDevice,
                              h->stream));
+    return BGF_OK;
+}
+
+// After a step's result reached the pinned slots: error word, loop update, parity.
+static int finish_step(bgf_handle* h, bgf_loop* loop)
+{
+    if (*(const int*)&h->h_misc[1]) {
+        g_last_error = "mesh has cross-level neighbours, which this build does not support yet";
+        return BGF_EINVAL;
+    }
+    const TimeState& nt = h->h_time[1];
+    loop->dt = nt.dt;
+    loop->dtmax = nt.dtmax;
+    h->cur = nt.cur;
+    h->parity ^= 1;
+    return BGF_OK;
+}
+
+// One flow step for parity p as a graph: the copies of the pinned time slot and dt
+// seed, the step's kernels, and the copies of the resulting time state and error
+// word into the pinned slots.  One launch per bgf_flow_step instead of six calls.
+static int build_step_graph(bgf_handle* h, int p)
+{
+    cudaGraph_t g;
+    BGF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(h->d_time + p, &h->h_time[0], sizeof(TimeState), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_dtmin + p, &h->h_misc[0], sizeof(unsigned long long), cudaMemcpyHostToDevice, h->stream);
+    h->step_graph_launches[p] = h->dbl ? enqueue_step<double>(h, p) : enqueue_step<float>(h, p);
+    cudaMemcpyAsync(&h->h_time[1], h->d_time + (p ^ 1), sizeof(TimeState), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(&h->h_misc[1], h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (e != cudaSuccess) {
+        g_last_error = std::string("graph capture: ") + cudaGetErrorString(e);
+        return BGF_ECUDA;
+    }
+    e = cudaGraphInstantiate(&h->step_graph[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->step_graph[p] = nullptr;
+        g_last_error = std::string("graph instantiate: ") + cudaGetErrorString(e);
+        return BGF_ECUDA;
+    }
     return BGF_OK;
 }
 
@@ -1169,6 +1226,16 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
     int rc = check_ready(h);
     if (rc) return rc;
     if (!loop) return BGF_EINVAL;
+    if (!h->profiling) {
+        const int p = h->parity;
+        if (!h->step_graph[p] && (rc = build_step_graph(h, p))) return rc;
+        // the host slots the graph copies from and to (not in use: the previous call synchronised)
+        set_time_slot_host(h, loop, INFINITY, 0.0, 1);
+        BGF_CUDA(cudaGraphLaunch(h->step_graph[p], h->stream));
+        h->launches += h->step_graph_launches[p];
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
+        return finish_step(h, loop);
+    }
     rc = write_time_slot(h, loop, INFINITY, 0.0, 1);
     if (rc) return rc;
     int n = 0;
@@ -1204,21 +1271,16 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
         h->update_ms += b;
         h->profiled_steps++;
     }
-    if (*(const int*)&h->h_misc[1]) {
-        g_last_error = "mesh has cross-level neighbours, which this build does not support yet";
-        return BGF_EINVAL;
-    }
-    const TimeState& nt = h->h_time[1];
-    loop->dt = nt.dt;
-    loop->dtmax = nt.dtmax;
-    h->cur = nt.cur;
-    h->parity ^= 1;
-    return BGF_OK;
+    return finish_step(h, loop);
 }
 
 static int build_graphs(bgf_handle* h)
 {
-    free_graphs(h);
+    for (int k = 0; k < 2; k++)  // the run graphs only; the single-step graphs stay valid
+        if (h->graph[k]) {
+            cudaGraphExecDestroy(h->graph[k]);
+            h->graph[k] = nullptr;
+        }
     for (int p0 = 0; p0 < 2; p0++) {
         cudaGraph_t g;
         BGF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));

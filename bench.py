@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--engine", type=int, default=1)
     ap.add_argument("--fastmath", type=int, default=1, help="1: fast-math kernels, 0: bit-exact kernels")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--only", choices=["amr", "ensemble", "serve"], default=None,
+                    help="run one secondary measurement alone and print it (profiling runs)")
     ap.add_argument("--amr", type=int, default=1024, help="level-0 cells per side of the AMR measurement (0: skip)")
     ap.add_argument("--ensemble", type=int, default=64, help="members of the batched-ensemble measurement (0: skip)")
     ap.add_argument("--ens-max-blocks", type=int, default=16384)
@@ -365,6 +367,16 @@ def main():
     from runners import make_gpu
 
     torch.cuda.set_device(local)
+    if args.only:
+        # one secondary measurement alone, for profiling its launches
+        if args.only == "amr":
+            r = amr_bench(args.amr, 2, args.steps, local, args.fastmath)
+        elif args.only == "ensemble":
+            r = ensemble_bench(args.ensemble, 2024, 64, args.ens_max_blocks, args.steps, local, args.fastmath)
+        else:
+            r = serving_bench(args.serve, 7, args.serve_rate, local, args.fastmath)
+        print(json.dumps({"measurement": args.only, **r}))
+        return
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
 

@@ -76,6 +76,8 @@ struct bgf_handle {
     TimeState* h_time = nullptr;  // pinned
     // pinned scalars: [0] dt-minimum seed (H2D), [1] device error word (D2H)
     unsigned long long* h_misc = nullptr;
+    // the per-block device arrays of bgf_create live in one allocation
+    void* d_slab = nullptr;
     int cur = 0, parity = 0;
     bool has_blocks = false, has_bed = false, has_state = false, has_cf = false, has_rainmask = false;
     int nseg_dev = 0, rain_n_dev = 0;
@@ -271,26 +273,116 @@ template <class T> static void buq_to(const void* src, int dbl, size_t n, std::v
 }
 
 // Pinned staging area of at least `bytes` (grown on demand, kept for the handle).
+// Page-locked staging buffers are kept in a process-wide cache by power-of-two size
+// class: handles come and go per scenario when serving, and cudaMallocHost /
+// cudaFreeHost of megabytes cost milliseconds.  The cache holds at most 1 GB.
+static std::mutex g_stage_mu;
+static std::vector<std::pair<size_t, void*>> g_stage_free;  // (bytes, buffer)
+static size_t g_stage_cached = 0;
+
+static void stage_release(void* p, size_t bytes)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    if (g_stage_cached + bytes > ((size_t)1 << 30)) {
+        cudaFreeHost(p);
+        return;
+    }
+    g_stage_free.push_back({bytes, p});
+    g_stage_cached += bytes;
+}
+
+static void* stage_acquire(size_t bytes, size_t* got)
+{
+    size_t cls = 1 << 16;
+    while (cls < bytes) cls <<= 1;
+    {
+        std::lock_guard<std::mutex> lk(g_stage_mu);
+        for (size_t k = 0; k < g_stage_free.size(); k++)
+            if (g_stage_free[k].first == cls) {
+                void* p = g_stage_free[k].second;
+                g_stage_free.erase(g_stage_free.begin() + k);
+                g_stage_cached -= cls;
+                *got = cls;
+                return p;
+            }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, cls) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    *got = cls;
+    return p;
+}
+
 static void* staging(bgf_handle* h, size_t bytes)
 {
     if (h->pinned_bytes < bytes) {
-        if (h->pinned) cudaFreeHost(h->pinned);
+        stage_release(h->pinned, h->pinned_bytes);
         h->pinned = nullptr;
         h->pinned_bytes = 0;
-        if (cudaMallocHost(&h->pinned, bytes) != cudaSuccess) return nullptr;
-        h->pinned_bytes = bytes;
+        size_t got = 0;
+        h->pinned = stage_acquire(bytes, &got);
+        if (!h->pinned) return nullptr;
+        h->pinned_bytes = got;
     }
     return h->pinned;
+}
+
+// Device buffers owned by a handle come from the stream-ordered allocator on the
+// handle's stream (released to the device's memory pool without a device-wide
+// synchronisation); an allocation is complete before it returns, so any stream may
+// use it.
+static cudaError_t dalloc(bgf_handle* h, void** p, size_t bytes)
+{
+    cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return e;
+}
+
+static void dfree(bgf_handle* h, void* p)
+{
+    if (p) cudaFreeAsync(p, h->stream);
+}
+
+// Page-locked host slots of 256 bytes for the per-step scalars of a handle (dt seed,
+// error word, two time states), handed out from 64 KB slabs that live until exit:
+// cudaMallocHost per handle would cost about a millisecond each time.
+static std::mutex g_pinned_mu;
+static std::vector<void*> g_pinned_free;
+
+static void* pinned_slot_get()
+{
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    if (g_pinned_free.empty()) {
+        char* slab = nullptr;
+        if (cudaMallocHost((void**)&slab, 65536) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        for (int k = 255; k >= 0; k--) g_pinned_free.push_back(slab + 256 * k);
+    }
+    void* p = g_pinned_free.back();
+    g_pinned_free.pop_back();
+    memset(p, 0, 256);
+    return p;
+}
+
+static void pinned_slot_put(void* p)
+{
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    g_pinned_free.push_back(p);
 }
 
 // Device tile scratch of at least `bytes` (grown on demand, kept for the handle).
 static void* tile_scratch(bgf_handle* h, size_t bytes)
 {
     if (h->tiles_bytes < bytes) {
-        if (h->d_tiles) cudaFree(h->d_tiles);
+        dfree(h, h->d_tiles);
         h->d_tiles = nullptr;
         h->tiles_bytes = 0;
-        if (cudaMalloc(&h->d_tiles, bytes) != cudaSuccess) {
+        if (dalloc(h, &h->d_tiles, bytes) != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
@@ -376,9 +468,14 @@ const char* bgf_last_error(void) { return g_last_error.c_str(); }
 
 int bgf_device_supported(int dev)
 {
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return 0;
-    return prop.major == 10 && prop.minor == 0;
+    // two attribute queries (cudaGetDeviceProperties takes milliseconds)
+    int major = 0, minor = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return major == 10 && minor == 0;
 }
 
 int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
@@ -404,11 +501,23 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         return BGF_ENOKERNEL;
     }
     h->fast = p->fastmath ? 1 : 0;
-    cudaError_t e = h->dbl ? (h->fast ? fa::configure_kernels<double>() : ex::configure_kernels<double>())
-                           : (h->fast ? fa::configure_kernels<float>() : ex::configure_kernels<float>());
-    if (e == cudaSuccess)
-        e = h->dbl ? (h->fast ? fa::configure_amr_kernels<double>() : ex::configure_amr_kernels<double>())
-                   : (h->fast ? fa::configure_amr_kernels<float>() : ex::configure_amr_kernels<float>());
+    // kernel attributes (dynamic shared memory) are set once per device, precision
+    // and arithmetic variant
+    static std::mutex cfg_mu;
+    static bool configured[64][2][2] = {};
+    cudaError_t e = cudaSuccess;
+    {
+        std::lock_guard<std::mutex> lk(cfg_mu);
+        bool& done = configured[h->dev & 63][h->dbl][h->fast];
+        if (!done) {
+            e = h->dbl ? (h->fast ? fa::configure_kernels<double>() : ex::configure_kernels<double>())
+                       : (h->fast ? fa::configure_kernels<float>() : ex::configure_kernels<float>());
+            if (e == cudaSuccess)
+                e = h->dbl ? (h->fast ? fa::configure_amr_kernels<double>() : ex::configure_amr_kernels<double>())
+                           : (h->fast ? fa::configure_amr_kernels<float>() : ex::configure_amr_kernels<float>());
+            done = e == cudaSuccess;
+        }
+    }
     if (e != cudaSuccess) {
         g_last_error = std::string("configure kernels: ") + cudaGetErrorString(e);
         delete h;
@@ -438,11 +547,38 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         {(void**)&h->d_flags, nb},                       {(void**)&h->d_child, 3 * nb * sizeof(int)},
         {&h->d_datum, nb * es},
     };
-    for (auto& a : allocs) {
-        if (cudaMalloc(a.p, a.bytes) != cudaSuccess) {
-            g_last_error = "cudaMalloc failed";
-            bgf_destroy(h);
-            return BGF_ENOMEM;
+    // one device allocation carved into 256-byte aligned pieces: handles are created
+    // and destroyed per scenario when serving, and each cudaMalloc / cudaFree costs
+    size_t total = 0;
+    for (auto& a : allocs) total += (a.bytes + 255) & ~(size_t)255;
+    // stream-ordered allocation from the device's memory pool, which keeps up to 4 GB
+    // of freed memory for reuse instead of returning it to the driver at each
+    // synchronisation (larger releases, e.g. of a pool's slots, still go back)
+    static std::mutex pool_mu;
+    static bool pool_set[64] = {};
+    {
+        std::lock_guard<std::mutex> lk(pool_mu);
+        if (!pool_set[h->dev & 63]) {
+            cudaMemPool_t mp;
+            if (cudaDeviceGetDefaultMemPool(&mp, h->dev) == cudaSuccess) {
+                uint64_t keep = (uint64_t)4 << 30;
+                cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            cudaGetLastError();
+            pool_set[h->dev & 63] = true;
+        }
+    }
+    if (cudaMallocAsync(&h->d_slab, total, h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        g_last_error = "cudaMalloc failed";
+        bgf_destroy(h);
+        return BGF_ENOMEM;
+    }
+    {
+        char* q = (char*)h->d_slab;
+        for (auto& a : allocs) {
+            *a.p = q;
+            q += (a.bytes + 255) & ~(size_t)255;
         }
     }
     cudaMemsetAsync(h->d_bndseg, 0xff, 4 * nb * sizeof(int), h->stream);
@@ -452,17 +588,21 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
     cudaMemsetAsync(h->d_dhu, 0, nb * 256 * es, h->stream);
     cudaMemsetAsync(h->d_dhv, 0, nb * 256 * es, h->stream);
     cudaMemsetAsync(h->d_datum, 0, nb * es, h->stream);
-    if (cudaMallocHost((void**)&h->h_misc, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    h->h_misc = (unsigned long long*)pinned_slot_get();
+    if (!h->h_misc) {
         bgf_destroy(h);
         return BGF_ENOMEM;
     }
-    if (cudaMallocHost((void**)&h->h_time, 2 * sizeof(TimeState)) != cudaSuccess) {
-        bgf_destroy(h);
-        return BGF_ENOMEM;
-    }
+    h->h_time = (TimeState*)(h->h_misc + 2);  // two time states after the two scalars
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
     for (int k = 0; k < 3; k++) cudaEventCreate(&h->pev[k]);
+    // the slab and its initial values are in place before any other stream uses them
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        g_last_error = "bgf_create: stream synchronisation failed";
+        bgf_destroy(h);
+        return BGF_ECUDA;
+    }
     *out = h;
     return BGF_OK;
 }
@@ -470,11 +610,11 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
 static void free_amr(bgf_handle* h)
 {
     for (auto& st : h->d_W)
-        for (void*& p : st) { if (p) cudaFree(p); p = nullptr; }
-    for (void*& p : h->d_G0) { if (p) cudaFree(p); p = nullptr; }
-    for (void*& p : h->d_F) { if (p) cudaFree(p); p = nullptr; }
-    if (h->d_pflag) cudaFree(h->d_pflag);
-    if (h->d_rank) cudaFree(h->d_rank);
+        for (void*& p : st) { dfree(h, p); p = nullptr; }
+    for (void*& p : h->d_G0) { dfree(h, p); p = nullptr; }
+    for (void*& p : h->d_F) { dfree(h, p); p = nullptr; }
+    dfree(h, h->d_pflag);
+    dfree(h, h->d_rank);
     h->d_pflag = nullptr;
     h->d_rank = nullptr;
 }
@@ -485,22 +625,20 @@ int bgf_destroy(bgf_handle* h)
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     free_graphs(h);
-    void* ptrs[] = {h->d_active, h->d_level, h->d_nbr, h->d_bndseg, h->d_err, h->d_zb, h->d_dzbdx, h->d_dzbdy,
-                    h->d_cf, h->d_rainmask, h->d_qmean, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t,
-                    h->d_rain_r, h->d_h[0], h->d_h[1], h->d_u[0], h->d_u[1], h->d_v[0], h->d_v[1], h->d_dh,
-                    h->d_dhu, h->d_dhv, h->d_time, h->d_dtmin, h->d_scratch, h->d_bxo, h->d_byo,
-                    h->d_flags, h->d_child, h->d_dem, h->d_datum, h->d_rivers, h->d_riv_t, h->d_riv_q,
-                    (void*)h->rmap.val, h->d_tiles};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    // the per-block arrays of bgf_create are pieces of d_slab (back to the memory pool in
+    // stream order); the rest are own allocations
+    void* ptrs[] = {h->d_slab, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t, h->d_rain_r, h->d_dem,
+                    h->d_rivers, h->d_riv_t, h->d_riv_q, (void*)h->rmap.val, h->d_tiles};
+    if (h->stream)
+        for (void* p : ptrs) dfree(h, p);
+    h->d_slab = nullptr;
     free_amr(h);
-    if (h->h_time) cudaFreeHost(h->h_time);
-    if (h->h_misc) cudaFreeHost(h->h_misc);
+    if (h->h_misc) pinned_slot_put(h->h_misc);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     for (int k = 0; k < 3; k++)
         if (h->pev[k]) cudaEventDestroy(h->pev[k]);
-    if (h->pinned) cudaFreeHost(h->pinned);
+    stage_release(h->pinned, h->pinned_bytes);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return BGF_OK;
@@ -516,11 +654,11 @@ static int alloc_amr(bgf_handle* h)
     const size_t nb = (size_t)h->nblkmem, es = h->esz;
     bool ok = true;
     for (auto& st : h->d_W)
-        for (void*& p : st) ok = ok && cudaMalloc(&p, nb * 324 * es) == cudaSuccess;
-    for (void*& p : h->d_G0) ok = ok && cudaMalloc(&p, nb * 324 * es) == cudaSuccess;
-    for (void*& p : h->d_F) ok = ok && cudaMalloc(&p, nb * NFX * es) == cudaSuccess;
-    ok = ok && cudaMalloc((void**)&h->d_pflag, nb * 64) == cudaSuccess;
-    ok = ok && cudaMalloc((void**)&h->d_rank, nb * sizeof(int)) == cudaSuccess;
+        for (void*& p : st) ok = ok && dalloc(h, &p, nb * 324 * es) == cudaSuccess;
+    for (void*& p : h->d_G0) ok = ok && dalloc(h, &p, nb * 324 * es) == cudaSuccess;
+    for (void*& p : h->d_F) ok = ok && dalloc(h, &p, nb * NFX * es) == cudaSuccess;
+    ok = ok && dalloc(h, (void**)&h->d_pflag, nb * 64) == cudaSuccess;
+    ok = ok && dalloc(h, (void**)&h->d_rank, nb * sizeof(int)) == cudaSuccess;
     if (!ok) {
         free_amr(h);
         g_last_error = "cudaMalloc failed (multi-level buffers)";
@@ -718,16 +856,16 @@ static int rebuild_segments(bgf_handle* h)
     // segment buffers only grow (pools rebuild them on every admission)
     size_t ns = std::max<size_t>(1, sd.size()), nser = std::max<size_t>(1, st.size());
     if (ns > h->seg_cap || !h->d_segs) {
-        if (h->d_segs) cudaFree(h->d_segs);
+        dfree(h, h->d_segs);
         h->seg_cap = std::max(ns, 2 * h->seg_cap);
-        BGF_CUDA(cudaMalloc((void**)&h->d_segs, h->seg_cap * sizeof(SegDev)));
+        BGF_CUDA(dalloc(h, (void**)&h->d_segs, h->seg_cap * sizeof(SegDev)));
     }
     if (nser > h->ser_cap || !h->d_seg_t) {
-        if (h->d_seg_t) cudaFree(h->d_seg_t);
-        if (h->d_seg_wl) cudaFree(h->d_seg_wl);
+        dfree(h, h->d_seg_t);
+        dfree(h, h->d_seg_wl);
         h->ser_cap = std::max(nser, 2 * h->ser_cap);
-        BGF_CUDA(cudaMalloc((void**)&h->d_seg_t, h->ser_cap * sizeof(double)));
-        BGF_CUDA(cudaMalloc((void**)&h->d_seg_wl, h->ser_cap * sizeof(double)));
+        BGF_CUDA(dalloc(h, (void**)&h->d_seg_t, h->ser_cap * sizeof(double)));
+        BGF_CUDA(dalloc(h, (void**)&h->d_seg_wl, h->ser_cap * sizeof(double)));
     }
     if (!sd.empty()) BGF_CUDA(cudaMemcpy(h->d_segs, sd.data(), sd.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
     if (!st.empty()) {
@@ -765,17 +903,18 @@ int bgf_set_rain_series(bgf_handle* h, int n, const double* t, const double* r)
     int rc = set_device(h);
     if (rc) return rc;
     BGF_CUDA(cudaStreamSynchronize(h->stream));
-    if (h->d_rain_t) { cudaFree(h->d_rain_t); h->d_rain_t = nullptr; }
-    if (h->d_rain_r) { cudaFree(h->d_rain_r); h->d_rain_r = nullptr; }
+    dfree(h, h->d_rain_t);
+    dfree(h, h->d_rain_r);
+    h->d_rain_t = h->d_rain_r = nullptr;
     h->rain_n_dev = n;
     h->rain_t.assign(t, t + n);
     h->rain_r.assign(r, r + n);
-    if (h->rmap.val) cudaFree((void*)h->rmap.val);  // a uniform series replaces a gridded one
+    dfree(h, (void*)h->rmap.val);  // a uniform series replaces a gridded one
     h->rmap = RainMapDev{};
     h->has_rmap = false;
     if (n > 0) {
-        BGF_CUDA(cudaMalloc((void**)&h->d_rain_t, n * sizeof(double)));
-        BGF_CUDA(cudaMalloc((void**)&h->d_rain_r, n * sizeof(double)));
+        BGF_CUDA(dalloc(h, (void**)&h->d_rain_t, n * sizeof(double)));
+        BGF_CUDA(dalloc(h, (void**)&h->d_rain_r, n * sizeof(double)));
         BGF_CUDA(cudaMemcpy(h->d_rain_t, t, n * sizeof(double), cudaMemcpyHostToDevice));
         BGF_CUDA(cudaMemcpy(h->d_rain_r, r, n * sizeof(double), cudaMemcpyHostToDevice));
     }
@@ -790,18 +929,19 @@ int bgf_set_rain_map(bgf_handle* h, int nx, int ny, double xo, double yo, double
     int rc = set_device(h);
     if (rc) return rc;
     BGF_CUDA(cudaStreamSynchronize(h->stream));
-    if (h->rmap.val) cudaFree((void*)h->rmap.val);
+    dfree(h, (void*)h->rmap.val);
     h->rmap = RainMapDev{};
     h->has_rmap = false;
     // a gridded series replaces a uniform one
-    if (h->d_rain_t) { cudaFree(h->d_rain_t); h->d_rain_t = nullptr; }
-    if (h->d_rain_r) { cudaFree(h->d_rain_r); h->d_rain_r = nullptr; }
+    dfree(h, h->d_rain_t);
+    dfree(h, h->d_rain_r);
+    h->d_rain_t = h->d_rain_r = nullptr;
     h->rain_n_dev = 0;
     h->rain_t.clear();
     h->rain_r.clear();
     const size_t n = (size_t)nx * ny * nt;
     float* d = nullptr;
-    BGF_CUDA(cudaMalloc((void**)&d, n * sizeof(float)));
+    BGF_CUDA(dalloc(h, (void**)&d, n * sizeof(float)));
     BGF_CUDA(cudaMemcpy(d, frames, n * sizeof(float), cudaMemcpyHostToDevice));
     RainMapDev& r = h->rmap;
     r.val = d;
@@ -863,10 +1003,10 @@ int bgf_add_river(bgf_handle* h, double xstart, double xend, double ystart, doub
     h->riv_t.insert(h->riv_t.end(), t, t + n);
     h->riv_q.insert(h->riv_q.end(), q, q + n);
     for (void** d : {(void**)&h->d_rivers, (void**)&h->d_riv_t, (void**)&h->d_riv_q})
-        if (*d) { cudaFree(*d); *d = nullptr; }
-    BGF_CUDA(cudaMalloc((void**)&h->d_rivers, h->rivers.size() * sizeof(RiverDev)));
-    BGF_CUDA(cudaMalloc((void**)&h->d_riv_t, h->riv_t.size() * sizeof(double)));
-    BGF_CUDA(cudaMalloc((void**)&h->d_riv_q, h->riv_q.size() * sizeof(double)));
+        if (*d) { dfree(h, *d); *d = nullptr; }
+    BGF_CUDA(dalloc(h, (void**)&h->d_rivers, h->rivers.size() * sizeof(RiverDev)));
+    BGF_CUDA(dalloc(h, (void**)&h->d_riv_t, h->riv_t.size() * sizeof(double)));
+    BGF_CUDA(dalloc(h, (void**)&h->d_riv_q, h->riv_q.size() * sizeof(double)));
     BGF_CUDA(cudaMemcpy(h->d_rivers, h->rivers.data(), h->rivers.size() * sizeof(RiverDev), cudaMemcpyHostToDevice));
     BGF_CUDA(cudaMemcpy(h->d_riv_t, h->riv_t.data(), h->riv_t.size() * sizeof(double), cudaMemcpyHostToDevice));
     BGF_CUDA(cudaMemcpy(h->d_riv_q, h->riv_q.data(), h->riv_q.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -1405,9 +1545,9 @@ int bgf_set_bathy(bgf_handle* h, int nx, int ny, double xo, double yo, double dx
     if (!h || nx < 2 || ny < 2 || !(dx > 0.0) || !val) return BGF_EINVAL;
     int rc = set_device(h);
     if (rc) return rc;
-    if (h->d_dem) cudaFree(h->d_dem);
+    dfree(h, h->d_dem);
     h->d_dem = nullptr;
-    BGF_CUDA(cudaMalloc((void**)&h->d_dem, sizeof(float) * (size_t)nx * ny));
+    BGF_CUDA(dalloc(h, (void**)&h->d_dem, sizeof(float) * (size_t)nx * ny));
     BGF_CUDA(cudaMemcpy(h->d_dem, val, sizeof(float) * (size_t)nx * ny, cudaMemcpyHostToDevice));
     h->dem_nx = nx;
     h->dem_ny = ny;

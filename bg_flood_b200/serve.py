@@ -11,6 +11,7 @@ gauge readings are sampled at every chunk boundary.  Time-to-solution is measure
 from arrival to retirement."""
 from __future__ import annotations
 
+import sys
 import threading
 import time
 from dataclasses import dataclass, field
@@ -72,36 +73,54 @@ class FloodServer:
         self.gpu_ms = 0.0
         self.host_s = {"admit": 0.0, "run": 0.0, "query": 0.0, "retire": 0.0, "fields": 0.0}
 
-    def serve(self, requests: list[Request], realtime: bool = True, prefetch: int = 8) -> list[Result]:
+    def serve(self, requests: list[Request], realtime: bool = True, prefetch: int = 8,
+              builders: int = 2) -> list[Result]:
         """Runs the stream to completion.  With realtime, a request becomes visible at
         its arrival time on the wall clock; otherwise all are queued at t = 0.
         Arrived requests are prepared (host set-up and upload into their own handle)
-        by a background thread while the pool computes, at most `prefetch` ahead."""
+        by `builders` background threads while the pool computes, at most `prefetch`
+        ahead; they are admitted in the order they become ready."""
+        self.gpu_ms = 0.0
+        self.host_s = {k: 0.0 for k in self.host_s}
         pending = sorted(requests, key=lambda r: r.arrival)
-        ready: list[tuple[Request, object]] = []   # (request, (FlowB200, Loop)) in arrival order
+        ready: list[tuple[Request, object]] = []   # (request, (FlowB200, Loop))
         lock = threading.Condition()
         stop = [False]
+        nexti = [0]
+        errors: list = []
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
 
         def builder():
-            for r in pending:
+            try:
+                while True:
+                    with lock:
+                        while len(ready) >= prefetch and not stop[0]:
+                            lock.wait(0.01)
+                        if stop[0] or nexti[0] >= len(pending):
+                            return
+                        r = pending[nexti[0]]
+                        nexti[0] += 1
+                    if realtime and r.arrival > now():
+                        time.sleep(r.arrival - now())
+                    if r.nblk > self.nblk_pool:
+                        raise ValueError(f"request {r.rid} needs {r.nblk} blocks, the pool holds {self.nblk_pool}")
+                    built = r.build()
+                    with lock:
+                        ready.append((r, built))
+                        lock.notify_all()
+            except Exception as e:  # reported by the serving loop
                 with lock:
-                    while len(ready) >= prefetch and not stop[0]:
-                        lock.wait(0.01)
-                    if stop[0]:
-                        return
-                if realtime and r.arrival > now():
-                    time.sleep(r.arrival - now())
-                if r.nblk > self.nblk_pool:
-                    raise ValueError(f"request {r.rid} needs {r.nblk} blocks, the pool holds {self.nblk_pool}")
-                built = r.build()
-                with lock:
-                    ready.append((r, built))
+                    errors.append(e)
                     lock.notify_all()
 
-        th = threading.Thread(target=builder, daemon=True)
-        th.start()
+        ths = [threading.Thread(target=builder, daemon=True) for _ in range(max(1, builders))]
+        # the serving loop makes many short calls; a short interpreter switch interval
+        # keeps the preparing threads from holding it off the GPU for milliseconds
+        switch = sys.getswitchinterval()
+        sys.setswitchinterval(min(switch, 0.0002))
+        for th in ths:
+            th.start()
         live: dict[int, tuple[Request, FlowB200, float, list]] = {}
         out: list[Result] = []
         nreq = len(pending)
@@ -119,8 +138,10 @@ class FloodServer:
                         ready.pop(0)
                         live[slot] = (r, f, now(), [])
                         lock.notify_all()
+                    if errors:
+                        raise RuntimeError(f"request preparation failed: {errors[0]}") from errors[0]
                     if not live:
-                        if not th.is_alive() and not ready:
+                        if not any(th.is_alive() for th in ths) and not ready:
                             raise RuntimeError("request preparation stopped before the stream ended")
                         lock.wait(0.01)
                         continue
@@ -156,7 +177,9 @@ class FloodServer:
             with lock:
                 stop[0] = True
                 lock.notify_all()
-            th.join(timeout=10)
+            for th in ths:
+                th.join(timeout=10)
+            sys.setswitchinterval(switch)
         return sorted(out, key=lambda x: x.rid)
 
 

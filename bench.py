@@ -206,7 +206,11 @@ def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, step
     t0 = time.perf_counter()
     pool = ScenarioPool(members[0].param, sum(blocks), nscen)
     t1 = time.perf_counter()
-    built = [make_gpu(c) for c in members]
+    # the members' host set-up in four threads (numpy and the C ABI release the
+    # interpreter lock); the plain loop above prepares one member at a time
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(4) as ex:
+        built = list(ex.map(make_gpu, members))
     t2 = time.perf_counter()
     for f, _, lp in built:
         pool.admit(f, lp, 1e30, maxsteps=steps)

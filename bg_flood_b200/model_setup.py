@@ -84,7 +84,10 @@ def read_param_file(path: str) -> Param:
         text = fh.read()
     lines = [ln for ln in text.splitlines() if ln and not ln.startswith("#")]
     _reject_unsupported(lines)
-    return read_param_text("\n".join(lines))
+    p = read_param_text("\n".join(lines))
+    if p.cf_file:
+        raise ValueError(f"roughness map '{p.cf_file}' (cf key) is not supported by this library")
+    return p
 
 
 # keys of inputs this library does not read (readparamstr, src/ReadInput.cu:890-1180)

@@ -96,6 +96,7 @@ class Param:
     rain: str = ""
     bathy: list = field(default_factory=list)  # bathymetry files, first one the base grid
     rivers: list = field(default_factory=list)  # (discharge file, xstart, xend, ystart, yend)
+    cf_file: str = ""  # a roughness map named by the cf key (not read by this library)
 
     @property
     def delta(self) -> float:
@@ -179,6 +180,14 @@ def _split_line(line: str):
     return key.strip(), val.strip()
 
 
+def _is_number(v: str) -> bool:
+    try:
+        float(v)
+        return True
+    except ValueError:
+        return False
+
+
 def _parse_bool(v: str) -> bool:
     # readparambool (src/ReadInput.cu): "1", "true", "yes", "on" (any case) are true
     return v.strip().lower() in ("1", "true", "yes", "on", "t", "y")
@@ -242,8 +251,8 @@ def read_param_text(text: str, param: Param | None = None) -> Param:
                     pass
                 elif typ is bool:
                     setattr(p, attr, _parse_bool(val))
-                elif attr == "cf" and any(c.isalpha() for c in val):
-                    pass  # a roughness map file: not read by this library
+                elif attr == "cf" and not _is_number(val):
+                    p.cf_file = val  # a roughness map file: not read by this library
                 else:
                     setattr(p, attr, typ(val))
                 break

@@ -117,6 +117,11 @@ def test_param_file_keys(tmp_path):
         read_param_file(str(tmp_path / "BG_param.txt"))
     (tmp_path / "BG_param.txt").write_text("bathy = bathy.asc\nriver = r.txt, 1,2,3,4\n")
     assert read_param_file(str(tmp_path / "BG_param.txt")).rivers == [("r.txt", 1.0, 2.0, 3.0, 4.0)]
+    (tmp_path / "BG_param.txt").write_text("bathy = bathy.asc\ncf = 1e-3\n")
+    assert read_param_file(str(tmp_path / "BG_param.txt")).cf == 1e-3
+    (tmp_path / "BG_param.txt").write_text("bathy = bathy.asc\ncf = manning.nc\n")
+    with pytest.raises(ValueError, match="roughness map"):
+        read_param_file(str(tmp_path / "BG_param.txt"))
     (tmp_path / "BG_param.txt").write_text("bathy = bathy.nc?z\n")
     with pytest.raises(ValueError, match="not supported"):
         prepare_model(str(tmp_path / "BG_param.txt"))

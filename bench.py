@@ -413,6 +413,8 @@ def main():
     case = workload_case(args.n, args.engine, local, args.fastmath)
     f, mesh, loop = make_gpu(case)
     ncell = mesh.nblk * 256
+    # launch shape from the autotuner (state restored afterwards)
+    tuned_grid, tuned_ms = f.autotune(loop, 20)
 
     for _ in range(args.warmup):
         loop.totaltime += f.flow_step(loop)
@@ -531,6 +533,8 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "cells": ncell, "blocks": mesh.nblk, "engine": args.engine,
                        "kernels": "fast-math (tolerance parity)" if args.fastmath else "bit-exact",
+                       "launch_grid": {"grid": tuned_grid, "tuned_ms_per_step": tuned_ms,
+                                       "meaning": "CTAs of the fused kernels, 0 = one per block (autotuned)"},
                        "l2": "flushed (256 MB write) before every timed step", "parallelism":
                        f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -1780,10 +1780,6 @@ int bgf_get_bed(bgf_handle* h, void* zb)
     return BGF_OK;
 }
 
-// ---------------------------------------------------------------- batched pools
-
-#include "bgf_pool.inc"
-
 int bgf_set_grid(bgf_handle* h, int grid)
 {
     if (!h || grid < 0) return BGF_EINVAL;
@@ -1791,3 +1787,122 @@ int bgf_set_grid(bgf_handle* h, int grid)
     free_graphs(h);
     return BGF_OK;
 }
+
+// ---------------------------------------------------------------- launch-shape autotuner
+
+// Launch shapes tried by the autotuner: one CTA per block (0), then persistent grids
+// of 2, 3, 4, 5, 6 and 8 CTAs per SM (only those smaller than the block count).
+static std::vector<int> tune_candidates(int dev, int nblk)
+{
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    std::vector<int> c = {0};
+    for (int k : {2, 3, 4, 5, 6, 8})
+        if (k * sms < nblk) c.push_back(k * sms);
+    return c;
+}
+
+// Device bytes to save and restore around tuning runs: (pointer, bytes) pairs.
+struct TuneSave {
+    std::vector<std::pair<void*, size_t>> areas;
+    void* d_copy = nullptr;
+    size_t total = 0;
+};
+
+static int tune_save(bgf_handle* h, TuneSave& t)
+{
+    for (auto& a : t.areas) t.total += a.second;
+    if (dalloc(h, &t.d_copy, std::max<size_t>(t.total, 1)) != cudaSuccess) return BGF_ENOMEM;
+    size_t off = 0;
+    for (auto& a : t.areas) {
+        BGF_CUDA(cudaMemcpyAsync((char*)t.d_copy + off, a.first, a.second, cudaMemcpyDeviceToDevice, h->stream));
+        off += a.second;
+    }
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    return BGF_OK;
+}
+
+static int tune_restore(bgf_handle* h, TuneSave& t)
+{
+    size_t off = 0;
+    for (auto& a : t.areas) {
+        BGF_CUDA(cudaMemcpyAsync(a.first, (char*)t.d_copy + off, a.second, cudaMemcpyDeviceToDevice, h->stream));
+        off += a.second;
+    }
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    dfree(h, t.d_copy);
+    t.d_copy = nullptr;
+    return BGF_OK;
+}
+
+// Times `steps` steps (after two untimed ones) of the handle's step graphs with the
+// current launch shape, from the time slot written by the caller.
+static int tune_time_handle(bgf_handle* h, int steps, double* ms)
+{
+    int rc = build_graphs(h);
+    if (rc) return rc;
+    const int p0 = h->parity;
+    BGF_CUDA(cudaGraphLaunch(h->graph[p0], h->stream));
+    BGF_CUDA(cudaEventRecord(h->ev0, h->stream));
+    for (int k = 0; k < (steps + 1) / 2; k++) BGF_CUDA(cudaGraphLaunch(h->graph[p0], h->stream));
+    BGF_CUDA(cudaEventRecord(h->ev1, h->stream));
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    float t = 0.f;
+    BGF_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    *ms = t / (2 * ((steps + 1) / 2));
+    return BGF_OK;
+}
+
+int bgf_autotune(bgf_handle* h, const bgf_loop* loop, int steps, int* grid, double* ms_per_step)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!loop || steps <= 0) return BGF_EINVAL;
+    if (h->amr) {
+        // the multi-level chain launches one CTA per block; nothing to choose
+        if (grid) *grid = 0;
+        if (ms_per_step) *ms_per_step = 0.0;
+        return BGF_OK;
+    }
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    const size_t nb = h->nblkmem, es = h->esz;
+    TuneSave save;
+    for (int b = 0; b < 2; b++)
+        for (void* a : {h->d_h[b], h->d_u[b], h->d_v[b]}) save.areas.push_back({a, nb * 256 * es});
+    save.areas.push_back({h->d_qmean, nb * 64 * sizeof(float)});
+    save.areas.push_back({h->d_time, 2 * sizeof(TimeState)});
+    if ((rc = tune_save(h, save))) return rc;
+    const int cur0 = h->cur, par0 = h->parity, grid0 = h->grid;
+    int best = grid0;
+    double best_ms = INFINITY;
+    for (int g : tune_candidates(h->dev, h->nblk)) {
+        h->grid = g;
+        h->cur = cur0;
+        h->parity = par0;
+        if ((rc = write_time_slot(h, loop, INFINITY, 0.0, (long long)1 << 60))) break;
+        double ms = 0.0;
+        if ((rc = tune_time_handle(h, steps, &ms))) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = g;
+        }
+    }
+    h->cur = cur0;
+    h->parity = par0;
+    int rc2 = tune_restore(h, save);
+    if (rc) {
+        h->grid = grid0;
+        free_graphs(h);
+        return rc;
+    }
+    if (rc2) return rc2;
+    h->grid = best;
+    free_graphs(h);
+    if (grid) *grid = best;
+    if (ms_per_step) *ms_per_step = best_ms;
+    return BGF_OK;
+}
+
+// ---------------------------------------------------------------- batched pools
+
+#include "bgf_pool.inc"

@@ -192,6 +192,16 @@ class FlowB200:
         """CTAs of the fused kernels (0: one per block; fewer: persistent launch)."""
         _check(lib().bgf_set_grid(self.handle, int(grid)), "bgf_set_grid")
 
+    def autotune(self, loop: Loop, steps: int = 20) -> tuple:
+        """Times the step kernels for each launch shape from the state of ``loop`` and
+        keeps the fastest; the state is unchanged afterwards.  Returns (grid, ms_per_step)."""
+        c = loop.to_c()
+        g = ctypes.c_int(0)
+        ms = ctypes.c_double(0.0)
+        _check(lib().bgf_autotune(self.handle, ctypes.byref(c), int(steps), ctypes.byref(g), ctypes.byref(ms)),
+               "bgf_autotune")
+        return g.value, ms.value
+
     def get_bed(self) -> np.ndarray:
         """zb on (nblkmem, 18, 18) tiles, halo included."""
         out = np.zeros((self.nblkmem, 18, 18), self.dev_dtype)

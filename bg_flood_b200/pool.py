@@ -107,3 +107,12 @@ class ScenarioPool:
 
     def set_grid(self, grid: int) -> None:
         _check(lib().bgf_pool_set_grid(self.handle, int(grid)), "bgf_pool_set_grid")
+
+    def autotune(self, steps: int = 20) -> tuple:
+        """Times the pool step for each launch shape over the live scenarios and keeps
+        the fastest; their state is unchanged afterwards.  Returns (grid, ms_per_step)."""
+        g = ctypes.c_int(0)
+        ms = ctypes.c_double(0.0)
+        _check(lib().bgf_pool_autotune(self.handle, int(steps), ctypes.byref(g), ctypes.byref(ms)),
+               "bgf_pool_autotune")
+        return g.value, ms.value

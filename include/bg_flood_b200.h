@@ -364,6 +364,19 @@ int bgf_pool_timing(bgf_pool* pool, double* gpu_ms, int64_t* steps, int* free_bl
 /* CTAs of the fused kernels (0: one per block; fewer CTAs loop over the blocks). */
 int bgf_pool_set_grid(bgf_pool* pool, int grid);
 
+/* ------------------------------------------------------------ launch-shape autotuner */
+/* Times the fused step kernels on the current mesh from the loop state `loop`
+ * (CUDA events; two untimed steps, then `steps` timed ones) for each launch shape -- one CTA per block, and
+ * persistent grids of 2, 3, 4, 5, 6 and 8 CTAs per SM smaller than the block count --
+ * keeps the fastest (as bgf_set_grid / bgf_pool_set_grid would) and reports it and
+ * its time per step.  The state, boundary means, maximum depths and time slots are
+ * restored afterwards, so the simulation continues as if no tuning run took place.
+ * Multi-level meshes launch one CTA per block: *grid = 0 and nothing is run.
+ * Threads per CTA are fixed (256: one per cell of a 16x16 block); the resident
+ * CTAs per SM are fixed at compile time (launch bounds). */
+int bgf_autotune(bgf_handle* h, const bgf_loop* loop, int steps, int* grid, double* ms_per_step);
+int bgf_pool_autotune(bgf_pool* pool, int steps, int* grid, double* ms_per_step);
+
 /* ------------------------------------------------------------ refinement pass */
 /* Criterion of the reference's "Adaptation" key (src/AdaptCriteria.cu:20-130):
  * a block is flagged for refinement when any of its cells has var > arg1

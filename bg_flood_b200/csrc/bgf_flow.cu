@@ -44,13 +44,32 @@ __device__ __forceinline__ T to_tile_datum(const DevModel<T>& m, T hv, int sb, i
     return SPLIT && sb != ib ? hv + (m.datum[sb] - D) : hv;
 }
 
-// Predictor tile: state n of the block and its two-cell ring.
+// Source of ring position k (< 128) of block ib; a cross-level side raises the
+// error word and falls back to the block's own clamped cell.
+template <class T>
+__device__ __forceinline__ void ring_source(const DevModel<T>& m, int ib, int k, int& x, int& y, int& sb, int& sx,
+                                            int& sy)
+{
+    ring_pos(k, x, y);
+    if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy, m.checklev != 0)) {
+        atomicOr(m.err, 1);
+        sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
+    }
+}
+
+// Predictor tile: state n of the block and its two-cell ring.  Threads 0..127 also
+// take one ring cell; its neighbour-table lookup is issued first, so that its
+// latency overlaps the interior loads instead of following them.
 template <class T, bool SPLIT>
 __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m, int ib, int cur, int tid, T D)
 {
+    static_assert(NTHREADS == 256, "one interior cell per thread, ring cells on threads 0..127");
     const T* H = m.h[cur];
     const T* U = m.u[cur];
     const T* V = m.v[cur];
+    int rx = 0, ry = 0, sb = ib, sx = 0, sy = 0;
+    const bool ring = tid < 128;
+    if (ring) ring_source<T>(m, ib, tid, rx, ry, sb, sx, sy);
     {
         int x = tid & 15, y = tid >> 4;
         size_t g = (size_t)ib * 256 + tid;
@@ -62,13 +81,8 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
         int c18 = si(x, y);
         s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
     }
-    if (tid < 128) {
-        int x, y, sb, sx, sy;
-        ring_pos(tid, x, y);
-        if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy, m.checklev != 0)) {
-            atomicOr(m.err, 1);
-            sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
-        }
+    if (ring) {
+        const int x = rx, y = ry;
         size_t g = (size_t)sb * 256 + sy * 16 + sx;
         T hv = to_tile_datum<T, SPLIT>(m, H[g], sb, ib, D), uv = U[g], vv = V[g];
         int c = ti(x, y);
@@ -81,48 +95,52 @@ __device__ __forceinline__ void load_state_tile(Smem<T>& s, const DevModel<T>& m
     }
 }
 
-// Corrector tile: half-step state h* = Advance(state n, adv, dt/2) at every tile
-// cell, evaluated from the source cell's state and flux divergence; state n is kept
-// on the 18x18 tile for the boundary fluxes and the full-step advance.
+// One cell of the corrector tile: h* = Advance(state n, adv, dt/2) of source cell
+// (sb, sx, sy) at tile position (x, y), and state n on the 18x18 tile.
 template <class T, bool SPLIT>
-__device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
-                                               int cur, T halfdt, int tid, T D, double time)
+__device__ __forceinline__ void half_tile_cell(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
+                                               int cur, T halfdt, T D, double time, int x, int y, int sb, int sx,
+                                               int sy)
 {
     const T* H = m.h[cur];
     const T* U = m.u[cur];
     const T* V = m.v[cur];
-    for (int k = tid; k < 256 + 128; k += NTHREADS) {
-        int x, y, sb = ib, sx, sy;
-        if (k < 256) {
-            x = k & 15; y = k >> 4; sx = x; sy = y;
-        } else {
-            ring_pos(k - 256, x, y);
-            if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy, m.checklev != 0)) {
-                atomicOr(m.err, 1);
-                sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
-            }
-        }
-        size_t g = (size_t)sb * 256 + sy * 16 + sx;
-        T hv = H[g], uv = U[g], vv = V[g];
-        // the predictor's river source (AddRiverForcing after updateEV) of the source cell
-        const T dhs = add_rivers<T>(m, p, sb, sx, sy, m.dh[g], time);
-        T ho, uo, vo;
-        if (SPLIT) {
-            const T Ds = sb == ib ? D : m.datum[sb];
-            advance_split<T>(halfdt, p.eps, p.forcemass != 0, Ds, hv, uv, vv, dhs, m.dhu[g], m.dhv[g], ho, uo, vo);
-            hv = to_tile_datum<T, SPLIT>(m, hv, sb, ib, D);
-            ho = to_tile_datum<T, SPLIT>(m, ho, sb, ib, D);
-        } else {
-            advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, dhs, m.dhu[g], m.dhv[g], ho, uo, vo);
-        }
-        int c = ti(x, y);
-        s.t[VH][c] = ho; s.t[VU][c] = uo; s.t[VV][c] = vo;
-        s.t[VZS][c] = tile_zb<T, SPLIT>(m, ib, x, y, sb, sx, sy, D) + ho;
-        if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
-            int c18 = si(x, y);
-            s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
-        }
+    size_t g = (size_t)sb * 256 + sy * 16 + sx;
+    T hv = H[g], uv = U[g], vv = V[g];
+    // the predictor's river source (AddRiverForcing after updateEV) of the source cell
+    const T dhs = add_rivers<T>(m, p, sb, sx, sy, m.dh[g], time);
+    T ho, uo, vo;
+    if (SPLIT) {
+        const T Ds = sb == ib ? D : m.datum[sb];
+        advance_split<T>(halfdt, p.eps, p.forcemass != 0, Ds, hv, uv, vv, dhs, m.dhu[g], m.dhv[g], ho, uo, vo);
+        hv = to_tile_datum<T, SPLIT>(m, hv, sb, ib, D);
+        ho = to_tile_datum<T, SPLIT>(m, ho, sb, ib, D);
+    } else {
+        advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, dhs, m.dhu[g], m.dhv[g], ho, uo, vo);
     }
+    int c = ti(x, y);
+    s.t[VH][c] = ho; s.t[VU][c] = uo; s.t[VV][c] = vo;
+    s.t[VZS][c] = tile_zb<T, SPLIT>(m, ib, x, y, sb, sx, sy, D) + ho;
+    if (x >= -1 && x <= BW && y >= -1 && y <= BW) {
+        int c18 = si(x, y);
+        s.h0[c18] = hv; s.u0[c18] = uv; s.v0[c18] = vv;
+    }
+}
+
+// Corrector tile: half-step state h* = Advance(state n, adv, dt/2) at every tile
+// cell, evaluated from the source cell's state and flux divergence; state n is kept
+// on the 18x18 tile for the boundary fluxes and the full-step advance.  As in the
+// predictor, threads 0..127 look up their ring cell's source before the interior.
+template <class T, bool SPLIT>
+__device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
+                                               int cur, T halfdt, int tid, T D, double time)
+{
+    static_assert(NTHREADS == 256, "one interior cell per thread, ring cells on threads 0..127");
+    int rx = 0, ry = 0, sb = ib, sx = 0, sy = 0;
+    const bool ring = tid < 128;
+    if (ring) ring_source<T>(m, ib, tid, rx, ry, sb, sx, sy);
+    half_tile_cell<T, SPLIT>(s, m, p, ib, cur, halfdt, D, time, tid & 15, tid >> 4, ib, tid & 15, tid >> 4);
+    if (ring) half_tile_cell<T, SPLIT>(s, m, p, ib, cur, halfdt, D, time, rx, ry, sb, sx, sy);
 }
 
 // ---------------------------------------------------------------- kernels

@@ -245,8 +245,10 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::update) update_kernel(DevMod
         __syncthreads();
         (void)tile_fluxes<T, ENGINE, false, SPLIT>(s, p, delta, tid, nullptr, D);
         __syncthreads();
-        apply_boundaries<T, SPLIT>(s, m, p, ib, ts.totaltime + dtd, tid, D);
-        __syncthreads();
+        if (block_has_segments<T>(m, ib)) {  // interior blocks skip the step and its barrier
+            apply_boundaries<T, SPLIT>(s, m, p, ib, ts.totaltime + dtd, tid, D);
+            __syncthreads();
+        }
         const int x = tid & 15, y = tid >> 4;
         const int c = ti(x, y);
         T dh, dhu, dhv;

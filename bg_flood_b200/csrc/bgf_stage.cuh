@@ -113,6 +113,14 @@ __device__ __forceinline__ T add_rivers(const DevModel<T>& m, const StepParams<T
 // bndFluxGPUSideCPU (src/Boundary.cu:587-745) for the four sides of one block.
 // Face arrays in s are modified in place; state n comes from s.h0/u0/v0 and the
 // bed tile (zs = zb + h, as RecalculateZs leaves it).
+// True when some side of block ib carries a boundary segment (the same for every
+// thread of the block, so a barrier may depend on it).
+template <class T> __device__ __forceinline__ bool block_has_segments(const DevModel<T>& m, int ib)
+{
+    const int* b = m.bndseg + (size_t)ib * 4;
+    return (b[0] & b[1] & b[2] & b[3]) >= 0;  // the sign bit survives only if all four are -1
+}
+
 template <class T, bool SPLIT = false>
 __device__ __forceinline__ void apply_boundaries(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
                                                  double tbnd, int tid, T D = (T)0)

@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) amr_flux_kernel(DevModel<T> m, Am
     const T celldt = tile_fluxes<T, ENGINE, true>(s, p, delta, tid, &sub);
     __syncthreads();
     if (stage == 0) {
-        T v = celldt;
+        T v = finite_state_dt<T>(s, tid, celldt);
         for (int o = 16; o > 0; o >>= 1) {
             T w = __shfl_xor_sync(0xffffffffu, v, o);
             v = w < v ? w : v;

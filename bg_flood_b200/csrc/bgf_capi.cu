@@ -1331,6 +1331,10 @@ static int finish_step(bgf_handle* h, bgf_loop* loop)
     loop->dtmax = nt.dtmax;
     h->cur = nt.cur;
     h->parity ^= 1;
+    if (nt.status == BGF_ENAN) {
+        g_last_error = "non-finite value in the state";
+        return BGF_ENAN;
+    }
     return BGF_OK;
 }
 
@@ -1491,7 +1495,7 @@ int bgf_run(bgf_handle* h, bgf_loop* loop, double endtime, double outputtimestep
     h->cur = ts.cur;
     // parity stays p0: every graph replay advances it by two
     if (nsteps) *nsteps = (int)ts.nstep;
-    if (ts.status == BGF_EDT_UNDERFLOW) return BGF_EDT_UNDERFLOW;
+    if (ts.status == BGF_EDT_UNDERFLOW || ts.status == BGF_ENAN) return ts.status;
     return BGF_OK;
 }
 

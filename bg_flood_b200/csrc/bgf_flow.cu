@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::flux) flux_kernel(DevModel<T
         load_state_tile<T, SPLIT>(s, m, ib, cur, tid, D);
         __syncthreads();
         T celldt = tile_fluxes<T, ENGINE, false, SPLIT>(s, p, delta, tid, nullptr, D);
+        celldt = finite_state_dt<T>(s, tid, celldt);
         __syncthreads();
         // CFL minimum: the interior dtmax values reduced with the warp shuffle, then one
         // atomic per block on the float bit pattern (dt > 0, so integer order == float order).

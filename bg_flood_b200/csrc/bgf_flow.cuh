@@ -45,7 +45,7 @@ struct TimeState {
     long long maxsteps;
     int cur;            // state buffer holding the current state
     int done;           // 1: the loop condition failed; further steps are no-ops
-    int status;         // 0 ok, BGF_EDT_UNDERFLOW
+    int status;         // 0 ok, BGF_EDT_UNDERFLOW, BGF_ENAN
     int pad;
 };
 

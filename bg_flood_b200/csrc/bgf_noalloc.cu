@@ -198,6 +198,10 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     }
     loop->dt = nt.dt;
     loop->dtmax = nt.dtmax;
+    if (nt.status == BGF_ENAN) {
+        bgf::set_last_error("non-finite value in the state");
+        return BGF_ENAN;
+    }
     return BGF_OK;
 }
 

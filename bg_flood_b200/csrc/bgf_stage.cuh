@@ -241,6 +241,16 @@ __device__ __forceinline__ bool step_live(const TimeState& ts)
     return !ts.done && ts.totaltime < ts.endtime && ts.nstep < ts.maxsteps;
 }
 
+// A cell whose state (h, u, v on the assembled tile) is not finite contributes a dt
+// of 0 to the CFL minimum: the step then ends its scenario with status BGF_ENAN (a
+// finite state always gives dt > 0).  The reference has no such check; a NaN there
+// propagates silently, since dry-face tests are false for it.
+template <class T> __device__ __forceinline__ T finite_state_dt(const Smem<T>& s, int tid, T celldt)
+{
+    const int c = ti(tid & 15, tid >> 4);
+    return isfinite(s.t[VH][c]) && isfinite(s.t[VU][c]) && isfinite(s.t[VV][c]) ? celldt : (T)0;
+}
+
 // dt of the step from the reduced minimum (CalctimestepGPU, src/Advection.cu:549-620
 // and CalctimestepCPU, :511-535): clamp to 1.5 * the previous dt, then split the
 // time to the next output into an integer number of equal steps.
@@ -269,6 +279,10 @@ __device__ __forceinline__ TimeState next_time_state(const TimeState& ts, const 
     nt.cur = nxt;
     if (dtd < p.dtmin && nt.totaltime < ts.endtime) {
         nt.status = 4;  // BGF_EDT_UNDERFLOW
+        nt.done = 1;
+    }
+    if (dtd == 0.0) {  // a non-finite state zeroed the dt minimum (finite_state_dt)
+        nt.status = 5;  // BGF_ENAN
         nt.done = 1;
     }
     if (ts.outputtimestep > 0.0 && nt.nextoutputtime - nt.totaltime <= dtd * 0.00001) {

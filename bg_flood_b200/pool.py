@@ -67,7 +67,8 @@ class ScenarioPool:
         return n.value
 
     def query(self, slot: int):
-        """(Loop, status, nsteps); status 0 running, 1 finished, 2 dt underflow."""
+        """(Loop, status, nsteps); status 0 running, 1 finished, 2 dt underflow,
+        3 non-finite state."""
         c = Loop().to_c()
         st = ctypes.c_int(0)
         n = ctypes.c_int64(0)

@@ -55,6 +55,7 @@ class Result:
     h: np.ndarray | None = None
     hmax: np.ndarray | None = None
     gauge_series: list = field(default_factory=list)  # (wall time, [h at each gauge])
+    status: int = 1            # as ScenarioPool.query: 1 finished, 2 dt underflow, 3 non-finite state
 
     @property
     def time_to_solution(self) -> float:
@@ -172,7 +173,7 @@ class FloodServer:
                     f.close()
                     self.host_s["retire"] += time.perf_counter() - tb
                     del live[slot]
-                    out.append(Result(r.rid, r.arrival, t_adm, now(), n, loop.totaltime, h, hmax, series))
+                    out.append(Result(r.rid, r.arrival, t_adm, now(), n, loop.totaltime, h, hmax, series, status))
         finally:
             with lock:
                 stop[0] = True

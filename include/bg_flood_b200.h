@@ -36,7 +36,8 @@ enum {
     BGF_ECUDA = 2,         /* a CUDA runtime call failed (see bgf_last_error)   */
     BGF_ENOMEM = 3,        /* device allocation failed                          */
     BGF_EDT_UNDERFLOW = 4, /* dt fell below dtmin before endtime (CrashDetection) */
-    BGF_ENAN = 5,          /* non-finite value detected in the state            */
+    BGF_ENAN = 5,          /* non-finite h, u or v at the start of a step: the  *
+                            * step's dt minimum is zeroed, the scenario stops   */
     BGF_ESTATE = 6,        /* call out of order (e.g. step before state upload) */
     BGF_EBUDGET = 7,       /* serving: request exceeds the HBM budget           */
     BGF_ETIMEOUT = 8,      /* bounded wait gave up                              */
@@ -354,7 +355,8 @@ int bgf_pool_retire(bgf_pool* pool, int slot, bgf_loop* loop, int* nsteps);
 /* Runs pool steps until every admitted scenario has finished or maxsteps steps
  * ran; *nlive receives the number still running. */
 int bgf_pool_run(bgf_pool* pool, int maxsteps, int* nlive);
-/* status: 0 running, 1 finished (end time or step budget), 2 dt underflow. */
+/* status: 0 running, 1 finished (end time or step budget), 2 dt underflow,
+ * 3 non-finite state (the scenario stops; see BGF_ENAN). */
 int bgf_pool_query(bgf_pool* pool, int slot, bgf_loop* loop, int* status, int64_t* nsteps);
 /* Interior depth (and running maximum depth, if tracked) of a scenario's blocks
  * in its active order, 256 values per block. */

@@ -129,16 +129,17 @@ __device__ __forceinline__ void half_tile_cell(Smem<T>& s, const DevModel<T>& m,
 
 // Corrector tile: half-step state h* = Advance(state n, adv, dt/2) at every tile
 // cell, evaluated from the source cell's state and flux divergence; state n is kept
-// on the 18x18 tile for the boundary fluxes and the full-step advance.  As in the
-// predictor, threads 0..127 look up their ring cell's source before the interior.
+// on the 18x18 tile for the boundary fluxes and the full-step advance.  Threads
+// 128..255 take the ring cells (threads 0..67 load the bed entries beyond 256 in
+// the same phase), looking up their source before the interior.
 template <class T, bool SPLIT>
 __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
                                                int cur, T halfdt, int tid, T D, double time)
 {
-    static_assert(NTHREADS == 256, "one interior cell per thread, ring cells on threads 0..127");
+    static_assert(NTHREADS == 256, "one interior cell per thread, ring cells on threads 128..255");
     int rx = 0, ry = 0, sb = ib, sx = 0, sy = 0;
-    const bool ring = tid < 128;
-    if (ring) ring_source<T>(m, ib, tid, rx, ry, sb, sx, sy);
+    const bool ring = tid >= 128;
+    if (ring) ring_source<T>(m, ib, tid - 128, rx, ry, sb, sx, sy);
     half_tile_cell<T, SPLIT>(s, m, p, ib, cur, halfdt, D, time, tid & 15, tid >> 4, ib, tid & 15, tid >> 4);
     if (ring) half_tile_cell<T, SPLIT>(s, m, p, ib, cur, halfdt, D, time, rx, ry, sb, sx, sy);
 }
@@ -180,7 +181,7 @@ __global__ void __launch_bounds__(NTHREADS, Occ<T>::flux) flux_kernel(DevModel<T
         const T D = SPLIT ? m.datum[ib] : (T)0;
 
         // bed and state tiles in one phase (the state tile takes zs from global zb)
-        load_bed<T, ENGINE, SPLIT>(s, m, ib, tid, D);
+        load_bed<T, ENGINE, SPLIT, true>(s, m, ib, tid, D);
         load_state_tile<T, SPLIT>(s, m, ib, cur, tid, D);
         __syncthreads();
         T celldt = tile_fluxes<T, ENGINE, false, SPLIT>(s, p, delta, tid, nullptr, D);

@@ -377,14 +377,16 @@ __device__ __forceinline__ T tile_fluxes(Smem<T>& s, const StepParams<T>& p, T d
     }
     __syncthreads();
     // Thread (tx,ty) owns the left (X) and bottom (Y) faces of its cell; threads
-    // 0..15 also take X face x=16 and threads 16..31 Y face y=16 (the faces the
+    // 0..15 also take X face x=16 and threads 32..47 Y face y=16 (the faces the
     // reference computes in the right / top halo column).
     Face<T> fx = tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, true, tx, ty, sub, D);
     T celldt = fx.dt;  // dtmax after the X sweep (hugeposval exceeds any finite dt)
     Face<T> fy = tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, false, tx, ty, sub, D);
     celldt = fy.wet ? (fy.dt < celldt ? fy.dt : celldt) : fy.dt;
+    // the extra X faces on warp 0 and the extra Y faces on warp 1: each warp runs one
+    // more face pass, instead of warp 0 running two half-empty ones
     if (tid < 16) tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, true, BW, tid, sub, D);
-    else if (tid < 32) tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, false, tid - 16, BW, sub, D);
+    else if (tid >= 32 && tid < 48) tile_face<T, ENGINE, SUB, SPLIT>(s, p, delta, false, tid - 32, BW, sub, D);
     return celldt;
 }
 

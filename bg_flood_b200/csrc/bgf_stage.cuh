@@ -8,22 +8,56 @@
 
 // Loads the bed halo tile and (engine 1) the bed-gradient rows/columns.
 // Split mode stores the tile's bed as the deviation zb + D of the block's datum.
-template <class T, int ENGINE, bool SPLIT = false>
+template <class T, int ENGINE, bool SPLIT = false, bool BALANCE = false>
 __device__ __forceinline__ void load_bed(Smem<T>& s, const DevModel<T>& m, int ib, int tid, T D = (T)0)
 {
     const T* zbt = m.zb + (size_t)ib * 324;
-    for (int k = tid; k < 324; k += NTHREADS) {
-        const int x = k % 18 - 1, y = k / 18 - 1;
-        s.zb[si(x, y)] = SPLIT ? zbt[k] + D : zbt[k];
-    }
-    if (ENGINE == 1) {
-        const T* gx = m.dzbdx + (size_t)ib * 324;
-        const T* gy = m.dzbdy + (size_t)ib * 324;
-        for (int k = tid; k < 18 * 16; k += NTHREADS) {
-            int x = k % 18 - 1, y = k / 18;
-            s.dzbx[gxi(x, y)] = gx[hi18(x, y)];
-            int xx = k % 16, yy = k / 16 - 1;
-            s.dzby[k] = gy[hi18(xx, yy)];
+    const T* gx = m.dzbdx + (size_t)ib * 324;
+    const T* gy = m.dzbdy + (size_t)ib * 324;
+    if constexpr (BALANCE) {
+        // one entry per thread, and the 68 (bed) and 32 (bed gradient) entries beyond
+        // 256 on threads 128..195 and 224..255: threads 0..127 load a ring cell of the
+        // state tile in the same phase.  (The corrector keeps the plain loops: there
+        // the extra live values cost register spills.)
+        static_assert(NTHREADS == 256, "entries 256.. go to threads 128..");
+        {
+            const int k = tid;
+            const int x = k % 18 - 1, y = k / 18 - 1;
+            s.zb[si(x, y)] = SPLIT ? zbt[k] + D : zbt[k];
+        }
+        if (tid >= 128 && tid < 128 + 324 - NTHREADS) {
+            const int k = tid + (NTHREADS - 128);
+            const int x = k % 18 - 1, y = k / 18 - 1;
+            s.zb[si(x, y)] = SPLIT ? zbt[k] + D : zbt[k];
+        }
+        if (ENGINE == 1) {
+            {
+                const int k = tid;
+                int x = k % 18 - 1, y = k / 18;
+                s.dzbx[gxi(x, y)] = gx[hi18(x, y)];
+                int xx = k % 16, yy = k / 16 - 1;
+                s.dzby[k] = gy[hi18(xx, yy)];
+            }
+            if (tid >= NTHREADS - (18 * 16 - NTHREADS)) {
+                const int k = tid + (18 * 16 - NTHREADS);
+                int x = k % 18 - 1, y = k / 18;
+                s.dzbx[gxi(x, y)] = gx[hi18(x, y)];
+                int xx = k % 16, yy = k / 16 - 1;
+                s.dzby[k] = gy[hi18(xx, yy)];
+            }
+        }
+    } else {
+        for (int k = tid; k < 324; k += NTHREADS) {
+            const int x = k % 18 - 1, y = k / 18 - 1;
+            s.zb[si(x, y)] = SPLIT ? zbt[k] + D : zbt[k];
+        }
+        if (ENGINE == 1) {
+            for (int k = tid; k < 18 * 16; k += NTHREADS) {
+                int x = k % 18 - 1, y = k / 18;
+                s.dzbx[gxi(x, y)] = gx[hi18(x, y)];
+                int xx = k % 16, yy = k / 16 - 1;
+                s.dzby[k] = gy[hi18(xx, yy)];
+            }
         }
     }
 }

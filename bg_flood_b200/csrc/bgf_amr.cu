@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(NTHREADS, 3) amr_flux_kernel(DevModel<T> m, Am
     T* const* W = a.W[stage];
     const size_t base = (size_t)ib * 324;
 
-    load_bed<T, ENGINE>(s, m, ib, tid);
+    load_bed<T, ENGINE, false, true>(s, m, ib, tid);  // entries beyond 256 on threads 128..
     {
         // interior and ring 1 (the block's halo, corners excluded)
         const int x = tid & 15, y = tid >> 4;
@@ -358,7 +358,11 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::update) amr_update_kernel
     const double dtd = (double)dt;
     const size_t base = (size_t)ib * 324;
     const size_t fb = (size_t)ib * NFX;
-    for (int k = tid; k < NFX; k += NTHREADS) {
+    // one face entry and one tile entry per thread; the 16 face entries beyond 256 go
+    // to threads 240..255 and the 68 tile entries beyond 256 to threads 128..195, so
+    // that no warp loads three rounds while others load two
+    static_assert(NTHREADS == 256 && NFX == 272, "entries beyond 256 on the upper threads");
+    auto load_faces = [&](int k) {
         s.Fhu[k] = a.F[0][fb + k];
         s.Fqux[k] = a.F[1][fb + k];
         s.Su[k] = a.F[2][fb + k];
@@ -367,15 +371,19 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::update) amr_update_kernel
         s.Fqvy[k] = a.F[5][fb + k];
         s.Sv[k] = a.F[6][fb + k];
         s.Fquy[k] = a.F[7][fb + k];
-    }
+    };
     // state n on the 18x18 tile (boundary segments, full-step advance) and the bed
-    for (int k = tid; k < 324; k += NTHREADS) {
+    auto load_tile = [&](int k) {
         const int q = si(k % 18 - 1, k / 18 - 1);
         s.zb[q] = a.zb[base + k];
         s.h0[q] = a.W[0][0][base + k];
         s.u0[q] = a.W[0][2][base + k];
         s.v0[q] = a.W[0][3][base + k];
-    }
+    };
+    load_faces(tid);
+    load_tile(tid);
+    if (tid >= 240) load_faces(tid + 16);
+    if (tid >= 128 && tid < 196) load_tile(tid + 128);
     __syncthreads();
     // HaloFluxCPULR / HaloFluxCPUBT (src/Halo.cu:1441-1540, 1766-1850): the faces of
     // a side with finer neighbours take the mean of the two fine faces
@@ -398,8 +406,10 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::update) amr_update_kernel
         }
     }
     __syncthreads();
-    apply_boundaries<T>(s, m, p, ib, stage == 0 ? ts.totaltime + ts.dt * 0.5 : ts.totaltime + dtd, tid);
-    __syncthreads();
+    if (block_has_segments<T>(m, ib)) {  // interior blocks skip the step and its barrier
+        apply_boundaries<T>(s, m, p, ib, stage == 0 ? ts.totaltime + ts.dt * 0.5 : ts.totaltime + dtd, tid);
+        __syncthreads();
+    }
     const int x = tid & 15, y = tid >> 4;
     const int c18 = hi18(x, y), q18 = si(x, y);
     const T hs = a.W[stage][0][base + c18], us = a.W[stage][2][base + c18], vs = a.W[stage][3][base + c18];

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <float.h>
 #include <math.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -40,6 +41,18 @@ struct HostSeg {
     std::vector<int> blk[4];
 };
 
+// Per-step control block of a handle: both time slots, both dt-minimum slots and the
+// device error word, laid out alike in device memory and in a page-locked host
+// mirror, so that a flow step moves its inputs with one copy in and its results
+// with one copy out.
+struct StepCtl {
+    TimeState t[2];
+    unsigned long long dtmin[2];
+    int err;
+    int pad[3];
+};
+static_assert(sizeof(StepCtl) <= 256, "the host mirror is one 256-byte page-locked slot");
+
 struct bgf_handle {
     bgf_param P;
     int nblkmem = 0, nblk = 0, dbl = 0, dev = 0, fast = 0;
@@ -70,9 +83,11 @@ struct bgf_handle {
     double *d_seg_t = nullptr, *d_seg_wl = nullptr, *d_rain_t = nullptr, *d_rain_r = nullptr;
     void *d_h[2] = {nullptr, nullptr}, *d_u[2] = {nullptr, nullptr}, *d_v[2] = {nullptr, nullptr};
     void *d_dh = nullptr, *d_dhu = nullptr, *d_dhv = nullptr;
+    StepCtl* d_ctl = nullptr;  // d_time, d_dtmin and d_err point into it
     TimeState* d_time = nullptr;
     unsigned long long* d_dtmin = nullptr;
     double* d_scratch = nullptr;
+    StepCtl* h_ctl = nullptr;  // pinned mirror of d_ctl (single flow steps)
     TimeState* h_time = nullptr;  // pinned
     // pinned scalars: [0] dt-minimum seed (H2D), [1] device error word (D2H)
     unsigned long long* h_misc = nullptr;
@@ -533,7 +548,7 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
     struct A { void** p; size_t bytes; } allocs[] = {
         {(void**)&h->d_active, nb * sizeof(int)},        {(void**)&h->d_level, nb * sizeof(int)},
         {(void**)&h->d_nbr, 8 * nb * sizeof(int)},       {(void**)&h->d_bndseg, 4 * nb * sizeof(int)},
-        {(void**)&h->d_err, sizeof(int)},                {&h->d_zb, nb * 324 * es},
+        {(void**)&h->d_ctl, sizeof(StepCtl)},            {&h->d_zb, nb * 324 * es},
         {&h->d_dzbdx, nb * 324 * es},                    {&h->d_dzbdy, nb * 324 * es},
         {&h->d_cf, nb * 256 * es},                       {(void**)&h->d_rainmask, nb * 256},
         {(void**)&h->d_qmean, nb * 64 * sizeof(float)},  {&h->d_h[0], nb * 256 * es},
@@ -541,7 +556,6 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         {&h->d_u[1], nb * 256 * es},                     {&h->d_v[0], nb * 256 * es},
         {&h->d_v[1], nb * 256 * es},                     {&h->d_dh, nb * 256 * es},
         {&h->d_dhu, nb * 256 * es},                      {&h->d_dhv, nb * 256 * es},
-        {(void**)&h->d_time, 2 * sizeof(TimeState)},     {(void**)&h->d_dtmin, 2 * sizeof(unsigned long long)},
         {(void**)&h->d_scratch, 8 * sizeof(double)},
         {(void**)&h->d_bxo, nb * sizeof(double)},        {(void**)&h->d_byo, nb * sizeof(double)},
         {(void**)&h->d_flags, nb},                       {(void**)&h->d_child, 3 * nb * sizeof(int)},
@@ -580,6 +594,9 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
             *a.p = q;
             q += (a.bytes + 255) & ~(size_t)255;
         }
+        h->d_time = h->d_ctl->t;
+        h->d_dtmin = h->d_ctl->dtmin;
+        h->d_err = &h->d_ctl->err;
     }
     cudaMemsetAsync(h->d_bndseg, 0xff, 4 * nb * sizeof(int), h->stream);
     cudaMemsetAsync(h->d_qmean, 0, nb * 64 * sizeof(float), h->stream);
@@ -594,6 +611,11 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         return BGF_ENOMEM;
     }
     h->h_time = (TimeState*)(h->h_misc + 2);  // two time states after the two scalars
+    h->h_ctl = (StepCtl*)pinned_slot_get();
+    if (!h->h_ctl) {
+        bgf_destroy(h);
+        return BGF_ENOMEM;
+    }
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
     for (int k = 0; k < 3; k++) cudaEventCreate(&h->pev[k]);
@@ -634,6 +656,7 @@ int bgf_destroy(bgf_handle* h)
     h->d_slab = nullptr;
     free_amr(h);
     if (h->h_misc) pinned_slot_put(h->h_misc);
+    if (h->h_ctl) pinned_slot_put(h->h_ctl);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     for (int k = 0; k < 3; k++)
@@ -1287,8 +1310,8 @@ template <class T> static int enqueue_step(bgf_handle* h, int parity)
 }
 
 // The host side of write_time_slot: fills the pinned time slot and dt seed.
-static void set_time_slot_host(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep,
-                               long long maxsteps)
+static TimeState make_time_state(const bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep,
+                                 long long maxsteps)
 {
     TimeState ts;
     memset(&ts, 0, sizeof(ts));
@@ -1303,7 +1326,13 @@ static void set_time_slot_host(bgf_handle* h, const bgf_loop* loop, double endti
     ts.cur = h->cur;
     ts.done = 0;
     ts.status = 0;
-    h->h_time[0] = ts;
+    return ts;
+}
+
+static void set_time_slot_host(bgf_handle* h, const bgf_loop* loop, double endtime, double outputtimestep,
+                               long long maxsteps)
+{
+    h->h_time[0] = make_time_state(h, loop, endtime, outputtimestep, maxsteps);
     h->h_misc[0] = dt_init_bits(h->dbl);
 }
 
@@ -1320,13 +1349,12 @@ static int write_time_slot(bgf_handle* h, const bgf_loop* loop, double endtime, 
 }
 
 // After a step's result reached the pinned slots: error word, loop update, parity.
-static int finish_step(bgf_handle* h, bgf_loop* loop)
+static int finish_step(bgf_handle* h, bgf_loop* loop, int err, const TimeState& nt)
 {
-    if (*(const int*)&h->h_misc[1]) {
+    if (err) {
         g_last_error = "mesh has cross-level neighbours, which this build does not support yet";
         return BGF_EINVAL;
     }
-    const TimeState& nt = h->h_time[1];
     loop->dt = nt.dt;
     loop->dtmax = nt.dtmax;
     h->cur = nt.cur;
@@ -1338,18 +1366,19 @@ static int finish_step(bgf_handle* h, bgf_loop* loop)
     return BGF_OK;
 }
 
-// One flow step for parity p as a graph: the copies of the pinned time slot and dt
-// seed, the step's kernels, and the copies of the resulting time state and error
-// word into the pinned slots.  One launch per bgf_flow_step instead of six calls.
+// One flow step for parity p as a graph: one copy of the control block's time and
+// dt slots in (slot p carries the step's loop state; the other slots are overwritten
+// by the step itself), the step's kernels, and one copy out from time slot p ^ 1 to
+// the error word.  One launch per bgf_flow_step.
 static int build_step_graph(bgf_handle* h, int p)
 {
     cudaGraph_t g;
     BGF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    cudaMemcpyAsync(h->d_time + p, &h->h_time[0], sizeof(TimeState), cudaMemcpyHostToDevice, h->stream);
-    cudaMemcpyAsync(h->d_dtmin + p, &h->h_misc[0], sizeof(unsigned long long), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_ctl, h->h_ctl, offsetof(StepCtl, err), cudaMemcpyHostToDevice, h->stream);
     h->step_graph_launches[p] = h->dbl ? enqueue_step<double>(h, p) : enqueue_step<float>(h, p);
-    cudaMemcpyAsync(&h->h_time[1], h->d_time + (p ^ 1), sizeof(TimeState), cudaMemcpyDeviceToHost, h->stream);
-    cudaMemcpyAsync(&h->h_misc[1], h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    const size_t off = offsetof(StepCtl, t) + (size_t)(p ^ 1) * sizeof(TimeState);
+    cudaMemcpyAsync((char*)h->h_ctl + off, (const char*)h->d_ctl + off, offsetof(StepCtl, err) + sizeof(int) - off,
+                    cudaMemcpyDeviceToHost, h->stream);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (e != cudaSuccess) {
         g_last_error = std::string("graph capture: ") + cudaGetErrorString(e);
@@ -1373,12 +1402,16 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
     if (!h->profiling) {
         const int p = h->parity;
         if (!h->step_graph[p] && (rc = build_step_graph(h, p))) return rc;
-        // the host slots the graph copies from and to (not in use: the previous call synchronised)
-        set_time_slot_host(h, loop, INFINITY, 0.0, 1);
+        // the host block the graph copies from and to (not in use: the previous call
+        // synchronised); both dt slots are armed, slot p ^ 1 is re-armed by the step too
+        StepCtl* c = h->h_ctl;
+        c->t[p] = make_time_state(h, loop, INFINITY, 0.0, 1);
+        c->t[p ^ 1] = c->t[p];
+        c->dtmin[0] = c->dtmin[1] = dt_init_bits(h->dbl);
         BGF_CUDA(cudaGraphLaunch(h->step_graph[p], h->stream));
         h->launches += h->step_graph_launches[p];
         BGF_CUDA(cudaStreamSynchronize(h->stream));
-        return finish_step(h, loop);
+        return finish_step(h, loop, c->err, c->t[p ^ 1]);
     }
     rc = write_time_slot(h, loop, INFINITY, 0.0, 1);
     if (rc) return rc;
@@ -1415,7 +1448,7 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
         h->update_ms += b;
         h->profiled_steps++;
     }
-    return finish_step(h, loop);
+    return finish_step(h, loop, *(const int*)&h->h_misc[1], h->h_time[1]);
 }
 
 static int build_graphs(bgf_handle* h)

@@ -439,7 +439,8 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::update) amr_update_kernel
             const T yc = (T)p.yo_d + (T)m.byo[ib] + (T)y * delta;
             Rainhh = rain_map_at<T>(m.rmap, xc, yc, ts.totaltime);
         } else {
-            Rainhh = (T)series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime);
+            Rainhh = (T)series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime,
+                                  p.rain_sorted != 0);
         }
         const T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
         Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;

@@ -203,6 +203,15 @@ template <class T> static AmrDev<T> amr_dev(bgf_handle* h)
     return a;
 }
 
+// Whether a series' times are non-decreasing (a NaN makes it unsorted); such series
+// are searched by bisection on the device.
+static bool series_sorted(const std::vector<double>& t)
+{
+    for (size_t k = 1; k < t.size(); k++)
+        if (!(t[k - 1] <= t[k])) return false;
+    return true;
+}
+
 template <class T> static StepParams<T> step_params(const bgf_handle* h)
 {
     const bgf_param& P = h->P;
@@ -235,6 +244,7 @@ template <class T> static StepParams<T> step_params(const bgf_handle* h)
     p.nseg = h->nseg_dev;
     p.rain_n = h->rain_n_dev;
     p.rain_off = 0;
+    p.rain_sorted = series_sorted(h->rain_t) ? 1 : 0;
     p.xo_d = std::isnan(P.xo) ? 0.0 : P.xo;
     p.yo_d = std::isnan(P.yo) ? 0.0 : P.yo;
     p.nriver = (int)h->rivers.size();
@@ -863,7 +873,7 @@ static int rebuild_segments(bgf_handle* h)
         d.type = s.type;
         d.n = (int)s.t.size();
         d.off = (int)st.size();
-        d.pad = 0;
+        d.sorted = series_sorted(s.t) ? 1 : 0;
         sd.push_back(d);
         st.insert(st.end(), s.t.begin(), s.t.end());
         swl.insert(swl.end(), s.wl.begin(), s.wl.end());

@@ -53,7 +53,7 @@ struct SegDev {
     int type;  // 0 wall, 1 Neumann, 2 Dirichlet, 3 absorbing
     int n;     // series length (0: no series, zsbnd from zsinit)
     int off;   // offset in the series arrays
-    int pad;
+    int sorted;  // 1: the series times are non-decreasing (the sample is found by bisection)
 };
 
 template <class T> struct StepParams {
@@ -65,6 +65,7 @@ template <class T> struct StepParams {
     int frictionmodel, forcemass, has_cf, has_rain, nseg, rain_n, rain_off;
     int nriver, riv_first;  // rivers of this scenario: entries riv_first .. riv_first + nriver - 1
     int rain_map;           // 1: the rain rate is a gridded series (m.rmap), else the uniform series
+    int rain_sorted;        // 1: the uniform rain series' times are non-decreasing
 };
 
 // A gridded rain series (the reference's DynForcingP<float> Rain read from a

@@ -147,6 +147,7 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     p.nseg = 4;
     p.rain_n = 0;
     p.rain_off = 0;
+    p.rain_sorted = 0;
     p.xo_d = 0.0;
     p.yo_d = 0.0;
     p.nriver = 0;

@@ -64,10 +64,23 @@ __device__ __forceinline__ void load_bed(Smem<T>& s, const DevModel<T>& m, int i
 
 // interptime (src/Util_CPU.cu:107-110) over a uniform series, stepping as
 // FlowbndFlux does (src/Boundary.cu:130-143).
-__device__ __forceinline__ double series_at(const double* t, const double* v, int n, double time)
+// The sample index is the first st in [1, n-1) whose time is not before `time`, else
+// n - 1.  For non-decreasing times that condition holds on a prefix, so bisection
+// finds the same index in log2(n) dependent loads instead of up to n (late in a long
+// series the scan dominated the boundary blocks); other series keep the scan.
+__device__ __forceinline__ double series_at(const double* t, const double* v, int n, double time, bool sorted)
 {
     int st = 1;
-    while (st < n - 1 && t[st] - time < 0.0) st++;
+    if (sorted) {
+        int hi = n - 1;
+        while (st < hi) {
+            const int mid = (st + hi) >> 1;
+            if (t[mid] - time < 0.0) st = mid + 1;
+            else hi = mid;
+        }
+    } else {
+        while (st < n - 1 && t[st] - time < 0.0) st++;
+    }
     return v[st - 1] + (time - t[st - 1]) / (t[st] - t[st - 1]) * (v[st] - v[st - 1]);
 }
 
@@ -170,7 +183,7 @@ __device__ __forceinline__ void apply_boundaries(Smem<T>& s, const DevModel<T>& 
     T taper = (T)1.0;
     if (sg.n > 0) {
         if (p.bndtaper > 0.0) taper = (T)fmin((tbnd - p.inittime) / p.bndtaper, 1.0);
-        zsbnd = series_at(m.seg_t + sg.off, m.seg_wl + sg.off, sg.n, tbnd);
+        zsbnd = series_at(m.seg_t + sg.off, m.seg_wl + sg.off, sg.n, tbnd, sg.sorted != 0);
     }
     int isright = side == 0 ? -1 : side == 1 ? 1 : 0;
     int istop = side == 2 ? 1 : side == 3 ? -1 : 0;

@@ -69,6 +69,25 @@ def dist_env():
     return rank, world, local
 
 
+def host_cpu() -> dict:
+    """The host the CPU baseline ran on: CPU model, logical CPUs and the cores this
+    process may use."""
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        allowed = len(os.sched_getaffinity(0))
+    except AttributeError:
+        allowed = os.cpu_count() or 1
+    return {"cpu_model": model, "nproc": os.cpu_count() or 1, "affinity_cores": allowed}
+
+
 def measured_peak_hbm():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -379,7 +398,7 @@ def run_reference_arm(args, rank, world):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample": "256x256 window of the workload", "engine": args.engine},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthreads, "kind": kind,
-                         "sample": f"{steps} FlowCPU steps on a 256x256 window ({secs:.1f} s)"},
+                         "sample": f"{steps} FlowCPU steps on a 256x256 window ({secs:.1f} s)", "host": host_cpu()},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -524,7 +543,7 @@ def main():
     if rank == 0 and world == 1:
         cv, kind, secs = cpu_reference_sample(8, 1, args.engine)
         cpu = {"value": cv, "unit": UNIT, "cores": min(8, os.cpu_count() or 1), "kind": kind,
-               "sample": f"8 FlowCPU steps on a 256x256 window of the workload ({secs:.1f} s)"}
+               "sample": f"8 FlowCPU steps on a 256x256 window of the workload ({secs:.1f} s)", "host": host_cpu()}
 
     if rank == 0:
         line = {

@@ -523,6 +523,17 @@ def main():
         ms, nl = f.last_run_timing()
         extra["device_loop_L2_resident"] = {"value": ncell * 400 / (ms / 1e3), "steps": 400, "ms": ms}
         del f
+        # the whole simulated run of the workload (20 s) in the device loop, from a
+        # fresh start: late steps read the far end of the boundary series
+        fr, mr, lr = make_gpu(workload_case(args.n, args.engine, local, args.fastmath))
+        lr.nextoutputtime = 1e30
+        t0 = time.perf_counter()
+        nfull = fr.run(lr, endtime=20.0)
+        wall_full = time.perf_counter() - t0
+        msf, _ = fr.last_run_timing()
+        extra["full_run_20s"] = {"value": mr.nblk * 256 * nfull / (msf / 1e3), "steps": nfull, "ms": msf,
+                                 "wall_s": wall_full, "simulated_s": lr.totaltime}
+        del fr
         # a grid well above L2 (4096^2 cells, ~1 GB of state): HBM-bound device loop
         big = workload_case(4096, args.engine, local, args.fastmath)
         fb, mb, lb = make_gpu(big)

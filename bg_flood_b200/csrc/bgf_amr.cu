@@ -87,9 +87,13 @@ __device__ __forceinline__ T wetdry_restrict(const Acc256<T>& h, const Acc324<T>
 
 // ---------------------------------------------------------------- stage kernels
 
+// Threads 0..255 copy the interior cells and threads 256..319 (two more warps) fill
+// the 64 halo cells, so that the halo rules do not wait behind an interior copy.
+constexpr int HALO_THREADS = NTHREADS + 64;
+
 template <class T>
-__global__ void __launch_bounds__(NTHREADS) amr_halo_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
-                                                             int stage)
+__global__ void __launch_bounds__(HALO_THREADS) amr_halo_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0,
+                                                                 int parity, int stage)
 {
     __shared__ T th[3][324];
     const int tid = threadIdx.x;
@@ -103,8 +107,8 @@ __global__ void __launch_bounds__(NTHREADS) amr_halo_kernel(DevModel<T> m, AmrDe
                        stage == 0 ? m.v[ts.cur] : m.dhv};
     T* const* W = a.W[stage];
     const size_t base = (size_t)ib * 324;
-    const int x = tid & 15, y = tid >> 4, c = hi18(x, y);
-    {
+    const int x = tid & 15, y = (tid >> 4) & 15, c = hi18(x, y);
+    if (tid < NTHREADS) {
         const size_t g = (size_t)ib * 256 + tid;
 #pragma unroll
         for (int f = 0; f < 3; f++) th[f][c] = src[f][g];
@@ -112,9 +116,8 @@ __global__ void __launch_bounds__(NTHREADS) amr_halo_kernel(DevModel<T> m, AmrDe
         W[2][base + c] = th[1][c];
         W[3][base + c] = th[2][c];
         W[1][base + c] = a.zb[base + c] + th[0][c];
-    }
-    if (tid < 64) {
-        const int s = tid >> 4, j = tid & 15;
+    } else {
+        const int s = (tid - NTHREADS) >> 4, j = tid & 15;
         const CellRule<T> r = halo_rule<T>(m.nbr, nbm, m.level, ib, s, j);
         T hv = rule_eval(r, Acc256<T>{src[0]});
         const T uv = rule_eval(r, Acc256<T>{src[1]});
@@ -137,6 +140,7 @@ __global__ void __launch_bounds__(NTHREADS) amr_halo_kernel(DevModel<T> m, AmrDe
     // finer neighbours' halos
     if (!has_finer_neighbour(m.nbr, nbm, m.level, ib)) return;
     __syncthreads();
+    if (tid >= NTHREADS) return;
     const T delta = calcres<T>(p.delta0, m.level[ib]);
     const T rdelta = (T)1.0 / delta;
 #pragma unroll
@@ -545,7 +549,7 @@ int launch_amr_stage(const DevModel<T>& m, const AmrDev<T>& a, const StepParams<
 {
     const int n = m.nblk;
     int launches = 0;
-    amr_halo_kernel<T><<<n, NTHREADS, 0, st>>>(m, a, p, parity, stage);
+    amr_halo_kernel<T><<<n, HALO_THREADS, 0, st>>>(m, a, p, parity, stage);
     amr_refine_kernel<T><<<n, 64, 0, st>>>(m, a, p, parity, stage);
     launches += 2;
     if (a.wetdryfix) {

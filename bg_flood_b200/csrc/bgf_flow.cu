@@ -151,7 +151,7 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
 // hides the tile loads; FP64 instantiations keep more registers.
 #if BGF_FAST
 template <class T> struct Occ {
-    static constexpr int flux = sizeof(T) == 4 ? 6 : 3, update = sizeof(T) == 4 ? 5 : 3;
+    static constexpr int flux = sizeof(T) == 4 ? 6 : 3, update = sizeof(T) == 4 ? 6 : 3;
 };
 #else
 template <class T> struct Occ {

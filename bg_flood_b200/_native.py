@@ -63,6 +63,9 @@ SIGNATURES = {
     "bgf_pool_timing": (ctypes.c_int, [c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64), c_int_p]),
     "bgf_pool_set_grid": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "bgf_autotune": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_double_p]),
+    "bgf_add_target_level_map": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_double, c_int_p]),
+    "bgf_clear_target_level_maps": (ctypes.c_int, [c_void_p]),
     "bgf_pool_autotune": (ctypes.c_int, [c_void_p, ctypes.c_int, c_int_p, c_double_p]),
     "bgf_set_rain_map": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,

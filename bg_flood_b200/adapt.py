@@ -1,8 +1,9 @@
 """Host mirror of the reference's adaptation pass (src/AdaptCriteria.cu,
 src/Adaptation.cu): criteria parsing and the table-level entry points of the C ABI.
 
-``parse_criterion`` reads the reference's ``Adaptation`` key ("Threshold,<z>,<var>"
-or "Inrange,<zmin>,<zmax>,<var>", src/ReadInput.cu:830-850).  ``refine_sanity`` and
+``parse_criterion`` reads the reference's ``Adaptation`` key ("Threshold,<z>,<var>",
+"Inrange,<zmin>,<zmax>,<var>" or "Targetlevel,<file>,...", src/ReadInput.cu:830-850,
+1155-1172).  ``refine_sanity`` and
 ``refine_tables`` call bgf_refine_sanity / bgf_refine_tables on block-id indexed
 host tables."""
 from __future__ import annotations
@@ -14,7 +15,7 @@ import numpy as np
 
 from ._native import lib
 
-THRESHOLD, INRANGE = 1, 2
+THRESHOLD, INRANGE, TARGETLEVEL = 1, 2, 3
 VARS = {"h": 0, "zs": 1, "u": 2, "v": 3, "zb": 4}
 
 
@@ -24,6 +25,7 @@ class Criterion:
     var: str
     arg1: float
     arg2: float = 0.0
+    maps: tuple = ()  # Targetlevel: the target-level map files, in order
 
     def flags(self, z: np.ndarray, dtype=np.float32) -> np.ndarray:
         """Refine flag per block from the interior cells z (nblk, 16, 16), as
@@ -40,6 +42,8 @@ def parse_criterion(text: str) -> Criterion:
         return Criterion(THRESHOLD, parts[2], float(parts[1]))
     if parts[0] == "Inrange":
         return Criterion(INRANGE, parts[3], float(parts[1]), float(parts[2]))
+    if parts[0].lower() == "targetlevel":
+        return Criterion(TARGETLEVEL, "h", 0.0, 0.0, tuple(p for p in parts[1:] if p))
     raise ValueError(f"unsupported adaptation criterion: {text}")
 
 

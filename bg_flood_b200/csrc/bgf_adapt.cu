@@ -41,6 +41,40 @@ __global__ void __launch_bounds__(256) adapt_criteria_kernel(DevModel<T> m, cons
     if (tid == 0) flags[ib] = any ? 1 : 0;
 }
 
+// targetlevelcriteria (src/AdaptCriteria.cu:179-232): at every cell of a block the
+// map's level, interp2BUQ's bilinear value (src/GridManip.cu:456-495, in double from
+// the clamped cell position) rounded in T; the block refines when some cell's level
+// is above its own and keeps its level (no coarsening) when some cell's level equals
+// it.  Every map rewrites the flags of all blocks, so the last map decides.
+template <class T>
+__global__ void __launch_bounds__(256) target_level_kernel(DevModel<T> m, TargetMapDev g, T xo, T yo, double dx0,
+                                                           uint8_t* refine, uint8_t* coarsen)
+{
+    const int ib = m.active[blockIdx.x];
+    const int tid = threadIdx.x, ix = tid & 15, iy = tid >> 4;
+    const int lev = m.level[ib];
+    const T delta = (T)calcres<double>(dx0, lev);
+    const T x = xo + (T)m.bxo[ib] + (T)ix * delta;
+    const T y = yo + (T)m.byo[ib] + (T)iy * delta;
+    const double xi = fmax(fmin((double)x, g.xmax), g.xo);
+    const double yi = fmax(fmin((double)y, g.ymax), g.yo);
+    const int cfi = min(max((int)floor((xi - g.xo) / g.dx), 0), g.nx - 2), cfip = cfi + 1;
+    const int cfj = min(max((int)floor((yi - g.yo) / g.dy), 0), g.ny - 2), cfjp = cfj + 1;
+    const double x1 = g.xo + g.dx * cfi, x2 = g.xo + g.dx * cfip;
+    const double y1 = g.yo + g.dy * cfj, y2 = g.yo + g.dy * cfjp;
+    const double q11 = g.val[cfi + cfj * g.nx], q12 = g.val[cfi + cfjp * g.nx];
+    const double q21 = g.val[cfip + cfj * g.nx], q22 = g.val[cfip + cfjp * g.nx];
+    const double x2x1 = x2 - x1, y2y1 = y2 - y1, x2x = x2 - xi, y2y = y2 - yi, yy1 = yi - y1, xx1 = xi - x1;
+    const T v = (T)(1.0 / (x2x1 * y2y1) * (q11 * x2x * y2y + q21 * xx1 * y2y + q12 * x2x * yy1 + q22 * xx1 * yy1));
+    const int target = (int)round(v);
+    const int up = __syncthreads_or(target > lev ? 1 : 0);
+    const int same = __syncthreads_or(target == lev ? 1 : 0);
+    if (tid == 0) {
+        refine[ib] = up ? 1 : 0;
+        coarsen[ib] = up || same ? 0 : 1;
+    }
+}
+
 template <class T> __global__ void __launch_bounds__(256) adapt_zs_kernel(DevModel<T> m, T* zs, int cur)
 {
     const int ib = m.active[blockIdx.x];
@@ -345,6 +379,13 @@ template <class T> void launch_criteria(const DevModel<T>& m, const T* z, int st
     adapt_criteria_kernel<T><<<m.nblk, 256, 0, st>>>(m, z, stride324, kind, a1, a2, flags);
 }
 
+template <class T>
+void launch_target_level(const DevModel<T>& m, const TargetMapDev& g, double xo, double yo, double dx0,
+                         uint8_t* refine, uint8_t* coarsen, cudaStream_t st)
+{
+    target_level_kernel<T><<<m.nblk, 256, 0, st>>>(m, g, (T)xo, (T)yo, dx0, refine, coarsen);
+}
+
 template <class T> void launch_zs(const DevModel<T>& m, T* zs, int cur, cudaStream_t st)
 {
     adapt_zs_kernel<T><<<m.nblk, 256, 0, st>>>(m, zs, cur);
@@ -369,6 +410,8 @@ template <class T> void launch_bed(const DevModel<T>& m, const AdaptDev<T>& a, c
 #define BGF_ADAPT_INST(T)                                                                                          \
     template void launch_criteria<T>(const DevModel<T>&, const T*, int, int, T, T, uint8_t*, cudaStream_t);       \
     template void launch_zs<T>(const DevModel<T>&, T*, int, cudaStream_t);                                         \
+    template void launch_target_level<T>(const DevModel<T>&, const TargetMapDev&, double, double, double, uint8_t*, \
+                                         uint8_t*, cudaStream_t);                                                  \
     template void launch_children<T>(const DevModel<T>&, const AdaptDev<T>&, int, T*, uint8_t*, cudaStream_t);      \
     template void launch_bed<T>(const DevModel<T>&, const AdaptDev<T>&, const StepParams<T>&, int, T*, double,      \
                                 double, const double*, const double*, double, uint8_t*, cudaStream_t);

@@ -310,6 +310,14 @@ __device__ __forceinline__ T refine_value(const A& z, const A& gx, const A& gy, 
 namespace adapt {
 
 // Device view of the refinement pass (bgf_adapt.cu).
+// A target-level map of the Targetlevel criterion: nx*ny nodes from (xo, yo) with
+// spacings dx, dy (integer levels held as float, which represents them exactly).
+struct TargetMapDev {
+    const float* val;
+    int nx, ny;
+    double xo, yo, dx, dy, xmax, ymax;
+};
+
 template <class T> struct AdaptDev {
     T* W[4];            // h, zs, u, v on 18x18 tiles of the old mesh
     T* zs;              // zs of the state, 256 per block

@@ -88,6 +88,8 @@ struct bgf_handle {
     unsigned long long* d_dtmin = nullptr;
     double* d_scratch = nullptr;
     StepCtl* h_ctl = nullptr;  // pinned mirror of d_ctl (single flow steps)
+    std::vector<adapt::TargetMapDev> tmaps;  // Targetlevel maps (device node values)
+    uint8_t* d_cflags = nullptr;             // coarsen flags of the Targetlevel criterion
     TimeState* h_time = nullptr;  // pinned
     // pinned scalars: [0] dt-minimum seed (H2D), [1] device error word (D2H)
     unsigned long long* h_misc = nullptr;
@@ -569,6 +571,7 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         {(void**)&h->d_scratch, 8 * sizeof(double)},
         {(void**)&h->d_bxo, nb * sizeof(double)},        {(void**)&h->d_byo, nb * sizeof(double)},
         {(void**)&h->d_flags, nb},                       {(void**)&h->d_child, 3 * nb * sizeof(int)},
+        {(void**)&h->d_cflags, nb},
         {&h->d_datum, nb * es},
     };
     // one device allocation carved into 256-byte aligned pieces: handles are created
@@ -661,8 +664,11 @@ int bgf_destroy(bgf_handle* h)
     // stream order); the rest are own allocations
     void* ptrs[] = {h->d_slab, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t, h->d_rain_r, h->d_dem,
                     h->d_rivers, h->d_riv_t, h->d_riv_q, (void*)h->rmap.val, h->d_tiles};
-    if (h->stream)
+    if (h->stream) {
         for (void* p : ptrs) dfree(h, p);
+        for (auto& g : h->tmaps) dfree(h, (void*)g.val);
+    }
+    h->tmaps.clear();
     h->d_slab = nullptr;
     free_amr(h);
     if (h->h_misc) pinned_slot_put(h->h_misc);
@@ -1604,6 +1610,39 @@ int bgf_set_bathy(bgf_handle* h, int nx, int ny, double xo, double yo, double dx
     return BGF_OK;
 }
 
+int bgf_add_target_level_map(bgf_handle* h, int nx, int ny, double xo, double yo, double dx, const int* levels)
+{
+    if (!h || nx < 2 || ny < 2 || !(dx > 0.0) || !levels) return BGF_EINVAL;
+    int rc = set_device(h);
+    if (rc) return rc;
+    const size_t n = (size_t)nx * ny;
+    std::vector<float> v(n);
+    for (size_t k = 0; k < n; k++) v[k] = (float)levels[k];
+    adapt::TargetMapDev g{};
+    BGF_CUDA(dalloc(h, (void**)&g.val, sizeof(float) * n));
+    BGF_CUDA(cudaMemcpy((void*)g.val, v.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    g.nx = nx;
+    g.ny = ny;
+    g.xo = xo;
+    g.yo = yo;
+    g.dx = dx;
+    g.dy = dx;
+    g.xmax = xo + (nx - 1) * dx;
+    g.ymax = yo + (ny - 1) * dx;
+    h->tmaps.push_back(g);
+    return BGF_OK;
+}
+
+int bgf_clear_target_level_maps(bgf_handle* h)
+{
+    if (!h) return BGF_EINVAL;
+    int rc = set_device(h);
+    if (rc) return rc;
+    for (auto& g : h->tmaps) dfree(h, (void*)g.val);
+    h->tmaps.clear();
+    return BGF_OK;
+}
+
 int bgf_get_blocks(bgf_handle* h, int* nblk, int* active, int* level, int* nbr8, double* xo, double* yo)
 {
     if (!h || !nblk) return BGF_EINVAL;
@@ -1645,6 +1684,35 @@ template <class T> static int adapt_flags_t(bgf_handle* h, const bgf_adapt_param
 {
     const int nb = h->nblkmem;
     DevModel<T> m = dev_model<T>(h);
+    if (ap->criterion == BGF_ADAPT_TARGETLEVEL) {
+        // AdaptCriteria runs targetlevelcriteria once per map (the last map decides)
+        if (h->tmaps.empty()) {
+            g_last_error = "the Targetlevel criterion needs at least one target-level map";
+            return BGF_EINVAL;
+        }
+        for (const auto& g : h->tmaps) {
+            adapt::launch_target_level<T>(m, g, std::isnan(h->P.xo) ? 0.0 : h->P.xo, std::isnan(h->P.yo) ? 0.0 : h->P.yo,
+                                          h->P.dx, h->d_flags, h->d_cflags, h->stream);
+            h->launches++;
+        }
+        BGF_CUDA(cudaGetLastError());
+        refine.assign(nb, 0);
+        coarsen.assign(nb, 0);
+        BGF_CUDA(cudaMemcpyAsync(refine.data(), h->d_flags, nb, cudaMemcpyDeviceToHost, h->stream));
+        BGF_CUDA(cudaMemcpyAsync(coarsen.data(), h->d_cflags, nb, cudaMemcpyDeviceToHost, h->stream));
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
+        std::vector<uint8_t> mask(nb, 0);
+        for (int ibl = 0; ibl < h->nblk; ibl++) mask[h->active[ibl]] = 1;
+        for (int ib = 0; ib < nb; ib++) {
+            refine[ib] = mask[ib] ? refine[ib] : 0;
+            coarsen[ib] = mask[ib] ? coarsen[ib] : 0;
+        }
+        std::vector<int> nbr8((size_t)8 * nb);
+        for (int ib = 0; ib < nb; ib++)
+            for (int k = 0; k < 8; k++) nbr8[8 * ib + k] = h->nbr[(size_t)k * nb + ib];
+        return bgf_refine_sanity(h->nblk, h->active.data(), h->level.data(), nbr8.data(), nb, h->P.minlevel,
+                                 h->P.maxlevel, refine.data(), coarsen.data());
+    }
     const T* z = nullptr;
     int stride324 = 0;
     switch (ap->var) {
@@ -1678,6 +1746,7 @@ template <class T> static int adapt_flags_t(bgf_handle* h, const bgf_adapt_param
 static int check_adapt_param(const bgf_adapt_param* ap)
 {
     if (!ap) return BGF_EINVAL;
+    if (ap->criterion == BGF_ADAPT_TARGETLEVEL) return BGF_OK;  // var, arg1 and arg2 are not used
     if (ap->criterion != BGF_ADAPT_THRESHOLD && ap->criterion != BGF_ADAPT_INRANGE) return BGF_EINVAL;
     if (ap->var < BGF_VAR_H || ap->var > BGF_VAR_ZB) return BGF_EINVAL;
     return BGF_OK;

@@ -47,6 +47,10 @@ template <class T> struct AdaptDev;
 template <class T> void launch_criteria(const DevModel<T>& m, const T* z, int stride324, int kind, T a1, T a2,
                                         uint8_t* flags, cudaStream_t st);
 template <class T> void launch_zs(const DevModel<T>& m, T* zs, int cur, cudaStream_t st);
+struct TargetMapDev;
+template <class T>
+void launch_target_level(const DevModel<T>& m, const TargetMapDev& g, double xo, double yo, double dx0,
+                         uint8_t* refine, uint8_t* coarsen, cudaStream_t st);
 template <class T> void launch_children(const DevModel<T>& m, const AdaptDev<T>& a, int cur, T* cf, uint8_t* rainmask,
                                         cudaStream_t st);
 template <class T> void launch_bed(const DevModel<T>& m, const AdaptDev<T>& a, const StepParams<T>& p, int cur, T* zb,

@@ -215,6 +215,18 @@ class FlowB200:
         ny, nx = g.shape
         _check(lib().bgf_set_bathy(self.handle, nx, ny, float(xo), float(yo), float(dx), _ptr(g)), "bgf_set_bathy")
 
+    def add_target_level_map(self, xo: float, yo: float, dx: float, levels: np.ndarray) -> None:
+        """Target-level map (ny, nx) of integer levels, node (0, 0) at (xo, yo), for the
+        Targetlevel criterion; maps apply in the order added (the last decides)."""
+        g = np.ascontiguousarray(levels, np.int32)
+        ny, nx = g.shape
+        _check(lib().bgf_add_target_level_map(self.handle, nx, ny, float(xo), float(yo), float(dx),
+                                              g.ctypes.data_as(ctypes.POINTER(ctypes.c_int))),
+               "bgf_add_target_level_map")
+
+    def clear_target_level_maps(self) -> None:
+        _check(lib().bgf_clear_target_level_maps(self.handle), "bgf_clear_target_level_maps")
+
     def _adapt_param(self, crit, maxiteration: int):
         from .adapt import VARS
         return CAdaptParam(crit.kind, VARS[crit.var], float(crit.arg1), float(crit.arg2), int(maxiteration))

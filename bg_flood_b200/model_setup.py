@@ -42,7 +42,7 @@ import numpy as np
 from ._native import lib
 from .mesh import Mesh, boundary_segments, uniform_mesh
 from .params import Param, read_param_text
-from .readforcing import BathyGrid, read_bathy, read_flow_file, read_uniform_series
+from .readforcing import BathyGrid, read_asc, read_bathy, read_flow_file, read_uniform_series
 
 __all__ = ["ModelInputs", "read_param_file", "prepare_model", "setup_model", "check_param_sanity", "inputs_on_mesh"]
 
@@ -368,6 +368,11 @@ def setup_model(param_file: str, basedir: str | None = None, nblkmem: int | None
         f = _load(inp, cap)
         f.set_bathy(inp.bathy.xo, inp.bathy.yo, inp.bathy.dx, inp.bathy.val)
         crit = parse_criterion(",".join([p.AdaptCrit] + list(p.Adapt_args)))
+        for fn in crit.maps:
+            # a target-level map (readstaticforcing into StaticForcingP<int>): the
+            # grid's values truncated to integers, as the int conversion does
+            g = read_asc(_resolve(fn, basedir or os.path.dirname(os.path.abspath(param_file))))
+            f.add_target_level_map(g.xo, g.yo, g.dx, np.trunc(g.val).astype(np.int32))
         f.adapt(crit, p.adaptmaxiteration)
         inp = _adapted_inputs(inp, f)
         f.close()

@@ -380,10 +380,14 @@ int bgf_autotune(bgf_handle* h, const bgf_loop* loop, int steps, int* grid, doub
 int bgf_pool_autotune(bgf_pool* pool, int steps, int* grid, double* ms_per_step);
 
 /* ------------------------------------------------------------ refinement pass */
-/* Criterion of the reference's "Adaptation" key (src/AdaptCriteria.cu:20-130):
+/* Criterion of the reference's "Adaptation" key (src/AdaptCriteria.cu:20-232):
  * a block is flagged for refinement when any of its cells has var > arg1
- * (Threshold) or arg1 <= var <= arg2 (Inrange), compared in the state precision. */
-enum { BGF_ADAPT_THRESHOLD = 1, BGF_ADAPT_INRANGE = 2 };
+ * (Threshold) or arg1 <= var <= arg2 (Inrange), compared in the state precision,
+ * or (Targetlevel) when the rounded bilinear value of a target-level map at any of
+ * its cells is above the block's level; Targetlevel keeps a block from coarsening
+ * when some cell's target equals its level, and each map rewrites the flags of the
+ * previous one (the last map decides), as the reference loops over its maps. */
+enum { BGF_ADAPT_THRESHOLD = 1, BGF_ADAPT_INRANGE = 2, BGF_ADAPT_TARGETLEVEL = 3 };
 enum { BGF_VAR_H = 0, BGF_VAR_ZS = 1, BGF_VAR_U = 2, BGF_VAR_V = 3, BGF_VAR_ZB = 4 };
 typedef struct bgf_adapt_param {
     int criterion;     /* BGF_ADAPT_THRESHOLD or BGF_ADAPT_INRANGE            */
@@ -397,6 +401,13 @@ typedef struct bgf_adapt_param {
  * re-interpolates the bed of every block from it, as the reference does
  * (interp2BUQ + setedges, src/GridManip.cu:222-575). */
 int bgf_set_bathy(bgf_handle* h, int nx, int ny, double xo, double yo, double dx, const float* val);
+
+/* Target-level maps of the Targetlevel criterion (the reference's
+ * Forcing.targetadapt, one per file of "Adaptation = Targetlevel,<file>,..."):
+ * nx*ny integer levels, row-major, node (0, 0) at (xo, yo), spacing dx in x and y.
+ * Maps are applied in the order they were added. */
+int bgf_add_target_level_map(bgf_handle* h, int nx, int ny, double xo, double yo, double dx, const int* levels);
+int bgf_clear_target_level_maps(bgf_handle* h);
 
 /* Refine / coarsen flags of one criterion + sanity pass on the current mesh and
  * state, one byte per active block (active order); the mesh is not changed. */

@@ -94,6 +94,8 @@ def ref_lib():
         l.ref_flags.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ubyte), ctypes.POINTER(ctypes.c_ubyte)]
         l.ref_set_bathy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, D]
+        l.ref_add_target_map.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         l.ref_nblkmem.argtypes = [ctypes.c_void_p]
         l.ref_create_from_file.restype = ctypes.c_void_p
         l.ref_create_from_file.argtypes = [ctypes.c_char_p, ctypes.c_int]
@@ -345,6 +347,14 @@ class Reference:
         v = np.ascontiguousarray(val, np.float64)
         ny, nx = v.shape
         self.lib.ref_set_bathy(self.h, nx, ny, xo, yo, dx, _dp(v))
+
+    def add_target_map(self, xo: float, yo: float, dx: float, levels: np.ndarray):
+        """Appends a target-level map (ny, nx) of integers with node (0, 0) at (xo, yo)
+        (the Targetlevel criterion; the last map decides)."""
+        v = np.ascontiguousarray(levels, np.int32)
+        ny, nx = v.shape
+        if self.lib.ref_add_target_map(self.h, nx, ny, xo, yo, dx, v.ctypes.data_as(ctypes.POINTER(ctypes.c_int))):
+            raise RuntimeError("ref_add_target_map failed")
 
     @property
     def nblkmem(self) -> int:

@@ -421,6 +421,27 @@ int ref_set_bathy(void* hdl, int nx, int ny, double xo, double yo, double dx, co
 {
     return ((RefBase*)hdl)->set_bathy(nx, ny, xo, yo, dx, val);
 }
+
+// Appends a target-level map (an entry of the reference's Forcing.targetadapt, which
+// readforcing fills from the files of "Adaptation = Targetlevel,<file>,..."): nx*ny
+// integer nodes from (xo, yo) with spacing dx in x and y.
+int ref_add_target_map(void* hdl, int nx, int ny, double xo, double yo, double dx, const int* val)
+{
+    StaticForcingP<int> m;
+    m.nx = nx;
+    m.ny = ny;
+    m.xo = xo;
+    m.yo = yo;
+    m.dx = dx;
+    m.dy = dx;
+    m.xmax = xo + (nx - 1) * dx;
+    m.ymax = yo + (ny - 1) * dx;
+    m.val = (int*)malloc(sizeof(int) * (size_t)nx * ny);
+    if (!m.val) return 1;
+    for (int k = 0; k < nx * ny; k++) m.val[k] = val[k];
+    ((RefBase*)hdl)->F.targetadapt.push_back(m);
+    return 0;
+}
 int ref_nblkmem(void* hdl) { return ((RefBase*)hdl)->P.nblkmem; }
 
 int ref_set_rain_series(void* hdl, int n, const double* t, const double* r)

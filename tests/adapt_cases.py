@@ -56,3 +56,31 @@ def id_tables(r: Reference, mem: int = MEM):
     xo[act] = xo_a
     yo[act] = yo_a
     return act, level, nbr, xo, yo
+
+
+# ---------------------------------------------------------------- Targetlevel criterion
+
+def target_case():
+    """The hump case with the Targetlevel criterion (maps added separately)."""
+    case = cases.amr_hump(64, 1, 2, 0.3)
+    case.paramtext = "\n".join("Adaptation = Targetlevel" if ln.startswith("Adaptation") else ln
+                               for ln in case.paramtext.splitlines()) + "\n"
+    return case
+
+
+def target_maps(case):
+    """Two target-level maps of 17 x 17 nodes over the level-0 domain, as
+    (xo, yo, dx, levels (ny, nx) int32).  The first asks for level 2 everywhere and
+    is overridden by the second (the reference applies the maps in turn and the
+    last decides): level 2 in a disc, 1 in a band around it and along the south
+    edge, 0 elsewhere."""
+    ext = case.n0 * case.dx
+    dxm = ext / 16.0
+    xs = case.xo + dxm * np.arange(17)
+    ys = case.yo + dxm * np.arange(17)
+    X, Y = np.meshgrid(xs, ys)
+    r = np.hypot(X - (case.xo + 0.3 * ext), Y - (case.yo + 0.6 * ext))
+    second = np.where(r < 0.2 * ext, 2, np.where(r < 0.3 * ext, 1, 0))
+    second[Y < case.yo + 0.15 * ext] = 1
+    first = np.full((17, 17), 2)
+    return [(case.xo, case.yo, dxm, first.astype(np.int32)), (case.xo, case.yo, dxm, second.astype(np.int32))]

@@ -177,7 +177,26 @@ def main_rainmap():
     print("rainmap48_e1", NSTEPS, dts[:3])
 
 
+def main_adapt_target():
+    """The reference's Adaptation() with the Targetlevel criterion and two target-level
+    maps (the last decides): final tables and interior fields (tests/test_gpu_adapt.py)."""
+    from adapt_cases import id_tables, reference_with_bathy, target_case, target_maps
+    case = target_case()
+    r = reference_with_bathy(case)
+    for xo, yo, dx, lv in target_maps(case):
+        r.add_target_map(xo, yo, dx, lv)
+    r.adaptation()
+    act, level, nbr, xo, yo = id_tables(r)
+    out = {k: interior(r.get(k)).astype(np.float32) for k in ("h", "zs", "u", "v", "zb")}
+    np.savez_compressed(os.path.join(HERE, "adapt_target_hump64.npz"), act=act, level=level[act], nbr=nbr[act],
+                        xo=xo[act], yo=yo[act], **out)
+    print("adapt Targetlevel", len(act), np.bincount(level[act]))
+
+
 if __name__ == "__main__":
+    if sys.argv[1:] == ["target"]:
+        main_adapt_target()
+        sys.exit(0)
     if sys.argv[1:] == ["setup"]:
         main_setup()
         sys.exit(0)

@@ -11,7 +11,8 @@ import os
 import numpy as np
 import pytest
 
-from adapt_cases import ADAPT_CASES, MEM, criterion_of, level0_grids
+from adapt_cases import ADAPT_CASES, MEM, criterion_of, level0_grids, target_case, target_maps
+from bg_flood_b200.adapt import TARGETLEVEL, Criterion
 from bg_flood_b200.flow import FlowB200, Loop
 from bg_flood_b200.mesh import boundary_segments, grid_to_buq, uniform_mesh
 from runners import interior
@@ -28,8 +29,8 @@ def _pad(a, n):
     return out
 
 
-def adapted_model(name, steps=0):
-    case = ADAPT_CASES[name]()
+def adapted_model(name, steps=0, case=None, maps=()):
+    case = case if case is not None else ADAPT_CASES[name]()
     zb0, h0 = level0_grids(case)
     mesh = uniform_mesh(case.n0, case.n0, case.dx)
     f = FlowB200(case.param, MEM)
@@ -45,7 +46,10 @@ def adapted_model(name, steps=0):
         f.init_dt(loop)
         for _ in range(steps):
             loop.totaltime += f.flow_step(loop)
-    n, it = f.adapt(criterion_of(case))
+    for xo, yo, dx, lv in maps:
+        f.add_target_level_map(xo, yo, dx, lv)
+    crit = Criterion(TARGETLEVEL, "h", 0.0) if maps else criterion_of(case)
+    n, it = f.adapt(crit)
     return case, f, n, it
 
 
@@ -69,6 +73,28 @@ def test_adaptation_matches_reference(name, steps):
     assert np.array_equal(interior(h[act]), g["h"])
     assert float(np.abs(interior(u[act]) - g["u"]).max()) <= UV_TOL
     assert float(np.abs(interior(v[act]) - g["v"]).max()) <= UV_TOL
+
+
+def test_targetlevel_adaptation_matches_reference():
+    """Targetlevel with two maps, the second overriding the first (the reference's
+    Adaptation() with the same maps: tests/golden/adapt_target_hump64.npz)."""
+    g = np.load(os.path.join(GOLDEN, "adapt_target_hump64.npz"))
+    case = target_case()
+    case, f, n, it = adapted_model("target", case=case, maps=target_maps(case))
+    act, lev, nb, xo, yo = f.get_blocks()
+    assert n == len(g["act"]) and set(np.unique(lev[act])) == {0, 1, 2}
+    assert np.array_equal(act, g["act"])
+    assert np.array_equal(lev[act], g["level"])
+    assert np.array_equal(nb[act], g["nbr"])
+    assert np.array_equal(xo[act].astype(np.float32), g["xo"].astype(np.float32))
+    assert np.array_equal(yo[act].astype(np.float32), g["yo"].astype(np.float32))
+    assert np.array_equal(interior(f.get_bed()[act]), g["zb"])
+    zs, h, u, v = f.get_state()
+    assert np.array_equal(interior(h[act]), g["h"])
+    # without a map the criterion is refused
+    f.clear_target_level_maps()
+    with pytest.raises(Exception):
+        f.adapt(Criterion(TARGETLEVEL, "h", 0.0))
 
 
 def test_adapted_mesh_steps_on_multilevel_path():

@@ -118,8 +118,16 @@ template <class T> __device__ __noinline__ T rain_map_at(const RainMapDev r, T x
 // interpolated discharge rounded to T, then divided by the discharge area.
 template <class T> __device__ __forceinline__ T river_rate(const RiverDev& r, const double* t, const double* q, double time)
 {
+    // the first st in [0, n-1) whose time is after `time`, else n - 1, by bisection:
+    // bgf_add_river takes strictly increasing times only, for which the reference's
+    // forward scan finds the same index
     int st = 0;
-    while (st < r.n - 1 && t[r.off + st] - time <= 0.0) st++;
+    int hi = r.n - 1;
+    while (st < hi) {
+        const int mid = (st + hi) >> 1;
+        if (t[r.off + mid] - time <= 0.0) st = mid + 1;
+        else hi = mid;
+    }
     const int pv = st > 0 ? st - 1 : 0;
     // before the first sample the reference divides by zero; the first value is used here
     const double qi = st == pv ? q[r.off + st]

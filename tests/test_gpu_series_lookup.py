@@ -1,13 +1,14 @@
-"""Uniform series late in a long record: the boundary water level and the rain
-rate are looked up by bisection when the series' times are non-decreasing and by
-the reference's forward scan otherwise; both give the oracle's values bit for bit.
+"""Uniform series late in a long record: the boundary water level, the rain rate
+and a river's discharge are looked up by bisection when the series' times are
+non-decreasing and by the reference's forward scan otherwise; both give the
+oracle's values bit for bit.
 The run starts 400 s into a 601-sample record, where the forward scan walks
 hundreds of samples per boundary cell and step."""
 import numpy as np
 import pytest
 
 import cases
-from bg_flood_b200.flow import Loop
+from bg_flood_b200.flow import BGFError, Loop
 from bg_flood_b200.params import BndSegmentSpec
 from runners import interior, make_gpu, make_oracle
 
@@ -15,6 +16,13 @@ pytestmark = pytest.mark.gpu
 
 T0 = 400.0
 NEXT = 1e9
+
+
+def _river(sorted_times: bool):
+    t = np.linspace(0.0, 600.0, 301)
+    if not sorted_times:
+        t[[100, 101]] = t[[101, 100]]
+    return (-0.02, 0.02, -0.02, 0.02, t, 0.002 + 0.001 * np.sin(t / 30.0))
 
 
 def _case(sorted_times: bool, rain: bool):
@@ -35,11 +43,20 @@ def _case(sorted_times: bool, rain: bool):
 
 
 @pytest.mark.parametrize("sorted_times", [True, False], ids=["sorted", "unsorted"])
-@pytest.mark.parametrize("rain", [False, True], ids=["bnd", "bnd+rain"])
-def test_late_series_lookup_bitexact(sorted_times, rain):
+@pytest.mark.parametrize("rain,river", [(False, False), (True, False), (False, True)],
+                         ids=["bnd", "bnd+rain", "bnd+river"])
+def test_late_series_lookup_bitexact(sorted_times, rain, river):
     case = _case(sorted_times, rain)
     f, mesh, loop0 = make_gpu(case)
     o, _ = make_oracle(case)
+    if river:
+        xs, xe, ys, ye, t, q = _river(sorted_times)
+        if not sorted_times:
+            # discharge series must have increasing times (readFlowfile's files do)
+            with pytest.raises(BGFError):
+                f.add_river(xs, xe, ys, ye, t, q)
+            return
+        assert f.add_river(xs, xe, ys, ye, t, q) == o.add_river(xs, xe, ys, ye, t, q) > 0
     loop = Loop(totaltime=T0, dt=loop0.dt, dtmax=loop0.dtmax, nextoutputtime=NEXT)
     o.set_loop(T0, NEXT, loop0.dtmax)
     for s in range(20):

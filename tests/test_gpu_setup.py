@@ -12,7 +12,7 @@ import pytest
 
 from bg_flood_b200.model_setup import setup_model
 from runners import make_oracle_inputs
-from setup_cases import CASES, RUN_CASES, write_case
+from setup_cases import CASES, RUN_CASES, asc_text, write_case
 
 pytestmark = pytest.mark.gpu
 
@@ -124,3 +124,27 @@ def test_river_scenario_in_a_pool(tmp_path):
         for a, b in zip(f.get_state()[1:], st[1:]):
             assert np.array_equal(a[:nb][I], b[:nb][I])
     pool.close()
+
+
+def test_targetlevel_maps_from_files(tmp_path):
+    """Adaptation = Targetlevel,<file>,<file>: setup_model reads each .asc map,
+    truncates its values to integers and applies the maps in order (the last
+    decides).  The first map asks for level 2 everywhere; the second asks for
+    level 1 west of x = 12 m and holds 0.9 (0 once truncated) up to x = 40 m, so
+    only the western column of level-0 blocks refines (maxlevel 1)."""
+    pf = write_case("adapt", str(tmp_path))
+    xs = np.arange(65, dtype=np.float64)
+    first = np.full((49, 65), 2.7, np.float32)
+    second = np.tile(np.where(xs < 12, 1.9, np.where(xs < 40, 0.9, 0.2)).astype(np.float32), (49, 1))
+    # node (0, 0) at (0, 0) (xllcenter / yllcorner: no half-cell shift)
+    (tmp_path / "t1.asc").write_text(asc_text(first, 1.0, 0.0, 0.0, "mixed"))
+    (tmp_path / "t2.asc").write_text(asc_text(second, 1.0, 0.0, 0.0, "mixed"))
+    text = (tmp_path / "BG_param.txt").read_text().replace("Adaptation = Threshold,0.3,h",
+                                                           "Adaptation = Targetlevel,t1.asc,t2.asc")
+    (tmp_path / "BG_param.txt").write_text(text)
+    f, inp, loop = setup_model(pf)
+    act, lev, nb, xo, yo = f.get_blocks()
+    level = lev[act]
+    assert len(act) == 21 and int((level == 1).sum()) == 12
+    assert np.all(xo[act][level == 1] < 16.0) and np.all(xo[act][level == 0] >= 16.0)
+    f.run(loop, endtime=1e30, maxsteps=5)

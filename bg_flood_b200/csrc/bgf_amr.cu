@@ -245,10 +245,17 @@ __global__ void __launch_bounds__(64) amr_apply_kernel(DevModel<T> m, AmrDev<T> 
 // without spills.
 template <class T> struct AmrOcc {
     static constexpr int update = sizeof(T) == 4 ? 4 : 3;
+    // the fast FP32 stage flux kernel runs six CTAs per SM (40 registers, no spills),
+    // 3 % faster on the multi-level mesh than five; the other builds keep their registers
+#if BGF_FAST
+    static constexpr int flux = sizeof(T) == 4 ? 6 : 3;
+#else
+    static constexpr int flux = 3;
+#endif
 };
 
 template <class T, int ENGINE>
-__global__ void __launch_bounds__(NTHREADS, 3) amr_flux_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
+__global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::flux) amr_flux_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
                                                                int stage)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -147,15 +147,16 @@ __device__ __forceinline__ void load_half_tile(Smem<T>& s, const DevModel<T>& m,
 // ---------------------------------------------------------------- kernels
 
 // Minimum resident CTAs per SM the register allocation must allow (launch
-// bounds): the fast build trades a few spilled registers for occupancy, which
-// hides the tile loads; FP64 instantiations keep more registers.
+// bounds): both FP32 builds trade a few spilled registers for six CTAs per SM
+// (the shared-memory limit), which hides the tile loads now that each phase's
+// work is spread over the warps; FP64 instantiations keep more registers.
 #if BGF_FAST
 template <class T> struct Occ {
     static constexpr int flux = sizeof(T) == 4 ? 6 : 3, update = sizeof(T) == 4 ? 6 : 3;
 };
 #else
 template <class T> struct Occ {
-    static constexpr int flux = sizeof(T) == 4 ? 4 : 3, update = sizeof(T) == 4 ? 4 : 3;
+    static constexpr int flux = sizeof(T) == 4 ? 6 : 3, update = sizeof(T) == 4 ? 6 : 3;
 };
 #endif
 

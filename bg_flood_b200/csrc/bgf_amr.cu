@@ -245,13 +245,9 @@ __global__ void __launch_bounds__(64) amr_apply_kernel(DevModel<T> m, AmrDev<T> 
 // without spills.
 template <class T> struct AmrOcc {
     static constexpr int update = sizeof(T) == 4 ? 4 : 3;
-    // the fast FP32 stage flux kernel runs six CTAs per SM (40 registers, no spills),
-    // 3 % faster on the multi-level mesh than five; the other builds keep their registers
-#if BGF_FAST
+    // the FP32 stage flux kernel runs six CTAs per SM: 3 % (fast build) and 10 %
+    // (bit-exact build) faster on the multi-level mesh than five or four
     static constexpr int flux = sizeof(T) == 4 ? 6 : 3;
-#else
-    static constexpr int flux = 3;
-#endif
 };
 
 template <class T, int ENGINE>

@@ -240,13 +240,12 @@ __global__ void __launch_bounds__(64) amr_apply_kernel(DevModel<T> m, AmrDev<T> 
     a.W[stage][1][o] = a.zb[o] + H[o];
 }
 
-// Minimum resident CTAs per SM for the register allocation of the stage kernels:
-// four CTAs of the FP32 update kernel (12 bytes of spill) run faster than three
-// without spills.
+// Resident CTAs per SM of the FP32 stage kernels (launch bounds): six, the shared-
+// memory limit.  Since the tile and face loads were spread over the warps, six beat
+// four or five in both builds (flux +3 % fast / +10 % bit-exact, update +6 % / +5 %)
+// despite a few spilled registers; FP64 instantiations keep more registers.
 template <class T> struct AmrOcc {
-    static constexpr int update = sizeof(T) == 4 ? 4 : 3;
-    // the FP32 stage flux kernel runs six CTAs per SM: 3 % (fast build) and 10 %
-    // (bit-exact build) faster on the multi-level mesh than five or four
+    static constexpr int update = sizeof(T) == 4 ? 6 : 3;
     static constexpr int flux = sizeof(T) == 4 ? 6 : 3;
 };
 

@@ -88,13 +88,20 @@ def build_oracle(force: bool = False) -> str:
     return out
 
 
-def build_reference_oracle(refsrc: str = "/root/reference/src") -> str | None:
-    """Builds oracle/_ref/libbgf_ref.so from the reference sources when they are present."""
-    if not os.path.isdir(refsrc):
+def build_reference_oracle(refsrc: str | None = None, faithful: bool = False) -> str | None:
+    """Builds the reference sources into oracle/_ref/libbgf_ref.so (test infrastructure and
+    the CPU baseline).  ``refsrc`` is the reference's src directory, else the environment
+    variable BG_FLOOD_REFERENCE_SRC; without either nothing is built.  ``faithful`` builds
+    oracle/_ref/faithful/libbgf_ref.so with the reference Makefile's host flags (no -O)."""
+    refsrc = refsrc or os.environ.get("BG_FLOOD_REFERENCE_SRC")
+    if not refsrc or not os.path.isdir(refsrc):
         return None
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle", "ref"), f"REFSRC={refsrc}", "-j8"],
-                   check=True, stdout=subprocess.DEVNULL)
-    return os.path.join(ROOT, "oracle", "_ref", "libbgf_ref.so")
+    out = os.path.join(ROOT, "oracle", "_ref", "faithful") if faithful else os.path.join(ROOT, "oracle", "_ref")
+    cmd = ["make", "-C", os.path.join(ROOT, "oracle", "ref"), f"REFSRC={refsrc}", f"OUT={out}", "-j8"]
+    if faithful:
+        cmd.append("HOSTOPT=-O0")
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+    return os.path.join(out, "libbgf_ref.so")
 
 
 if __name__ == "__main__":

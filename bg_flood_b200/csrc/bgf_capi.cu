@@ -361,9 +361,19 @@ static void* staging(bgf_handle* h, size_t bytes)
 // handle's stream (released to the device's memory pool without a device-wide
 // synchronisation); an allocation is complete before it returns, so any stream may
 // use it.
+// Debug aid: with BGF_DEBUG_FILL set in the environment, every device array of a
+// handle starts as all-ones bytes (a NaN in both precisions) instead of whatever the
+// memory pool held, so that a read of a cell no kernel wrote shows up in the results.
+static bool debug_fill()
+{
+    static const bool on = getenv("BGF_DEBUG_FILL") != nullptr;
+    return on;
+}
+
 static cudaError_t dalloc(bgf_handle* h, void** p, size_t bytes)
 {
     cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
+    if (e == cudaSuccess && debug_fill()) e = cudaMemsetAsync(*p, 0xff, bytes, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     return e;
 }
@@ -371,6 +381,23 @@ static cudaError_t dalloc(bgf_handle* h, void** p, size_t bytes)
 static void dfree(bgf_handle* h, void* p)
 {
     if (p) cudaFreeAsync(p, h->stream);
+}
+
+// Host <-> device copies and fills of a handle's arrays, issued on the handle's
+// stream and complete when they return.  Handle streams are created non-blocking,
+// so the synchronous cudaMemcpy / cudaMemset (legacy default stream) would not be
+// ordered with the handle's kernels: a bed upload could still be landing, or a
+// fill of the bed gradients could run after the kernels that compute them.
+static cudaError_t copy_on(cudaStream_t st, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+}
+
+static cudaError_t fill_on(cudaStream_t st, void* p, int value, size_t bytes)
+{
+    cudaError_t e = cudaMemsetAsync(p, value, bytes, st);
+    return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
 }
 
 // Page-locked host slots of 256 bytes for the per-step scalars of a handle (dt seed,
@@ -601,6 +628,7 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         bgf_destroy(h);
         return BGF_ENOMEM;
     }
+    if (debug_fill()) cudaMemsetAsync(h->d_slab, 0xff, total, h->stream);
     {
         char* q = (char*)h->d_slab;
         for (auto& a : allocs) {
@@ -805,21 +833,21 @@ static int set_bed_t(bgf_handle* h, const void* zb, const void* dzbdx, const voi
             h->datum[ib] = std::max(0.0, std::round(-sum / 256.0));
             dt[ib] = (T)h->datum[ib];
         }
-        BGF_CUDA(cudaMemcpy(h->d_datum, dt.data(), nb * sizeof(T), cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_datum, dt.data(), nb * sizeof(T), cudaMemcpyHostToDevice));
     }
-    BGF_CUDA(cudaMemcpy(h->d_zb, z.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
+    BGF_CUDA(copy_on(h->stream, h->d_zb, z.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
     if (dzbdx && dzbdy) {
         // the caller's bed halo and gradients are taken as they are
         std::vector<T> gx, gy;
         buq_to<T>(dzbdx, h->iodbl, nb * 324, gx);
         buq_to<T>(dzbdy, h->iodbl, nb * 324, gy);
-        BGF_CUDA(cudaMemcpy(h->d_dzbdx, gx.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
-        BGF_CUDA(cudaMemcpy(h->d_dzbdy, gy.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_dzbdx, gx.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_dzbdy, gy.data(), nb * 324 * sizeof(T), cudaMemcpyHostToDevice));
     } else {
         // bed halo and bed gradients from the interior, as the reference prepares
         // them at initialisation (src/InitialConditions.cu:140-144)
-        BGF_CUDA(cudaMemset(h->d_dzbdx, 0, nb * 324 * sizeof(T)));
-        BGF_CUDA(cudaMemset(h->d_dzbdy, 0, nb * 324 * sizeof(T)));
+        BGF_CUDA(fill_on(h->stream, h->d_dzbdx, 0, nb * 324 * sizeof(T)));
+        BGF_CUDA(fill_on(h->stream, h->d_dzbdy, 0, nb * 324 * sizeof(T)));
         DevModel<T> m = dev_model<T>(h);
         StepParams<T> p = step_params<T>(h);
         int n = h->fast ? fa::launch_bed_init<T>(m, p, (T*)h->d_zb, (T*)h->d_dzbdx, (T*)h->d_dzbdy, h->stream)
@@ -837,7 +865,7 @@ static int set_bed_t(bgf_handle* h, const void* zb, const void* dzbdx, const voi
                     size_t s = ib * 324 + (i + 1) + (j + 1) * 18;
                     c[ib * 256 + j * 16 + i] = h->iodbl ? (T)((const double*)cf)[s] : (T)((const float*)cf)[s];
                 }
-        BGF_CUDA(cudaMemcpy(h->d_cf, c.data(), nb * 256 * sizeof(T), cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_cf, c.data(), nb * 256 * sizeof(T), cudaMemcpyHostToDevice));
     }
     h->has_rainmask = activeCell != nullptr;
     if (activeCell) {
@@ -845,7 +873,7 @@ static int set_bed_t(bgf_handle* h, const void* zb, const void* dzbdx, const voi
         for (size_t ib = 0; ib < nb; ib++)
             for (int j = 0; j < 16; j++)
                 for (int i = 0; i < 16; i++) r[ib * 256 + j * 16 + i] = (uint8_t)(activeCell[ib * 324 + (i + 1) + (j + 1) * 18] != 0);
-        BGF_CUDA(cudaMemcpy(h->d_rainmask, r.data(), nb * 256, cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_rainmask, r.data(), nb * 256, cudaMemcpyHostToDevice));
     }
     h->has_bed = true;
     free_graphs(h);
@@ -906,12 +934,12 @@ static int rebuild_segments(bgf_handle* h)
         BGF_CUDA(dalloc(h, (void**)&h->d_seg_t, h->ser_cap * sizeof(double)));
         BGF_CUDA(dalloc(h, (void**)&h->d_seg_wl, h->ser_cap * sizeof(double)));
     }
-    if (!sd.empty()) BGF_CUDA(cudaMemcpy(h->d_segs, sd.data(), sd.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
+    if (!sd.empty()) BGF_CUDA(copy_on(h->stream, h->d_segs, sd.data(), sd.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
     if (!st.empty()) {
-        BGF_CUDA(cudaMemcpy(h->d_seg_t, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
-        BGF_CUDA(cudaMemcpy(h->d_seg_wl, swl.data(), swl.size() * sizeof(double), cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_seg_t, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_seg_wl, swl.data(), swl.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
-    BGF_CUDA(cudaMemcpy(h->d_bndseg, side.data(), side.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BGF_CUDA(copy_on(h->stream, h->d_bndseg, side.data(), side.size() * sizeof(int), cudaMemcpyHostToDevice));
     h->nseg_dev = (int)sd.size();
     free_graphs(h);
     return BGF_OK;
@@ -954,8 +982,8 @@ int bgf_set_rain_series(bgf_handle* h, int n, const double* t, const double* r)
     if (n > 0) {
         BGF_CUDA(dalloc(h, (void**)&h->d_rain_t, n * sizeof(double)));
         BGF_CUDA(dalloc(h, (void**)&h->d_rain_r, n * sizeof(double)));
-        BGF_CUDA(cudaMemcpy(h->d_rain_t, t, n * sizeof(double), cudaMemcpyHostToDevice));
-        BGF_CUDA(cudaMemcpy(h->d_rain_r, r, n * sizeof(double), cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_rain_t, t, n * sizeof(double), cudaMemcpyHostToDevice));
+        BGF_CUDA(copy_on(h->stream, h->d_rain_r, r, n * sizeof(double), cudaMemcpyHostToDevice));
     }
     free_graphs(h);
     return BGF_OK;
@@ -981,7 +1009,7 @@ int bgf_set_rain_map(bgf_handle* h, int nx, int ny, double xo, double yo, double
     const size_t n = (size_t)nx * ny * nt;
     float* d = nullptr;
     BGF_CUDA(dalloc(h, (void**)&d, n * sizeof(float)));
-    BGF_CUDA(cudaMemcpy(d, frames, n * sizeof(float), cudaMemcpyHostToDevice));
+    BGF_CUDA(copy_on(h->stream, d, frames, n * sizeof(float), cudaMemcpyHostToDevice));
     RainMapDev& r = h->rmap;
     r.val = d;
     r.nx = nx;
@@ -1046,9 +1074,9 @@ int bgf_add_river(bgf_handle* h, double xstart, double xend, double ystart, doub
     BGF_CUDA(dalloc(h, (void**)&h->d_rivers, h->rivers.size() * sizeof(RiverDev)));
     BGF_CUDA(dalloc(h, (void**)&h->d_riv_t, h->riv_t.size() * sizeof(double)));
     BGF_CUDA(dalloc(h, (void**)&h->d_riv_q, h->riv_q.size() * sizeof(double)));
-    BGF_CUDA(cudaMemcpy(h->d_rivers, h->rivers.data(), h->rivers.size() * sizeof(RiverDev), cudaMemcpyHostToDevice));
-    BGF_CUDA(cudaMemcpy(h->d_riv_t, h->riv_t.data(), h->riv_t.size() * sizeof(double), cudaMemcpyHostToDevice));
-    BGF_CUDA(cudaMemcpy(h->d_riv_q, h->riv_q.data(), h->riv_q.size() * sizeof(double), cudaMemcpyHostToDevice));
+    BGF_CUDA(copy_on(h->stream, h->d_rivers, h->rivers.data(), h->rivers.size() * sizeof(RiverDev), cudaMemcpyHostToDevice));
+    BGF_CUDA(copy_on(h->stream, h->d_riv_t, h->riv_t.data(), h->riv_t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    BGF_CUDA(copy_on(h->stream, h->d_riv_q, h->riv_q.data(), h->riv_q.size() * sizeof(double), cudaMemcpyHostToDevice));
     free_graphs(h);
     return BGF_OK;
 }
@@ -1246,7 +1274,7 @@ static int check_ready(bgf_handle* h)
 static int check_err_word(bgf_handle* h)
 {
     int err = 0;
-    BGF_CUDA(cudaMemcpy(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    BGF_CUDA(copy_on(h->stream, &err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) {
         g_last_error = "mesh has cross-level neighbours, which this build does not support yet";
         return BGF_EINVAL;
@@ -1601,7 +1629,7 @@ int bgf_set_bathy(bgf_handle* h, int nx, int ny, double xo, double yo, double dx
     dfree(h, h->d_dem);
     h->d_dem = nullptr;
     BGF_CUDA(dalloc(h, (void**)&h->d_dem, sizeof(float) * (size_t)nx * ny));
-    BGF_CUDA(cudaMemcpy(h->d_dem, val, sizeof(float) * (size_t)nx * ny, cudaMemcpyHostToDevice));
+    BGF_CUDA(copy_on(h->stream, h->d_dem, val, sizeof(float) * (size_t)nx * ny, cudaMemcpyHostToDevice));
     h->dem_nx = nx;
     h->dem_ny = ny;
     h->dem_xo = xo;
@@ -1620,7 +1648,7 @@ int bgf_add_target_level_map(bgf_handle* h, int nx, int ny, double xo, double yo
     for (size_t k = 0; k < n; k++) v[k] = (float)levels[k];
     adapt::TargetMapDev g{};
     BGF_CUDA(dalloc(h, (void**)&g.val, sizeof(float) * n));
-    BGF_CUDA(cudaMemcpy((void*)g.val, v.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    BGF_CUDA(copy_on(h->stream, (void*)g.val, v.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
     g.nx = nx;
     g.ny = ny;
     g.xo = xo;
@@ -1892,7 +1920,7 @@ int bgf_get_bed(bgf_handle* h, void* zb)
     int rc = set_device(h);
     if (rc) return rc;
     BGF_CUDA(cudaStreamSynchronize(h->stream));
-    BGF_CUDA(cudaMemcpy(zb, h->d_zb, (size_t)h->nblkmem * 324 * h->esz, cudaMemcpyDeviceToHost));
+    BGF_CUDA(copy_on(h->stream, zb, h->d_zb, (size_t)h->nblkmem * 324 * h->esz, cudaMemcpyDeviceToHost));
     return BGF_OK;
 }
 

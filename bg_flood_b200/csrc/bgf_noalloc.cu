@@ -13,7 +13,10 @@
 // The scratch array is sized for at most BGF_NOALLOC_MAX_BLOCKS blocks in double
 // precision; every GPU that loads the library holds it until the process exits.
 // All calls share it and it keeps the contents of the last call, so calls whose
-// GPU work overlaps (two streams, two host threads) race on it.
+// GPU work overlaps (two streams, two host threads) race on it.  The absorbing-
+// boundary running means live in it too and carry from call to call, as the
+// reference's qmean carries from step to step (src/Boundary.cu:481-537); they are
+// cleared at the first set-up on a device and when the caller asks (reset_means).
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -47,7 +50,10 @@ constexpr int kMaxDevices = 64;
 unsigned char* g_scratch_ptr[kMaxDevices] = {nullptr};
 std::mutex g_setup_mutex;
 
-int scratch_for_device(int dev, unsigned char** out)
+// The set-up copies run on the caller's stream and complete before the step is
+// queued behind them (a non-blocking caller stream is not ordered with the legacy
+// default stream of cudaMemcpy).
+int scratch_for_device(int dev, cudaStream_t st, unsigned char** out)
 {
     if (dev < 0 || dev >= kMaxDevices) return BGF_EINVAL;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -61,7 +67,15 @@ int scratch_for_device(int dev, unsigned char** out)
         // segment table: entry k is a boundary of type k without a water-level series
         SegDev segs[4];
         for (int k = 0; k < 4; k++) segs[k] = SegDev{k, 0, 0, 0};
-        e = cudaMemcpy((unsigned char*)p + kOffSegs, segs, sizeof(segs), cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync((unsigned char*)p + kOffSegs, segs, sizeof(segs), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            bgf::set_last_error(std::string("scratch set-up: ") + cudaGetErrorString(e));
+            return BGF_ECUDA;
+        }
+        // the running means start from zero, as the reference's segment sides do
+        e = cudaMemsetAsync((unsigned char*)p + kOffQmean, 0, kQmean, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
             bgf::set_last_error(std::string("scratch set-up: ") + cudaGetErrorString(e));
             return BGF_ECUDA;
@@ -154,8 +168,8 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     p.rain_map = 0;
     p.riv_first = 0;
 
-    // per-call state: time slot 0 from the caller's loop, the dt minimum, the error
-    // word and the absorbing-boundary running means start from zero
+    // per-call state: time slot 0 from the caller's loop, the dt minimum and the error
+    // word; the absorbing-boundary running means persist unless the caller resets them
     TimeState ts;
     memset(&ts, 0, sizeof(ts));
     ts.totaltime = loop->totaltime;
@@ -170,7 +184,8 @@ int step_noalloc(const bgf_param* P, const bgf_noalloc_args* a, bgf_loop* loop, 
     if ((e = cudaMemcpyAsync(m.time, &ts, sizeof(ts), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(m.dtmin, &bits, sizeof(bits), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemsetAsync(m.err, 0, sizeof(int), st)) != cudaSuccess ||
-        (e = cudaMemsetAsync(m.qmean, 0, (size_t)a->nblkmem * 64 * sizeof(float), st)) != cudaSuccess) {
+        (a->reset_means &&
+         (e = cudaMemsetAsync(m.qmean, 0, (size_t)a->nblkmem * 64 * sizeof(float), st)) != cudaSuccess)) {
         bgf::set_last_error(std::string("scratch reset: ") + cudaGetErrorString(e));
         return BGF_ECUDA;
     }
@@ -222,11 +237,19 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* a, bgf_loo
         return BGF_EINVAL;
     if (p->engine == 1 && (!a->dzbdx || !a->dzbdy)) return BGF_EINVAL;
     if (p->frictionmodel != 0 && p->frictionmodel != -1 && p->frictionmodel != 1) return BGF_EINVAL;
+    if (p->splitprecision || p->conserveElevation) {
+        bgf::set_last_error("the allocation-free step takes neither split precision nor conserveElevation");
+        return BGF_EINVAL;
+    }
+    int caller_dev = 0;
+    if (cudaGetDevice(&caller_dev) != cudaSuccess) return BGF_ECUDA;
     if (cudaSetDevice(p->GPUDEVICE) != cudaSuccess) return BGF_ECUDA;
     unsigned char* sc = nullptr;
-    int rc = scratch_for_device(p->GPUDEVICE, &sc);
-    if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    return p->doubleprecision ? step_noalloc<double>(p, a, loop, st, sc) : step_noalloc<float>(p, a, loop, st, sc);
+    int rc = scratch_for_device(p->GPUDEVICE, st, &sc);
+    if (!rc) {
+        rc = p->doubleprecision ? step_noalloc<double>(p, a, loop, st, sc) : step_noalloc<float>(p, a, loop, st, sc);
+    }
+    cudaSetDevice(caller_dev);
+    return rc;
 }
-

@@ -221,15 +221,28 @@ int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches);
  * lives in one static device array sized for BGF_NOALLOC_MAX_BLOCKS blocks in
  * double precision (about 3.3 MB), which every GPU that loads the library keeps
  * until the process exits.
- * - The first call on a device finds the array's device address and writes its
- *   constant part; make that first call before any stream capture.
- * - Every call shares the array and it keeps the last call's contents; the parts
- *   that must start at zero are cleared on each call.  Calls whose GPU work
- *   overlaps (other streams, other threads) race on it.
+ * - The first call on a device finds the array's device address, writes its
+ *   constant part and clears the boundary running means; make that first call
+ *   before any stream capture.  The set-up is cached per device for the life of
+ *   the process and does not survive a cudaDeviceReset.  The caller's current
+ *   device is restored before the call returns.
+ * - Every call shares the array and it keeps the last call's contents.  The time
+ *   slot, the dt minimum and the error word are rewritten by each call.  The
+ *   absorbing-boundary running means (the reference's per-side qmean, carried
+ *   from step to step) persist in the array between calls; set reset_means = 1
+ *   on the first step of a run to clear them.  Calls whose GPU work overlaps
+ *   (other streams, other threads) race on the array, and two runs interleaved
+ *   step by step share one set of running means.
  * - nblkmem > BGF_NOALLOC_MAX_BLOCKS is rejected with BGF_EINVAL.
- * - Single-level meshes only; no rain, uniform friction coefficient.  Boundary
- *   sides carry a type (0 wall, 1 Neumann, 2 Dirichlet at Param.zsinit,
- *   3 absorbing 1D) or -1 for a side with a neighbour.
+ * - Single-level meshes only (a cross-level neighbour gives BGF_EINVAL), FP32 or
+ *   FP64 state, uniform friction coefficient, no rain, no rivers, no split
+ *   precision (splitprecision = 1 and conserveElevation != 0 are rejected).
+ *   Boundary sides carry a type (0 wall, 1 Neumann, 2 Dirichlet at the constant
+ *   level Param.zsinit, or 0 when zsinit is NaN -- the reference's level for a
+ *   segment without a water-level series -- 3 absorbing 1D) or -1 for a side
+ *   with a neighbour; time series are not taken.
+ * - active must hold nblk distinct ids < nblkmem and nbr ids < nblkmem: the
+ *   kernels index with them unchecked.
  * State layout here is the kernels' own: 256 values per block slot, cell
  * (i, j) at j * 16 + i; the output arrays must not alias the inputs.
  * Synchronises `stream` (dt is returned to the host, as bgf_flow_step does). */
@@ -244,6 +257,8 @@ typedef struct bgf_noalloc_args {
     const void *zb, *dzbdx, *dzbdy; /* device BUQ tiles, 324 per block slot    */
     const void *h_in, *u_in, *v_in; /* device, 256 per block slot              */
     void *h_out, *u_out, *v_out;    /* device, 256 per block slot              */
+    int reset_means;      /* 1: clear the absorbing-boundary running means
+                             before this step (first step of a run)           */
 } bgf_noalloc_args;
 int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* args, bgf_loop* loop, void* stream);
 

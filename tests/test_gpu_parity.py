@@ -242,3 +242,76 @@ def test_fp32_eta_error_against_fp64_oracle(fast):
     zs, h, u, v = f.get_state()
     err = float(np.abs(interior(zs).astype(np.float64) - interior(o.get("zs"))).max())
     assert err <= 1e-3, err
+
+
+# ---------------------------------------------------------------- the benchmarked configurations
+
+RUNUP_STEPS = 40
+RUNUP_EXACT_TOL = 1e-5   # m, m/s: Manning's cbrtf rounds differently in glibc and CUDA
+RUNUP_FP64_ETA_TOL = 1e-3  # m: FP32 surface against the FP64 oracle
+
+
+@pytest.fixture(scope="module")
+def runup_oracles():
+    """The FP32 and FP64 oracles over the first RUNUP_STEPS steps of the benchmarked
+    workload (1024x1024 run-up), with their dt sequences."""
+    out = {}
+    for dbl in (False, True):
+        o, _ = make_oracle(cases.conical_island(1024, 1, dx=0.05), use_double=dbl)
+        dts = [float(o.step(1)[0]) for _ in range(RUNUP_STEPS)]
+        out[dbl] = (dts, {k: interior(o.get(k)).astype(np.float64) for k in ("zs", "h", "u", "v")})
+    return out
+
+
+@pytest.mark.parametrize("fast", [0, 1], ids=["exact", "fast"])
+def test_runup1024_bench_workload_vs_oracle(fast, runup_oracles):
+    """The workload bench.py times (1024x1024 cells, conical island, solitary wave,
+    Manning n = 0.01), both kernel builds, against the FP32 oracle step by step and
+    against the FP64 oracle at the end."""
+    case = cases.conical_island(1024, 1, dx=0.05)
+    case.param.fastmath = fast
+    f, _, loop = make_gpu(case)
+    dts, ref = runup_oracles[False]
+    dt_rtol = FAST_DT_RTOL if fast else DT_RTOL
+    for s in range(RUNUP_STEPS):
+        dt = f.flow_step(loop)
+        loop.totaltime += dt
+        assert abs(dt - dts[s]) <= dt_rtol * dts[s], (s, dt, dts[s])
+    zs, h, u, v = f.get_state()
+    tol = FAST_FIELD_TOL if fast else RUNUP_EXACT_TOL
+    for nm, a in (("h", h), ("u", u), ("v", v)):
+        assert float(np.abs(interior(a).astype(np.float64) - ref[nm]).max()) <= tol, nm
+    _, ref64 = runup_oracles[True]
+    eta_err = float(np.abs(interior(zs).astype(np.float64) - ref64["zs"]).max())
+    assert eta_err <= RUNUP_FP64_ETA_TOL, eta_err
+
+
+@pytest.mark.parametrize("fast", [0, 1], ids=["exact", "fast"])
+def test_config1_hump256_full_run_vs_oracle(fast):
+    """The plain-method configuration run in full: 256x256 cells, Gaussian hump on a
+    flat bed 1 m deep, walls, Kurganov, no friction, 10 s simulated.  The exact build
+    matches the oracle bit for bit at every step and in the fields; the fast build
+    within the fast-math tolerances.  Volume is conserved either way."""
+    case = cases.hump_walls(256, 2)
+    case.param.fastmath = fast
+    f, _, loop = make_gpu(case)
+    o, _ = make_oracle(case)
+    loop.nextoutputtime = 10.0
+    o.set_loop(0.0, 10.0, loop.dtmax)
+    v0 = f.volume()
+    steps = 0
+    while o.totaltime < 10.0:
+        dt = f.flow_step(loop)
+        loop.totaltime += dt
+        do = float(o.step(1)[0])
+        if fast:
+            assert abs(dt - do) <= FAST_DT_RTOL * do, (steps, dt, do)
+        else:
+            assert dt == do, (steps, dt, do)
+        steps += 1
+    assert o.totaltime >= 10.0 and loop.totaltime == pytest.approx(o.totaltime, rel=1e-6 if fast else 0.0)
+    zs, h, u, v = f.get_state()
+    for nm, a in (("h", h), ("u", u), ("v", v)):
+        d = float(np.abs(interior(a).astype(np.float64) - interior(o.get(nm))).max())
+        assert d <= (FAST_FIELD_TOL if fast else 0.0), (nm, d)
+    assert abs(f.volume() - v0) / v0 < 2e-6

@@ -23,7 +23,8 @@ pytestmark = pytest.mark.gpu
 class NoallocArgs(ctypes.Structure):
     _fields_ = [("nblk", ctypes.c_int), ("nblkmem", ctypes.c_int)] + \
         [(n, ctypes.c_void_p) for n in ("active", "level", "nbr", "bndtype", "zb", "dzbdx", "dzbdy",
-                                        "h_in", "u_in", "v_in", "h_out", "u_out", "v_out")]
+                                        "h_in", "u_in", "v_in", "h_out", "u_out", "v_out")] + \
+        [("reset_means", ctypes.c_int)]
 
 
 def _device_inputs(case, mesh, torch):
@@ -49,8 +50,9 @@ def _device_inputs(case, mesh, torch):
     return t, state
 
 
-def _step(case, t, state_in, state_out, loop):
+def _step(case, t, state_in, state_out, loop, reset=False):
     a = NoallocArgs()
+    a.reset_means = 1 if reset else 0
     a.nblk = a.nblkmem = t["active"].numel()
     for k in ("active", "level", "nbr", "bndtype", "zb", "dzbdx", "dzbdy"):
         setattr(a, k, t[k].data_ptr())
@@ -77,7 +79,7 @@ def test_noalloc_step_matches_handle_step(mk):
     for step in range(2):  # two calls in a row: the static scratch is reused
         dt_ref = f.flow_step(loop)
         loop.totaltime += dt_ref
-        dt_na = _step(case, t, cur, nxt, nloop)
+        dt_na = _step(case, t, cur, nxt, nloop, reset=step == 0)
         nloop.totaltime += dt_na
         assert dt_na == dt_ref, (step, dt_na, dt_ref)
         zs, h, u, v = f.get_state()
@@ -85,6 +87,49 @@ def test_noalloc_step_matches_handle_step(mk):
             ref_i = interior(ref).reshape(mesh.nblk, 256)
             assert np.array_equal(got.cpu().numpy(), ref_i), (step, name)
         cur, nxt = nxt, cur
+
+
+def test_noalloc_absorbing_means_carry_across_calls():
+    """An absorbing edge with the dt key set: the boundary's running means (the time
+    filter of ABS1DQ, src/Boundary.cu:481-537) carry from call to call in the static
+    array, so 30 calls follow bgf_flow_step and the oracle step by step, bit for bit,
+    while the wave leaves the domain."""
+    torch = pytest.importorskip("torch")
+    case = cases.gauss(48, 1, 3)
+    case.param.dt = 0.01
+    case.param.bndfiltertime = 0.05
+    f, mesh, loop = make_gpu(case)
+    o, _ = make_oracle(case)
+    t, cur = _device_inputs(case, mesh, torch)
+    init = [x.clone() for x in cur]
+    nxt = [torch.empty_like(x) for x in cur]
+    loop0 = (loop.totaltime, loop.dt, loop.dtmax, loop.nextoutputtime)
+    nloop = Loop(*loop0)
+    torch.cuda.synchronize()
+    nsteps = 30
+    for step in range(nsteps):
+        dt_ref = f.flow_step(loop)
+        loop.totaltime += dt_ref
+        dt_na = _step(case, t, cur, nxt, nloop, reset=step == 0)
+        nloop.totaltime += dt_na
+        dt_o = float(o.step(1)[0])
+        assert dt_na == dt_ref == dt_o, (step, dt_na, dt_ref, dt_o)
+        zs, h, u, v = f.get_state()
+        for name, ref, got in (("h", h, nxt[0]), ("u", u, nxt[1]), ("v", v, nxt[2])):
+            ref_i = interior(ref).reshape(mesh.nblk, 256)
+            assert np.array_equal(got.cpu().numpy(), ref_i), (step, name)
+            assert np.array_equal(got.cpu().numpy(), interior(o.get(name)).reshape(mesh.nblk, 256)), (step, name)
+        cur, nxt = nxt, cur
+    final_h = cur[0].cpu().numpy().copy()
+    # the case is sensitive to the running means: clearing them on every call
+    # (what the step did before they were kept) ends elsewhere
+    cur = [x.clone() for x in init]
+    nxt = [torch.empty_like(x) for x in cur]
+    nloop = Loop(*loop0)
+    for step in range(nsteps):
+        nloop.totaltime += _step(case, t, cur, nxt, nloop, reset=True)
+        cur, nxt = nxt, cur
+    assert not np.array_equal(cur[0].cpu().numpy(), final_h)
 
 
 def test_noalloc_rejects_too_many_blocks():

@@ -51,6 +51,7 @@ SIGNATURES = {
     "bgf_get_blocks": (ctypes.c_int, [c_void_p, c_int_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "bgf_get_bed": (ctypes.c_int, [c_void_p, c_void_p]),
     "bgf_set_grid": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "bgf_set_kernel_layout": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "bgf_pool_create": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p,
                                        ctypes.POINTER(c_void_p)]),
     "bgf_pool_destroy": (ctypes.c_int, [c_void_p]),

@@ -122,6 +122,7 @@ struct bgf_handle {
     // multi-level meshes: stage tiles with halos, pre-prolongation gradients, face
     // arrays, wet/dry prolongation decisions and the active-list rank of each block
     bool amr = false;
+    int gen = 2;  // single-level stage kernels: 1 one cell per thread, 2 two cells per thread
     int minlev = 0, maxlev = 0;
     int steps_launches = 2;  // kernel launches per step
     int grid = 0;            // CTAs of the fused kernels (0: one per block)
@@ -186,6 +187,7 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.hmax = nullptr;
     m.checklev = 0;
     m.datum = h->split ? (const T*)h->d_datum : nullptr;
+    m.gen = h->gen;
     return m;
 }
 
@@ -1928,6 +1930,14 @@ int bgf_set_grid(bgf_handle* h, int grid)
 {
     if (!h || grid < 0) return BGF_EINVAL;
     h->grid = grid;
+    free_graphs(h);
+    return BGF_OK;
+}
+
+int bgf_set_kernel_layout(bgf_handle* h, int cells_per_thread)
+{
+    if (!h || (cells_per_thread != 1 && cells_per_thread != 2)) return BGF_EINVAL;
+    h->gen = cells_per_thread;
     free_graphs(h);
     return BGF_OK;
 }

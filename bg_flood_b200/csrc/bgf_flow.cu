@@ -5,6 +5,7 @@
 // BGF_VARIANT=fast (FMA contraction, approximate division and square root,
 // flush-to-zero).  Each build puts its kernels and launchers in its own namespace.
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdio.h>
 
 #include "bgf_flow.cuh"
@@ -18,6 +19,8 @@ namespace bgf {
 namespace BGF_VARIANT {
 
 #include "bgf_stage.cuh"
+#include "bgf_pair.cuh"
+#include "bgf_flow2.cuh"
 
 // ---------------------------------------------------------------- tile assembly
 
@@ -364,7 +367,14 @@ template <class T, int ENGINE, bool SPLIT, bool POOL> cudaError_t configure_one(
     const int sm = (int)smem_bytes<T>();
     cudaError_t e = cudaFuncSetAttribute(flux_kernel<T, ENGINE, SPLIT, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(update_kernel<T, ENGINE, SPLIT, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    e = cudaFuncSetAttribute(update_kernel<T, ENGINE, SPLIT, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess || SPLIT) return e;
+    // two cells per thread (split precision keeps the one-cell kernels)
+    e = cudaFuncSetAttribute(flux2_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem2_pred<T>());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(update2_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem2_corr<T>());
 }
 
 template <class T, int ENGINE> cudaError_t configure_engine()
@@ -394,6 +404,17 @@ static void launch_step_kernel(const DevModel<T>& m, const StepParams<T>& p, int
     const bool pool = m.scen != nullptr;
     bool split = false;
     if constexpr (sizeof(T) == 4) split = m.datum != nullptr;
+    if (!split && m.gen != 1) {
+        // two cells per thread
+        if constexpr (FLUX) {
+            if (pool) flux2_kernel<T, ENGINE, true><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);
+            else flux2_kernel<T, ENGINE, false><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);
+        } else {
+            if (pool) update2_kernel<T, ENGINE, true><<<g, NT2, smem2_corr<T>(), st>>>(m, p, parity);
+            else update2_kernel<T, ENGINE, false><<<g, NT2, smem2_corr<T>(), st>>>(m, p, parity);
+        }
+        return;
+    }
     if constexpr (FLUX) {
         if constexpr (sizeof(T) == 4) {
             if (split) {

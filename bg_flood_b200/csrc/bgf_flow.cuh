@@ -124,6 +124,8 @@ template <class T> struct DevModel {
     T* hmax;                          // per cell (256 per block): running maximum depth, or null
     const T* datum;                   // per block slot: datum depth of split mode, or null
     int checklev;                     // fused kernels: verify that neighbours share the block's level
+    int gen;                          // thread layout of the single-level stage kernels: 1 one cell per
+                                      // thread, otherwise two cells per thread (read by the launchers)
 };
 
 // Positive floating-point values order like their bit patterns.

@@ -192,6 +192,10 @@ class FlowB200:
         """CTAs of the fused kernels (0: one per block; fewer: persistent launch)."""
         _check(lib().bgf_set_grid(self.handle, int(grid)), "bgf_set_grid")
 
+    def set_kernel_layout(self, cells_per_thread: int) -> None:
+        """Thread layout of the fused single-level kernels: 2 cells per thread (default) or 1."""
+        _check(lib().bgf_set_kernel_layout(self.handle, int(cells_per_thread)), "bgf_set_kernel_layout")
+
     def autotune(self, loop: Loop, steps: int = 20) -> tuple:
         """Times the step kernels for each launch shape from the state of ``loop`` and
         keeps the fastest; the state is unchanged afterwards.  Returns (grid, ms_per_step)."""

@@ -206,6 +206,12 @@ int bgf_kernel_timing(bgf_handle* h, double* flux_ms, double* update_ms, int64_t
  * active block; a smaller count makes each CTA loop over blocks (a persistent
  * launch).  Results do not depend on it. */
 int bgf_set_grid(bgf_handle* h, int grid);
+/* Thread layout of the two fused single-level kernels: 2 (default) gives each
+ * thread two vertically adjacent cells of a block (128 threads per block, paired
+ * FP32 arithmetic in the fast-math build), 1 one cell per thread (256 threads per
+ * block).  The exact build gives the same results bit for bit with either;
+ * split-precision handles always use layout 1.  No counterpart in the reference. */
+int bgf_set_kernel_layout(bgf_handle* h, int cells_per_thread);
 /* Device time (ms) and kernel launches of the last bgf_run (events around its graphs). */
 int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches);
 

@@ -40,6 +40,7 @@ UNIT = "cell-updates/s"
 WORKLOAD = "wet/dry run-up 1024x1024 cells (16x16 blocks), dx=0.05 m, conical island, solitary wave, Manning n=0.01"
 ALG_BYTES_FLUX = 28    # h,u,v,zb read + dh,dhu,dhv written (FP32)
 ALG_BYTES_UPDATE = 40  # h,u,v,dh,dhu,dhv,zb read + h,u,v written (FP32)
+REF_WINDOW = 256       # the reference's FlowCPU is timed on a window of this many cells per side
 
 
 def parse():
@@ -59,6 +60,10 @@ def parse():
     ap.add_argument("--ens-max-blocks", type=int, default=16384)
     ap.add_argument("--serve", type=int, default=48, help="requests of the serving measurement (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="run this many flow steps of the workload and exit (for ncu captures of the stage kernels)")
+    ap.add_argument("--cpu-sample", choices=["O2", "makefile"], default=None,
+                    help="internal: time the reference FlowCPU build in this process and print one JSON line")
     return ap.parse_args()
 
 
@@ -171,28 +176,98 @@ def flushed_steps(f, loop, steps, flush):
     return a, b
 
 
-def cpu_reference_sample(steps: int, warmup: int, engine: int):
-    """The reference FlowCPU on a 256x256 window of the workload (oracle/_ref), or the
-    C restatement when the reference build is absent.  Returns (cells/s, kind, steps)."""
+def _cpu_sample_here(build: str, steps: int, warmup: int, engine: int) -> dict:
+    """The reference FlowCPU (built from its sources: "O2" host optimisation, or
+    "makefile", the reference Makefile's own host flags without -O) on a
+    REF_WINDOW x REF_WINDOW window of the workload, in this process.  Records the
+    wall time, the CPU time (user + system) and the largest number of threads the
+    process ran, so the parallelism is measured, not assumed."""
+    import resource
     import cases
-    from oracle.pyoracle import ref_available
-    case = cases.conical_island(256, engine=engine, dx=0.05)
-    ncell = 256 * 256
-    if ref_available():
+    from oracle.pyoracle import REF_LIB, REF_LIB_FAITHFUL, ref_available
+    case = cases.conical_island(REF_WINDOW, engine=engine, dx=0.05)
+    ncell = REF_WINDOW * REF_WINDOW
+    faithful = build == "makefile"
+    if ref_available(faithful):
         from runners import make_reference
-        r = make_reference(case)
-        r.step(warmup)
-        t0 = time.perf_counter()
-        r.step(steps)
-        dt = time.perf_counter() - t0
-        return ncell * steps / dt, "reference", dt
-    from runners import make_oracle
-    o, _ = make_oracle(case)
-    o.step(warmup)
+        r = make_reference(case, lib_path=REF_LIB_FAITHFUL if faithful else REF_LIB)
+        kind, run = "reference", r.step
+    else:
+        from runners import make_oracle
+        r, _ = make_oracle(case)
+        kind, run = "port", r.step
+    run(warmup)
+
+    def nthreads() -> int:
+        try:
+            with open("/proc/self/status") as fh:
+                for ln in fh:
+                    if ln.startswith("Threads:"):
+                        return int(ln.split()[1])
+        except OSError:
+            pass
+        return 0
+    idle = nthreads()  # the interpreter's own (and any idle library pool) threads
+    peak = [idle]
+    stop = threading.Event()
+
+    def watch():
+        while not stop.is_set():
+            peak[0] = max(peak[0], nthreads() - 1)  # less this watcher
+            time.sleep(0.005)
+    th = threading.Thread(target=watch, daemon=True)
+    th.start()
+    ru0 = resource.getrusage(resource.RUSAGE_SELF)
     t0 = time.perf_counter()
+    run(steps)
+    wall = time.perf_counter() - t0
+    ru1 = resource.getrusage(resource.RUSAGE_SELF)
+    stop.set()
+    th.join()
+    cpu = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)
+    return {"value": ncell * steps / wall, "kind": kind, "build": build, "wall_s": wall, "steps": steps,
+            "cpu_s": cpu, "parallelism": cpu / wall, "threads_max": 1 + peak[0] - idle}
+
+
+def cpu_reference_sample(steps: int, warmup: int, engine: int, build: str = "O2") -> dict:
+    """_cpu_sample_here in a child process (the two reference builds export the same
+    symbols, so each is loaded alone)."""
+    import subprocess
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-sample", build, "--steps", str(steps), "--warmup",
+           str(warmup), "--engine", str(engine)]
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
+    return json.loads(out.strip().splitlines()[-1])
+
+
+def cpu_baseline_entry(r: dict) -> dict:
+    hc = host_cpu()
+    return {"value": r["value"], "unit": UNIT, "cores": r["threads_max"], "kind": r["kind"],
+            "sample": f"{r['steps']} FlowCPU steps on a {REF_WINDOW}x{REF_WINDOW} window of the workload "
+                      f"({r['wall_s']:.1f} s), reference host build {r['build']}",
+            "measured_parallelism": round(r["parallelism"], 2),
+            "cores_meaning": "largest number of threads the reference ran at once (its per-variable std::threads plus "
+                             "the calling thread); measured_parallelism = CPU time / wall time",
+            "host": hc, "taskset_cores": sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else None}
+
+
+def accuracy_vs_fp64(n: int, engine: int, dev: int, fastmath: int, steps: int = 20) -> dict:
+    """The headline build from the workload's start against the FP64 oracle over the
+    same number of steps: max |eta| and max |h u| differences over all cells."""
+    from runners import make_gpu, make_oracle
+    case = workload_case(n, engine, dev, fastmath)
+    f, mesh, loop = make_gpu(case)
+    for _ in range(steps):
+        loop.totaltime += f.flow_step(loop)
+    zs, h, u, v = f.get_state()
+    o, _ = make_oracle(workload_case(n, engine, dev, fastmath), use_double=True)
     o.step(steps)
-    dt = time.perf_counter() - t0
-    return ncell * steps / dt, "port", dt
+    it = (slice(None), slice(1, 17), slice(1, 17))
+    eta_err = float(np.abs(zs[it].astype(np.float64) - o.get("zs")[it]).max())
+    hu_err = float(np.abs((h[it].astype(np.float64) * u[it]) - o.get("h")[it] * o.get("u")[it]).max())
+    hv_err = float(np.abs((h[it].astype(np.float64) * v[it]) - o.get("h")[it] * o.get("v")[it]).max())
+    return {"vs": "FP64 oracle (CPU restatement of FlowCPU, pinned to the reference)", "steps": steps,
+            "simulated_s": loop.totaltime, "max_abs_eta_m": eta_err, "max_abs_hu_m2s": hu_err, "max_abs_hv_m2s": hv_err,
+            "target_eta_m": 1e-3}
 
 
 def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, steps: int, dev: int, fastmath: int):
@@ -389,17 +464,18 @@ def _serving_at_rate(nreq: int, seed: int, rate: float, dev: int, fastmath: int,
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    nthreads = min(8, os.cpu_count() or 1)
     steps = max(1, args.steps if args.steps <= 20 else 10)
-    val, kind, secs = cpu_reference_sample(steps, min(args.warmup, 3), args.engine)
+    r = cpu_reference_sample(steps, min(args.warmup, 3), args.engine, "O2")
+    cb = cpu_baseline_entry(r)
     line = {
-        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": min(args.warmup, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": "256x256 window of the workload", "engine": args.engine},
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthreads, "kind": kind,
-                         "sample": f"{steps} FlowCPU steps on a 256x256 window ({secs:.1f} s)", "host": host_cpu()},
-        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": WORKLOAD, "engine": args.engine,
+                   "sample": f"{REF_WINDOW}x{REF_WINDOW} window of the workload (the reference's FlowCPU takes about "
+                             f"a second per step on it; the full 1024x1024 grid is 16x that per step)"},
+        "cpu_baseline": cb,
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -407,6 +483,9 @@ def run_reference_arm(args, rank, world):
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.cpu_sample:
+        print(json.dumps(_cpu_sample_here(args.cpu_sample, args.steps, args.warmup, args.engine)), flush=True)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         return
@@ -425,6 +504,12 @@ def main():
         else:
             r = serving_bench(args.serve, 7, args.serve_rate, local, args.fastmath)
         print(json.dumps({"measurement": args.only, **r}))
+        return
+    if args.profile_steps:
+        f, mesh, loop = make_gpu(workload_case(args.n, args.engine, local, args.fastmath))
+        for _ in range(args.profile_steps):
+            loop.totaltime += f.flow_step(loop)
+        print(json.dumps({"profile_steps": args.profile_steps, "totaltime": loop.totaltime}))
         return
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
@@ -463,7 +548,8 @@ def main():
 
     # dominant kernel roofline
     peak, peak_kind = measured_peak_hbm()
-    kern = {"flux_kernel": (flux_ms / nprof, ALG_BYTES_FLUX), "update_kernel": (update_ms / nprof, ALG_BYTES_UPDATE)}
+    # the handle runs the two-cells-per-thread stage kernels (its default layout)
+    kern = {"flux2_kernel": (flux_ms / nprof, ALG_BYTES_FLUX), "update2_kernel": (update_ms / nprof, ALG_BYTES_UPDATE)}
     dom = max(kern, key=lambda k: kern[k][0])
     dom_ms, dom_b = kern[dom]
     achieved = dom_b * ncell / (dom_ms / 1e3) / 1e9
@@ -552,9 +638,13 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1:
-        cv, kind, secs = cpu_reference_sample(8, 1, args.engine)
-        cpu = {"value": cv, "unit": UNIT, "cores": min(8, os.cpu_count() or 1), "kind": kind,
-               "sample": f"8 FlowCPU steps on a 256x256 window of the workload ({secs:.1f} s)", "host": host_cpu()}
+        # the reference's FlowCPU on the host cores: the -O2 build is the baseline, the
+        # Makefile-flags build (no host optimisation, as the reference ships) beside it
+        cpu = cpu_baseline_entry(cpu_reference_sample(8, 1, args.engine, "O2"))
+        if not args.no_extra:
+            extra["cpu_baseline_makefile_flags"] = cpu_baseline_entry(
+                cpu_reference_sample(2, 0, args.engine, "makefile"))
+        extra["accuracy"] = accuracy_vs_fp64(args.n, args.engine, local, args.fastmath)
 
     if rank == 0:
         line = {
@@ -565,16 +655,22 @@ def main():
                        "kernels": "fast-math (tolerance parity)" if args.fastmath else "bit-exact",
                        "launch_grid": {"grid": tuned_grid, "tuned_ms_per_step": tuned_ms,
                                        "meaning": "CTAs of the fused kernels, 0 = one per block (autotuned)"},
-                       "l2": "flushed (256 MB write) before every timed step", "parallelism":
+                       "l2": "flushed (256 MB write) before every timed step",
+                       "reference_arm_sample": f"{REF_WINDOW}x{REF_WINDOW} window of the workload",
+                       "kernel_layout": "two cells per thread (bgf_set_kernel_layout 2)", "parallelism":
                        f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "alg_bytes_per_cell": dom_b},
+                         "alg_bytes_per_cell": dom_b,
+                         "step": {"alg_bytes_per_cell_update": ALG_BYTES_FLUX + ALG_BYTES_UPDATE,
+                                  "achieved": (ALG_BYTES_FLUX + ALG_BYTES_UPDATE) * value / world / 1e9,
+                                  "frac": (ALG_BYTES_FLUX + ALG_BYTES_UPDATE) * value / world / 1e9 / peak}},
+            "accuracy": extra.pop("accuracy", None),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
-            "kernels_ms_per_step": {"flux_kernel": flux_ms / nprof, "update_kernel": update_ms / nprof},
+            "kernels_ms_per_step": {"flux2_kernel": flux_ms / nprof, "update2_kernel": update_ms / nprof},
             "extra": extra,
         }
         print(json.dumps(line), flush=True)

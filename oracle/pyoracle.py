@@ -33,7 +33,6 @@ class OraParam(ctypes.Structure):
 
 
 _olib = None
-_rlib = None
 
 
 def oracle_lib():
@@ -67,49 +66,55 @@ def oracle_lib():
     return _olib
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_LIB)
+# the same sources built with the reference Makefile's own host flags (no -O)
+REF_LIB_FAITHFUL = os.path.join(HERE, "_ref", "faithful", "libbgf_ref.so")
+_rlibs = {}
 
 
-def ref_lib():
-    global _rlib
-    if _rlib is None:
-        l = ctypes.CDLL(REF_LIB)
-        l.ref_create.restype = ctypes.c_void_p
-        l.ref_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
-                                 ctypes.c_double, ctypes.c_double, D, D, D, D, D, ctypes.c_double]
-        l.ref_step.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
-        l.ref_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, D]
-        l.ref_get_blocks.argtypes = [ctypes.c_void_p, I, D, D, I]
-        l.ref_nblk.argtypes = [ctypes.c_void_p]
-        l.ref_nseg.argtypes = [ctypes.c_void_p]
-        l.ref_set_segment_series.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D, D]
-        l.ref_set_rain_series.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
-        l.ref_destroy.argtypes = [ctypes.c_void_p]
-        l.ref_adapt.argtypes = [ctypes.c_void_p]
-        l.ref_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, D]
-        l.ref_reinit.argtypes = [ctypes.c_void_p, ctypes.c_double]
-        l.ref_get_active.argtypes = [ctypes.c_void_p, I]
-        l.ref_adaptation.argtypes = [ctypes.c_void_p]
-        l.ref_flags.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ubyte), ctypes.POINTER(ctypes.c_ubyte)]
-        l.ref_set_bathy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
-                                    ctypes.c_double, D]
-        l.ref_add_target_map.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
-                                         ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
-        l.ref_nblkmem.argtypes = [ctypes.c_void_p]
-        l.ref_create_from_file.restype = ctypes.c_void_p
-        l.ref_create_from_file.argtypes = [ctypes.c_char_p, ctypes.c_int]
-        l.ref_read_asc_head.argtypes = [ctypes.c_char_p, I, I, D, D, D, D]
-        l.ref_read_asc.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
-        l.ref_param.argtypes = [ctypes.c_void_p, D]
-        l.ref_rain.argtypes = [ctypes.c_void_p, D, D]
-        l.ref_segment.argtypes = [ctypes.c_void_p, ctypes.c_int, I, D, D]
-        l.ref_get_active_cell.argtypes = [ctypes.c_void_p, I]
-        l.ref_set_rain_map.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
-                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
-                                       ctypes.c_double, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
-        _rlib = l
-    return _rlib
+def ref_available(faithful: bool = False) -> bool:
+    return os.path.exists(REF_LIB_FAITHFUL if faithful else REF_LIB)
+
+
+def ref_lib(path: str | None = None):
+    path = path or REF_LIB
+    if path in _rlibs:
+        return _rlibs[path]
+    l = ctypes.CDLL(path)
+    l.ref_create.restype = ctypes.c_void_p
+    l.ref_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                             ctypes.c_double, ctypes.c_double, D, D, D, D, D, ctypes.c_double]
+    l.ref_step.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
+    l.ref_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, D]
+    l.ref_get_blocks.argtypes = [ctypes.c_void_p, I, D, D, I]
+    l.ref_nblk.argtypes = [ctypes.c_void_p]
+    l.ref_nseg.argtypes = [ctypes.c_void_p]
+    l.ref_set_segment_series.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, D, D]
+    l.ref_set_rain_series.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
+    l.ref_destroy.argtypes = [ctypes.c_void_p]
+    l.ref_adapt.argtypes = [ctypes.c_void_p]
+    l.ref_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p, D]
+    l.ref_reinit.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    l.ref_get_active.argtypes = [ctypes.c_void_p, I]
+    l.ref_adaptation.argtypes = [ctypes.c_void_p]
+    l.ref_flags.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ubyte), ctypes.POINTER(ctypes.c_ubyte)]
+    l.ref_set_bathy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                ctypes.c_double, D]
+    l.ref_add_target_map.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
+    l.ref_nblkmem.argtypes = [ctypes.c_void_p]
+    l.ref_create_from_file.restype = ctypes.c_void_p
+    l.ref_create_from_file.argtypes = [ctypes.c_char_p, ctypes.c_int]
+    l.ref_read_asc_head.argtypes = [ctypes.c_char_p, I, I, D, D, D, D]
+    l.ref_read_asc.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    l.ref_param.argtypes = [ctypes.c_void_p, D]
+    l.ref_rain.argtypes = [ctypes.c_void_p, D, D]
+    l.ref_segment.argtypes = [ctypes.c_void_p, ctypes.c_int, I, D, D]
+    l.ref_get_active_cell.argtypes = [ctypes.c_void_p, I]
+    l.ref_set_rain_map.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+    _rlibs[path] = l
+    return l
 
 
 def _dp(a):
@@ -238,8 +243,8 @@ class Reference:
     """The reference BG_Flood flow step (FlowCPU, or FlowGPU with gpudevice >= 0)."""
 
     def __init__(self, paramtext: str, nx, ny, dx, xo, yo, zb, h, u, v, cf=None, nextoutputtime=0.0,
-                 use_double=False):
-        self.lib = ref_lib()
+                 use_double=False, lib_path: str | None = None):
+        self.lib = ref_lib(lib_path)
         cfa = None if cf is None else np.ascontiguousarray(cf, np.float64)
         arrs = [np.ascontiguousarray(a, np.float64) for a in (zb, h, u, v)]
         self.h = self.lib.ref_create(paramtext.encode(), 1 if use_double else 0, nx, ny, dx, xo, yo,

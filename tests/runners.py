@@ -38,9 +38,9 @@ def make_oracle(case: Case, use_double: bool = False, mesh=None):
     return o, mesh
 
 
-def make_reference(case: Case, use_double: bool = False) -> Reference:
+def make_reference(case: Case, use_double: bool = False, lib_path: str | None = None) -> Reference:
     r = Reference(case.paramtext, case.nx, case.ny, case.dx, case.xo, case.yo, case.zb, case.h, case.u, case.v,
-                  case.cf, case.nextoutputtime, use_double)
+                  case.cf, case.nextoutputtime, use_double, lib_path=lib_path)
     for k, seg in enumerate(case.param.segments):
         if seg.times:
             r.set_segment_series(k, seg.times, seg.levels)

@@ -52,6 +52,10 @@ SIGNATURES = {
     "bgf_get_bed": (ctypes.c_int, [c_void_p, c_void_p]),
     "bgf_set_grid": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "bgf_set_kernel_layout": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "bgf_set_gauges": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p]),
+    "bgf_read_gauges": (ctypes.c_int, [c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "bgf_pool_set_gauges": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p, c_void_p]),
+    "bgf_pool_read_gauges": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p, c_void_p]),
     "bgf_pool_create": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p,
                                        ctypes.POINTER(c_void_p)]),
     "bgf_pool_destroy": (ctypes.c_int, [c_void_p]),

@@ -35,6 +35,7 @@ SOURCES = [
     ("bgf_adapt_host.cpp", "bgf_adapt_host.o", ["-x", "cu", "--fmad=false"]),
     ("bgf_io.cpp", "bgf_io.o", ["-x", "cu", "--fmad=false"]),
     ("bgf_layout.cu", "bgf_layout.o", ["--fmad=false"]),
+    ("bgf_gauge.cu", "bgf_gauge.o", ["--fmad=false"]),
 ]
 
 

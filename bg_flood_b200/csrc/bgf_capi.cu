@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -52,6 +53,19 @@ struct StepCtl {
     int pad[3];
 };
 static_assert(sizeof(StepCtl) <= 256, "the host mirror is one 256-byte page-locked slot");
+
+// Host side of a device ring of gauge samples (GaugeRingDev): the gauges' cells and
+// scenarios, the ring, and how many samples the host has drained.
+struct GaugeRing {
+    int n = 0, cap = 0;
+    int* d_cell = nullptr;
+    int* d_scen = nullptr;
+    void* d_vals = nullptr;
+    double* d_time = nullptr;
+    unsigned long long* d_count = nullptr;
+    unsigned long long read = 0;  // samples drained so far
+    int64_t lost = 0;             // samples overwritten before they were drained
+};
 
 struct bgf_handle {
     bgf_param P;
@@ -140,6 +154,12 @@ struct bgf_handle {
     double *d_bxo = nullptr, *d_byo = nullptr;
     uint8_t* d_flags = nullptr;
     int* d_child = nullptr;
+    // gauges: the device ring, and the drained samples on the host ([sample][gauge]
+    // times and [sample][gauge][4] values h, zs, u, v; gauge_nhost gauges per sample)
+    GaugeRing gauges;
+    std::vector<double> gauge_t, gauge_v;
+    int gauge_nhost = 0;
+    int64_t gauge_lost = 0;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -400,6 +420,101 @@ static cudaError_t fill_on(cudaStream_t st, void* p, int value, size_t bytes)
 {
     cudaError_t e = cudaMemsetAsync(p, value, bytes, st);
     return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+}
+
+// ---------------------------------------------------------------- gauge rings
+
+static void gauge_free(bgf_handle* h, GaugeRing& g)
+{
+    for (void* q : {(void*)g.d_cell, (void*)g.d_scen, g.d_vals, (void*)g.d_time, (void*)g.d_count}) dfree(h, q);
+    g = GaugeRing();
+}
+
+// A ring of cap samples for the given cells (block slot * 256 + j * 16 + i) and, for
+// pools, their scenarios; allocated on h's stream, counter at zero.
+static int gauge_alloc(bgf_handle* h, GaugeRing& g, const std::vector<int>& cells, const std::vector<int>& scen,
+                       int cap)
+{
+    gauge_free(h, g);
+    const int n = (int)cells.size();
+    if (n == 0) return BGF_OK;
+    bool ok = dalloc(h, (void**)&g.d_cell, sizeof(int) * n) == cudaSuccess &&
+              dalloc(h, &g.d_vals, (size_t)cap * n * 4 * h->esz) == cudaSuccess &&
+              dalloc(h, (void**)&g.d_time, (size_t)cap * n * sizeof(double)) == cudaSuccess &&
+              dalloc(h, (void**)&g.d_count, sizeof(unsigned long long)) == cudaSuccess;
+    if (ok && !scen.empty()) ok = dalloc(h, (void**)&g.d_scen, sizeof(int) * n) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        gauge_free(h, g);
+        g_last_error = "cudaMalloc failed (gauge ring)";
+        return BGF_ENOMEM;
+    }
+    g.n = n;
+    g.cap = cap;
+    BGF_CUDA(copy_on(h->stream, g.d_cell, cells.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (!scen.empty()) BGF_CUDA(copy_on(h->stream, g.d_scen, scen.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    BGF_CUDA(fill_on(h->stream, g.d_count, 0, sizeof(unsigned long long)));
+    return BGF_OK;
+}
+
+template <class T> static GaugeRingDev<T> gauge_dev(const GaugeRing& g)
+{
+    return GaugeRingDev<T>{g.d_cell, g.d_scen, g.n, g.cap, (T*)g.d_vals, g.d_time, g.d_count};
+}
+
+// Copies the samples written since the last drain (ordered after the work queued on
+// h's stream) and hands each (sample row, gauge, time, values) to sink.  Samples
+// overwritten before this drain are counted in g.lost.
+template <class T, class Sink> static int gauge_drain_t(bgf_handle* h, GaugeRing& g, Sink sink)
+{
+    if (g.n == 0) return BGF_OK;
+    unsigned long long count = 0;
+    BGF_CUDA(copy_on(h->stream, &count, g.d_count, sizeof(count), cudaMemcpyDeviceToHost));
+    if (count <= g.read) return BGF_OK;
+    if (count - g.read > (unsigned long long)g.cap) {
+        g.lost += (int64_t)(count - g.read - g.cap);
+        g.read = count - g.cap;
+    }
+    const size_t rows = (size_t)(count - g.read);
+    std::vector<T> v(rows * g.n * 4);
+    std::vector<double> t(rows * g.n);
+    size_t done = 0;
+    while (done < rows) {
+        // contiguous run of ring rows from row (read + done) % cap
+        const size_t r0 = (size_t)((g.read + done) % g.cap);
+        const size_t nr = std::min(rows - done, (size_t)g.cap - r0);
+        BGF_CUDA(cudaMemcpyAsync(v.data() + done * g.n * 4, (const T*)g.d_vals + r0 * g.n * 4, nr * g.n * 4 * sizeof(T),
+                                 cudaMemcpyDeviceToHost, h->stream));
+        BGF_CUDA(cudaMemcpyAsync(t.data() + done * g.n, g.d_time + r0 * g.n, nr * g.n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, h->stream));
+        done += nr;
+    }
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    for (size_t r = 0; r < rows; r++)
+        for (int q = 0; q < g.n; q++) {
+            const T* x = v.data() + (r * g.n + q) * 4;
+            const double vals[4] = {(double)x[0], (double)x[1], (double)x[2], (double)x[3]};
+            sink(r, q, t[r * g.n + q], vals);
+        }
+    g.read = count;
+    return BGF_OK;
+}
+
+// Drains a handle's own ring into its host buffer.
+static int gauge_drain_handle(bgf_handle* h)
+{
+    if (h->gauges.n == 0) return BGF_OK;
+    const int n = h->gauges.n;
+    auto sink = [&](size_t, int, double t, const double* v) {
+        if (std::isnan(t)) return;  // a replayed step after the loop ended
+        h->gauge_t.push_back(t);
+        h->gauge_v.insert(h->gauge_v.end(), v, v + 4);
+    };
+    const int64_t lost0 = h->gauges.lost;
+    const int rc = h->dbl ? gauge_drain_t<double>(h, h->gauges, sink) : gauge_drain_t<float>(h, h->gauges, sink);
+    h->gauge_lost += h->gauges.lost - lost0;
+    h->gauge_nhost = n;
+    return rc;
 }
 
 // Page-locked host slots of 256 bytes for the per-step scalars of a handle (dt seed,
@@ -699,6 +814,7 @@ int bgf_destroy(bgf_handle* h)
         for (auto& g : h->tmaps) dfree(h, (void*)g.val);
     }
     h->tmaps.clear();
+    if (h->stream) gauge_free(h, h->gauges);
     h->d_slab = nullptr;
     free_amr(h);
     if (h->h_misc) pinned_slot_put(h->h_misc);
@@ -748,6 +864,8 @@ static int upload_tables(bgf_handle* h)
     int nt = 0;
     for (int ibl = 0; ibl < h->nblk; ibl++) nt = std::max(nt, h->active[ibl] + 1);
     h->ntab = nt;
+    // gauge cells name block slots of the previous mesh
+    if (h->gauges.n) gauge_free(h, h->gauges);
     BGF_CUDA(cudaMemcpyAsync(h->d_active, h->active.data(), sizeof(int) * h->nblk, cudaMemcpyHostToDevice, h->stream));
     BGF_CUDA(cudaMemcpyAsync(h->d_level, h->level.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, h->stream));
     for (int k = 0; k < 8; k++)
@@ -1349,10 +1467,19 @@ template <class T> static int enqueue_update(bgf_handle* h, int parity)
     return 1;
 }
 
+// The gauge samples of a step, after its corrector.
+template <class T> static int enqueue_gauges(bgf_handle* h, int parity)
+{
+    if (h->gauges.n == 0) return 0;
+    launch_gauges<T>(dev_model<T>(h), gauge_dev<T>(h->gauges), parity, h->stream);
+    return 1;
+}
+
 template <class T> static int enqueue_step(bgf_handle* h, int parity)
 {
     int n = enqueue_flux<T>(h, parity);
-    return n + enqueue_update<T>(h, parity);
+    n += enqueue_update<T>(h, parity);
+    return n + enqueue_gauges<T>(h, parity);
 }
 
 // The host side of write_time_slot: fills the pinned time slot and dt seed.
@@ -1474,6 +1601,7 @@ int bgf_flow_step(bgf_handle* h, bgf_loop* loop)
             n += enqueue_update<float>(h, h->parity);
         }
         BGF_CUDA(cudaEventRecord(h->pev[2], h->stream));
+        n += h->dbl ? enqueue_gauges<double>(h, h->parity) : enqueue_gauges<float>(h, h->parity);
     } else if (h->dbl) {
         n = enqueue_step<double>(h, h->parity);
     } else {
@@ -1559,6 +1687,8 @@ int bgf_run(bgf_handle* h, bgf_loop* loop, double endtime, double outputtimestep
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
         gpu_ms += ms;
         ts = h->h_time[1];
+        // at most 1024 steps per batch: the 4096-sample gauge ring cannot overflow
+        if ((rc = gauge_drain_handle(h))) return rc;
         if (ts.dt > 0) dtguess = ts.dt;
         if (ts.done || ts.totaltime >= endtime || ts.nstep >= maxsteps) break;
     }
@@ -1931,6 +2061,54 @@ int bgf_set_grid(bgf_handle* h, int grid)
     if (!h || grid < 0) return BGF_EINVAL;
     h->grid = grid;
     free_graphs(h);
+    return BGF_OK;
+}
+
+int bgf_set_gauges(bgf_handle* h, int n, const int* block, const int* i, const int* j)
+{
+    if (!h || n < 0 || (n > 0 && (!block || !i || !j))) return BGF_EINVAL;
+    if (!h->has_blocks) return BGF_ESTATE;
+    int rc = set_device(h);
+    if (rc) return rc;
+    std::vector<int> cells(n);
+    std::vector<uint8_t> isact(h->nblkmem, 0);
+    for (int ibl = 0; ibl < h->nblk; ibl++) isact[h->active[ibl]] = 1;
+    for (int k = 0; k < n; k++) {
+        if (block[k] < 0 || block[k] >= h->nblkmem || !isact[block[k]] || i[k] < 0 || i[k] >= 16 || j[k] < 0 ||
+            j[k] >= 16) {
+            g_last_error = "gauge outside the active blocks";
+            return BGF_EINVAL;
+        }
+        cells[k] = block[k] * 256 + j[k] * 16 + i[k];
+    }
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if ((rc = gauge_drain_handle(h))) return rc;
+    if ((rc = gauge_alloc(h, h->gauges, cells, {}, 4096))) return rc;
+    h->gauge_t.clear();
+    h->gauge_v.clear();
+    h->gauge_nhost = n;
+    free_graphs(h);
+    return BGF_OK;
+}
+
+int bgf_read_gauges(bgf_handle* h, int max_samples, double* times, double* values, int* nsamples, int64_t* lost)
+{
+    if (!h || max_samples < 0 || !nsamples) return BGF_EINVAL;
+    int rc = set_device(h);
+    if (rc) return rc;
+    if ((rc = gauge_drain_handle(h))) return rc;
+    const int n = h->gauge_nhost;
+    const size_t have = n > 0 ? h->gauge_t.size() / n : 0;
+    const size_t take = std::min(have, (size_t)max_samples);
+    if (take && (!times || !values)) return BGF_EINVAL;
+    if (take) {
+        std::copy(h->gauge_t.begin(), h->gauge_t.begin() + take * n, times);
+        std::copy(h->gauge_v.begin(), h->gauge_v.begin() + take * n * 4, values);
+        h->gauge_t.erase(h->gauge_t.begin(), h->gauge_t.begin() + take * n);
+        h->gauge_v.erase(h->gauge_v.begin(), h->gauge_v.begin() + take * n * 4);
+    }
+    *nsamples = (int)take;
+    if (lost) *lost = h->gauge_lost;
     return BGF_OK;
 }
 

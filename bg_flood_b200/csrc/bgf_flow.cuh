@@ -128,6 +128,17 @@ template <class T> struct DevModel {
                                       // thread, otherwise two cells per thread (read by the launchers)
 };
 
+// Device ring of gauge samples (bgf_gauge.cu): row k % cap holds, for each of the n
+// gauges, the time of sample k and h, zs, u, v at the gauge cell.
+template <class T> struct GaugeRingDev {
+    const int* cell;   // per gauge: block slot * 256 + j * 16 + i
+    const int* scen;   // per gauge: scenario index (pools), or null
+    int n, cap;
+    T* vals;           // [cap][n][4]
+    double* time;      // [cap][n]
+    unsigned long long* count;  // samples written
+};
+
 // Positive floating-point values order like their bit patterns.
 __device__ __forceinline__ unsigned long long dt_bits(float v) { return (unsigned long long)__float_as_uint(v); }
 __device__ __forceinline__ unsigned long long dt_bits(double v) { return (unsigned long long)__double_as_longlong(v); }

@@ -13,6 +13,11 @@ struct SegDev;
 template <class T> struct DevModel;
 template <class T> struct StepParams;
 template <class T> struct AmrDev;
+template <class T> struct GaugeRingDev;
+
+// Gauge sampling after a step (bgf_gauge.cu), built once: it does no arithmetic
+// beyond zs = zb + h.
+template <class T> void launch_gauges(const DevModel<T>& m, const GaugeRingDev<T>& r, int parity, cudaStream_t st);
 
 // Kernel launchers, built twice (bgf_flow.cu, bgf_amr.cu): "exact" reproduces the reference
 // CPU arithmetic bit for bit, "fast" trades the last bits for speed.

@@ -192,6 +192,26 @@ class FlowB200:
         """CTAs of the fused kernels (0: one per block; fewer: persistent launch)."""
         _check(lib().bgf_set_grid(self.handle, int(grid)), "bgf_set_grid")
 
+    def set_gauges(self, gauges) -> None:
+        """Gauge cells (block id, i, j) sampled after every step (the reference's
+        time-series output nodes)."""
+        g = np.asarray(list(gauges), np.int32).reshape(-1, 3)
+        cols = [np.ascontiguousarray(g[:, k]) for k in range(3)]
+        _check(lib().bgf_set_gauges(self.handle, len(g), *[_ptr(c) for c in cols]), "bgf_set_gauges")
+        self._ngauges = len(g)
+
+    def read_gauges(self, max_samples: int = 1 << 20):
+        """(times (s, n), values (s, n, 4) as h, zs, u, v, lost) of the samples
+        recorded since the last read."""
+        n = max(getattr(self, "_ngauges", 0), 1)
+        t = np.zeros((max_samples, n))
+        v = np.zeros((max_samples, n, 4))
+        ns = ctypes.c_int(0)
+        lost = ctypes.c_int64(0)
+        _check(lib().bgf_read_gauges(self.handle, int(max_samples), _ptr(t), _ptr(v), ctypes.byref(ns),
+                                     ctypes.byref(lost)), "bgf_read_gauges")
+        return t[:ns.value], v[:ns.value], lost.value
+
     def set_kernel_layout(self, cells_per_thread: int) -> None:
         """Thread layout of the fused single-level kernels: 2 cells per thread (default) or 1."""
         _check(lib().bgf_set_kernel_layout(self.handle, int(cells_per_thread)), "bgf_set_kernel_layout")

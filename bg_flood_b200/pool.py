@@ -85,7 +85,11 @@ class ScenarioPool:
         _check(lib().bgf_pool_retire(self.handle, int(slot), ctypes.byref(c), ctypes.byref(n)), "bgf_pool_retire")
         loop = Loop()
         loop.from_c(c)
-        return self.members.pop(slot), loop, n.value
+        f = self.members.pop(slot)
+        ng = getattr(self, "_ngauges", {}).pop(slot, 0)
+        if ng:
+            f._ngauges = ng  # its unread gauge samples came with it
+        return f, loop, n.value
 
     def depth(self, slot: int, nblk: int, with_max: bool = False):
         """Interior depth (nblk, 16, 16) of a scenario in its active order, and its
@@ -96,6 +100,27 @@ class ScenarioPool:
                                         None if hm is None else hm.ctypes.data_as(ctypes.c_void_p)),
                "bgf_pool_get_depth")
         return (h, hm) if with_max else h
+
+    def set_gauges(self, slot: int, gauges) -> None:
+        """Gauges of a scenario: (block index in its active order, i, j)."""
+        g = np.asarray(list(gauges), np.int32).reshape(-1, 3)
+        cols = [np.ascontiguousarray(g[:, k]) for k in range(3)]
+        _check(lib().bgf_pool_set_gauges(self.handle, int(slot), len(g),
+                                         *[c.ctypes.data_as(ctypes.c_void_p) for c in cols]), "bgf_pool_set_gauges")
+        self._ngauges = getattr(self, "_ngauges", {})
+        self._ngauges[slot] = len(g)
+
+    def read_gauges(self, slot: int, max_samples: int = 1 << 16):
+        """(times (s, n), values (s, n, 4) as h, zs, u, v) of a scenario's samples
+        since the last read."""
+        n = max(getattr(self, "_ngauges", {}).get(slot, 0), 1)
+        t = np.zeros((max_samples, n))
+        v = np.zeros((max_samples, n, 4))
+        ns = ctypes.c_int(0)
+        _check(lib().bgf_pool_read_gauges(self.handle, int(slot), int(max_samples),
+                                          t.ctypes.data_as(ctypes.c_void_p), v.ctypes.data_as(ctypes.c_void_p),
+                                          ctypes.byref(ns)), "bgf_pool_read_gauges")
+        return t[:ns.value], v[:ns.value]
 
     def timing(self):
         """(gpu_ms, steps) of the last run() and the free block slots."""

@@ -7,7 +7,8 @@ requests in arrival order while the pool's block slots -- sized from an HBM
 budget -- and scenario slots allow, keeps admitted scenarios resident, advances
 all of them together in chunks of pool steps, and retires each one as soon as it
 finishes, copying its final depth and maximum-depth map back to the host.  Its
-gauge readings are sampled at every chunk boundary.  Time-to-solution is measured
+gauges are recorded on the device after every step (the reference's time-series
+output) and the server collects them once per chunk.  Time-to-solution is measured
 from arrival to retirement."""
 from __future__ import annotations
 
@@ -54,7 +55,7 @@ class Result:
     totaltime: float
     h: np.ndarray | None = None
     hmax: np.ndarray | None = None
-    gauge_series: list = field(default_factory=list)  # (wall time, [h at each gauge])
+    gauge_series: list = field(default_factory=list)  # per step: (simulated time, [h at each gauge])
     status: int = 1            # as ScenarioPool.query: 1 finished, 2 dt underflow, 3 non-finite state
 
     @property
@@ -137,6 +138,8 @@ class FloodServer:
                         if slot is None:
                             break
                         ready.pop(0)
+                        if r.gauges:
+                            self.pool.set_gauges(slot, [(b, c % 16, c // 16) for b, c in r.gauges])
                         live[slot] = (r, f, now(), [])
                         lock.notify_all()
                     if errors:
@@ -156,8 +159,8 @@ class FloodServer:
                     loop, status, n = self.pool.query(slot)
                     self.host_s["query"] += time.perf_counter() - ta
                     if r.gauges:
-                        h = self.pool.depth(slot, r.nblk)
-                        series.append((now(), [float(h[b].reshape(-1)[c]) for b, c in r.gauges]))
+                        t, v = self.pool.read_gauges(slot)
+                        series.extend((float(tk), [float(x) for x in vk[:, 0]]) for tk, vk in zip(t[:, 0], v))
                     if status == 0:
                         continue
                     h = hmax = None

@@ -212,6 +212,23 @@ int bgf_set_grid(bgf_handle* h, int grid);
  * block).  The exact build gives the same results bit for bit with either;
  * split-precision handles always use layout 1.  No counterpart in the reference. */
 int bgf_set_kernel_layout(bgf_handle* h, int cells_per_thread);
+
+/* ------------------------------------------------------------ gauges */
+/* Gauges, the reference's time-series output nodes (TSnodesout; pointoutputstep /
+ * storeTSout, src/Mainloop.cu:359-500): after every step the library records, on
+ * the device, the step's time and h, zs, u, v at each gauge cell (block id, i, j,
+ * 0 <= i, j < 16, as the reference's TSnodesout block/i/j).  zs is zb + h.  The
+ * samples wait in a device ring of 4096 steps; bgf_run drains it after every
+ * batch of graphs, bgf_read_gauges drains it and hands out the samples in step
+ * order.  After more than 4096 single bgf_flow_step calls without a read the oldest
+ * samples are overwritten and counted in *lost.  Setting gauges replaces earlier
+ * ones and drops their unread samples; bgf_set_blocks (or a refinement pass) clears
+ * them, since they name block ids of the old mesh. */
+int bgf_set_gauges(bgf_handle* h, int n, const int* block, const int* i, const int* j);
+/* Up to max_samples samples: times[s * n + g], values[(s * n + g) * 4 + q] with q
+ * = h, zs, u, v; *nsamples receives the number returned, *lost (optional) the
+ * samples overwritten so far. */
+int bgf_read_gauges(bgf_handle* h, int max_samples, double* times, double* values, int* nsamples, int64_t* lost);
 /* Device time (ms) and kernel launches of the last bgf_run (events around its graphs). */
 int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches);
 
@@ -383,6 +400,14 @@ int bgf_pool_query(bgf_pool* pool, int slot, bgf_loop* loop, int* status, int64_
  * in its active order, 256 values per block. */
 int bgf_pool_get_depth(bgf_pool* pool, int slot, void* h, void* hmax);
 /* Device time (ms) and pool steps of the last bgf_pool_run; free block slots. */
+/* Gauges of a pooled scenario: block is the index in the scenario's active order
+ * (0 .. nblk-1), i, j the cell.  Every pool step records them on the device
+ * (bgf_set_gauges); bgf_pool_run drains the ring after each batch, and
+ * bgf_pool_read_gauges hands out the scenario's samples in step order (same
+ * layout as bgf_read_gauges).  Unread samples of a retired scenario go with it to
+ * its handle (bgf_read_gauges).  No counterpart in the reference. */
+int bgf_pool_set_gauges(bgf_pool* P, int slot, int n, const int* block, const int* i, const int* j);
+int bgf_pool_read_gauges(bgf_pool* P, int slot, int max_samples, double* times, double* values, int* nsamples);
 int bgf_pool_timing(bgf_pool* pool, double* gpu_ms, int64_t* steps, int* free_blocks);
 /* CTAs of the fused kernels (0: one per block; fewer CTAs loop over the blocks). */
 int bgf_pool_set_grid(bgf_pool* pool, int grid);

@@ -34,11 +34,18 @@ def test_served_results_equal_alone():
     assert len(res) == len(reqs)
     for r, q in zip(res, reqs):
         f, loop = q.build()
+        act = f.get_blocks()[0]
+        f.set_gauges([(int(act[b]), c % 16, c // 16) for b, c in q.gauges])
         n = f.run(loop, endtime=q.endtime, maxsteps=q.maxsteps)
         h = f.get_state()[1][: q.nblk, 1:17, 1:17]
         assert r.nsteps == n and r.totaltime == loop.totaltime
         assert np.array_equal(r.h, h)
         assert np.all(r.hmax >= r.h)
-        assert len(r.gauge_series) >= 1 and r.time_to_solution > 0
+        assert r.time_to_solution > 0
+        # gauges recorded on the device after every step, alone and served
+        t, v, lost = f.read_gauges()
+        assert lost == 0 and len(t) == n == len(r.gauge_series)
+        assert [s[0] for s in r.gauge_series] == t[:, 0].tolist()
+        assert np.array_equal(np.array([s[1] for s in r.gauge_series]), v[:, :, 0])
     seq = serve_sequential(reqs, realtime=False)
     assert [s.nsteps for s in seq] == [r.nsteps for r in res]

@@ -378,14 +378,19 @@ def amr_bench(n0: int, maxlevel: int, steps: int, dev: int, fastmath: int):
     t0 = time.perf_counter()
     nblk, it = f.adapt(Criterion(INRANGE, "zb", 0.0, 60.0), maxiteration=maxlevel + 1)
     adapt_s = time.perf_counter() - t0
-    act, lev, _, _, _ = f.get_blocks()
+    act, lev, nbr, _, _ = f.get_blocks()
     hist = np.bincount(lev[act], minlength=maxlevel + 1).tolist()
+    # blocks with a side facing another level run the multi-level chain, the rest the
+    # single-level kernels
+    act = act[:nblk]
+    cross = int(np.count_nonzero((lev[nbr[act]] != lev[act][:, None]).any(axis=1)))
     loop = Loop(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=1e30)
     f.init_dt(loop)
     f.run(loop, endtime=1e30, maxsteps=10)
     f.run(loop, endtime=1e30, maxsteps=steps)
     ms, launches = f.last_run_timing()
     return {"level0_cells": n0 * n0, "blocks": int(nblk), "blocks_per_level": hist, "adapt_passes": it,
+            "blocks_multilevel_chain": cross, "blocks_single_level_kernels": int(nblk) - cross,
             "adapt_s": adapt_s, "steps": steps, "ms": ms, "launches_per_step": launches / steps,
             "cell_updates_per_s": nblk * 256 * steps / (ms / 1e3)}
 

@@ -59,8 +59,8 @@ __device__ __forceinline__ bool has_finer_neighbour(const int* nbr, int nbm, con
 // wetdryrestriction (src/ConserveElevation.cu:676-726): a halo cell next to a finer
 // neighbour whose four cells are partly wet takes the depth-weighted surface of the
 // wet ones minus its own bed.  hv is the restricted depth from the halo fill.
-template <class T>
-__device__ __forceinline__ T wetdry_restrict(const Acc256<T>& h, const Acc324<T>& zb, T eps, T zbw, int nb, int s, int j,
+template <class T, class HA>
+__device__ __forceinline__ T wetdry_restrict(const HA& h, const Acc324<T>& zb, T eps, T zbw, int nb, int s, int j,
                                              T hv)
 {
     const int jj = j < BW / 2 ? 2 * j : (j - BW / 2) * 2;
@@ -85,6 +85,64 @@ __device__ __forceinline__ T wetdry_restrict(const Acc256<T>& h, const Acc324<T>
     return hv;
 }
 
+// ---------------------------------------------------------------- stage state
+
+// State of any cell as a stage reads it: state n in the predictor; in the corrector
+// the half-step state h* = Advance(state n, predictor tendencies, dt / 2), rebuilt
+// from the stored tendencies (the predictor advance is pointwise, so this is the
+// value the reference's half-step state holds at that cell).  Blocks on one level
+// among same-level neighbours run the single-level kernels, which store the same
+// tendencies, so every block reads its neighbours the same way.
+template <class T> struct StageState {
+    const DevModel<T>& m;
+    const StepParams<T>& p;
+    int cur;
+    bool half;
+    T halfdt;
+    double time;
+    __device__ __forceinline__ void get(int b, int x, int y, T& ho, T& uo, T& vo) const
+    {
+        const size_t g = (size_t)b * 256 + y * 16 + x;
+        const T hv = m.h[cur][g], uv = m.u[cur][g], vv = m.v[cur][g];
+        if (!half) {
+            ho = hv; uo = uv; vo = vv;
+            return;
+        }
+        // the predictor's river source of the cell (AddRiverForcing after updateEV)
+        const T dhs = add_rivers<T>(m, p, b, x, y, m.dh[g], time);
+        advance<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hv, uv, vv, dhs, m.dhu[g], m.dhv[g], ho, uo, vo);
+    }
+};
+template <class T> struct StageComp {
+    const StageState<T>& s;
+    int f;
+    __device__ __forceinline__ T operator()(int b, int x, int y) const
+    {
+        T a0, a1, a2;
+        s.get(b, x, y, a0, a1, a2);
+        return f == 0 ? a0 : f == 1 ? a1 : a2;
+    }
+};
+
+// rule_eval of the three state components of a rule, each cell's state formed once;
+// the arithmetic of each component is rule_eval's.
+template <class T>
+__device__ __forceinline__ void rule_eval_state(const CellRule<T>& r, const StageState<T>& S, T& ho, T& uo, T& vo)
+{
+    T c[4][3];
+    const int nc = r.kind == 0 ? 1 : r.kind == 2 ? 3 : 4;
+    for (int k = 0; k < nc; k++) S.get(r.b[k], r.x[k], r.y[k], c[k][0], c[k][1], c[k][2]);
+    T out[3];
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+        if (r.kind == 0) out[f] = c[0][f];
+        else if (r.kind == 1) out[f] = (T)0.25 * (c[0][f] + c[1][f] + c[2][f] + c[3][f]);
+        else if (r.kind == 2) out[f] = r.w1 * c[0][f] + r.w2 * c[1][f] + r.w3 * c[2][f];
+        else out[f] = bilinear01<T>(c[0][f], c[1][f], c[2][f], c[3][f], r.w1, r.w2);
+    }
+    ho = out[0]; uo = out[1]; vo = out[2];
+}
+
 // ---------------------------------------------------------------- stage kernels
 
 // Threads 0..255 copy the interior cells and threads 256..319 (two more warps) fill
@@ -103,15 +161,13 @@ __global__ void __launch_bounds__(HALO_THREADS) amr_halo_kernel(DevModel<T> m, A
     if (!step_live(ts)) return;
     const StepParams<T>& p = m.sparams ? m.sparams[sc] : p0;
     const int nbm = m.nblkmem;
-    const T* src[3] = {stage == 0 ? m.h[ts.cur] : m.dh, stage == 0 ? m.u[ts.cur] : m.dhu,
-                       stage == 0 ? m.v[ts.cur] : m.dhv};
+    const T halfdt = stage == 0 ? (T)0 : step_dt<T>(ts, m.dtmin[2 * sc + parity]) * (T)0.5;
+    const StageState<T> S{m, p, ts.cur, stage != 0, halfdt, ts.totaltime};
     T* const* W = a.W[stage];
     const size_t base = (size_t)ib * 324;
     const int x = tid & 15, y = (tid >> 4) & 15, c = hi18(x, y);
     if (tid < NTHREADS) {
-        const size_t g = (size_t)ib * 256 + tid;
-#pragma unroll
-        for (int f = 0; f < 3; f++) th[f][c] = src[f][g];
+        S.get(ib, x, y, th[0][c], th[1][c], th[2][c]);
         W[0][base + c] = th[0][c];
         W[2][base + c] = th[1][c];
         W[3][base + c] = th[2][c];
@@ -119,15 +175,14 @@ __global__ void __launch_bounds__(HALO_THREADS) amr_halo_kernel(DevModel<T> m, A
     } else {
         const int s = (tid - NTHREADS) >> 4, j = tid & 15;
         const CellRule<T> r = halo_rule<T>(m.nbr, nbm, m.level, ib, s, j);
-        T hv = rule_eval(r, Acc256<T>{src[0]});
-        const T uv = rule_eval(r, Acc256<T>{src[1]});
-        const T vv = rule_eval(r, Acc256<T>{src[2]});
+        T hv, uv, vv;
+        rule_eval_state<T>(r, S, hv, uv, vv);
         int hx, hy;
         halo_xy(s, j, hx, hy);
         const int hc = hi18(hx, hy);
         const int nbh = m.nbr[(2 * s + (j >= BW / 2 ? 1 : 0)) * nbm + ib];
         if (a.wetdryfix && m.level[nbh] > m.level[ib])
-            hv = wetdry_restrict<T>(Acc256<T>{src[0]}, Acc324<T>{a.zb}, p.eps, a.zb[base + hc], nbh, s, j, hv);
+            hv = wetdry_restrict<T>(StageComp<T>{S, 0}, Acc324<T>{a.zb}, p.eps, a.zb[base + hc], nbh, s, j, hv);
         th[0][hc] = hv;
         th[1][hc] = uv;
         th[2][hc] = vv;
@@ -302,8 +357,28 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::flux) amr_flux_kernel(Dev
         else if (sd == 2) y = -2;
         else y = BW + 1;
         const int c = ti(x, y);
+        if (r.kind == 3) {
+            // inside a coarser neighbour's 2x2 patch, which may reach into its halo:
+            // that neighbour has a finer neighbour, so it runs this chain and its
+            // stage tile is filled
 #pragma unroll
-        for (int v = 0; v < 4; v++) s.t[v][c] = rule_eval(r, Acc324<T>{W[v]});
+            for (int v = 0; v < 4; v++) s.t[v][c] = rule_eval(r, Acc324<T>{W[v]});
+        } else {
+            // interior cells of this block or of a same-level or finer neighbour,
+            // read as the stage reads any cell (the neighbour may run the single-level
+            // kernels and have no stage tile)
+            const T halfdt = stage == 0 ? (T)0 : step_dt<T>(ts, m.dtmin[2 * sc + parity]) * (T)0.5;
+            const StageState<T> S{m, p, ts.cur, stage != 0, halfdt, ts.totaltime};
+            T cv[4][4];  // per rule cell: h, zs, u, v
+            const int nc = r.kind == 0 ? 1 : 4;
+            for (int q = 0; q < nc; q++) {
+                S.get(r.b[q], r.x[q], r.y[q], cv[q][0], cv[q][2], cv[q][3]);
+                cv[q][1] = a.zb[(size_t)r.b[q] * 324 + hi18(r.x[q], r.y[q])] + cv[q][0];
+            }
+#pragma unroll
+            for (int v = 0; v < 4; v++)
+                s.t[v][c] = r.kind == 0 ? cv[0][v] : (T)0.25 * (cv[0][v] + cv[1][v] + cv[2][v] + cv[3][v]);
+        }
     }
     __syncthreads();
     const T celldt = tile_fluxes<T, ENGINE, true>(s, p, delta, tid, &sub);
@@ -421,18 +496,18 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::update) amr_update_kernel
     const T hs = a.W[stage][0][base + c18], us = a.W[stage][2][base + c18], vs = a.W[stage][3][base + c18];
     T dh, dhu, dhv;
     flux_divergence<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, y, hs, us, vs, dh, dhu, dhv);
-    dh = add_rivers<T>(m, p, ib, x, y, dh, ts.totaltime);
-    const T hold = s.h0[q18], uold = s.u0[q18], vold = s.v0[q18];
     const size_t g = (size_t)ib * 256 + tid;
-    T ho, uo, vo;
     if (stage == 0) {
-        // predictor: half step from state n into the scratch arrays (read back by the corrector's halo fill)
-        advance<T>(dt * (T)0.5, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
-        m.dh[g] = ho;
-        m.dhu[g] = uo;
-        m.dhv[g] = vo;
+        // predictor: the tendencies (before the river source), from which the
+        // corrector rebuilds the half-step state of any cell (StageState)
+        m.dh[g] = dh;
+        m.dhu[g] = dhu;
+        m.dhv[g] = dhv;
         return;
     }
+    dh = add_rivers<T>(m, p, ib, x, y, dh, ts.totaltime);
+    const T hold = s.h0[q18], uold = s.u0[q18], vold = s.v0[q18];
+    T ho, uo, vo;
     advance<T>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
     const T cfv = p.has_cf ? m.cf[g] : p.cf;
     bottom_friction<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);

@@ -147,6 +147,12 @@ struct bgf_handle {
     void* d_F[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     uint8_t* d_pflag = nullptr;
     int* d_rank = nullptr;
+    // multi-level meshes split their active blocks: the chain runs on blocks with a
+    // side facing another level, the single-level kernels on the rest ("pure")
+    int* d_active_chain = nullptr;
+    int* d_active_pure = nullptr;
+    uint8_t* d_nolead = nullptr;  // zeros: the chain's kernels do not write the time slot
+    int nchain = 0, npure = 0;
     // refinement pass: bathymetry grid, block origins, flags, children
     float* d_dem = nullptr;
     int dem_nx = 0, dem_ny = 0;
@@ -795,8 +801,13 @@ static void free_amr(bgf_handle* h)
     for (void*& p : h->d_F) { dfree(h, p); p = nullptr; }
     dfree(h, h->d_pflag);
     dfree(h, h->d_rank);
+    dfree(h, h->d_active_chain);
+    dfree(h, h->d_active_pure);
+    dfree(h, h->d_nolead);
     h->d_pflag = nullptr;
     h->d_rank = nullptr;
+    h->d_active_chain = h->d_active_pure = nullptr;
+    h->d_nolead = nullptr;
 }
 
 int bgf_destroy(bgf_handle* h)
@@ -844,12 +855,16 @@ static int alloc_amr(bgf_handle* h)
     for (void*& p : h->d_F) ok = ok && dalloc(h, &p, nb * NFX * es) == cudaSuccess;
     ok = ok && dalloc(h, (void**)&h->d_pflag, nb * 64) == cudaSuccess;
     ok = ok && dalloc(h, (void**)&h->d_rank, nb * sizeof(int)) == cudaSuccess;
+    ok = ok && dalloc(h, (void**)&h->d_active_chain, nb * sizeof(int)) == cudaSuccess;
+    ok = ok && dalloc(h, (void**)&h->d_active_pure, nb * sizeof(int)) == cudaSuccess;
+    ok = ok && dalloc(h, (void**)&h->d_nolead, nb) == cudaSuccess;
     if (!ok) {
         free_amr(h);
         g_last_error = "cudaMalloc failed (multi-level buffers)";
         return BGF_ENOMEM;
     }
     BGF_CUDA(cudaMemsetAsync(h->d_pflag, 0, nb * 64, h->stream));
+    BGF_CUDA(cudaMemsetAsync(h->d_nolead, 0, nb, h->stream));
     return BGF_OK;
 }
 
@@ -892,6 +907,22 @@ static int upload_tables(bgf_handle* h)
         std::vector<int> rank(nt, 0);
         for (int ibl = 0; ibl < h->nblk; ibl++) rank[h->active[ibl]] = ibl;
         BGF_CUDA(cudaMemcpyAsync(h->d_rank, rank.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, h->stream));
+        // chain: blocks with a side facing another level; pure: the rest, in active order
+        std::vector<int> chain, pure;
+        for (int ibl = 0; ibl < h->nblk; ibl++) {
+            const int ib = h->active[ibl];
+            bool cross = false;
+            for (int k = 0; k < 8; k++) cross = cross || h->level[h->nbr[(size_t)k * nb + ib]] != h->level[ib];
+            (cross ? chain : pure).push_back(ib);
+        }
+        h->nchain = (int)chain.size();
+        h->npure = (int)pure.size();
+        if (h->nchain)
+            BGF_CUDA(cudaMemcpyAsync(h->d_active_chain, chain.data(), sizeof(int) * h->nchain, cudaMemcpyHostToDevice,
+                                     h->stream));
+        if (h->npure)
+            BGF_CUDA(cudaMemcpyAsync(h->d_active_pure, pure.data(), sizeof(int) * h->npure, cudaMemcpyHostToDevice,
+                                     h->stream));
         BGF_CUDA(cudaStreamSynchronize(h->stream));
     }
     BGF_CUDA(cudaStreamSynchronize(h->stream));
@@ -1440,16 +1471,56 @@ int bgf_init_dt(bgf_handle* h, bgf_loop* loop)
     return h->dbl ? init_dt_t<double>(h, loop) : init_dt_t<float>(h, loop);
 }
 
+// A multi-level mesh's two block sets: the multi-level chain over the blocks with a
+// side facing another level, and the fused single-level kernels over the rest.
+// Without pools only one kernel may write the time slot: the single-level
+// corrector's first block when it has blocks, else the chain's.
+template <class T> static DevModel<T> chain_model(const bgf_handle* h, DevModel<T> m, bool pool)
+{
+    m.active = h->d_active_chain;
+    m.nblk = h->nchain;
+    if (!pool && h->npure) m.lead = h->d_nolead;
+    return m;
+}
+template <class T> static DevModel<T> pure_model(const bgf_handle* h, DevModel<T> m)
+{
+    m.active = h->d_active_pure;
+    m.nblk = h->npure;
+    return m;
+}
+
+// One stage of a multi-level step over model m (a handle's or a pool's): predictor
+// (stage 0) = single-level flux kernel on the pure blocks and the chain's predictor;
+// corrector = the chain's corrector and the single-level update kernel.
+template <class T>
+static int enqueue_amr_stage(bgf_handle* h, const DevModel<T>& m, const StepParams<T>& p, int parity, int stage,
+                             bool pool)
+{
+    int n = 0;
+    const DevModel<T> mc = chain_model<T>(h, m, pool), mp = pure_model<T>(h, m);
+    if (stage == 0 && h->npure) {
+        if (h->fast) fa::launch_flux<T>(mp, p, h->P.engine, parity, h->stream, 0);
+        else ex::launch_flux<T>(mp, p, h->P.engine, parity, h->stream, 0);
+        n++;
+    }
+    n += h->fast ? fa::launch_amr_stage<T>(mc, amr_dev<T>(h), p, h->P.engine, parity, stage, h->minlev, h->maxlev,
+                                          h->stream)
+                 : ex::launch_amr_stage<T>(mc, amr_dev<T>(h), p, h->P.engine, parity, stage, h->minlev, h->maxlev,
+                                          h->stream);
+    if (stage == 1 && h->npure) {
+        if (h->fast) fa::launch_update<T>(mp, p, h->P.engine, parity, h->stream, 0);
+        else ex::launch_update<T>(mp, p, h->P.engine, parity, h->stream, 0);
+        n++;
+    }
+    return n;
+}
+
 // First and second half of a step: the fused predictor / corrector kernels, or
-// the predictor / corrector stages of the multi-level chain.  Return the number
-// of kernels launched.
+// the predictor / corrector stages of a multi-level mesh.  Return the number of
+// kernels launched.
 template <class T> static int enqueue_flux(bgf_handle* h, int parity)
 {
-    if (h->amr)
-        return h->fast ? fa::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
-                                                 0, h->minlev, h->maxlev, h->stream)
-                       : ex::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
-                                                 0, h->minlev, h->maxlev, h->stream);
+    if (h->amr) return enqueue_amr_stage<T>(h, dev_model<T>(h), step_params<T>(h), parity, 0, false);
     if (h->fast) fa::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream, h->grid);
     else ex::launch_flux<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream, h->grid);
     return 1;
@@ -1457,11 +1528,7 @@ template <class T> static int enqueue_flux(bgf_handle* h, int parity)
 
 template <class T> static int enqueue_update(bgf_handle* h, int parity)
 {
-    if (h->amr)
-        return h->fast ? fa::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
-                                                 1, h->minlev, h->maxlev, h->stream)
-                       : ex::launch_amr_stage<T>(dev_model<T>(h), amr_dev<T>(h), step_params<T>(h), h->P.engine, parity,
-                                                 1, h->minlev, h->maxlev, h->stream);
+    if (h->amr) return enqueue_amr_stage<T>(h, dev_model<T>(h), step_params<T>(h), parity, 1, false);
     if (h->fast) fa::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream, h->grid);
     else ex::launch_update<T>(dev_model<T>(h), step_params<T>(h), h->P.engine, parity, h->stream, h->grid);
     return 1;

@@ -75,8 +75,8 @@ class FloodServer:
         self.gpu_ms = 0.0
         self.host_s = {"admit": 0.0, "run": 0.0, "query": 0.0, "retire": 0.0, "fields": 0.0}
 
-    def serve(self, requests: list[Request], realtime: bool = True, prefetch: int = 8,
-              builders: int = 2) -> list[Result]:
+    def serve(self, requests: list[Request], realtime: bool = True, prefetch: int = 16,
+              builders: int = 4) -> list[Result]:
         """Runs the stream to completion.  With realtime, a request becomes visible at
         its arrival time on the wall clock; otherwise all are queued at t = 0.
         Arrived requests are prepared (host set-up and upload into their own handle)

@@ -403,8 +403,8 @@ int bgf_pool_get_depth(bgf_pool* pool, int slot, void* h, void* hmax);
 /* Gauges of a pooled scenario: block is the index in the scenario's active order
  * (0 .. nblk-1), i, j the cell.  Every pool step records them on the device
  * (bgf_set_gauges); bgf_pool_run drains the ring after each batch, and
- * bgf_pool_read_gauges hands out the scenario's samples in step order (same
- * layout as bgf_read_gauges).  Unread samples of a retired scenario go with it to
+ * bgf_pool_read_gauges hands out the scenario's samples collected so far, in step
+ * order, without touching the device (same layout as bgf_read_gauges).  Unread samples of a retired scenario go with it to
  * its handle (bgf_read_gauges).  No counterpart in the reference. */
 int bgf_pool_set_gauges(bgf_pool* P, int slot, int n, const int* block, const int* i, const int* j);
 int bgf_pool_read_gauges(bgf_pool* P, int slot, int max_samples, double* times, double* values, int* nsamples);

@@ -88,6 +88,11 @@ SIGNATURES = {
                                          ctypes.c_int, c_void_p, c_void_p]),
     "bgf_refine_tables": (ctypes.c_int, [c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, ctypes.c_int,
                                          ctypes.c_double, ctypes.c_int, c_void_p, c_int_p]),
+    "bgf_adapt_sanity": (ctypes.c_int, [ctypes.c_int, c_int_p, c_int_p, c_int_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, c_double_p, c_double_p, ctypes.c_double, ctypes.c_int,
+                                        c_void_p, c_void_p]),
+    "bgf_adapt_tables": (ctypes.c_int, [c_int_p, c_int_p, c_int_p, c_int_p, c_double_p, c_double_p, ctypes.c_int,
+                                        ctypes.c_double, ctypes.c_int, c_void_p, c_void_p, c_int_p, c_int_p]),
 }
 
 

@@ -2,6 +2,7 @@
 // 435-532, with AdaptCriteria, src/AdaptCriteria.cu:20-238):
 //
 //   adapt_criteria_kernel   Threshold / Inrange criterion per block (any cell)
+//   adapt_hgrad_kernel      depth-or-slope criterion with coarsening (extension)
 //   adapt_halo_kernel       halos of the old mesh as the reference's adaptation
 //                           fills them: h and zs like the flow step, u and v with
 //                           the flux-type rules (fillHaloF)
@@ -11,6 +12,7 @@
 //   adapt_children_kernel   bilinear interpolation of h, zs, u, v from the parent
 //                           tile (with halo and corners) into its four children;
 //                           per-cell friction and rain mask by covering cell
+//   adapt_coarsen_kernel    quads merged into their parent (mean of four cells)
 //   adapt_bed_kernel        bed re-interpolated from the bathymetry grid for every
 //                           block (interp2BUQ), domain-edge cells copied from the
 //                           next row (setedges), then the wet/dry fix-up of h, zs
@@ -39,6 +41,46 @@ __global__ void __launch_bounds__(256) adapt_criteria_kernel(DevModel<T> m, cons
     const bool hit = kind == 1 ? v > a1 : (v >= a1 && v <= a2);
     const int any = __syncthreads_or(hit ? 1 : 0);
     if (tid == 0) flags[ib] = any ? 1 : 0;
+}
+
+// Depth-or-slope criterion (extension): refine when some cell has h > hthr or a
+// wet-surface slope above gthr, coarsening candidate when every cell has h <=
+// hthr/2 and slope <= gthr/2.  The slope comes from wet cells of the block only:
+// central difference over two wet neighbours, one-sided towards a single wet one,
+// 0 with none; squares are compared, in T, without contraction.
+template <class T>
+__global__ void __launch_bounds__(256) adapt_hgrad_kernel(DevModel<T> m, const T* zs, int cur, T eps, T hthr, T gthr,
+                                                          double dx0, uint8_t* refine, uint8_t* coarsen)
+{
+    __shared__ T sh[256], sz[256];
+    const int ib = m.active[blockIdx.x];
+    const int tid = threadIdx.x, x = tid & 15, y = tid >> 4;
+    const size_t g = (size_t)ib * 256 + tid;
+    const T hv = m.h[cur][g];
+    sh[tid] = hv;
+    sz[tid] = zs[g];
+    __syncthreads();
+    const T dxl = (T)calcres<double>(dx0, m.level[ib]);
+    auto wet = [&](int k) { return sh[k] > eps; };
+    auto slope = [&](int km, bool okm, int kp, bool okp) -> T {
+        if (okm && okp) return (sz[kp] - sz[km]) / ((T)2 * dxl);
+        if (okp) return (sz[kp] - sz[tid]) / dxl;
+        if (okm) return (sz[tid] - sz[km]) / dxl;
+        return (T)0;
+    };
+    T g2 = (T)0;
+    if (wet(tid)) {
+        const T gx = slope(tid - 1, x > 0 && wet(tid - 1), tid + 1, x < 15 && wet(tid + 1));
+        const T gy = slope(tid - 16, y > 0 && wet(tid - 16), tid + 16, y < 15 && wet(tid + 16));
+        g2 = gx * gx + gy * gy;  // this file is compiled without contraction
+    }
+    const T hh = hthr * (T)0.5, gh = gthr * (T)0.5;
+    const int up = __syncthreads_or(hv > hthr || g2 > gthr * gthr ? 1 : 0);
+    const int keep = __syncthreads_or(hv > hh || g2 > gh * gh ? 1 : 0);
+    if (tid == 0) {
+        refine[ib] = up ? 1 : 0;
+        coarsen[ib] = keep ? 0 : 1;
+    }
 }
 
 // targetlevelcriteria (src/AdaptCriteria.cu:179-232): at every cell of a block the
@@ -285,6 +327,56 @@ __global__ void __launch_bounds__(256) adapt_children_kernel(DevModel<T> m, Adap
     }
 }
 
+// ---------------------------------------------------------------- coarsening
+
+// coarsen, step 1 (src/Adaptation.cu:690-770): the parent (the quad's lower-left
+// block, which keeps its id) takes at cell (ix, iy) the mean of the four cells of
+// the quadrant's block it covers, T(0.25) * (((c00 + c10) + c01) + c11), for h, zs,
+// u and v, read from the old mesh's tiles; per-cell friction is averaged the same
+// way and the rain mask is set when any covered cell has it (the bed pass
+// recomputes it from the new bed).  quads[4k..4k+3] = parent, right, top, top-right.
+template <class T>
+__global__ void __launch_bounds__(256) adapt_coarsen_kernel(DevModel<T> m, AdaptDev<T> a, const int* quads, int cur,
+                                                            T* cf, uint8_t* rainmask)
+{
+    __shared__ T cfq[4][256];
+    __shared__ uint8_t rmq[4][256];
+    const int* q = quads + 4 * (size_t)blockIdx.x;
+    const int ib = q[0];
+    const int tid = threadIdx.x, ix = tid & 15, iy = tid >> 4;
+    if (cf || rainmask) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (cf) cfq[k][tid] = cf[(size_t)q[k] * 256 + tid];
+            if (rainmask) rmq[k][tid] = rainmask[(size_t)q[k] * 256 + tid];
+        }
+    }
+    __syncthreads();
+    const int kq = (ix >= 8 ? 1 : 0) + (iy >= 8 ? 2 : 0);
+    const int src = q[kq];
+    const int cx = 2 * (ix & 7), cy = 2 * (iy & 7);
+    const size_t sb = (size_t)src * 324;
+    const int ii = hi18(cx, cy), ir = hi18(cx + 1, cy), it = hi18(cx, cy + 1), itr = hi18(cx + 1, cy + 1);
+    T* dst[4] = {m.h[cur], a.zs, m.u[cur], m.v[cur]};
+    const size_t o = (size_t)ib * 256 + tid;
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        const T* W = a.W[f] + sb;
+        dst[f][o] = (T)0.25 * (((W[ii] + W[ir]) + W[it]) + W[itr]);
+    }
+    const int c00 = cy * 16 + cx;
+    if (cf) {
+        const T* c = cfq[kq];
+        cf[o] = (T)0.25 * (((c[c00] + c[c00 + 1]) + c[c00 + 16]) + c[c00 + 17]);
+    }
+    if (rainmask) {
+        const uint8_t* r = rmq[kq];
+        rainmask[o] = (r[c00] | r[c00 + 1] | r[c00 + 16] | r[c00 + 17]) ? 1 : 0;
+    }
+    // boundary running means of the merged block start at zero
+    if (tid < 64) m.qmean[(size_t)ib * 64 + tid] = 0.f;
+}
+
 // ---------------------------------------------------------------- bed
 
 // interp2BUQ (src/GridManip.cu:456-575): bilinear between grid nodes when the
@@ -391,13 +483,29 @@ template <class T> void launch_zs(const DevModel<T>& m, T* zs, int cur, cudaStre
     adapt_zs_kernel<T><<<m.nblk, 256, 0, st>>>(m, zs, cur);
 }
 
-template <class T> void launch_children(const DevModel<T>& m, const AdaptDev<T>& a, int cur, T* cf, uint8_t* rainmask,
-                                        cudaStream_t st)
+template <class T>
+void launch_hgrad(const DevModel<T>& m, const T* zs, int cur, double eps, double hthr, double gthr, double dx0,
+                  uint8_t* refine, uint8_t* coarsen, cudaStream_t st)
+{
+    adapt_hgrad_kernel<T><<<m.nblk, 256, 0, st>>>(m, zs, cur, (T)eps, (T)hthr, (T)gthr, dx0, refine, coarsen);
+}
+
+template <class T> int launch_children(const DevModel<T>& m, const AdaptDev<T>& a, int cur, T* cf, uint8_t* rainmask,
+                                       const int* quads, int nquads, bool refine, cudaStream_t st)
 {
     adapt_halo_kernel<T><<<m.nblk, 256, 0, st>>>(m, a, cur);
     adapt_halo_late_kernel<T><<<m.nblk, 32, 0, st>>>(m, a);
     adapt_corner_kernel<T><<<m.nblk, 4, 0, st>>>(m, a);
-    adapt_children_kernel<T><<<m.nblk, 256, 0, st>>>(m, a, cur, cf, rainmask);
+    int n = 3;
+    if (refine) {
+        adapt_children_kernel<T><<<m.nblk, 256, 0, st>>>(m, a, cur, cf, rainmask);
+        n++;
+    }
+    if (nquads > 0) {
+        adapt_coarsen_kernel<T><<<nquads, 256, 0, st>>>(m, a, quads, cur, cf, rainmask);
+        n++;
+    }
+    return n;
 }
 
 template <class T> void launch_bed(const DevModel<T>& m, const AdaptDev<T>& a, const StepParams<T>& p, int cur, T* zb,
@@ -412,7 +520,10 @@ template <class T> void launch_bed(const DevModel<T>& m, const AdaptDev<T>& a, c
     template void launch_zs<T>(const DevModel<T>&, T*, int, cudaStream_t);                                         \
     template void launch_target_level<T>(const DevModel<T>&, const TargetMapDev&, double, double, double, uint8_t*, \
                                          uint8_t*, cudaStream_t);                                                  \
-    template void launch_children<T>(const DevModel<T>&, const AdaptDev<T>&, int, T*, uint8_t*, cudaStream_t);      \
+    template int launch_children<T>(const DevModel<T>&, const AdaptDev<T>&, int, T*, uint8_t*, const int*, int, bool, \
+                                    cudaStream_t);                                                                 \
+    template void launch_hgrad<T>(const DevModel<T>&, const T*, int, double, double, double, double, uint8_t*,      \
+                                  uint8_t*, cudaStream_t);                                                         \
     template void launch_bed<T>(const DevModel<T>&, const AdaptDev<T>&, const StepParams<T>&, int, T*, double,      \
                                 double, const double*, const double*, double, uint8_t*, cudaStream_t);
 BGF_ADAPT_INST(float)

@@ -39,23 +39,46 @@ inline int block_index(double o, double dxl) { return (int)floor((o / dxl - 0.5)
 
 }  // namespace
 
-// refinesanitycheck (src/Adaptation.cu:157-296): no refinement at maxlevel; no
-// coarsening at all (the reference cancels every coarsen flag); a refining block
-// forces its coarser first neighbours (top, bottom, left, right) to refine, until
-// nothing changes, so that the refined mesh keeps neighbours within one level.
-extern "C" int bgf_refine_sanity(int nblk, const int* active, const int* level, const int* nbr8, int nblkmem,
-                                 int minlevel, int maxlevel, uint8_t* refine, uint8_t* coarsen)
+// refinesanitycheck (src/Adaptation.cu:157-296), checkneighbourrefine (:298-312).
+// The reference cancels every coarsening flag (:173-175); with allow_coarsen the
+// flags are kept and its coarsening rules apply, in its order.
+extern "C" int bgf_adapt_sanity(int nblk, const int* active, const int* level, const int* nbr8, int nblkmem,
+                                int minlevel, int maxlevel, const double* xo, const double* yo, double dx,
+                                int allow_coarsen, uint8_t* refine, uint8_t* coarsen)
 {
     if (nblk <= 0 || nblkmem < nblk || !active || !level || !nbr8 || !refine || !coarsen) return BGF_EINVAL;
+    if (allow_coarsen && (!xo || !yo || !(dx > 0.0))) return BGF_EINVAL;
     for (int ibl = 0; ibl < nblk; ibl++) {
         const int ib = active[ibl];
         if (ib < 0 || ib >= nblkmem) return BGF_EINVAL;
+        for (int k = 0; k < 8; k++)
+            if (nbr8[8 * ib + k] < 0 || nbr8[8 * ib + k] >= nblkmem) return BGF_EINVAL;
         if (refine[ib] && level[ib] == maxlevel) refine[ib] = 0;
         if (coarsen[ib] && level[ib] == minlevel) coarsen[ib] = 0;
-        coarsen[ib] = 0;
+        if (!allow_coarsen || refine[ib]) coarsen[ib] = 0;
     }
-    // first neighbours in the reference's order: top-left, bottom-left, left-bottom, right-bottom
-    static const int side_first[4] = {6, 4, 0, 2};
+    auto N = [&](int ib, int k) { return nbr8[8 * ib + k]; };
+    enum { LB = 0, LT = 1, RB = 2, RT = 3, BL = 4, BR = 5, TL = 6, TR = 7 };
+    if (allow_coarsen) {
+        // no coarsening next to a refining block
+        for (int ibl = 0; ibl < nblk; ibl++) {
+            const int ib = active[ibl];
+            if (refine[ib])
+                for (int k = 0; k < 8; k++) coarsen[N(ib, k)] = 0;
+        }
+        // no coarsening next to a finer block (first neighbour of each side)
+        for (int ibl = 0; ibl < nblk; ibl++) {
+            const int ib = active[ibl];
+            const int l = level[ib];
+            if (coarsen[ib] && (l < level[N(ib, LB)] || l < level[N(ib, RB)] || l < level[N(ib, TL)] ||
+                                l < level[N(ib, BL)]))
+                coarsen[ib] = 0;
+        }
+    }
+    // a refining block forces its coarser first neighbours (top-left, bottom-left,
+    // left-bottom, right-bottom) to refine and keeps same-level ones from coarsening,
+    // until nothing changes
+    static const int side_first[4] = {TL, BL, LB, RB};
     bool changed = true;
     while (changed) {
         changed = false;
@@ -63,30 +86,60 @@ extern "C" int bgf_refine_sanity(int nblk, const int* active, const int* level, 
             const int ib = active[ibl];
             if (!refine[ib]) continue;
             for (int k : side_first) {
-                const int nb = nbr8[8 * ib + k];
+                const int nb = N(ib, k);
                 if (!refine[nb] && level[nb] < level[ib]) {
                     refine[nb] = 1;
                     coarsen[nb] = 0;
                     changed = true;
                 }
+                if (level[nb] == level[ib]) coarsen[nb] = 0;
             }
         }
+    }
+    if (!allow_coarsen) return BGF_OK;
+    // a block keeps its flag only as the lower-left block of a quad whose right, top
+    // and top-right blocks are on its level and flagged; active order, in place
+    for (int ibl = 0; ibl < nblk; ibl++) {
+        const int ib = active[ibl];
+        if (!coarsen[ib]) continue;
+        const double dxl = calcres_d(dx, level[ib]);
+        const int ix = (int)(xo[ib] / dxl / 16.0), iy = (int)(yo[ib] / dxl / 16.0);
+        const int r = N(ib, RB), t = N(ib, TL), tr = N(N(ib, TR), RB);
+        const int l = level[ib];
+        const bool corner = ix % 2 == 0 && iy % 2 == 0 && r != ib && t != ib && tr != N(ib, TR);
+        if (!(corner && level[r] == l && level[t] == l && level[tr] == l && coarsen[r] && coarsen[t] && coarsen[tr]))
+            coarsen[ib] = 0;
     }
     return BGF_OK;
 }
 
-// Refinement of the flagged blocks on host tables (CalcAvailblk, refine and
-// Adaptationcleanup, src/Adaptation.cu:535-596, 1017-1876).  Arrays are indexed by
-// block id and sized nblkmem; nbr8 is [nblkmem][8] (LB, LT, RB, RT, BL, BR, TL, TR).
-// A refined block keeps its id as the bottom-left child; the k-th refined block of
-// the active list takes the free ids 3k, 3k+1, 3k+2 (ascending) of the inactive
-// ones for its bottom-right, top-left and top-right children, which are appended
-// to the active list in that order.  children[3*ib + 0..2] receives those ids (or
-// -1).  Returns BGF_ENOMEM when nblkmem has too few free block slots.
-extern "C" int bgf_refine_tables(int* nblk_io, int* active, int* level, int* nbr8, double* xo, double* yo,
-                                 int nblkmem, double dx, int doubleprecision, const uint8_t* refine, int* children)
+extern "C" int bgf_refine_sanity(int nblk, const int* active, const int* level, const int* nbr8, int nblkmem,
+                                 int minlevel, int maxlevel, uint8_t* refine, uint8_t* coarsen)
+{
+    return bgf_adapt_sanity(nblk, active, level, nbr8, nblkmem, minlevel, maxlevel, nullptr, nullptr, 0.0, 0, refine,
+                            coarsen);
+}
+
+// Coarsening and refinement of the flagged blocks on host tables (CalcAvailblk,
+// coarsen, refine and Adaptationcleanup, src/Adaptation.cu:535-596, 677-1015,
+// 1017-1876).  Arrays are indexed by block id and sized nblkmem; nbr8 is
+// [nblkmem][8] (LB, LT, RB, RT, BL, BR, TL, TR).
+//   coarsen: a flagged quad parent keeps its id at level - 1; its right, top and
+//   top-right blocks (siblings[3*ib + 0..2]) leave the active list and join the
+//   free ids only after this pass, as the reference appends them behind the free
+//   list that the refinement draws from.
+//   refine: a refined block keeps its id as the bottom-left child; the k-th refined
+//   block of the active list takes the free ids 3k, 3k+1, 3k+2 (ascending) of the
+//   ids inactive before the pass for its bottom-right, top-left and top-right
+//   children, which are appended to the active list in that order.
+//   children[3*ib + 0..2] receives those ids (or -1).
+// Returns BGF_ENOMEM when nblkmem has too few free block slots.
+extern "C" int bgf_adapt_tables(int* nblk_io, int* active, int* level, int* nbr8, double* xo, double* yo,
+                                int nblkmem, double dx, int doubleprecision, const uint8_t* refine,
+                                const uint8_t* coarsen, int* children, int* siblings)
 {
     if (!nblk_io || !active || !level || !nbr8 || !xo || !yo || !refine || !children) return BGF_EINVAL;
+    if (coarsen && !siblings) return BGF_EINVAL;
     const int nblk = *nblk_io;
     if (nblk <= 0 || nblk > nblkmem) return BGF_EINVAL;
     std::vector<char> isactive(nblkmem, 0);
@@ -102,18 +155,56 @@ extern "C" int bgf_refine_tables(int* nblk_io, int* active, int* level, int* nbr
         if (!isactive[ib]) avail.push_back(ib);
     if ((int)avail.size() < 3 * nref) return BGF_ENOMEM;
     for (int ib = 0; ib < nblkmem; ib++) children[3 * ib] = children[3 * ib + 1] = children[3 * ib + 2] = -1;
+    if (siblings)
+        for (int ib = 0; ib < nblkmem; ib++) siblings[3 * ib] = siblings[3 * ib + 1] = siblings[3 * ib + 2] = -1;
 
     auto round_t = [&](double v) { return doubleprecision ? v : (double)(float)v; };
-    // integer positions before refinement
+    // integer positions before the pass
     std::vector<int> bx(nblkmem, 0), by(nblkmem, 0);
+    std::unordered_map<uint64_t, int> old;
+    old.reserve((size_t)nblk * 2);
     for (int ibl = 0; ibl < nblk; ibl++) {
         const int ib = active[ibl];
         const double dxl = calcres_d(dx, level[ib]);
         bx[ib] = block_index(xo[ib], dxl);
         by[ib] = block_index(yo[ib], dxl);
+        old[key(level[ib], bx[ib], by[ib])] = ib;
     }
-    int n = nblk, k = 0;
-    for (int ibl = 0; ibl < nblk; ibl++) {
+    // coarsening: quads merge into their lower-left block
+    std::vector<char> gone(nblkmem, 0);
+    if (coarsen) {
+        for (int ibl = 0; ibl < nblk; ibl++) {
+            const int ib = active[ibl];
+            if (!coarsen[ib]) continue;
+            const int l = level[ib], x = bx[ib], y = by[ib];
+            if (refine[ib] || gone[ib] || (x & 1) || (y & 1)) return BGF_EINVAL;
+            int sib[3];
+            for (int q = 1; q < 4; q++) {
+                auto it = old.find(key(l, x + (q & 1), y + (q >> 1)));
+                if (it == old.end()) return BGF_EINVAL;
+                const int s = it->second;
+                if (refine[s] || coarsen[s] || gone[s]) return BGF_EINVAL;
+                sib[q - 1] = s;
+            }
+            for (int q = 0; q < 3; q++) {
+                siblings[3 * ib + q] = sib[q];
+                gone[sib[q]] = 1;
+            }
+            // the reference adds T(calcres(dx, level + 1)) to the T origin
+            const double c = round_t(calcres_d(dx, l + 1));
+            xo[ib] = round_t(xo[ib] + c);
+            yo[ib] = round_t(yo[ib] + c);
+            level[ib] = l - 1;
+            bx[ib] = x >> 1;
+            by[ib] = y >> 1;
+        }
+    }
+    int n = 0;
+    for (int ibl = 0; ibl < nblk; ibl++)
+        if (!gone[active[ibl]]) active[n++] = active[ibl];
+    const int nkeep = n;
+    int k = 0;
+    for (int ibl = 0; ibl < nkeep; ibl++) {
         const int ib = active[ibl];
         if (!refine[ib]) continue;
         const int ibr = avail[3 * k], ibtl = avail[3 * k + 1], ibtr = avail[3 * k + 2];
@@ -144,6 +235,7 @@ extern "C" int bgf_refine_tables(int* nblk_io, int* active, int* level, int* nbr
         active[n + 2] = ibtr;
         n += 3;
     }
+    for (int ibl = n; ibl < nblk; ibl++) active[ibl] = -1;
     // neighbours from the geometry of the new quadtree
     std::unordered_map<uint64_t, int> at;
     at.reserve((size_t)n * 2);
@@ -190,4 +282,11 @@ extern "C" int bgf_refine_tables(int* nblk_io, int* active, int* level, int* nbr
     }
     *nblk_io = n;
     return BGF_OK;
+}
+
+extern "C" int bgf_refine_tables(int* nblk_io, int* active, int* level, int* nbr8, double* xo, double* yo,
+                                 int nblkmem, double dx, int doubleprecision, const uint8_t* refine, int* children)
+{
+    return bgf_adapt_tables(nblk_io, active, level, nbr8, xo, yo, nblkmem, dx, doubleprecision, refine, nullptr,
+                            children, nullptr);
 }

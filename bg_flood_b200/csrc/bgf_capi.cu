@@ -160,6 +160,7 @@ struct bgf_handle {
     double *d_bxo = nullptr, *d_byo = nullptr;
     uint8_t* d_flags = nullptr;
     int* d_child = nullptr;
+    int* d_quads = nullptr;  // coarsened quads of an adaptation pass, 4 ids each
     // gauges: the device ring, and the drained samples on the host ([sample][gauge]
     // times and [sample][gauge][4] values h, zs, u, v; gauge_nhost gauges per sample)
     GaugeRing gauges;
@@ -721,7 +722,7 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         {(void**)&h->d_scratch, 8 * sizeof(double)},
         {(void**)&h->d_bxo, nb * sizeof(double)},        {(void**)&h->d_byo, nb * sizeof(double)},
         {(void**)&h->d_flags, nb},                       {(void**)&h->d_child, 3 * nb * sizeof(int)},
-        {(void**)&h->d_cflags, nb},
+        {(void**)&h->d_cflags, nb},                      {(void**)&h->d_quads, nb * sizeof(int)},
         {&h->d_datum, nb * es},
     };
     // one device allocation carved into 256-byte aligned pieces: handles are created
@@ -1904,6 +1905,20 @@ template <class T> static adapt::AdaptDev<T> adapt_dev(bgf_handle* h)
     return a;
 }
 
+// refinesanitycheck on the handle's tables (bgf_adapt_sanity); coarsening flags
+// survive only with allow_coarsen.
+static int sanity(bgf_handle* h, const bgf_adapt_param* ap, std::vector<uint8_t>& refine,
+                  std::vector<uint8_t>& coarsen)
+{
+    const int nb = h->nblkmem;
+    std::vector<int> nbr8((size_t)8 * nb);
+    for (int ib = 0; ib < nb; ib++)
+        for (int k = 0; k < 8; k++) nbr8[8 * ib + k] = h->nbr[(size_t)k * nb + ib];
+    return bgf_adapt_sanity(h->nblk, h->active.data(), h->level.data(), nbr8.data(), nb, h->P.minlevel, h->P.maxlevel,
+                            h->bxo.data(), h->byo.data(), h->P.dx, ap->allow_coarsen ? 1 : 0, refine.data(),
+                            coarsen.data());
+}
+
 // AdaptCriteria (src/AdaptCriteria.cu:20-130) on the device, then the host sanity
 // pass.  refine/coarsen are indexed by block id (nblkmem bytes each).
 template <class T> static int adapt_flags_t(bgf_handle* h, const bgf_adapt_param* ap, std::vector<uint8_t>& refine,
@@ -1934,11 +1949,25 @@ template <class T> static int adapt_flags_t(bgf_handle* h, const bgf_adapt_param
             refine[ib] = mask[ib] ? refine[ib] : 0;
             coarsen[ib] = mask[ib] ? coarsen[ib] : 0;
         }
-        std::vector<int> nbr8((size_t)8 * nb);
-        for (int ib = 0; ib < nb; ib++)
-            for (int k = 0; k < 8; k++) nbr8[8 * ib + k] = h->nbr[(size_t)k * nb + ib];
-        return bgf_refine_sanity(h->nblk, h->active.data(), h->level.data(), nbr8.data(), nb, h->P.minlevel,
-                                 h->P.maxlevel, refine.data(), coarsen.data());
+        return sanity(h, ap, refine, coarsen);
+    }
+    if (ap->criterion == BGF_ADAPT_HGRAD) {
+        adapt::launch_hgrad<T>(m, (const T*)h->d_dh, h->cur, h->P.eps, ap->arg1, ap->arg2, h->P.dx, h->d_flags,
+                               h->d_cflags, h->stream);
+        h->launches++;
+        BGF_CUDA(cudaGetLastError());
+        refine.assign(nb, 0);
+        coarsen.assign(nb, 0);
+        BGF_CUDA(cudaMemcpyAsync(refine.data(), h->d_flags, nb, cudaMemcpyDeviceToHost, h->stream));
+        BGF_CUDA(cudaMemcpyAsync(coarsen.data(), h->d_cflags, nb, cudaMemcpyDeviceToHost, h->stream));
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
+        std::vector<uint8_t> mask(nb, 0);
+        for (int ibl = 0; ibl < h->nblk; ibl++) mask[h->active[ibl]] = 1;
+        for (int ib = 0; ib < nb; ib++) {
+            refine[ib] = mask[ib] ? refine[ib] : 0;
+            coarsen[ib] = mask[ib] ? coarsen[ib] : 0;
+        }
+        return sanity(h, ap, refine, coarsen);
     }
     const T* z = nullptr;
     int stride324 = 0;
@@ -1963,17 +1992,15 @@ template <class T> static int adapt_flags_t(bgf_handle* h, const bgf_adapt_param
         refine[ib] = mask[ib] ? refine[ib] : 0;
         coarsen[ib] = mask[ib] ? !refine[ib] : 0;  // Thresholdcriteria: coarsen = !refine
     }
-    std::vector<int> nbr8((size_t)8 * nb);
-    for (int ib = 0; ib < nb; ib++)
-        for (int k = 0; k < 8; k++) nbr8[8 * ib + k] = h->nbr[(size_t)k * nb + ib];
-    return bgf_refine_sanity(h->nblk, h->active.data(), h->level.data(), nbr8.data(), nb, h->P.minlevel, h->P.maxlevel,
-                             refine.data(), coarsen.data());
+    return sanity(h, ap, refine, coarsen);
 }
 
 static int check_adapt_param(const bgf_adapt_param* ap)
 {
     if (!ap) return BGF_EINVAL;
+    if (ap->allow_coarsen != 0 && ap->allow_coarsen != 1) return BGF_EINVAL;
     if (ap->criterion == BGF_ADAPT_TARGETLEVEL) return BGF_OK;  // var, arg1 and arg2 are not used
+    if (ap->criterion == BGF_ADAPT_HGRAD) return ap->arg1 >= 0.0 && ap->arg2 >= 0.0 ? BGF_OK : BGF_EINVAL;
     if (ap->criterion != BGF_ADAPT_THRESHOLD && ap->criterion != BGF_ADAPT_INRANGE) return BGF_EINVAL;
     if (ap->var < BGF_VAR_H || ap->var > BGF_VAR_ZB) return BGF_EINVAL;
     return BGF_OK;
@@ -2021,31 +2048,52 @@ template <class T> static int adapt_t(bgf_handle* h, const bgf_adapt_param* ap, 
     bool changed_any = false;
     while (it < maxit) {
         it++;
-        const int oldn = h->nblk;
         std::vector<uint8_t> refine, coarsen;
         if ((rc = adapt_flags_t<T>(h, ap, refine, coarsen))) return rc;
-        std::vector<int> act(nb, -1), lev = h->level, nbr8((size_t)8 * nb), child((size_t)3 * nb, -1);
+        std::vector<int> act(nb, -1), lev = h->level, nbr8((size_t)8 * nb), child((size_t)3 * nb, -1),
+            sib((size_t)3 * nb, -1);
         std::copy(h->active.begin(), h->active.end(), act.begin());
         for (int ib = 0; ib < nb; ib++)
             for (int k = 0; k < 8; k++) nbr8[8 * ib + k] = h->nbr[(size_t)k * nb + ib];
         std::vector<double> xo = h->bxo, yo = h->byo;
         int n = h->nblk;
-        rc = bgf_refine_tables(&n, act.data(), lev.data(), nbr8.data(), xo.data(), yo.data(), nb, h->P.dx, h->dbl,
-                               refine.data(), child.data());
+        rc = bgf_adapt_tables(&n, act.data(), lev.data(), nbr8.data(), xo.data(), yo.data(), nb, h->P.dx, h->dbl,
+                              refine.data(), ap->allow_coarsen ? coarsen.data() : nullptr, child.data(), sib.data());
         if (rc) {
             if (rc == BGF_ENOMEM) g_last_error = "refinement needs more block slots than nblkmem";
             return rc;
         }
+        bool refined = false;
+        std::vector<int> quads;
+        for (int ibl = 0; ibl < h->nblk; ibl++) {
+            const int ib = h->active[ibl];
+            refined = refined || child[3 * ib] >= 0;
+            if (sib[3 * ib] >= 0) {
+                quads.push_back(ib);
+                for (int q = 0; q < 3; q++) quads.push_back(sib[3 * ib + q]);
+            }
+        }
+        const int nquads = (int)quads.size() / 4;
+        const bool changed = refined || nquads > 0;
         adapt::AdaptDev<T> a = adapt_dev<T>(h);
         DevModel<T> m = dev_model<T>(h);
-        if (n != oldn) {
-            // children from the old mesh (old tables still on the device)
-            BGF_CUDA(cudaMemcpyAsync(h->d_child, child.data(), sizeof(int) * 3 * nb, cudaMemcpyHostToDevice, h->stream));
-            adapt::launch_children<T>(m, a, h->cur, h->has_cf ? (T*)h->d_cf : nullptr,
-                                      h->has_rainmask ? h->d_rainmask : nullptr, h->stream);
-            h->launches += 4;
+        if (changed) {
+            // children and merged quads from the old mesh (old tables still on the device)
+            if (refined)
+                BGF_CUDA(cudaMemcpyAsync(h->d_child, child.data(), sizeof(int) * 3 * nb, cudaMemcpyHostToDevice,
+                                         h->stream));
+            if (nquads)
+                BGF_CUDA(cudaMemcpyAsync(h->d_quads, quads.data(), sizeof(int) * quads.size(), cudaMemcpyHostToDevice,
+                                         h->stream));
+            h->launches += adapt::launch_children<T>(m, a, h->cur, h->has_cf ? (T*)h->d_cf : nullptr,
+                                                     h->has_rainmask ? h->d_rainmask : nullptr, h->d_quads, nquads,
+                                                     refined, h->stream);
             BGF_CUDA(cudaGetLastError());
-            // segments: the children on a listed side inherit it
+            // segments: the children on a listed side inherit it; a merged quad's
+            // blocks give way to the parent, listed once
+            std::vector<int> parent_of(nb, -1);
+            for (int k = 0; k < nquads; k++)
+                for (int q = 0; q < 4; q++) parent_of[quads[4 * k + q]] = quads[4 * k];
             const int kids_side[4][2] = {{0, 2}, {1, 3}, {2, 3}, {0, 1}};  // left, right, top, bot: child slots
             for (HostSeg& sg : h->segs)
                 for (int sidx = 0; sidx < 4; sidx++) {
@@ -2055,6 +2103,9 @@ template <class T> static int adapt_t(bgf_handle* h, const bgf_adapt_param* ap, 
                             const int kids[4] = {ib, child[3 * ib], child[3 * ib + 1], child[3 * ib + 2]};
                             out.push_back(kids[kids_side[sidx][0]]);
                             out.push_back(kids[kids_side[sidx][1]]);
+                        } else if (ib >= 0 && ib < nb && parent_of[ib] >= 0) {
+                            const int p = parent_of[ib];
+                            if (std::find(out.begin(), out.end(), p) == out.end()) out.push_back(p);
                         } else {
                             out.push_back(ib);
                         }
@@ -2077,7 +2128,7 @@ template <class T> static int adapt_t(bgf_handle* h, const bgf_adapt_param* ap, 
                              h->has_rainmask ? h->d_rainmask : nullptr, h->stream);
         h->launches++;
         BGF_CUDA(cudaGetLastError());
-        if (n == oldn) break;
+        if (!changed) break;
     }
     // bed halo and gradients of the new mesh
     BGF_CUDA(cudaMemsetAsync(h->d_dzbdx, 0, (size_t)nb * 324 * sizeof(T), h->stream));

@@ -56,8 +56,13 @@ struct TargetMapDev;
 template <class T>
 void launch_target_level(const DevModel<T>& m, const TargetMapDev& g, double xo, double yo, double dx0,
                          uint8_t* refine, uint8_t* coarsen, cudaStream_t st);
-template <class T> void launch_children(const DevModel<T>& m, const AdaptDev<T>& a, int cur, T* cf, uint8_t* rainmask,
-                                        cudaStream_t st);
+// Old-mesh halos, then the children of refined blocks (refine) and the merged
+// quads (nquads > 0, quads[4k..4k+3] on the device); returns the launch count.
+template <class T> int launch_children(const DevModel<T>& m, const AdaptDev<T>& a, int cur, T* cf, uint8_t* rainmask,
+                                       const int* quads, int nquads, bool refine, cudaStream_t st);
+template <class T>
+void launch_hgrad(const DevModel<T>& m, const T* zs, int cur, double eps, double hthr, double gthr, double dx0,
+                  uint8_t* refine, uint8_t* coarsen, cudaStream_t st);
 template <class T> void launch_bed(const DevModel<T>& m, const AdaptDev<T>& a, const StepParams<T>& p, int cur, T* zb,
                                    double xo0, double yo0, const double* bxo, const double* byo, double mask,
                                    uint8_t* rainmask, cudaStream_t st);

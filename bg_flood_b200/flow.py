@@ -43,7 +43,7 @@ class CBlockP(ctypes.Structure):
 
 class CAdaptParam(ctypes.Structure):
     _fields_ = [("criterion", ctypes.c_int), ("var", ctypes.c_int), ("arg1", ctypes.c_double),
-                ("arg2", ctypes.c_double), ("maxiteration", ctypes.c_int)]
+                ("arg2", ctypes.c_double), ("maxiteration", ctypes.c_int), ("allow_coarsen", ctypes.c_int)]
 
 
 class CEvolving(ctypes.Structure):
@@ -251,23 +251,26 @@ class FlowB200:
     def clear_target_level_maps(self) -> None:
         _check(lib().bgf_clear_target_level_maps(self.handle), "bgf_clear_target_level_maps")
 
-    def _adapt_param(self, crit, maxiteration: int):
+    def _adapt_param(self, crit, maxiteration: int, allow_coarsen: bool = False):
         from .adapt import VARS
-        return CAdaptParam(crit.kind, VARS[crit.var], float(crit.arg1), float(crit.arg2), int(maxiteration))
+        return CAdaptParam(crit.kind, VARS[crit.var], float(crit.arg1), float(crit.arg2), int(maxiteration),
+                           1 if allow_coarsen else 0)
 
-    def adapt_flags(self, crit):
-        """(refine, coarsen) per active block of one criterion + sanity pass."""
+    def adapt_flags(self, crit, allow_coarsen: bool = False):
+        """(refine, coarsen) per active block of one criterion + sanity pass; with
+        allow_coarsen, coarsen marks the parents of the quads that would merge."""
         n = ctypes.c_int(0)
         _check(lib().bgf_get_blocks(self.handle, ctypes.byref(n), None, None, None, None, None), "bgf_get_blocks")
         r = np.zeros(n.value, np.uint8)
         c = np.zeros(n.value, np.uint8)
-        p = self._adapt_param(crit, 1)
+        p = self._adapt_param(crit, 1, allow_coarsen)
         _check(lib().bgf_adapt_flags(self.handle, ctypes.byref(p), _ptr(r), _ptr(c)), "bgf_adapt_flags")
         return r, c
 
-    def adapt(self, crit, maxiteration: int = 20):
-        """Adaptation of the mesh and state; returns (nblk, passes)."""
-        p = self._adapt_param(crit, maxiteration)
+    def adapt(self, crit, maxiteration: int = 20, allow_coarsen: bool = False):
+        """Adaptation of the mesh and state; returns (nblk, passes).  allow_coarsen
+        (an extension; the reference cancels coarsening) also merges quads."""
+        p = self._adapt_param(crit, maxiteration, allow_coarsen)
         n, it = ctypes.c_int(0), ctypes.c_int(0)
         _check(lib().bgf_adapt(self.handle, ctypes.byref(p), ctypes.byref(n), ctypes.byref(it)), "bgf_adapt")
         return n.value, it.value

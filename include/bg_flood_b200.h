@@ -432,14 +432,32 @@ int bgf_pool_autotune(bgf_pool* pool, int steps, int* grid, double* ms_per_step)
  * or (Targetlevel) when the rounded bilinear value of a target-level map at any of
  * its cells is above the block's level; Targetlevel keeps a block from coarsening
  * when some cell's target equals its level, and each map rewrites the flags of the
- * previous one (the last map decides), as the reference loops over its maps. */
-enum { BGF_ADAPT_THRESHOLD = 1, BGF_ADAPT_INRANGE = 2, BGF_ADAPT_TARGETLEVEL = 3 };
+ * previous one (the last map decides), as the reference loops over its maps.
+ * Threshold and Inrange mark every block that does not refine as a coarsening
+ * candidate (coarsen = !refine).
+ *
+ * Extension (no counterpart key in the reference): BGF_ADAPT_HGRAD flags a block
+ * for refinement when some cell has h > arg1 or a wet-surface slope |grad eta| >
+ * arg2, and as a coarsening candidate when every cell has h <= arg1/2 and |grad
+ * eta| <= arg2/2 (var is not used).  The slope is taken inside the block from wet
+ * cells only: along x, (eta(x+1) - eta(x-1)) / (2 dx_l) when both neighbours are
+ * wet cells of the block, the one-sided difference to the wet one otherwise, 0
+ * with none (likewise along y); a cell is wet when h > eps; |grad eta|^2 =
+ * gx^2 + gy^2 is compared with the squared threshold, all in the state precision.
+ *
+ * allow_coarsen (extension, 0 = the reference's behaviour): the reference's sanity
+ * pass cancels every coarsening flag (src/Adaptation.cu:173-175).  With 1 the
+ * pass keeps them and applies the reference's coarsening rules instead (see
+ * bgf_adapt_sanity), and bgf_adapt merges each complete quad of coarsening blocks
+ * into its parent (the reference's coarsen, src/Adaptation.cu:677-1015). */
+enum { BGF_ADAPT_THRESHOLD = 1, BGF_ADAPT_INRANGE = 2, BGF_ADAPT_TARGETLEVEL = 3, BGF_ADAPT_HGRAD = 4 };
 enum { BGF_VAR_H = 0, BGF_VAR_ZS = 1, BGF_VAR_U = 2, BGF_VAR_V = 3, BGF_VAR_ZB = 4 };
 typedef struct bgf_adapt_param {
-    int criterion;     /* BGF_ADAPT_THRESHOLD or BGF_ADAPT_INRANGE            */
-    int var;           /* BGF_VAR_*                                          */
-    double arg1, arg2; /* threshold, or zmin and zmax                         */
+    int criterion;     /* BGF_ADAPT_*                                          */
+    int var;           /* BGF_VAR_* (Threshold, Inrange)                       */
+    double arg1, arg2; /* threshold, or zmin and zmax, or h and slope thresholds */
     int maxiteration;  /* adaptmaxiteration, 20 when <= 0                     */
+    int allow_coarsen; /* extension: 0 as the reference (no coarsening)       */
 } bgf_adapt_param;
 
 /* Bathymetry forcing (the reference's Forcing.Bathy[0]): nx*ny float nodes,
@@ -468,7 +486,12 @@ int bgf_adapt_flags(bgf_handle* h, const bgf_adapt_param* a, uint8_t* refine, ui
  * and every boundary segment lists the children of its refined blocks on the
  * same side.  Per-cell friction and rain-mask inputs are carried to the children
  * from the covering parent cell.  Writes the new block count and the number of
- * passes. */
+ * passes.  With allow_coarsen, a pass also merges every quad of coarsening blocks:
+ * the parent keeps the lower-left block's id and takes h, zs, u, v (and friction)
+ * as T(0.25) * (((c00 + c10) + c01) + c11) of the four cells it covers, its
+ * boundary running means restart at zero, the three other ids become free for the
+ * next pass, and boundary segments list the parent in their place; passes stop
+ * when a pass neither refines nor coarsens. */
 int bgf_adapt(bgf_handle* h, const bgf_adapt_param* a, int* nblk, int* niter);
 
 /* Host copies of the current block tables: active (nblk entries), level and
@@ -499,6 +522,34 @@ int bgf_refine_sanity(int nblk, const int* active, const int* level, const int* 
  * slots per flagged block exist below nblkmem. */
 int bgf_refine_tables(int* nblk, int* active, int* level, int* nbr8, double* xo, double* yo, int nblkmem, double dx,
                       int doubleprecision, const uint8_t* refine, int* children);
+
+/* refinesanitycheck with coarsening kept (extension; allow_coarsen = 0 is
+ * bgf_refine_sanity).  The reference's rules without its cancelling line, in its
+ * order: (1) no refinement at maxlevel, no coarsening at minlevel; (2) no
+ * coarsening of any neighbour entry of a refining block; (3) no coarsening of a
+ * block with a finer side neighbour; (4) until nothing changes, every refining
+ * block forces its coarser first neighbours to refine and keeps its same-level
+ * first neighbours from coarsening (checkneighbourrefine); (5) in active order, a block
+ * keeps its flag only when it is the lower-left block of a quad -- its origin
+ * xo / dx_l / 16 and yo / dx_l / 16 truncate to even numbers, its right, top and
+ * top-right neighbours exist, are on its level and are flagged; every other
+ * block's flag is cleared, so that afterwards coarsen[ib] marks the parents.  xo
+ * and yo are the block origins as in bgf_get_blocks, dx the level-0 spacing. */
+int bgf_adapt_sanity(int nblk, const int* active, const int* level, const int* nbr8, int nblkmem, int minlevel,
+                     int maxlevel, const double* xo, const double* yo, double dx, int allow_coarsen, uint8_t* refine,
+                     uint8_t* coarsen);
+/* bgf_refine_tables with coarsening (extension; coarsen may be NULL): first every
+ * flagged quad parent ib (coarsen[ib], after bgf_adapt_sanity) merges its quad
+ * (coarsen, src/Adaptation.cu:677-1015): level - 1, origin xo += dx_{l+1} and yo +=
+ * dx_{l+1} (the reference's T(calcres(dx, level + 1)) added in T), its right, top
+ * and top-right blocks leave the active list (siblings[3*ib..3*ib+2], else -1) and
+ * become free for the next pass only; then the refinement as bgf_refine_tables.
+ * The active list keeps its order without the removed blocks, followed by the new
+ * children.  BGF_EINVAL when a flagged parent is not the lower-left block of a
+ * complete quad on its level or also refines. */
+int bgf_adapt_tables(int* nblk, int* active, int* level, int* nbr8, double* xo, double* yo, int nblkmem, double dx,
+                     int doubleprecision, const uint8_t* refine, const uint8_t* coarsen, int* children,
+                     int* siblings);
 
 #ifdef __cplusplus
 }

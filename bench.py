@@ -53,9 +53,9 @@ def parse():
     ap.add_argument("--engine", type=int, default=1)
     ap.add_argument("--fastmath", type=int, default=1, help="1: fast-math kernels, 0: bit-exact kernels")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
-    ap.add_argument("--only", choices=["amr", "ensemble", "serve"], default=None,
+    ap.add_argument("--only", choices=["amr", "ensemble", "ensemble_small", "serve"], default=None,
                     help="run one secondary measurement alone and print it (profiling runs)")
-    ap.add_argument("--amr", type=int, default=1024, help="level-0 cells per side of the AMR measurement (0: skip)")
+    ap.add_argument("--amr", type=int, default=2048, help="level-0 cells per side of the AMR measurement (0: skip)")
     ap.add_argument("--ensemble", type=int, default=64, help="members of the batched-ensemble measurement (0: skip)")
     ap.add_argument("--ens-max-blocks", type=int, default=16384)
     ap.add_argument("--serve", type=int, default=48, help="requests of the serving measurement (0: skip)")
@@ -270,7 +270,65 @@ def accuracy_vs_fp64(n: int, engine: int, dev: int, fastmath: int, steps: int = 
             "target_eta_m": 1e-3}
 
 
-def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, steps: int, dev: int, fastmath: int):
+ACC_T = 300.0       # simulated seconds of the ensemble accuracy runs
+ACC_MAX_BLOCKS = 1024
+
+
+def _oracle_member(args):
+    """The FP64 or FP32 oracle on ensemble member k to ACC_T; (zs, hu) interiors."""
+    k, seed, min_blocks, use_double = args
+    import cases
+    from runners import interior, make_oracle
+    c = cases.ensemble_member(k, seed, min_blocks, ACC_MAX_BLOCKS)
+    c.nextoutputtime = ACC_T
+    o, _ = make_oracle(c, use_double=use_double)
+    while o.totaltime < ACC_T:
+        o.step(1)
+    zs, h, u = (interior(o.get(n)) for n in ("zs", "h", "u"))
+    return zs, h * u
+
+
+def ensemble_accuracy(seed: int, min_blocks: int, dev: int, fastmath: int, members=(0, 1, 3, 7)) -> dict:
+    """Split-precision FP32 members (two rain, two tsunami; block counts capped at
+    ACC_MAX_BLOCKS) after ACC_T simulated seconds against the FP64 oracle, with the
+    reference's own FP32 arithmetic (the oracle's FP32 build) against the same FP64
+    oracle beside it.  The oracle runs in spawned processes while the GPU runs."""
+    import multiprocessing as mp
+    import cases
+    from runners import interior, make_gpu
+    ctx = mp.get_context("spawn")
+    jobs = [(k, seed, min_blocks, dbl) for k in members for dbl in (True, False)]
+    with ctx.Pool(min(len(jobs), max(1, (os.cpu_count() or 2) - 1))) as pool:
+        pending = pool.map_async(_oracle_member, jobs)
+        gpu = {}
+        for k in members:
+            c = cases.ensemble_member(k, seed, min_blocks, ACC_MAX_BLOCKS)
+            c.param.GPUDEVICE = dev
+            c.param.fastmath = fastmath
+            c.param.splitprecision = 1
+            c.nextoutputtime = ACC_T
+            f, _, lp = make_gpu(c)
+            f.run(lp, endtime=ACC_T)
+            zs, h, u, v = f.get_state()
+            gpu[k] = (c.name, interior(zs).astype(np.float64), (interior(h).astype(np.float64) * interior(u)))
+            del f
+        ora = dict(zip(jobs, pending.get()))
+    acc = {}
+    for k in members:
+        name, zs, hu = gpu[k]
+        z64, q64 = ora[(k, seed, min_blocks, True)]
+        z32, q32 = ora[(k, seed, min_blocks, False)]
+        acc[name] = {"kind": "tsunami" if k % 4 == 3 else "rain", "simulated_s": ACC_T,
+                     "max_eta_err_m": float(np.abs(zs - z64).max()), "max_hu_err_m2s": float(np.abs(hu - q64).max()),
+                     "reference_fp32_eta_err_m": float(np.abs(z32 - z64).max()),
+                     "reference_fp32_hu_err_m2s": float(np.abs(q32 - q64).max())}
+    return {"vs": "FP64 oracle (CPU restatement of FlowCPU, pinned to the reference)",
+            "reference_fp32": "the oracle's FP32 build against the same FP64 oracle: the error of evaluating the "
+                              "reference's algorithm in FP32", "members": acc}
+
+
+def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, steps: int, dev: int, fastmath: int,
+                   accuracy: bool = True, peak_rate: float | None = None):
     """Batched ensemble against the plain one-scenario-at-a-time loop on the same
     seeded members (block counts log-uniform in [min_blocks, max_blocks], rain on
     fractal terrain and deep-water tsunamis), each member advanced by `steps`
@@ -291,12 +349,27 @@ def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, step
     f.run(lp, endtime=1e30, maxsteps=4)
     del f
     plain_ms, t0 = 0.0, time.perf_counter()
+    member_ms = []
     for c in members:
         f, _, lp = make_gpu(c)
         f.run(lp, endtime=1e30, maxsteps=steps)
-        plain_ms += f.last_run_timing()[0]
+        member_ms.append(f.last_run_timing()[0])
+        plain_ms += member_ms[-1]
         del f
     plain_wall = time.perf_counter() - t0
+    # the reference's loop structure: one host call per step, the step's dt read back
+    # before the next (Mainloop); wall clock of the steps alone, set-up excluded
+    step_loop_s = 0.0
+    for c in members:
+        f, _, lp = make_gpu(c)
+        lp.totaltime += f.flow_step(lp)
+        ts = time.perf_counter()
+        for _ in range(steps):
+            lp.totaltime += f.flow_step(lp)
+        step_loop_s += time.perf_counter() - ts
+        del f
+    cells = [256 * b for b in blocks]
+    best_member_rate = max(cl * steps / (ms / 1e3) for cl, ms in zip(cells, member_ms))
     t0 = time.perf_counter()
     pool = ScenarioPool(members[0].param, sum(blocks), nscen)
     t1 = time.perf_counter()
@@ -315,84 +388,105 @@ def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, step
     phases = {"pool_create_s": t1 - t0, "build_s": t2 - t1, "admit_s": t3 - t2, "run_s": time.perf_counter() - t3}
     assert left == 0
     del pool, built
-    # accuracy: split-precision FP32 against the FP64 build at the same simulated time
-    acc = {}
-    for k in range(min(nscen, 8)):
-        if len(acc) >= 4:
-            break
-        kind = "tsunami" if k % 4 == 3 else "rain"
-        if kind == "rain" and sum(1 for v in acc.values() if v["kind"] == "rain") >= 2:
-            continue
-        res = {}
-        for mode in ("split", "fp64"):
-            c = cases.ensemble_member(k, seed, min_blocks, min(max_blocks, 1024))
-            c.param.GPUDEVICE = dev
-            c.param.fastmath = fastmath
-            c.param.splitprecision = 1 if mode == "split" else 0
-            c.param.doubleprecision = 1 if mode == "fp64" else 0
-            c.nextoutputtime = 300.0
-            f, _, lp = make_gpu(c)
-            f.run(lp, endtime=300.0)
-            zs, h, u, v = f.get_state()
-            res[mode] = (zs[:, 1:17, 1:17].astype(np.float64), (h * u)[:, 1:17, 1:17].astype(np.float64))
-            del f
-        acc[c.name] = {"kind": kind, "max_eta_err_m": float(np.abs(res["split"][0] - res["fp64"][0]).max()),
-                       "max_hu_err_m2s": float(np.abs(res["split"][1] - res["fp64"][1]).max()),
-                       "simulated_s": 300.0}
+    batched_rate = sum(blocks) * 256 * steps / (batched_ms / 1e3)
+    acc = ensemble_accuracy(seed, min_blocks, dev, fastmath) if accuracy else None
     return {"scenarios": nscen, "precision": "FP32 split (deviations from FP64 block datums)",
             "accuracy_vs_fp64": acc, "blocks_total": int(sum(blocks)), "blocks_min": int(min(blocks)),
             "blocks_max": int(max(blocks)), "steps_per_scenario": steps,
             "plain_device_ms": plain_ms, "batched_device_ms": batched_ms,
             "plain_scenarios_per_s": nscen / (plain_ms / 1e3), "batched_scenarios_per_s": nscen / (batched_ms / 1e3),
             "speedup_device": plain_ms / batched_ms,
+            "best_member_cell_rate": best_member_rate,
+            "speedup_device_bound": plain_ms / (sum(cells) * steps / max(best_member_rate, batched_rate) * 1e3),
+            "speedup_device_bound_at_peak": None if peak_rate is None else
+            plain_ms / (sum(cells) * steps / max(peak_rate, best_member_rate, batched_rate) * 1e3),
+            "speedup_bound_meaning": "plain device time / (all members' cell-updates at the best cell rate measured: "
+                                     "the best single member, the batched run or, at_peak, the large single-grid "
+                                     "device loop): what batching could gain at most if every member ran that fast",
+            "plain_per_step_loop_s": step_loop_s,
+            "speedup_vs_per_step_loop": step_loop_s / (batched_ms / 1e3),
+            "per_step_loop_meaning": "one bgf_flow_step call per step with its dt read back (the reference's "
+                                     "Mainloop structure), wall clock of the steps, against the batched device time",
             "plain_wall_s": plain_wall, "batched_wall_s": batched_wall,
             "speedup_wall": plain_wall / batched_wall, "batched_phases": phases,
             "cell_updates_per_s_batched": sum(blocks) * 256 * steps / (batched_ms / 1e3)}
 
 
-def amr_bench(n0: int, maxlevel: int, steps: int, dev: int, fastmath: int):
-    """Quadtree rain-on-grid: seeded fractal terrain (0-300 m relief) on an n0 x n0
-    level-0 grid (dx = 10 m), refined by the library's own adaptation pass up to
-    maxlevel where the bed lies in the lowest 60 m (Inrange criterion), rain of 50
-    mm/h, Manning n = 0.035; the device loop's cell-updates/s over all levels."""
+def amr_bench(n0: int, maxlevel: int, steps: int, dev: int, fastmath: int, readapt_every: int = 50,
+              mem_factor: int = 16):
+    """Quadtree rain-on-grid: seeded fractal terrain (0-300 m relief, carved valley) on
+    an n0 x n0 level-0 grid (dx = 10 m), rain of 50 mm/h, Manning n = 0.035, a lake
+    filling the lowest 3 % of the terrain at the start.  The mesh follows the
+    depth-or-slope criterion (refine where h > 0.01 m or |grad eta| > 1e-3, coarsen
+    below half of both; coarsening is an extension, the reference cancels it) up to
+    maxlevel: adapted at the start and again every readapt_every steps while the
+    device loop runs.  Reports the device loop's cell-updates/s over all levels, the
+    adaptation passes' wall time and the rate with that time included."""
     import cases
-    from bg_flood_b200.adapt import Criterion, INRANGE
+    from bg_flood_b200.adapt import depth_or_slope
     from bg_flood_b200.flow import FlowB200, Loop
     from bg_flood_b200.mesh import boundary_segments, grid_to_buq, uniform_mesh
     case = cases.rain_on_terrain(n0, engine=1, dx=10.0, seed=11)
     case.param.GPUDEVICE = dev
     case.param.fastmath = fastmath
     case.param.maxlevel, case.param.minlevel, case.param.initlevel = maxlevel, 0, 0
+    zfill = float(np.quantile(case.zb, 0.03))
+    h0 = np.maximum(np.float32(zfill) - case.zb, 0.0).astype(np.float32)
     mesh = uniform_mesh(n0, n0, case.dx)
-    mem = mesh.nblk * (4 ** maxlevel)
+    mem = mesh.nblk * mem_factor
     f = FlowB200(case.param, mem)
     f.set_blocks(mesh.active, mesh.level, mesh.nbr, mesh.xo, mesh.yo)
     pad = lambda a: np.concatenate([a, np.zeros((mem - len(a), 18, 18), a.dtype)])
-    f.set_bed(pad(grid_to_buq(case.zb, mesh)))
+    f.set_bed(pad(grid_to_buq(case.zb, mesh, np.float32)))
     for typ, times, levels, sides in boundary_segments(mesh, case.param.segments, case.param.aoibnd, 0.0, 0.0):
         f.add_segment(typ, times, levels, sides)
     f.set_rain(*case.rain)
     z = np.zeros_like(case.zb)
-    f.set_state(*(pad(grid_to_buq(a, mesh)) for a in (case.h, z, z)))
+    f.set_state(*(pad(grid_to_buq(a, mesh, np.float32)) for a in (h0, z, z)))
     f.set_bathy(0.5 * case.dx, 0.5 * case.dx, case.dx, case.zb)
+    crit = depth_or_slope(0.01, 1e-3)
     t0 = time.perf_counter()
-    nblk, it = f.adapt(Criterion(INRANGE, "zb", 0.0, 60.0), maxiteration=maxlevel + 1)
-    adapt_s = time.perf_counter() - t0
-    act, lev, nbr, _, _ = f.get_blocks()
-    hist = np.bincount(lev[act], minlength=maxlevel + 1).tolist()
-    # blocks with a side facing another level run the multi-level chain, the rest the
-    # single-level kernels
-    act = act[:nblk]
-    cross = int(np.count_nonzero((lev[nbr[act]] != lev[act][:, None]).any(axis=1)))
+    nblk, it = f.adapt(crit, maxiteration=maxlevel + 1, allow_coarsen=True)
+    adapt0_s = time.perf_counter() - t0
+
+    def mesh_stats():
+        act, lev, nbr, _, _ = f.get_blocks()
+        act = act[: f.nblk]
+        hist = np.bincount(lev[act], minlength=maxlevel + 1).tolist()
+        cross = int(np.count_nonzero((lev[nbr[act]] != lev[act][:, None]).any(axis=1)))
+        return hist, cross
+
+    hist0, cross0 = mesh_stats()
     loop = Loop(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=1e30)
     f.init_dt(loop)
     f.run(loop, endtime=1e30, maxsteps=10)
-    f.run(loop, endtime=1e30, maxsteps=steps)
-    ms, launches = f.last_run_timing()
-    return {"level0_cells": n0 * n0, "blocks": int(nblk), "blocks_per_level": hist, "adapt_passes": it,
-            "blocks_multilevel_chain": cross, "blocks_single_level_kernels": int(nblk) - cross,
-            "adapt_s": adapt_s, "steps": steps, "ms": ms, "launches_per_step": launches / steps,
-            "cell_updates_per_s": nblk * 256 * steps / (ms / 1e3)}
+    ms_total, cells_total, launches, passes = 0.0, 0, 0, []
+    done = 0
+    while done < steps:
+        k = min(readapt_every, steps - done)
+        n = f.nblk
+        f.run(loop, endtime=1e30, maxsteps=k)
+        ms, nl = f.last_run_timing()
+        ms_total += ms
+        launches += nl
+        cells_total += n * 256 * k
+        done += k
+        if done < steps:
+            t0 = time.perf_counter()
+            n2, it2 = f.adapt(crit, maxiteration=maxlevel + 1, allow_coarsen=True)
+            passes.append({"after_step": done, "s": time.perf_counter() - t0, "blocks_before": n, "blocks_after": n2,
+                           "passes": it2})
+    hist1, cross1 = mesh_stats()
+    adapt_total = sum(p["s"] for p in passes)
+    return {"level0_cells": n0 * n0, "maxlevel": maxlevel, "nblkmem": mem,
+            "criterion": "h > 0.01 m or |grad eta| > 1e-3, coarsen below half (extension)",
+            "blocks_start": int(nblk), "blocks_per_level_start": hist0, "adapt_passes_start": it,
+            "adapt_start_s": adapt0_s, "blocks_multilevel_chain_start": cross0,
+            "blocks_end": int(f.nblk), "blocks_per_level_end": hist1, "blocks_multilevel_chain_end": cross1,
+            "steps": steps, "readapt_every": readapt_every, "readaptations": passes,
+            "simulated_s": loop.totaltime, "ms": ms_total, "launches_per_step": launches / steps,
+            "cell_updates_per_s": cells_total / (ms_total / 1e3),
+            "cell_updates_per_s_with_adaptation": cells_total / (ms_total / 1e3 + adapt_total)}
 
 
 def serving_bench(nreq: int, seed: int, rate: float, dev: int, fastmath: int, budget_gb: float = 150.0,
@@ -503,9 +597,11 @@ def main():
     if args.only:
         # one secondary measurement alone, for profiling its launches
         if args.only == "amr":
-            r = amr_bench(args.amr, 2, args.steps, local, args.fastmath)
+            r = amr_bench(args.amr, 3, args.steps, local, args.fastmath)
         elif args.only == "ensemble":
             r = ensemble_bench(args.ensemble, 2024, 64, args.ens_max_blocks, args.steps, local, args.fastmath)
+        elif args.only == "ensemble_small":
+            r = ensemble_bench(args.ensemble, 2025, 40, 512, args.steps, local, args.fastmath, accuracy=False)
         else:
             r = serving_bench(args.serve, 7, args.serve_rate, local, args.fastmath)
         print(json.dumps({"measurement": args.only, **r}))
@@ -634,10 +730,15 @@ def main():
         extra["device_loop_4096x4096"] = {"value": mb.nblk * 256 * 100 / (msb / 1e3), "steps": 100, "ms": msb}
         del fb
         if args.amr > 0:
-            extra["amr_rain_on_grid"] = amr_bench(args.amr, 2, 100, local, args.fastmath)
+            extra["amr_rain_on_grid"] = amr_bench(args.amr, 3, 200, local, args.fastmath)
         if args.ensemble > 0:
+            peak = extra["device_loop_4096x4096"]["value"]
             extra["ensemble"] = ensemble_bench(args.ensemble, 2024, 64, args.ens_max_blocks, 100, local,
-                                               args.fastmath)
+                                               args.fastmath, peak_rate=peak)
+            # the small end of the stated member sizes (1e4 to 1.3e5 cells), where one
+            # member alone cannot fill the GPU
+            extra["ensemble_small_members"] = ensemble_bench(args.ensemble, 2025, 40, 512, 100, local,
+                                                             args.fastmath, accuracy=False, peak_rate=peak)
         if args.serve > 0:
             extra["serving"] = serving_bench(args.serve, 7, args.serve_rate, local, args.fastmath)
 

@@ -101,6 +101,13 @@ class FlowB200:
         except Exception:
             pass
 
+    @property
+    def nblk(self) -> int:
+        """Active blocks of the current mesh."""
+        n = ctypes.c_int(0)
+        _check(lib().bgf_get_blocks(self.handle, ctypes.byref(n), None, None, None, None, None), "bgf_get_blocks")
+        return n.value
+
     # -- set-up -------------------------------------------------------------------
     def set_blocks(self, active: np.ndarray, level: np.ndarray, nbr: np.ndarray, xo=None, yo=None) -> None:
         """Block tables; nbr is (nblkmem, 8) in LeftBot, LeftTop, RightBot, RightTop,

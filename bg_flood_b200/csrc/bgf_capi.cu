@@ -2232,7 +2232,7 @@ int bgf_read_gauges(bgf_handle* h, int max_samples, double* times, double* value
 
 int bgf_set_kernel_layout(bgf_handle* h, int cells_per_thread)
 {
-    if (!h || (cells_per_thread != 1 && cells_per_thread != 2)) return BGF_EINVAL;
+    if (!h || cells_per_thread < 1 || cells_per_thread > 3) return BGF_EINVAL;
     h->gen = cells_per_thread;
     free_graphs(h);
     return BGF_OK;

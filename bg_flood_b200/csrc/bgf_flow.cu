@@ -21,6 +21,7 @@ namespace BGF_VARIANT {
 #include "bgf_stage.cuh"
 #include "bgf_pair.cuh"
 #include "bgf_flow2.cuh"
+#include "bgf_flow3.cuh"
 
 // ---------------------------------------------------------------- tile assembly
 
@@ -373,8 +374,31 @@ template <class T, int ENGINE, bool SPLIT, bool POOL> cudaError_t configure_one(
     e = cudaFuncSetAttribute(flux2_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem2_pred<T>());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(update2_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem2_corr<T>());
+    e = cudaFuncSetAttribute(update2_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem2_corr<T>());
+    if (e != cudaSuccess) return e;
+    // staged tiles (persistent CTAs with a producer warp)
+    e = cudaFuncSetAttribute(flux3_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem3_pred<T>());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(update3_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem3_corr<T>());
+}
+
+// Persistent grid of the staged kernels: CTAs resident on all SMs at once (from the
+// occupancy of the kernel at its shared memory), at most one per block.
+template <class KERN> static int resident_grid(KERN k, size_t smem, int nblk)
+{
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, NT3, smem) != cudaSuccess || per <= 0) per = 1;
+    const int g = sms * per;
+    return g < nblk ? g : nblk;
 }
 
 template <class T, int ENGINE> cudaError_t configure_engine()
@@ -404,6 +428,19 @@ static void launch_step_kernel(const DevModel<T>& m, const StepParams<T>& p, int
     const bool pool = m.scen != nullptr;
     bool split = false;
     if constexpr (sizeof(T) == 4) split = m.datum != nullptr;
+    if (!split && m.gen == 3) {
+        // staged tiles, persistent CTAs (the grid argument, when set, is the CTA count)
+        if constexpr (FLUX) {
+            auto k = pool ? flux3_kernel<T, ENGINE, true> : flux3_kernel<T, ENGINE, false>;
+            const int gg = g < m.nblk ? g : resident_grid(k, smem3_pred<T>(), m.nblk);
+            k<<<gg, NT3, smem3_pred<T>(), st>>>(m, p, parity);
+        } else {
+            auto k = pool ? update3_kernel<T, ENGINE, true> : update3_kernel<T, ENGINE, false>;
+            const int gg = g < m.nblk ? g : resident_grid(k, smem3_corr<T>(), m.nblk);
+            k<<<gg, NT3, smem3_corr<T>(), st>>>(m, p, parity);
+        }
+        return;
+    }
     if (!split && m.gen != 1) {
         // two cells per thread
         if constexpr (FLUX) {

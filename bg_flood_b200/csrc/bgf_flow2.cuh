@@ -59,8 +59,8 @@ template <class T> struct Smem2 {
     // corrector only (the predictor's launch leaves these out of its shared memory)
     T h0[360], u0[360], v0[360];  // state n on the 18x18 tile (boundary fluxes)
 };
-template <class T> constexpr size_t smem2_pred() { return offsetof(Smem2<T>, h0); }
-template <class T> constexpr size_t smem2_corr() { return sizeof(Smem2<T>); }
+template <class T> __host__ __device__ constexpr size_t smem2_pred() { return offsetof(Smem2<T>, h0); }
+template <class T> __host__ __device__ constexpr size_t smem2_corr() { return sizeof(Smem2<T>); }
 
 // 64-bit shared access of the pair of rows (2p, 2p+1) at index i (even).
 template <class T> __device__ __forceinline__ V2<T> ld2(const T* a, int i)

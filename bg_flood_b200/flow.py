@@ -220,7 +220,8 @@ class FlowB200:
         return t[:ns.value], v[:ns.value], lost.value
 
     def set_kernel_layout(self, cells_per_thread: int) -> None:
-        """Thread layout of the fused single-level kernels: 2 cells per thread (default) or 1."""
+        """Thread layout of the fused single-level kernels: 2 cells per thread (default),
+        1, or 3 (two cells per thread in persistent CTAs with a staging warp)."""
         _check(lib().bgf_set_kernel_layout(self.handle, int(cells_per_thread)), "bgf_set_kernel_layout")
 
     def autotune(self, loop: Loop, steps: int = 20) -> tuple:

@@ -134,6 +134,10 @@ class ScenarioPool:
     def set_grid(self, grid: int) -> None:
         _check(lib().bgf_pool_set_grid(self.handle, int(grid)), "bgf_pool_set_grid")
 
+    def set_kernel_layout(self, layout: int) -> None:
+        """Thread layout of the single-level kernels (1, 2 or 3), as FlowB200.set_kernel_layout."""
+        _check(lib().bgf_pool_set_kernel_layout(self.handle, int(layout)), "bgf_pool_set_kernel_layout")
+
     def autotune(self, steps: int = 20) -> tuple:
         """Times the pool step for each launch shape over the live scenarios and keeps
         the fastest; their state is unchanged afterwards.  Returns (grid, ms_per_step)."""

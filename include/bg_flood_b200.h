@@ -209,8 +209,11 @@ int bgf_set_grid(bgf_handle* h, int grid);
 /* Thread layout of the two fused single-level kernels: 2 (default) gives each
  * thread two vertically adjacent cells of a block (128 threads per block, paired
  * FP32 arithmetic in the fast-math build), 1 one cell per thread (256 threads per
- * block).  The exact build gives the same results bit for bit with either;
- * split-precision handles always use layout 1.  No counterpart in the reference. */
+ * block), 3 the two-cell arithmetic in persistent CTAs whose fifth warp stages the
+ * next block's tile into shared memory with bulk asynchronous copies while the
+ * other four compute (the grid then defaults to the CTAs resident on all SMs).
+ * The exact build gives the same results bit for bit with each; split-precision
+ * handles always use layout 1.  No counterpart in the reference. */
 int bgf_set_kernel_layout(bgf_handle* h, int cells_per_thread);
 
 /* ------------------------------------------------------------ gauges */
@@ -411,6 +414,8 @@ int bgf_pool_read_gauges(bgf_pool* P, int slot, int max_samples, double* times, 
 int bgf_pool_timing(bgf_pool* pool, double* gpu_ms, int64_t* steps, int* free_blocks);
 /* CTAs of the fused kernels (0: one per block; fewer CTAs loop over the blocks). */
 int bgf_pool_set_grid(bgf_pool* pool, int grid);
+/* Thread layout of the pool's single-level kernels, as bgf_set_kernel_layout. */
+int bgf_pool_set_kernel_layout(bgf_pool* pool, int layout);
 
 /* ------------------------------------------------------------ launch-shape autotuner */
 /* Times the fused step kernels on the current mesh from the loop state `loop`

@@ -1,8 +1,10 @@
-"""The two thread layouts of the fused single-level kernels (bgf_set_kernel_layout:
-two cells per thread, or one cell per thread) give the same results: bit for bit
-in the exact build, within the fast-math tolerance in the fast build (there the
-two-cell kernels use paired FP32 instructions and contract other products into
-fused multiply-adds).  Both run through the C ABI on the same inputs."""
+"""The thread layouts of the fused single-level kernels (bgf_set_kernel_layout: one
+cell per thread, two cells per thread, or two cells per thread in persistent CTAs
+whose producer warp stages each block's tile with bulk asynchronous copies) give
+the same results: bit for bit in the exact build, within the fast-math tolerance in
+the fast build (there the two-cell kernels use paired FP32 instructions and
+contract other products into fused multiply-adds).  All run through the C ABI on
+the same inputs, handles and pools."""
 import numpy as np
 import pytest
 
@@ -39,36 +41,82 @@ def _run(mk, layout, fast, nsteps, dbl=False):
     return dts, f.get_state()
 
 
+@pytest.mark.parametrize("layout", [2, 3])
 @pytest.mark.parametrize("name,mk,nsteps", CASES, ids=[c[0] for c in CASES])
-def test_layouts_bit_identical_exact(name, mk, nsteps):
+def test_layouts_bit_identical_exact(name, mk, nsteps, layout):
     d1, s1 = _run(mk, 1, 0, nsteps)
-    d2, s2 = _run(mk, 2, 0, nsteps)
+    d2, s2 = _run(mk, layout, 0, nsteps)
     assert d1 == d2
     for k, a, b in zip("zs h u v".split(), s1, s2):
         assert np.array_equal(interior(a), interior(b)), (k, float(np.abs(interior(a) - interior(b)).max()))
 
 
+@pytest.mark.parametrize("layout", [2, 3])
 @pytest.mark.parametrize("name,mk,nsteps", CASES, ids=[c[0] for c in CASES])
-def test_layouts_close_fast(name, mk, nsteps):
+def test_layouts_close_fast(name, mk, nsteps, layout):
     d1, s1 = _run(mk, 1, 1, nsteps)
-    d2, s2 = _run(mk, 2, 1, nsteps)
+    d2, s2 = _run(mk, layout, 1, nsteps)
     for a, b in zip(d1, d2):
         assert abs(a - b) <= FAST_DT_RTOL * a
     for k, a, b in zip("zs h u v".split(), s1, s2):
         assert float(np.abs(interior(a).astype(np.float64) - interior(b)).max()) <= FAST_TOL, k
 
 
-def test_layouts_bit_identical_double():
+@pytest.mark.parametrize("layout", [2, 3])
+def test_layouts_bit_identical_double(layout):
     mk = lambda: cases.dam_break(32, 1)
     d1, s1 = _run(mk, 1, 0, 30, dbl=True)
-    d2, s2 = _run(mk, 2, 0, 30, dbl=True)
+    d2, s2 = _run(mk, layout, 0, 30, dbl=True)
     assert d1 == d2
     for a, b in zip(s1, s2):
         assert np.array_equal(interior(a), interior(b))
 
 
+@pytest.mark.parametrize("grid", [0, 7])
+def test_staged_layout_persistent_grids(grid):
+    """The staged kernels with their default resident grid and with 7 CTAs (many
+    blocks per CTA, so every CTA refills its stage many times)."""
+    mk = lambda: cases.conical_island(128, 1)
+    d1, s1 = _run(mk, 1, 0, 25)
+    case = mk()
+    f, _, loop = make_gpu(case)
+    f.set_kernel_layout(3)
+    f.set_grid(grid)
+    d3 = []
+    for _ in range(25):
+        dt = f.flow_step(loop)
+        loop.totaltime += dt
+        d3.append(dt)
+    assert d1 == d3
+    for a, b in zip(s1, f.get_state()):
+        assert np.array_equal(interior(a), interior(b))
+
+
+def test_staged_layout_in_a_pool():
+    """Scenarios of different sizes and step budgets in one pool with the staged
+    kernels (finished scenarios stop swapping their state buffers while others run)
+    end as each does alone with one cell per thread."""
+    from bg_flood_b200.pool import ScenarioPool
+    mks = [lambda: cases.gauss(48, 1, 3), lambda: cases.conical_island(64, 1), lambda: cases.dam_break(48, 1)]
+    budgets = [17, 30, 23]
+    alone = []
+    for mk, n in zip(mks, budgets):
+        _, st = _run(mk, 1, 0, n)
+        alone.append(st)
+    built = [make_gpu(mk()) for mk in mks]
+    pool = ScenarioPool(mks[0]().param, sum(b[1].nblk for b in built), 4)
+    pool.set_kernel_layout(3)
+    slots = [pool.admit(f, lp, 1e30, maxsteps=n) for (f, _, lp), n in zip(built, budgets)]
+    assert pool.run(64) == 0
+    for slot, (f, m, _), st in zip(slots, built, alone):
+        h = pool.depth(slot, m.nblk)
+        assert np.array_equal(h, interior(st[1])[: m.nblk])
+    pool.close()
+
+
 def test_layout_rejects_other_values():
     f, _, _ = make_gpu(cases.hump_walls(32, 2))
     from bg_flood_b200.flow import BGFError
-    with pytest.raises(BGFError):
-        f.set_kernel_layout(3)
+    for bad in (0, 4):
+        with pytest.raises(BGFError):
+            f.set_kernel_layout(bad)

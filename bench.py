@@ -250,6 +250,32 @@ def cpu_baseline_entry(r: dict) -> dict:
             "host": hc, "taskset_cores": sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else None}
 
 
+def reference_gpu_baseline(n: int, engine: int, steps: int) -> dict:
+    """The reference's own FlowGPU (its CUDA sources compiled for sm_100a by
+    oracle/ref/Makefile) on the same workload and GPU, through the oracle harness:
+    wall clock of `steps` steps after 3 untimed ones (each reference step reads its dt
+    back to the host, so the clock covers its work), and its distance from FlowCPU."""
+    import torch
+    from runners import interior, make_oracle, make_reference
+    case = workload_case(n, engine, 0, 0)
+    case.paramtext = case.paramtext.replace("gpudevice = -1", "gpudevice = 0")
+    r = make_reference(case)
+    r.step(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r.step(steps)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    o, _ = make_oracle(workload_case(n, engine, 0, 0))
+    o.step(3 + steps)
+    diff = float(np.abs(interior(r.get("zs")) - interior(o.get("zs"))).max())
+    del r
+    return {"value": n * n * steps / wall, "unit": UNIT, "ms_per_step": wall / steps * 1e3,
+            "sample": f"{steps} FlowGPU steps of the {n}x{n} workload after 3 untimed ones, wall clock",
+            "build": "reference sources compiled for sm_100a (nvcc defaults: FMA contraction)",
+            "max_abs_zs_vs_flowcpu_m": diff}
+
+
 def accuracy_vs_fp64(n: int, engine: int, dev: int, fastmath: int, steps: int = 20) -> dict:
     """The headline build from the workload's start against the FP64 oracle over the
     same number of steps: max |eta| and max |h u| differences over all cells."""
@@ -751,6 +777,8 @@ def main():
             extra["cpu_baseline_makefile_flags"] = cpu_baseline_entry(
                 cpu_reference_sample(2, 0, args.engine, "makefile"))
         extra["accuracy"] = accuracy_vs_fp64(args.n, args.engine, local, args.fastmath)
+        if not args.no_extra:
+            extra["reference_flowgpu_b200"] = reference_gpu_baseline(args.n, args.engine, 20)
 
     if rank == 0:
         line = {

@@ -68,6 +68,10 @@ SIGNATURES = {
     "bgf_pool_timing": (ctypes.c_int, [c_void_p, c_double_p, ctypes.POINTER(ctypes.c_int64), c_int_p]),
     "bgf_pool_set_grid": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "bgf_pool_set_kernel_layout": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "bgf_pool_run_async": (ctypes.c_int, [c_void_p, ctypes.c_int]),
+    "bgf_pool_wait": (ctypes.c_int, [c_void_p, c_int_p]),
+    "bgf_pool_finish": (ctypes.c_int, [c_void_p, ctypes.c_int, c_int_p, c_void_p, c_void_p, c_void_p,
+                                       ctypes.POINTER(ctypes.c_int64), c_int_p]),
     "bgf_autotune": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_double_p]),
     "bgf_add_target_level_map": (ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                 ctypes.c_double, ctypes.c_double, c_int_p]),

@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 
 from ._native import lib
-from .flow import BGFError, FlowB200, Loop, _check
+from .flow import BGFError, CLoop, FlowB200, Loop, _check
 
 __all__ = ["ScenarioPool"]
 
@@ -65,6 +65,43 @@ class ScenarioPool:
         n = ctypes.c_int(0)
         _check(lib().bgf_pool_run(self.handle, int(maxsteps), ctypes.byref(n)), "bgf_pool_run")
         return n.value
+
+    def run_async(self, maxsteps: int) -> None:
+        """Enqueues maxsteps (<= 512) pool steps and returns at once; wait() completes them."""
+        _check(lib().bgf_pool_run_async(self.handle, int(maxsteps)), "bgf_pool_run_async")
+
+    def wait(self) -> int:
+        """Waits for the steps run_async enqueued; returns the number still running."""
+        n = ctypes.c_int(0)
+        _check(lib().bgf_pool_wait(self.handle, ctypes.byref(n)), "bgf_pool_wait")
+        return n.value
+
+    def finish(self, slots, nblks, with_max: bool = False):
+        """Retires finished scenarios for their fields only (bgf_pool_finish): returns,
+        per slot, (FlowB200, h (nblk, 16, 16), hmax or None, Loop, nsteps, status).
+        The scenarios' handles are not updated; may overlap steps from run_async."""
+        n = len(slots)
+        if n == 0:
+            return []
+        hs = [np.zeros((nb, 16, 16), self.dtype) for nb in nblks]
+        hm = [np.zeros((nb, 16, 16), self.dtype) for nb in nblks] if with_max else None
+        ptrs = (ctypes.c_void_p * n)(*[a.ctypes.data for a in hs])
+        mptrs = (ctypes.c_void_p * n)(*[a.ctypes.data for a in hm]) if with_max else None
+        loops = (CLoop * n)()
+        steps = (ctypes.c_int64 * n)()
+        status = (ctypes.c_int * n)()
+        sl = (ctypes.c_int * n)(*[int(x) for x in slots])
+        _check(lib().bgf_pool_finish(self.handle, n, sl, ptrs, mptrs, loops, steps, status), "bgf_pool_finish")
+        out = []
+        for k, slot in enumerate(slots):
+            lp = Loop()
+            lp.from_c(loops[k])
+            f = self.members.pop(slot)
+            ng = getattr(self, "_ngauges", {}).pop(slot, 0)
+            if ng:
+                f._ngauges = ng
+            out.append((f, hs[k], hm[k] if with_max else None, lp, int(steps[k]), int(status[k])))
+        return out
 
     def query(self, slot: int):
         """(Loop, status, nsteps); status 0 running, 1 finished, 2 dt underflow,

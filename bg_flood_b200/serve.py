@@ -81,7 +81,10 @@ class FloodServer:
         its arrival time on the wall clock; otherwise all are queued at t = 0.
         Arrived requests are prepared (host set-up and upload into their own handle)
         by `builders` background threads while the pool computes, at most `prefetch`
-        ahead; they are admitted in the order they become ready."""
+        ahead; they are admitted in the order they become ready.  Each chunk of pool
+        steps is enqueued before the host retires the scenarios that finished in
+        the previous chunk (their fields gathered on the pool's copy stream), so
+        retirement overlaps the device work."""
         self.gpu_ms = 0.0
         self.host_s = {k: 0.0 for k in self.host_s}
         pending = sorted(requests, key=lambda r: r.arrival)
@@ -125,10 +128,25 @@ class FloodServer:
             th.start()
         live: dict[int, tuple[Request, FlowB200, float, list]] = {}
         out: list[Result] = []
+        finished: list[int] = []  # slots that finished in the last chunk, retired during the next one
         nreq = len(pending)
+
+        def retire(slots):
+            ta = time.perf_counter()
+            res = self.pool.finish(slots, [live[s][0].nblk for s in slots], with_max=self.track_hmax)
+            tb = time.perf_counter()
+            self.host_s["fields"] += tb - ta
+            for slot, (f, h, hmax, loop, n, status) in zip(slots, res):
+                r, _, t_adm, series = live.pop(slot)
+                f.close()
+                out.append(Result(r.rid, r.arrival, t_adm, now(), n, loop.totaltime,
+                                  h if self.keep_fields else None, hmax if self.keep_fields else None, series, status))
+            self.host_s["retire"] += time.perf_counter() - tb
+
         try:
             while len(out) < nreq:
-                # admission in arrival order while block and scenario slots allow
+                # admission in arrival order while block and scenario slots allow (no
+                # pool steps are in flight here)
                 with lock:
                     while ready:
                         r, (f, loop) = ready[0]
@@ -149,8 +167,20 @@ class FloodServer:
                             raise RuntimeError("request preparation stopped before the stream ended")
                         lock.wait(0.01)
                         continue
+                running = len(live) > len(finished)
+                if running:
+                    # the next chunk runs on the device while the host retires the
+                    # scenarios that finished in the last one (their state is frozen)
+                    ta = time.perf_counter()
+                    self.pool.run_async(self.chunk)
+                    self.host_s["run"] += time.perf_counter() - ta
+                if finished:
+                    retire(finished)
+                    finished = []
+                if not running:
+                    continue
                 ta = time.perf_counter()
-                self.pool.run(self.chunk)
+                self.pool.wait()
                 self.host_s["run"] += time.perf_counter() - ta
                 self.gpu_ms += self.pool.timing()[0]
                 for slot in list(live):
@@ -161,22 +191,8 @@ class FloodServer:
                     if r.gauges:
                         t, v = self.pool.read_gauges(slot)
                         series.extend((float(tk), [float(x) for x in vk[:, 0]]) for tk, vk in zip(t[:, 0], v))
-                    if status == 0:
-                        continue
-                    h = hmax = None
-                    ta = time.perf_counter()
-                    if self.keep_fields:
-                        if self.track_hmax:
-                            h, hmax = self.pool.depth(slot, r.nblk, with_max=True)
-                        else:
-                            h = self.pool.depth(slot, r.nblk)
-                    tb = time.perf_counter()
-                    self.host_s["fields"] += tb - ta
-                    f, loop, n = self.pool.retire(slot)
-                    f.close()
-                    self.host_s["retire"] += time.perf_counter() - tb
-                    del live[slot]
-                    out.append(Result(r.rid, r.arrival, t_adm, now(), n, loop.totaltime, h, hmax, series, status))
+                    if status != 0:
+                        finished.append(slot)
         finally:
             with lock:
                 stop[0] = True

@@ -412,6 +412,26 @@ int bgf_pool_get_depth(bgf_pool* pool, int slot, void* h, void* hmax);
 int bgf_pool_set_gauges(bgf_pool* P, int slot, int n, const int* block, const int* i, const int* j);
 int bgf_pool_read_gauges(bgf_pool* P, int slot, int max_samples, double* times, double* values, int* nsamples);
 int bgf_pool_timing(bgf_pool* pool, double* gpu_ms, int64_t* steps, int* free_blocks);
+/* bgf_pool_run in two halves, so that the host can work while the pool steps run.
+ * bgf_pool_run_async applies pending admissions and retirements and enqueues
+ * maxsteps (<= 512) pool steps plus a copy of the time slots, then returns;
+ * bgf_pool_wait waits for them, refreshes what bgf_pool_query reports, drains the
+ * gauge ring, records the device time and writes the scenarios still running.
+ * Between the two only bgf_pool_finish may be called (admit, retire, run and
+ * get_depth return BGF_ESTATE). */
+int bgf_pool_run_async(bgf_pool* pool, int maxsteps);
+int bgf_pool_wait(bgf_pool* pool, int* nlive);
+/* Retirement of n finished scenarios (bgf_pool_query status != 0) for a caller
+ * that needs only their fields: final depth h and maximum depth hmax (either may
+ * be NULL; per scenario an array of nblk * 256 values of the field type in the
+ * scenario's active order), loop state, step count and status (1 finished, 2 dt
+ * underflow, 3 non-finite).  The state is not copied back into the scenarios'
+ * handles.  Runs on the pool's own copy stream, also while a run enqueued by
+ * bgf_pool_run_async is in flight (finished scenarios are no longer written);
+ * the freed slots serve admissions after that run.  BGF_ESTATE for a scenario
+ * that is still running. */
+int bgf_pool_finish(bgf_pool* pool, int n, const int* slots, void* const* h, void* const* hmax, bgf_loop* loops,
+                    int64_t* nsteps, int* status);
 /* CTAs of the fused kernels (0: one per block; fewer CTAs loop over the blocks). */
 int bgf_pool_set_grid(bgf_pool* pool, int grid);
 /* Thread layout of the pool's single-level kernels, as bgf_set_kernel_layout. */

@@ -128,3 +128,52 @@ def test_pool_with_multilevel_scenarios():
         assert nn == n and loop.totaltime == loop_a.totaltime and loop.dt == loop_a.dt
         for a, b in zip(f.get_state()[1:], st[1:]):
             assert np.array_equal(interior(a), interior(b))
+
+
+def test_async_run_and_batched_finish():
+    """Chunks enqueued with run_async while the scenarios that finished in the last
+    chunk are retired with finish (fields gathered on the pool's copy stream): every
+    scenario's final depth, maximum depth, time and step count equal its run alone,
+    a later admission reuses freed slots, and a scenario still running cannot be
+    finished."""
+    from bg_flood_b200.flow import BGFError
+    ref = [alone(mk, n) for mk, n in zip(MIX, BUDGET)]
+    case0 = MIX[0]()
+    pool = ScenarioPool(case0.param, 4096, 8, track_hmax=True)
+    built = [make_gpu(mk()) for mk in MIX]
+    slots = {pool.admit(f, loop, ENDTIME, maxsteps=n): k for k, ((f, mesh, loop), n) in enumerate(zip(built, BUDGET))}
+    # a running scenario is refused
+    pool.run(4)
+    with pytest.raises(BGFError):
+        pool.finish([next(iter(slots))], [built[slots[next(iter(slots))]][1].nblk])
+    got, finished = {}, []
+    while slots:
+        running = len(slots) > len(finished)
+        if running:
+            pool.run_async(16)
+        if finished:
+            res = pool.finish(finished, [built[slots[s]][1].nblk for s in finished], with_max=True)
+            for s, (f, h, hmax, loop, n, status) in zip(finished, res):
+                got[slots.pop(s)] = (h, hmax, loop, n, status)
+            finished = []
+        if not running:
+            continue
+        pool.wait()
+        for s in slots:
+            _, status, _ = pool.query(s)
+            if status != 0:
+                finished.append(s)
+    for k, (st, loop_a, n_a) in enumerate(ref):
+        h, hmax, loop, n, status = got[k]
+        assert status == 1 and n == n_a and loop.totaltime == loop_a.totaltime, k
+        nblk = built[k][1].nblk
+        assert np.array_equal(h, interior(st[1])[:nblk]), k
+        assert (hmax >= h).all(), k
+    # the freed slots take a new scenario, which again matches its run alone
+    (st, loop_a, n_a) = alone(MIX[1], 30)
+    f, mesh, loop = make_gpu(MIX[1]())
+    s = pool.admit(f, loop, ENDTIME, maxsteps=30)
+    assert pool.run(1000) == 0
+    (_, h, _, loop_p, n_p, _), = pool.finish([s], [mesh.nblk])
+    assert n_p == n_a and np.array_equal(h, interior(st[1])[: mesh.nblk])
+    pool.close()

@@ -18,7 +18,7 @@ def run_to(case, endtime, mode):
     case.nextoutputtime = endtime
     f, mesh, loop = make_gpu(case)
     f.run(loop, endtime=endtime)
-    assert loop.totaltime == endtime
+    assert abs(loop.totaltime - endtime) < 1e-6  # the FP32 builds take their last dt in FP32
     zs, h, u, v = f.get_state()
     zs, h, u = (interior(a).astype(np.float64) for a in (zs, h, u))
     return zs, h * u

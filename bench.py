@@ -764,13 +764,13 @@ def main():
         if args.amr > 0:
             extra["amr_rain_on_grid"] = amr_bench(args.amr, 3, 200, local, args.fastmath)
         if args.ensemble > 0:
-            peak = extra["device_loop_4096x4096"]["value"]
+            grid_rate = extra["device_loop_4096x4096"]["value"]
             extra["ensemble"] = ensemble_bench(args.ensemble, 2024, 64, args.ens_max_blocks, 100, local,
-                                               args.fastmath, peak_rate=peak)
+                                               args.fastmath, peak_rate=grid_rate)
             # the small end of the stated member sizes (1e4 to 1.3e5 cells), where one
             # member alone cannot fill the GPU
             extra["ensemble_small_members"] = ensemble_bench(args.ensemble, 2025, 40, 512, 100, local,
-                                                             args.fastmath, accuracy=False, peak_rate=peak)
+                                                             args.fastmath, accuracy=False, peak_rate=grid_rate)
         if args.serve > 0:
             extra["serving"] = serving_bench(args.serve, 7, args.serve_rate, local, args.fastmath)
 

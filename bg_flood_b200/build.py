@@ -36,6 +36,7 @@ SOURCES = [
     ("bgf_io.cpp", "bgf_io.o", ["-x", "cu", "--fmad=false"]),
     ("bgf_layout.cu", "bgf_layout.o", ["--fmad=false"]),
     ("bgf_gauge.cu", "bgf_gauge.o", ["--fmad=false"]),
+    ("bgf_adapt_dev.cu", "bgf_adapt_dev.o", ["--fmad=false"]),
 ]
 
 

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <unordered_map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -161,6 +162,11 @@ struct bgf_handle {
     uint8_t* d_flags = nullptr;
     int* d_child = nullptr;
     int* d_quads = nullptr;  // coarsened quads of an adaptation pass, 4 ids each
+    // device table work of bgf_adapt (bgf_adapt_dev.cu): 1 when the mesh allows it
+    int adapt_mode = 1;
+    void* d_adapt = nullptr;      // scratch, carved into adapt::DevAdaptScratch
+    int* d_agrids = nullptr;      // per-level block index grids
+    long long agrids_cap = 0;
     // gauges: the device ring, and the drained samples on the host ([sample][gauge]
     // times and [sample][gauge][4] values h, zs, u, v; gauge_nhost gauges per sample)
     GaugeRing gauges;
@@ -820,7 +826,8 @@ int bgf_destroy(bgf_handle* h)
     // the per-block arrays of bgf_create are pieces of d_slab (back to the memory pool in
     // stream order); the rest are own allocations
     void* ptrs[] = {h->d_slab, h->d_segs, h->d_seg_t, h->d_seg_wl, h->d_rain_t, h->d_rain_r, h->d_dem,
-                    h->d_rivers, h->d_riv_t, h->d_riv_q, (void*)h->rmap.val, h->d_tiles};
+                    h->d_rivers, h->d_riv_t, h->d_riv_q, (void*)h->rmap.val, h->d_tiles, h->d_adapt,
+                    (void*)h->d_agrids};
     if (h->stream) {
         for (void* p : ptrs) dfree(h, p);
         for (auto& g : h->tmaps) dfree(h, (void*)g.val);
@@ -2037,15 +2044,24 @@ int bgf_adapt_flags(bgf_handle* h, const bgf_adapt_param* ap, uint8_t* refine, u
 // bed re-interpolation, wet/dry fix-up} until the block count stops changing or
 // maxiteration passes ran, then prepares the bed halo and gradients of the new
 // mesh and carries the boundary segments over to the children of refined blocks.
-template <class T> static int adapt_t(bgf_handle* h, const bgf_adapt_param* ap, int* niter)
+template <class T>
+static int adapt_dev_t(bgf_handle* h, const bgf_adapt_param* ap, const adapt::GridSpec& gs, int* niter,
+                       bool& changed_any);
+
+// gs: the level grids when the table work runs on the device (adapt_dev_t), else
+// NULL for the host tables.
+template <class T> static int adapt_t(bgf_handle* h, const bgf_adapt_param* ap, int* niter, const adapt::GridSpec* gs)
 {
     const int nb = h->nblkmem;
     int rc = alloc_amr(h);  // stage tiles double as the old-mesh halo tiles
     if (rc) return rc;
-    zs_from_state<T>(h);
     const int maxit = ap->maxiteration > 0 ? ap->maxiteration : 20;
     int it = 0;
     bool changed_any = false;
+    if (gs) {
+        if ((rc = adapt_dev_t<T>(h, ap, *gs, &it, changed_any))) return rc;
+    } else {
+    zs_from_state<T>(h);
     while (it < maxit) {
         it++;
         std::vector<uint8_t> refine, coarsen;
@@ -2130,6 +2146,7 @@ template <class T> static int adapt_t(bgf_handle* h, const bgf_adapt_param* ap, 
         BGF_CUDA(cudaGetLastError());
         if (!changed) break;
     }
+    }
     // bed halo and gradients of the new mesh
     BGF_CUDA(cudaMemsetAsync(h->d_dzbdx, 0, (size_t)nb * 324 * sizeof(T), h->stream));
     BGF_CUDA(cudaMemsetAsync(h->d_dzbdy, 0, (size_t)nb * 324 * sizeof(T), h->stream));
@@ -2142,6 +2159,272 @@ template <class T> static int adapt_t(bgf_handle* h, const bgf_adapt_param* ap, 
     if (changed_any && (rc = rebuild_segments(h))) return rc;
     free_graphs(h);
     if (niter) *niter = it;
+    return BGF_OK;
+}
+
+// ---------------------------------------------------------------- adaptation tables on the device
+
+// The level grids of the device table rebuild: levels 0..maxlevel of the domain's
+// level-0 block extent.  False when the mesh or its size leaves the device path
+// out (a level below 0, more than 16 levels, grids above 64 M entries).
+static bool adapt_grid_spec(const bgf_handle* h, int maxlevel, adapt::GridSpec& gs)
+{
+    if (h->P.minlevel < 0 || maxlevel < 0 || maxlevel > 15) return false;
+    const int nb = h->nblkmem;
+    (void)nb;
+    int nbx0 = 0, nby0 = 0;
+    for (int ibl = 0; ibl < h->nblk; ibl++) {
+        const int ib = h->active[ibl];
+        const int l = h->level[ib];
+        if (l < 0 || l > maxlevel) return false;
+        const double dxl = h->P.dx / (double)(1 << l);
+        const int bx = (int)floor((h->bxo[ib] / dxl - 0.5) / 16.0 + 0.5);
+        const int by = (int)floor((h->byo[ib] / dxl - 0.5) / 16.0 + 0.5);
+        if (bx < 0 || by < 0) return false;
+        nbx0 = std::max(nbx0, (bx >> l) + 1);
+        nby0 = std::max(nby0, (by >> l) + 1);
+    }
+    gs.nlev = maxlevel + 1;
+    long long tot = 0;
+    for (int l = 0; l < 16; l++) {
+        gs.off[l] = 0;
+        gs.w[l] = gs.h[l] = 0;
+        if (l >= gs.nlev) continue;
+        gs.off[l] = (int)tot;
+        gs.w[l] = nbx0 << l;
+        gs.h[l] = nby0 << l;
+        tot += (long long)gs.w[l] * gs.h[l];
+        if (tot > (64ll << 20)) return false;
+    }
+    gs.total = tot;
+    return true;
+}
+
+// Scratch of the device table work, carved from one allocation sized for nblkmem.
+static int adapt_scratch(bgf_handle* h, const adapt::GridSpec& gs, adapt::DevAdaptScratch& S, int*& d_err)
+{
+    const size_t nb = (size_t)h->nblkmem;
+    struct Piece {
+        void** p;
+        size_t bytes;
+    };
+    const size_t ntile = nb / 1024 + 2;
+    Piece pieces[] = {
+        {(void**)&S.pos, nb * 4},     {(void**)&S.parent, nb},     {(void**)&S.gone, nb},
+        {(void**)&S.fr, nb * 4},      {(void**)&S.fq, nb * 4},     {(void**)&S.fk, nb * 4},
+        {(void**)&S.ff, nb * 4},      {(void**)&S.sr, nb * 4},     {(void**)&S.sq, nb * 4},
+        {(void**)&S.sk, nb * 4},      {(void**)&S.sf, nb * 4},     {(void**)&S.tiles, ntile * 4},
+        {(void**)&S.counts, 64},      {(void**)&S.avail, nb * 4},  {(void**)&S.nact, nb * 4},
+        {(void**)&S.nlev, nb * 4},    {(void**)&S.nxo, nb * 8},    {(void**)&S.nyo, nb * 8},
+        {(void**)&S.reflist, nb * 16}, {(void**)&S.bx, nb * 4},    {(void**)&S.by, nb * 4},
+        {(void**)&S.nnbr, nb * 32},   {(void**)&d_err, 64},
+    };
+    size_t total = 0;
+    for (auto& q : pieces) total += (q.bytes + 255) & ~(size_t)255;
+    if (!h->d_adapt) {
+        BGF_CUDA(dalloc(h, &h->d_adapt, total));
+    }
+    unsigned char* base = (unsigned char*)h->d_adapt;
+    for (auto& q : pieces) {
+        *q.p = base;
+        base += (q.bytes + 255) & ~(size_t)255;
+    }
+    if (gs.total > h->agrids_cap) {
+        if (h->d_agrids) dfree(h, (void*)h->d_agrids);
+        h->d_agrids = nullptr;
+        h->agrids_cap = 0;
+        BGF_CUDA(dalloc(h, (void**)&h->d_agrids, sizeof(int) * (size_t)gs.total));
+        h->agrids_cap = gs.total;
+    }
+    S.grids = h->d_agrids;
+    return BGF_OK;
+}
+
+// The criterion on the device into d_flags (refine) and, for the criteria that
+// have one, d_cflags (coarsen).  Returns in fill whether coarsen is !refine.
+template <class T> static int launch_flag_criteria(bgf_handle* h, const bgf_adapt_param* ap, int& fill)
+{
+    DevModel<T> m = dev_model<T>(h);
+    fill = 0;
+    if (ap->criterion == BGF_ADAPT_TARGETLEVEL) {
+        if (h->tmaps.empty()) {
+            g_last_error = "the Targetlevel criterion needs at least one target-level map";
+            return BGF_EINVAL;
+        }
+        for (const auto& g : h->tmaps) {
+            adapt::launch_target_level<T>(m, g, std::isnan(h->P.xo) ? 0.0 : h->P.xo, std::isnan(h->P.yo) ? 0.0 : h->P.yo,
+                                          h->P.dx, h->d_flags, h->d_cflags, h->stream);
+            h->launches++;
+        }
+    } else if (ap->criterion == BGF_ADAPT_HGRAD) {
+        adapt::launch_hgrad<T>(m, (const T*)h->d_dh, h->cur, h->P.eps, ap->arg1, ap->arg2, h->P.dx, h->d_flags,
+                               h->d_cflags, h->stream);
+        h->launches++;
+    } else {
+        const T* z = nullptr;
+        int stride324 = 0;
+        switch (ap->var) {
+        case BGF_VAR_H: z = (const T*)h->d_h[h->cur]; break;
+        case BGF_VAR_ZS: z = (const T*)h->d_dh; break;
+        case BGF_VAR_U: z = (const T*)h->d_u[h->cur]; break;
+        case BGF_VAR_V: z = (const T*)h->d_v[h->cur]; break;
+        case BGF_VAR_ZB: z = (const T*)h->d_zb; stride324 = 1; break;
+        default: return BGF_EINVAL;
+        }
+        adapt::launch_criteria<T>(m, z, stride324, ap->criterion, (T)ap->arg1, (T)ap->arg2, h->d_flags, h->stream);
+        h->launches++;
+        fill = 1;
+    }
+    BGF_CUDA(cudaGetLastError());
+    return BGF_OK;
+}
+
+// Boundary segments after a pass: the children on a listed side inherit it; a
+// merged quad's blocks give way to the parent, listed once.  kids(ib, out[3]) and
+// parent(ib) describe the pass.
+template <class Kids, class Parent> static void segments_after_pass(bgf_handle* h, Kids kids, Parent parent)
+{
+    const int nb = h->nblkmem;
+    const int kids_side[4][2] = {{0, 2}, {1, 3}, {2, 3}, {0, 1}};  // left, right, top, bot: child slots
+    for (HostSeg& sg : h->segs)
+        for (int sidx = 0; sidx < 4; sidx++) {
+            std::vector<int> out;
+            for (int ib : sg.blk[sidx]) {
+                int k3[3];
+                if (ib >= 0 && ib < nb && kids(ib, k3)) {
+                    const int q4[4] = {ib, k3[0], k3[1], k3[2]};
+                    out.push_back(q4[kids_side[sidx][0]]);
+                    out.push_back(q4[kids_side[sidx][1]]);
+                } else if (ib >= 0 && ib < nb && parent(ib) >= 0) {
+                    const int p = parent(ib);
+                    if (std::find(out.begin(), out.end(), p) == out.end()) out.push_back(p);
+                } else {
+                    out.push_back(ib);
+                }
+            }
+            sg.blk[sidx] = out;
+        }
+}
+
+// adapt_t with the sanity pass and the tables on the device (same results); the
+// host mirrors of the tables are refreshed once at the end.
+template <class T>
+static int adapt_dev_t(bgf_handle* h, const bgf_adapt_param* ap, const adapt::GridSpec& gs, int* niter,
+                       bool& changed_any)
+{
+    const int nb = h->nblkmem;
+    int rc = alloc_amr(h);  // stage tiles double as the old-mesh halo tiles
+    if (rc) return rc;
+    adapt::DevAdaptScratch S;
+    int* d_err = nullptr;
+    if ((rc = adapt_scratch(h, gs, S, d_err))) return rc;
+    BGF_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), h->stream));
+    zs_from_state<T>(h);
+    const int maxit = ap->maxiteration > 0 ? ap->maxiteration : 20;
+    const int allow = ap->allow_coarsen ? 1 : 0;
+    int it = 0;
+    changed_any = false;
+    while (it < maxit) {
+        it++;
+        int fill = 0;
+        if ((rc = launch_flag_criteria<T>(h, ap, fill))) return rc;
+        const adapt::DevTables t{h->d_active, h->nblk, nb, h->d_level, h->d_nbr, h->d_bxo, h->d_byo};
+        h->launches += adapt::dev_sanity(t, S, h->d_flags, h->d_cflags, h->P.minlevel, h->P.maxlevel, allow, fill,
+                                         h->P.dx, h->stream);
+        h->launches += adapt::dev_tables_count(t, S, h->d_flags, h->d_cflags, h->stream);
+        BGF_CUDA(cudaGetLastError());
+        int cnt[5];
+        BGF_CUDA(cudaMemcpyAsync(cnt, S.counts, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->stream));
+        BGF_CUDA(cudaMemcpyAsync(cnt + 4, d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        BGF_CUDA(cudaStreamSynchronize(h->stream));
+        const int nref = cnt[0], nq = cnt[1], nkeep = cnt[2], nfree = cnt[3];
+        if (cnt[4]) {
+            g_last_error = "device adaptation: a block lies outside the level grids";
+            return BGF_EINVAL;
+        }
+        if (3 * nref > nfree) {
+            g_last_error = "refinement needs more block slots than nblkmem";
+            return BGF_ENOMEM;
+        }
+        const bool changed = nref > 0 || nq > 0;
+        adapt::AdaptDev<T> a = adapt_dev<T>(h);
+        DevModel<T> m = dev_model<T>(h);
+        if (changed) {
+            const int nnew = nkeep + 3 * nref;
+            h->launches += adapt::dev_tables_build(t, S, h->d_flags, h->d_cflags, h->P.dx, h->dbl, nkeep, nnew,
+                                                   h->d_child, h->d_quads, gs, d_err, h->stream);
+            // children and merged quads from the old mesh (old tables still in place)
+            h->launches += adapt::launch_children<T>(m, a, h->cur, h->has_cf ? (T*)h->d_cf : nullptr,
+                                                     h->has_rainmask ? h->d_rainmask : nullptr, h->d_quads, nq,
+                                                     nref > 0, h->stream);
+            BGF_CUDA(cudaGetLastError());
+            if (!h->segs.empty()) {
+                std::vector<int> rl((size_t)4 * nref), ql((size_t)4 * nq);
+                if (nref)
+                    BGF_CUDA(cudaMemcpyAsync(rl.data(), S.reflist, sizeof(int) * rl.size(), cudaMemcpyDeviceToHost,
+                                             h->stream));
+                if (nq)
+                    BGF_CUDA(cudaMemcpyAsync(ql.data(), h->d_quads, sizeof(int) * ql.size(), cudaMemcpyDeviceToHost,
+                                             h->stream));
+                BGF_CUDA(cudaStreamSynchronize(h->stream));
+                std::unordered_map<int, int> kid_at, parent_of;
+                for (int k = 0; k < nref; k++) kid_at[rl[4 * k]] = k;
+                for (int k = 0; k < nq; k++)
+                    for (int q = 0; q < 4; q++) parent_of[ql[4 * k + q]] = ql[4 * k];
+                segments_after_pass(
+                    h,
+                    [&](int ib, int* out) {
+                        auto f = kid_at.find(ib);
+                        if (f == kid_at.end()) return false;
+                        for (int q = 0; q < 3; q++) out[q] = rl[4 * f->second + 1 + q];
+                        return true;
+                    },
+                    [&](int ib) {
+                        auto f = parent_of.find(ib);
+                        return f == parent_of.end() ? -1 : f->second;
+                    });
+            }
+            // the new tables replace the old ones
+            BGF_CUDA(cudaMemcpyAsync(h->d_active, S.nact, sizeof(int) * nnew, cudaMemcpyDeviceToDevice, h->stream));
+            BGF_CUDA(cudaMemcpyAsync(h->d_level, S.nlev, sizeof(int) * nb, cudaMemcpyDeviceToDevice, h->stream));
+            BGF_CUDA(cudaMemcpyAsync(h->d_nbr, S.nnbr, sizeof(int) * 8 * (size_t)nb, cudaMemcpyDeviceToDevice, h->stream));
+            BGF_CUDA(cudaMemcpyAsync(h->d_bxo, S.nxo, sizeof(double) * nb, cudaMemcpyDeviceToDevice, h->stream));
+            BGF_CUDA(cudaMemcpyAsync(h->d_byo, S.nyo, sizeof(double) * nb, cudaMemcpyDeviceToDevice, h->stream));
+            h->nblk = nnew;
+            changed_any = true;
+            m = dev_model<T>(h);
+        }
+        adapt::launch_bed<T>(m, a, step_params<T>(h), h->cur, (T*)h->d_zb, std::isnan(h->P.xo) ? 0.0 : h->P.xo,
+                             std::isnan(h->P.yo) ? 0.0 : h->P.yo, h->d_bxo, h->d_byo, h->P.mask,
+                             h->has_rainmask ? h->d_rainmask : nullptr, h->stream);
+        h->launches++;
+        BGF_CUDA(cudaGetLastError());
+        if (!changed) break;
+    }
+    // host mirrors of the final tables
+    int err = 0;
+    h->active.assign(h->nblk, 0);
+    std::vector<int> nbrT((size_t)8 * nb);
+    BGF_CUDA(cudaMemcpyAsync(h->active.data(), h->d_active, sizeof(int) * h->nblk, cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->level.data(), h->d_level, sizeof(int) * nb, cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->nbr.data(), h->d_nbr, sizeof(int) * 8 * (size_t)nb, cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->bxo.data(), h->d_bxo, sizeof(double) * nb, cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(h->byo.data(), h->d_byo, sizeof(double) * nb, cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if (err) {
+        g_last_error = "device adaptation: a block lies outside the level grids";
+        return BGF_EINVAL;
+    }
+    if ((rc = upload_tables(h))) return rc;
+    if (niter) *niter = it;
+    return BGF_OK;
+}
+
+int bgf_set_adapt_mode(bgf_handle* h, int mode)
+{
+    if (!h || (mode != 0 && mode != 1)) return BGF_EINVAL;
+    h->adapt_mode = mode;
     return BGF_OK;
 }
 
@@ -2158,7 +2441,10 @@ int bgf_adapt(bgf_handle* h, const bgf_adapt_param* ap, int* nblk, int* niter)
         g_last_error = "bgf_adapt does not support split precision";
         return BGF_EINVAL;
     }
-    rc = h->dbl ? adapt_t<double>(h, ap, niter) : adapt_t<float>(h, ap, niter);
+    adapt::GridSpec gs;
+    const bool on_device = h->adapt_mode && adapt_grid_spec(h, std::max(h->P.maxlevel, h->maxlev), gs);
+    rc = h->dbl ? adapt_t<double>(h, ap, niter, on_device ? &gs : nullptr)
+                : adapt_t<float>(h, ap, niter, on_device ? &gs : nullptr);
     if (nblk) *nblk = h->nblk;
     return rc;
 }

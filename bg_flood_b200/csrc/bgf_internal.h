@@ -66,6 +66,43 @@ void launch_hgrad(const DevModel<T>& m, const T* zs, int cur, double eps, double
 template <class T> void launch_bed(const DevModel<T>& m, const AdaptDev<T>& a, const StepParams<T>& p, int cur, T* zb,
                                    double xo0, double yo0, const double* bxo, const double* byo, double mask,
                                    uint8_t* rainmask, cudaStream_t st);
+
+// Device side of the sanity pass and the table rebuild (bgf_adapt_dev.cu).
+struct DevTables {
+    const int* active;
+    int nblk, nblkmem;
+    const int* level;
+    const int* nbr;        // [8][nblkmem]
+    const double *xo, *yo;
+};
+struct DevAdaptScratch {
+    int* pos;              // position in the active list, -1 when inactive
+    uint8_t *parent, *gone;
+    int *fr, *fq, *fk, *ff;  // refine, parent, kept flags per active position; free flag per id
+    int *sr, *sq, *sk, *sf;  // their exclusive prefix sums
+    int* tiles;            // scan tile totals
+    int* counts;           // refined, parents, kept, free
+    int* avail;            // free ids in ascending order
+    int *nact, *nlev;      // new active list and levels
+    double *nxo, *nyo;     // new origins
+    int* reflist;          // refined blocks and their children, 4 ids each
+    int* grids;            // per-level block index grids
+    int *bx, *by;          // block coordinates in the new mesh
+    int* nnbr;             // new neighbour tables [8][nblkmem]
+};
+struct GridSpec {
+    int nlev;              // levels 0..nlev-1
+    int off[16], w[16], h[16];
+    long long total;
+};
+void scan_excl(const int* in, int* out, int n, int* tile_sum, int* total, cudaStream_t st);
+int dev_sanity(const DevTables& t, const DevAdaptScratch& s, uint8_t* refine, uint8_t* coarsen, int minlevel,
+               int maxlevel, int allow, int fill_coarsen, double dx, cudaStream_t st);
+int dev_tables_count(const DevTables& t, const DevAdaptScratch& s, const uint8_t* refine, const uint8_t* coarsen,
+                     cudaStream_t st);
+int dev_tables_build(const DevTables& t, const DevAdaptScratch& s, const uint8_t* refine, const uint8_t* coarsen,
+                     double dx, int dbl, int nkeep, int nnew, int* child, int* quads, const GridSpec& gs, int* err,
+                     cudaStream_t st);
 }  // namespace adapt
 
 // Tile <-> compact layout kernels (bgf_layout.cu) for pinned host arrays.

@@ -283,6 +283,10 @@ class FlowB200:
         _check(lib().bgf_adapt(self.handle, ctypes.byref(p), ctypes.byref(n), ctypes.byref(it)), "bgf_adapt")
         return n.value, it.value
 
+    def set_adapt_mode(self, mode: int) -> None:
+        """1 (default): adaptation tables on the device when the mesh allows; 0: host tables."""
+        _check(lib().bgf_set_adapt_mode(self.handle, int(mode)), "bgf_set_adapt_mode")
+
     def get_blocks(self):
         """(active, level, nbr (nblkmem, 8), xo, yo) host copies of the tables."""
         n = ctypes.c_int(0)

@@ -518,6 +518,13 @@ int bgf_adapt_flags(bgf_handle* h, const bgf_adapt_param* a, uint8_t* refine, ui
  * next pass, and boundary segments list the parent in their place; passes stop
  * when a pass neither refines nor coarsens. */
 int bgf_adapt(bgf_handle* h, const bgf_adapt_param* a, int* nblk, int* niter);
+/* Where bgf_adapt does the sanity pass and the new tables: 1 (default) on the
+ * device when the mesh allows it (levels 0..15, per-level block grids of at most
+ * 64 M entries), else and with 0 in host C++ (bgf_adapt_sanity,
+ * bgf_adapt_tables).  Both give the same flags, ids, active list, levels, origins
+ * and neighbour tables; the device path copies the tables to the host once per
+ * call instead of every pass. */
+int bgf_set_adapt_mode(bgf_handle* h, int mode);
 
 /* Host copies of the current block tables: active (nblk entries), level and
  * origins per block slot, neighbours as [nblkmem][8] (LB, LT, RB, RT, BL, BR, TL,

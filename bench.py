@@ -276,6 +276,51 @@ def reference_gpu_baseline(n: int, engine: int, steps: int) -> dict:
             "max_abs_zs_vs_flowcpu_m": diff}
 
 
+def accuracy_full_run(n: int, engine: int, dev: int, fastmath: int, endtime: float = 20.0) -> dict:
+    """The whole simulated run of the workload (as the configuration states it) in the
+    headline build against the reference's own FP64 FlowGPU (its CUDA sources built
+    for sm_100a) over the same simulated time, both on this GPU: max |eta|, |hu|,
+    |hv| over all cells at the end, and the step counts."""
+    import torch
+    from runners import interior, make_gpu, make_reference
+    case = workload_case(n, engine, dev, fastmath)
+    case.nextoutputtime = endtime
+    f, mesh, loop = make_gpu(case)
+    nsteps = f.run(loop, endtime=endtime)
+    zs, h, u, v = f.get_state()
+    def reference_run(use_double):
+        rc = workload_case(n, engine, dev, fastmath)
+        rc.nextoutputtime = endtime
+        rc.paramtext = rc.paramtext.replace("gpudevice = -1", "gpudevice = 0")
+        r = make_reference(rc, use_double=use_double)
+        rsteps, rtime = 0, 0.0
+        t0 = time.perf_counter()
+        while rtime < endtime - 1e-12 and rsteps < 200000:
+            rtime += float(r.step(1)[0])  # the harness adds dt to its FP64 time the same way
+            rsteps += 1
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        fields = [interior(r.get(k)).astype(np.float64) for k in ("zs", "h", "u", "v")]
+        del r
+        return fields, rtime, rsteps, wall
+
+    def errors(a, b):
+        (za, ha, ua, va), (zb, hb, ub, vb) = a, b
+        return {"max_abs_eta_m": float(np.abs(za - zb).max()), "max_abs_hu_m2s": float(np.abs(ha * ua - hb * ub).max()),
+                "max_abs_hv_m2s": float(np.abs(ha * va - hb * vb).max())}
+
+    r64, rtime, rsteps, wall64 = reference_run(True)
+    r32, _, rsteps32, _ = reference_run(False)
+    ours = [interior(a).astype(np.float64) for a in (zs, h, u, v)]
+    out = {"vs": "reference FlowGPU, FP64 build, same GPU", "simulated_s": loop.totaltime,
+           "reference_simulated_s": rtime, "steps": nsteps, "reference_steps": rsteps,
+           "reference_fp64_wall_s": wall64, **errors(ours, r64),
+           "reference_fp32": {"steps": rsteps32, **errors(r32, r64)},
+           "reference_fp32_meaning": "the reference's own FP32 FlowGPU against its FP64 build over the same run",
+           "target_eta_m": 1e-3}
+    return out
+
+
 def accuracy_vs_fp64(n: int, engine: int, dev: int, fastmath: int, steps: int = 20) -> dict:
     """The headline build from the workload's start against the FP64 oracle over the
     same number of steps: max |eta| and max |h u| differences over all cells."""
@@ -353,31 +398,83 @@ def ensemble_accuracy(seed: int, min_blocks: int, dev: int, fastmath: int, membe
                               "reference's algorithm in FP32", "members": acc}
 
 
+def _member_levels(k: int, seed: int, amr: bool) -> int:
+    """Refinement levels above level 0 of ensemble member k: 0, 1 or 2 (seeded) for
+    rain members when the ensemble has AMR members, 0 for tsunamis (split precision
+    runs on single-level meshes)."""
+    if not amr or k % 4 == 3:
+        return 0
+    return int(np.random.default_rng([seed, k, 7]).integers(0, 3))
+
+
+def _build_member(c, levels: int):
+    """The handle of an ensemble member: single-level (make_gpu) or refined to
+    `levels` levels above level 0 where the bed lies in the lowest 10 % of the
+    member's relief (Inrange criterion on zb), from its own bathymetry grid."""
+    from runners import make_gpu
+    if levels == 0:
+        f, mesh, lp = make_gpu(c)
+        return f, lp
+    from bg_flood_b200.adapt import Criterion, INRANGE
+    from bg_flood_b200.flow import FlowB200, Loop
+    from bg_flood_b200.mesh import boundary_segments, grid_to_buq, uniform_mesh
+    c.param.maxlevel, c.param.minlevel, c.param.initlevel = levels, 0, 0
+    mesh = uniform_mesh(c.nx, c.ny, c.dx)
+    lo = float(c.zb.min())
+    hi = lo + 0.1 * (float(c.zb.max()) - lo)
+    mem = 3 * mesh.nblk
+    while True:
+        f = FlowB200(c.param, mem)
+        pad = lambda a: np.concatenate([a, np.zeros((mem - len(a), 18, 18), a.dtype)])
+        f.set_blocks(mesh.active, mesh.level, mesh.nbr, mesh.xo, mesh.yo)
+        f.set_bed(pad(grid_to_buq(c.zb, mesh, np.float32)))
+        for typ, times, lv, sides in boundary_segments(mesh, c.param.segments, c.param.aoibnd, 0.0, 0.0):
+            f.add_segment(typ, times, lv, sides)
+        if c.rain is not None:
+            f.set_rain(*c.rain)
+        f.set_state(*(pad(grid_to_buq(a, mesh, np.float32)) for a in (c.h, c.u, c.v)))
+        f.set_bathy(0.5 * c.dx, 0.5 * c.dx, c.dx, c.zb)
+        try:
+            f.adapt(Criterion(INRANGE, "zb", lo, hi), maxiteration=levels + 1)
+            break
+        except RuntimeError:
+            f.close()
+            if mem >= mesh.nblk * 4 ** levels:
+                raise
+            mem *= 2
+    lp = Loop(totaltime=0.0, dt=0.0, dtmax=0.0, nextoutputtime=c.nextoutputtime)
+    f.init_dt(lp)
+    return f, lp
+
+
 def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, steps: int, dev: int, fastmath: int,
-                   accuracy: bool = True, peak_rate: float | None = None):
+                   accuracy: bool = True, peak_rate: float | None = None, amr: bool = True):
     """Batched ensemble against the plain one-scenario-at-a-time loop on the same
-    seeded members (block counts log-uniform in [min_blocks, max_blocks], rain on
-    fractal terrain and deep-water tsunamis), each member advanced by `steps`
-    steps.  Device time of the steps (CUDA events around the graphs) and wall
-    clock including the host set-up of every member."""
+    seeded members (level-0 block counts log-uniform in [min_blocks, max_blocks];
+    rain on fractal terrain, with 0-2 refinement levels when amr, in FP32; and
+    deep-water tsunamis in split precision), each member advanced by `steps` steps.
+    The batched form runs two pools (split and FP32 members), one after the other.
+    Device time of the steps (CUDA events around the graphs) and wall clock
+    including the host set-up of every member."""
     import cases
     from bg_flood_b200.pool import ScenarioPool
-    from runners import make_gpu
     members = [cases.ensemble_member(k, seed, min_blocks, max_blocks) for k in range(nscen)]
-    for c in members:
+    levels = [_member_levels(k, seed, amr) for k in range(nscen)]
+    for k, c in enumerate(members):
         c.param.GPUDEVICE = dev
         c.param.fastmath = fastmath
-        c.param.splitprecision = 1   # FP32 bulk, deviations from FP64 block datums
-    blocks = [(c.nx // 16) * (c.ny // 16) for c in members]
+        c.param.splitprecision = 1 if k % 4 == 3 else 0   # tsunamis: FP32 deviations from FP64 block datums
+    build = lambda k: _build_member(members[k], levels[k])
     # warm-up of both paths on the smallest member
-    small = members[int(np.argmin(blocks))]
-    f, _, lp = make_gpu(small)
+    small = int(np.argmin([(c.nx // 16) * (c.ny // 16) for c in members]))
+    f, lp = build(small)
     f.run(lp, endtime=1e30, maxsteps=4)
     del f
     plain_ms, t0 = 0.0, time.perf_counter()
-    member_ms = []
-    for c in members:
-        f, _, lp = make_gpu(c)
+    member_ms, blocks = [], []
+    for k in range(nscen):
+        f, lp = build(k)
+        blocks.append(f.nblk)
         f.run(lp, endtime=1e30, maxsteps=steps)
         member_ms.append(f.last_run_timing()[0])
         plain_ms += member_ms[-1]
@@ -386,8 +483,8 @@ def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, step
     # the reference's loop structure: one host call per step, the step's dt read back
     # before the next (Mainloop); wall clock of the steps alone, set-up excluded
     step_loop_s = 0.0
-    for c in members:
-        f, _, lp = make_gpu(c)
+    for k in range(nscen):
+        f, lp = build(k)
         lp.totaltime += f.flow_step(lp)
         ts = time.perf_counter()
         for _ in range(steps):
@@ -397,26 +494,32 @@ def ensemble_bench(nscen: int, seed: int, min_blocks: int, max_blocks: int, step
     cells = [256 * b for b in blocks]
     best_member_rate = max(cl * steps / (ms / 1e3) for cl, ms in zip(cells, member_ms))
     t0 = time.perf_counter()
-    pool = ScenarioPool(members[0].param, sum(blocks), nscen)
+    groups = [[k for k in range(nscen) if members[k].param.splitprecision == sp] for sp in (1, 0)]
+    groups = [g for g in groups if g]
+    pools = [ScenarioPool(members[g[0]].param, sum(blocks[k] for k in g), len(g)) for g in groups]
     t1 = time.perf_counter()
     # the members' host set-up in four threads (numpy and the C ABI release the
     # interpreter lock); the plain loop above prepares one member at a time
     from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(4) as ex:
-        built = list(ex.map(make_gpu, members))
+        built = list(ex.map(build, range(nscen)))
     t2 = time.perf_counter()
-    for f, _, lp in built:
-        pool.admit(f, lp, 1e30, maxsteps=steps)
+    for g, pool in zip(groups, pools):
+        for k in g:
+            f, lp = built[k]
+            pool.admit(f, lp, 1e30, maxsteps=steps)
     t3 = time.perf_counter()
-    left = pool.run(steps + 2)
-    batched_ms = pool.timing()[0]
+    batched_ms = 0.0
+    for pool in pools:
+        assert pool.run(steps + 2) == 0
+        batched_ms += pool.timing()[0]
     batched_wall = time.perf_counter() - t0
     phases = {"pool_create_s": t1 - t0, "build_s": t2 - t1, "admit_s": t3 - t2, "run_s": time.perf_counter() - t3}
-    assert left == 0
-    del pool, built
+    del pools, built
     batched_rate = sum(blocks) * 256 * steps / (batched_ms / 1e3)
     acc = ensemble_accuracy(seed, min_blocks, dev, fastmath) if accuracy else None
-    return {"scenarios": nscen, "precision": "FP32 split (deviations from FP64 block datums)",
+    return {"scenarios": nscen, "precision": "tsunamis FP32 split (deviations from FP64 block datums), rain FP32",
+            "members_per_level_count": {str(n + 1): int(sum(1 for x in levels if x == n)) for n in range(3)},
             "accuracy_vs_fp64": acc, "blocks_total": int(sum(blocks)), "blocks_min": int(min(blocks)),
             "blocks_max": int(max(blocks)), "steps_per_scenario": steps,
             "plain_device_ms": plain_ms, "batched_device_ms": batched_ms,
@@ -633,7 +736,7 @@ def main():
         elif args.only == "ensemble":
             r = ensemble_bench(args.ensemble, 2024, 64, args.ens_max_blocks, args.steps, local, args.fastmath)
         elif args.only == "ensemble_small":
-            r = ensemble_bench(args.ensemble, 2025, 40, 512, args.steps, local, args.fastmath, accuracy=False)
+            r = ensemble_bench(args.ensemble, 2025, 40, 512, args.steps, local, args.fastmath, accuracy=False, amr=False)
         else:
             r = serving_bench(args.serve, 7, args.serve_rate, local, args.fastmath)
         print(json.dumps({"measurement": args.only, **r}))
@@ -770,7 +873,8 @@ def main():
             # the small end of the stated member sizes (1e4 to 1.3e5 cells), where one
             # member alone cannot fill the GPU
             extra["ensemble_small_members"] = ensemble_bench(args.ensemble, 2025, 40, 512, 100, local,
-                                                             args.fastmath, accuracy=False, peak_rate=grid_rate)
+                                                             args.fastmath, accuracy=False, peak_rate=grid_rate,
+                                                             amr=False)
         if args.serve > 0:
             extra["serving"] = serving_bench(args.serve, 7, args.serve_rate, local, args.fastmath)
 
@@ -785,6 +889,7 @@ def main():
         extra["accuracy"] = accuracy_vs_fp64(args.n, args.engine, local, args.fastmath)
         if not args.no_extra:
             extra["reference_flowgpu_b200"] = reference_gpu_baseline(args.n, args.engine, 20)
+            extra["accuracy_full_run"] = accuracy_full_run(args.n, args.engine, local, args.fastmath)
 
     if rank == 0:
         line = {

@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--n", type=int, default=1024, help="grid cells per side")
     ap.add_argument("--engine", type=int, default=1)
     ap.add_argument("--fastmath", type=int, default=1, help="1: fast-math kernels, 0: bit-exact kernels")
+    ap.add_argument("--layout", type=int, default=2, help="thread layout of the single-level kernels (profiling runs)")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--only", choices=["amr", "ensemble", "ensemble_small", "serve"], default=None,
                     help="run one secondary measurement alone and print it (profiling runs)")
@@ -743,6 +744,7 @@ def main():
         return
     if args.profile_steps:
         f, mesh, loop = make_gpu(workload_case(args.n, args.engine, local, args.fastmath))
+        f.set_kernel_layout(args.layout)
         for _ in range(args.profile_steps):
             loop.totaltime += f.flow_step(loop)
         print(json.dumps({"profile_steps": args.profile_steps, "totaltime": loop.totaltime}))

@@ -164,6 +164,7 @@ struct bgf_handle {
     int* d_quads = nullptr;  // coarsened quads of an adaptation pass, 4 ids each
     // device table work of bgf_adapt (bgf_adapt_dev.cu): 1 when the mesh allows it
     int adapt_mode = 1;
+    int regular_nbx = 0;          // > 0: single-level mesh that is a full regular grid of blocks
     void* d_adapt = nullptr;      // scratch, carved into adapt::DevAdaptScratch
     int* d_agrids = nullptr;      // per-level block index grids
     long long agrids_cap = 0;
@@ -221,6 +222,7 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.checklev = 0;
     m.datum = h->split ? (const T*)h->d_datum : nullptr;
     m.gen = h->gen;
+    m.regular_nbx = h->amr ? 0 : h->regular_nbx;
     return m;
 }
 
@@ -908,6 +910,25 @@ static int upload_tables(bgf_handle* h)
     if (h->amr && h->split) {
         g_last_error = "split precision supports single-level meshes only";
         return BGF_EINVAL;
+    }
+    // a full regular grid of blocks in row-major ids: the two-cell kernels derive the
+    // ids the tables hold instead of loading them
+    h->regular_nbx = 0;
+    if (!h->amr) {
+        int nbx = 0;
+        for (int k = 0; k < h->nblk && !nbx; k++)
+            if (h->active[k] != k) break;
+            else if (h->nbr[(size_t)2 * nb + k] == k) nbx = k + 1;
+        bool ok = nbx > 0 && h->nblk % nbx == 0;
+        const int nby = ok ? h->nblk / nbx : 0;
+        for (int k = 0; ok && k < h->nblk; k++) {
+            const int bx = k % nbx, by = k / nbx;
+            const int want[4] = {bx > 0 ? k - 1 : k, bx < nbx - 1 ? k + 1 : k, by > 0 ? k - nbx : k,
+                                 by < nby - 1 ? k + nbx : k};
+            ok = h->active[k] == k;
+            for (int q = 0; ok && q < 8; q++) ok = h->nbr[(size_t)q * nb + k] == want[q >> 1];
+        }
+        if (ok) h->regular_nbx = nbx;
     }
     if (h->amr) {
         rc = alloc_amr(h);

@@ -126,6 +126,10 @@ template <class T> struct DevModel {
     int checklev;                     // fused kernels: verify that neighbours share the block's level
     int gen;                          // thread layout of the single-level stage kernels: 1 one cell per
                                       // thread, otherwise two cells per thread (read by the launchers)
+    int regular_nbx;                  // > 0: the mesh is a full regular grid of regular_nbx blocks per
+                                      // row in row-major ids (active[w] == w, neighbours at +-1 and
+                                      // +-regular_nbx, a domain edge its own block); the two-cell
+                                      // kernels then derive ids instead of loading them
 };
 
 // Device ring of gauge samples (bgf_gauge.cu): row k % cap holds, for each of the n

@@ -303,11 +303,24 @@ __device__ __forceinline__ void friction_v(int model, T g, T eps, T dt, V2<T> cf
 
 // ---------------------------------------------------------------- phases
 
-// Ring cell r (0..127) of the tile: source block and cell, as ring_source.
+// Ring cell r (0..127) of the tile: source block and cell, as ring_source.  On a
+// regular grid of blocks the neighbour comes from the block's row and column (the
+// same ids the tables hold) instead of a dependent table load.
 template <class T>
 __device__ __forceinline__ void ring_src2(const DevModel<T>& m, int ib, int r, int& x, int& y, int& sb, int& sx, int& sy)
 {
     ring_pos(r, x, y);
+    if (m.regular_nbx > 0) {
+        const int nbx = m.regular_nbx, bx = ib % nbx, by = ib / nbx, nby = m.nblk / nbx;
+        sb = ib;
+        sx = x;
+        sy = y;
+        if (x < 0) { if (bx > 0) { sb = ib - 1; sx = BW + x; } else sx = 0; }
+        else if (x >= BW) { if (bx < nbx - 1) { sb = ib + 1; sx = x - BW; } else sx = BW - 1; }
+        else if (y < 0) { if (by > 0) { sb = ib - nbx; sy = BW + y; } else sy = 0; }
+        else if (y >= BW) { if (by < nby - 1) { sb = ib + nbx; sy = y - BW; } else sy = BW - 1; }
+        return;
+    }
     if (!tile_source(m.nbr, m.nblkmem, m.level, ib, x, y, sb, sx, sy, m.checklev != 0)) {
         atomicOr(m.err, 1);
         sb = ib; sx = min(max(x, 0), BW - 1); sy = min(max(y, 0), BW - 1);
@@ -628,7 +641,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
     const int py = (w4 & 1) + 4 * (w4 >> 1) + 2 * (lane >> 4);
     const int y = 2 * py;
     for (int w = blockIdx.x; w < m.nblk; w += gridDim.x) {
-        const int ib = m.active[w];
+        const int ib = m.regular_nbx > 0 ? w : m.active[w];
         const int sc = POOL ? m.scen[ib] : 0;
         const TimeState ts = m.time[2 * sc + parity];
         if (!step_live(ts)) continue;
@@ -707,7 +720,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
     const int py = (w4 & 1) + 4 * (w4 >> 1) + 2 * (lane >> 4);
     const int y = 2 * py;
     for (int w = blockIdx.x; w < m.nblk; w += gridDim.x) {
-        const int ib = m.active[w];
+        const int ib = m.regular_nbx > 0 ? w : m.active[w];
         const int sc = POOL ? m.scen[ib] : 0;
         const TimeState ts = m.time[2 * sc + parity];
         const bool lead = POOL ? m.lead[ib] != 0 : w == 0;

@@ -83,8 +83,9 @@ class FloodServer:
         by `builders` background threads while the pool computes, at most `prefetch`
         ahead; they are admitted in the order they become ready.  Each chunk of pool
         steps is enqueued before the host retires the scenarios that finished in
-        the previous chunk (their fields gathered on the pool's copy stream), so
-        retirement overlaps the device work."""
+        the previous chunk (their fields gathered on the pool's copy stream) and
+        admits ready requests (queued behind the chunk), so both overlap the device
+        work."""
         self.gpu_ms = 0.0
         self.host_s = {k: 0.0 for k in self.host_s}
         pending = sorted(requests, key=lambda r: r.arrival)
@@ -143,41 +144,45 @@ class FloodServer:
                                   h if self.keep_fields else None, hmax if self.keep_fields else None, series, status))
             self.host_s["retire"] += time.perf_counter() - tb
 
+        def admit_ready():
+            # arrival order while block and scenario slots allow; with a chunk in
+            # flight the admission is queued behind it and joins the next chunk
+            with lock:
+                while ready:
+                    r, (f, loop) = ready[0]
+                    ta = time.perf_counter()
+                    slot = self.pool.try_admit(f, loop, r.endtime, maxsteps=r.maxsteps)
+                    self.host_s["admit"] += time.perf_counter() - ta
+                    if slot is None:
+                        break
+                    ready.pop(0)
+                    if r.gauges:
+                        self.pool.set_gauges(slot, [(b, c % 16, c // 16) for b, c in r.gauges])
+                    live[slot] = (r, f, now(), [])
+                    lock.notify_all()
+                if errors:
+                    raise RuntimeError(f"request preparation failed: {errors[0]}") from errors[0]
+
         try:
             while len(out) < nreq:
-                # admission in arrival order while block and scenario slots allow (no
-                # pool steps are in flight here)
-                with lock:
-                    while ready:
-                        r, (f, loop) = ready[0]
-                        ta = time.perf_counter()
-                        slot = self.pool.try_admit(f, loop, r.endtime, maxsteps=r.maxsteps)
-                        self.host_s["admit"] += time.perf_counter() - ta
-                        if slot is None:
-                            break
-                        ready.pop(0)
-                        if r.gauges:
-                            self.pool.set_gauges(slot, [(b, c % 16, c // 16) for b, c in r.gauges])
-                        live[slot] = (r, f, now(), [])
-                        lock.notify_all()
-                    if errors:
-                        raise RuntimeError(f"request preparation failed: {errors[0]}") from errors[0]
-                    if not live:
-                        if not any(th.is_alive() for th in ths) and not ready:
-                            raise RuntimeError("request preparation stopped before the stream ended")
-                        lock.wait(0.01)
-                        continue
                 running = len(live) > len(finished)
                 if running:
                     # the next chunk runs on the device while the host retires the
                     # scenarios that finished in the last one (their state is frozen)
+                    # and admits the requests that became ready
                     ta = time.perf_counter()
                     self.pool.run_async(self.chunk)
                     self.host_s["run"] += time.perf_counter() - ta
                 if finished:
                     retire(finished)
                     finished = []
+                admit_ready()
                 if not running:
+                    if not live and len(out) < nreq:
+                        with lock:
+                            if not any(th.is_alive() for th in ths) and not ready:
+                                raise RuntimeError("request preparation stopped before the stream ended")
+                            lock.wait(0.01)
                     continue
                 ta = time.perf_counter()
                 self.pool.wait()

@@ -417,8 +417,10 @@ int bgf_pool_timing(bgf_pool* pool, double* gpu_ms, int64_t* steps, int* free_bl
  * maxsteps (<= 512) pool steps plus a copy of the time slots, then returns;
  * bgf_pool_wait waits for them, refreshes what bgf_pool_query reports, drains the
  * gauge ring, records the device time and writes the scenarios still running.
- * Between the two only bgf_pool_finish may be called (admit, retire, run and
- * get_depth return BGF_ESTATE). */
+ * Between the two, bgf_pool_finish retires finished scenarios, and
+ * bgf_pool_admit and bgf_pool_set_gauges queue new scenarios behind the running
+ * steps (they join the next run; their index lists come from page-locked
+ * staging); retire, run and get_depth return BGF_ESTATE. */
 int bgf_pool_run_async(bgf_pool* pool, int maxsteps);
 int bgf_pool_wait(bgf_pool* pool, int* nlive);
 /* Retirement of n finished scenarios (bgf_pool_query status != 0) for a caller

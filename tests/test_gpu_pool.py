@@ -177,3 +177,28 @@ def test_async_run_and_batched_finish():
     (_, h, _, loop_p, n_p, _), = pool.finish([s], [mesh.nblk])
     assert n_p == n_a and np.array_equal(h, interior(st[1])[: mesh.nblk])
     pool.close()
+
+
+def test_admission_queued_behind_a_running_chunk():
+    """Scenarios admitted (with gauges) while a chunk is in flight join the next
+    chunk and end as they do alone; the running scenario is unaffected."""
+    ref = [alone(mk, n) for mk, n in zip(MIX[:3], [60, 45, 50])]
+    case0 = MIX[0]()
+    pool = ScenarioPool(case0.param, 4096, 8, track_hmax=True)
+    built = [make_gpu(mk()) for mk in MIX[:3]]
+    s0 = pool.admit(built[0][0], built[0][2], ENDTIME, maxsteps=60)
+    pool.run_async(16)
+    s1 = pool.admit(built[1][0], built[1][2], ENDTIME, maxsteps=45)   # queued behind the chunk
+    s2 = pool.admit(built[2][0], built[2][2], ENDTIME, maxsteps=50)
+    pool.set_gauges(s2, [(0, 3, 4)])
+    assert pool.wait() >= 1
+    _, st1, n1 = pool.query(s1)
+    assert st1 == 0 and n1 == 0   # not yet stepped
+    assert pool.run(1000) == 0
+    for s, (st, loop_a, n_a), (f, mesh, _) in zip((s0, s1, s2), ref, built):
+        loop, status, n = pool.query(s)
+        assert n == n_a and loop.totaltime == loop_a.totaltime
+        assert np.array_equal(pool.depth(s, mesh.nblk), interior(st[1])[: mesh.nblk])
+    t, v = pool.read_gauges(s2)
+    assert len(t) == 50
+    pool.close()

@@ -97,6 +97,20 @@ template <class V> __device__ __forceinline__ V cst(typename LaneOf<V>::T x)
 template <class V> __device__ __forceinline__ V minmod_v(V theta, V s0, V s1, V s2)
 {
     using T = typename LaneOf<V>::T;
+#if BGF_FAST
+    if constexpr (sizeof(T) == 4) {
+        // Fast build: the same limiter as a sign test and one three-way minimum of
+        // magnitudes.  s0 < s1 < s2 (or s0 > s1 > s2) holds exactly when the two
+        // one-sided differences have the same strict sign, i.e. when their product is
+        // positive (a product flushed to zero only drops a subnormal slope); the
+        // result is then the candidate of least magnitude with that sign.
+        const V a = sub(s1, s0), b = sub(s2, s1);
+        const V d1 = mul(theta, a), d3 = mul(theta, b);
+        const V d2 = mul(sub(s2, s0), cst<V>((T)0.5));
+        const V m = vmin(vmin(vabs(d1), vabs(d2)), vabs(d3));
+        return sel(gt(mul(a, b), cst<V>((T)0.0)), vcopysign(m, a), cst<V>((T)0.0));
+    }
+#endif
     const auto inc = lt(s0, s1) && lt(s1, s2);
     const auto dec = gt(s0, s1) && gt(s1, s2);
     const V d1 = mul(theta, sub(s1, s0));
@@ -117,6 +131,25 @@ template <class T> __device__ __forceinline__ V2<T> divd_v(V2<T> x, T d, T r)
 #else
     return V2<T>{div_by<T>(x.a, d, r), div_by<T>(x.b, d, r)};
 #endif
+}
+
+// Limited slope minmod2(theta, s0, s1, s2) / delta.  The fast build folds 1 / delta
+// into the limiter's factors (theta / delta and 0.5 / delta) and evaluates the
+// sign-test form of minmod_v, one product fewer per slope.
+template <class V> __device__ __forceinline__ V slope_v(V th, V thr, V hr, V s0, V s1, V s2,
+                                                        typename LaneOf<V>::T delta, typename LaneOf<V>::T rdelta)
+{
+    using T = typename LaneOf<V>::T;
+#if BGF_FAST
+    if constexpr (sizeof(T) == 4) {
+        const V a = sub(s1, s0), b = sub(s2, s1);
+        const V m = vmin(vmin(vabs(mul(thr, a)), vabs(mul(hr, sub(s2, s0)))), vabs(mul(thr, b)));
+        return sel(gt(mul(a, b), cst<V>((T)0.0)), vcopysign(m, a), cst<V>((T)0.0));
+    }
+#endif
+    (void)thr;
+    (void)hr;
+    return divd_v(minmod_v<V>(th, s0, s1, s2), delta, rdelta);
 }
 
 // Wet-slope reset (wetslope)
@@ -159,8 +192,17 @@ __device__ __forceinline__ V hllc_v(V g, V CFLdelta, V epsi, V hm, V hp, V um, V
     const V fup = mul(hp, add(mul(up, up), mul(mul(g, hp), half)));
     const V SLSR = mul(SL, SR);
     const V den = sub(SR, SL);
-    const V fhM = dv(add(sub(mul(SR, fhm), mul(SL, fhp)), mul(SLSR, sub(hp, hm))), den);
-    const V fqM = dv(add(sub(mul(SR, fum), mul(SL, fup)), mul(SLSR, sub(mul(hp, up), mul(hm, um)))), den);
+    const V nh = add(sub(mul(SR, fhm), mul(SL, fhp)), mul(SLSR, sub(hp, hm)));
+    const V nq = add(sub(mul(SR, fum), mul(SL, fup)), mul(SLSR, sub(mul(hp, up), mul(hm, um))));
+#if BGF_FAST
+    // one reciprocal of the wave-speed spread for both star-region fluxes
+    const V rden = dv(cst<V>((T)1.0), den);
+    const V fhM = mul(nh, rden);
+    const V fqM = mul(nq, rden);
+#else
+    const V fhM = dv(nh, den);
+    const V fqM = dv(nq, den);
+#endif
     const auto caseL = le(zero, SL);
     const auto caseR = ge(zero, SR);
     fh = sel(caseL, fhm, sel(caseR, fhp, fhM));
@@ -258,7 +300,7 @@ template <class T>
 __device__ __forceinline__ T edt_lane(T dt, double eps_d, bool forcemass, T hold, T dhi)
 {
 #if BGF_FAST
-    return forcemass ? dt : dhi >= (T)0.0 ? dt : M<T>::fmin_(dt, M<T>::fmax_(hold, (T)eps_d) / M<T>::fabs_(dhi));
+    return forcemass ? dt : dhi >= (T)0.0 ? dt : M<T>::fmin_(dt, dv(M<T>::fmax_(hold, (T)eps_d), M<T>::fabs_(dhi)));
 #else
     return forcemass ? dt : dhi >= (T)0.0 ? dt : (T)fmin((double)dt, fmax((double)hold, eps_d) / (double)M<T>::fabs_(dhi));
 #endif
@@ -284,6 +326,14 @@ __device__ __forceinline__ void advance_v(typename LaneOf<V>::T dt, typename Lan
     vo = sel(wet, dv(mad(hold, vold, mul(edt, dhvi)), ho), cst<V>((T)0.0));
 }
 
+template <class T> __device__ __forceinline__ V2<T> cbrt_v(V2<T> h)
+{
+#if BGF_FAST
+    if constexpr (sizeof(T) == 4) return V2<T>{cbrta(h.a), cbrta(h.b)};
+#endif
+    return V2<T>{M<T>::cbrt_(h.a), M<T>::cbrt_(h.b)};
+}
+
 // bottomfriction (src/Friction.cu:17-143) on a pair; model is uniform.
 template <class T>
 __device__ __forceinline__ void friction_v(int model, T g, T eps, T dt, V2<T> cfv, V2<T> hi, V2<T>& ui, V2<T>& vi)
@@ -292,7 +342,7 @@ __device__ __forceinline__ void friction_v(int model, T g, T eps, T dt, V2<T> cf
     V2<T> cfi;
     if (model == 0) cfi = cfv;
     else if (model == 1) cfi = V2<T>{smartfriction<T>(hi.a, cfv.a), smartfriction<T>(hi.b, cfv.b)};
-    else if (model == -1) cfi = dv(mul(mul(V2<T>{g, g}, cfv), cfv), V2<T>{M<T>::cbrt_(hi.a), M<T>::cbrt_(hi.b)});
+    else if (model == -1) cfi = dv(mul(mul(V2<T>{g, g}, cfv), cfv), cbrt_v<T>(hi));
     else cfi = V2<T>{(T)0.0, (T)0.0};
     const V2<T> tb = mul(dv(mul(cfi, normu), hi), V2<T>{dt, dt});
     const V2<T> den = add(V2<T>{(T)1.0, (T)1.0}, tb);
@@ -367,6 +417,8 @@ __device__ __forceinline__ void gradients2(Smem2<T>& s, const BedGrad<T>& bg, T 
     using V = V2<T>;
     const T rdelta = (T)1.0 / delta;
     const V th = V{theta, theta};
+    const T thr_s = theta * rdelta, hr_s = (T)0.5 * rdelta;
+    const V thr{thr_s, thr_s}, hr{hr_s, hr_s};
     const int ct = p2t(x, 2 * py);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -375,8 +427,8 @@ __device__ __forceinline__ void gradients2(Smem2<T>& s, const BedGrad<T>& bg, T 
         const V xp = ld2<T>(a, ct + 2);
         ym[k] = a[ct - 39];        // (x, 2p-1)
         const T yp = a[ct + 40];   // (x, 2p+2)
-        gxo[k] = divd_v(minmod_v<V>(th, xm[k], c[k], xp), delta, rdelta);
-        gyo[k] = divd_v(minmod_v<V>(th, V{ym[k], c[k].a}, c[k], V{c[k].b, yp}), delta, rdelta);
+        gxo[k] = slope_v<V>(th, thr, hr, xm[k], c[k], xp, delta, rdelta);
+        gyo[k] = slope_v<V>(th, thr, hr, V{ym[k], c[k].a}, c[k], V{c[k].b, yp}, delta, rdelta);
     }
     // ring gradients: ring cell r = tid / 2 (side r / 16, position r % 16), variables
     // h, zs (even tid) or u, v (odd tid); x-gradients on the left / right columns,
@@ -392,7 +444,7 @@ __device__ __forceinline__ void gradients2(Smem2<T>& s, const BedGrad<T>& bg, T 
 #pragma unroll
     for (int j = 0; j < 2; j++) {
         const T* a = s.t[k0 + j];
-        rg[j] = divd_v(minmod_v<T>(theta, a[cm], a[cr], a[cp]), delta, rdelta);
+        rg[j] = slope_v<T>(theta, thr_s, hr_s, a[cm], a[cr], a[cp], delta, rdelta);
     }
     if (ENGINE == 1) {
         const T hd = delta * (T)0.5;

@@ -85,6 +85,31 @@ __device__ __forceinline__ V2<float> mad(V2<float> x, V2<float> y, V2<float> z)
     asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk(x)), "l"(pk(y)), "l"(pk(z)));
     return upk(r);
 }
+// Quotients in the fast build: the numerator times the hardware reciprocal
+// approximation of the denominator (rcp.approx.ftz.f32, at most 1 ulp off, one
+// multi-function-unit instruction), so a pair of quotients costs two reciprocals and
+// one paired product instead of two full-range divisions.  A zero denominator gives
+// an infinite reciprocal, as the division gives an infinite or NaN quotient; every
+// caller selects such a lane away (dry cells, faces with no wave speed).
+__device__ __forceinline__ float rcpa(float y)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
+    return r;
+}
+__device__ __forceinline__ float dv(float x, float y) { return x * rcpa(y); }
+__device__ __forceinline__ V2<float> dv(V2<float> x, V2<float> y) { return mul(x, V2<float>{rcpa(y.a), rcpa(y.b)}); }
+// Cube root for Manning's friction factor: h^(1/3) = 2^(log2(h) / 3) with the
+// hardware base-2 logarithm and exponential approximations (relative error about
+// 1e-7 |log2 h| on the depths of wet cells; h = 0 gives 0).
+__device__ __forceinline__ float cbrta(float h)
+{
+    float l, r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(h));
+    l *= 0.333333343f;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l));
+    return r;
+}
 #else
 __device__ __forceinline__ V2<float> add(V2<float> x, V2<float> y) { return V2<float>{__fadd_rn(x.a, y.a), __fadd_rn(x.b, y.b)}; }
 __device__ __forceinline__ V2<float> sub(V2<float> x, V2<float> y) { return V2<float>{__fsub_rn(x.a, y.a), __fsub_rn(x.b, y.b)}; }
@@ -113,6 +138,15 @@ template <class T> __device__ __forceinline__ V2<T> vmax(V2<T> x, V2<T> y)
     return V2<T>{M<T>::fmax_(x.a, y.a), M<T>::fmax_(x.b, y.b)};
 }
 template <class T> __device__ __forceinline__ V2<T> vabs(V2<T> x) { return V2<T>{M<T>::fabs_(x.a), M<T>::fabs_(x.b)}; }
+template <class T> __device__ __forceinline__ T vcopysign(T x, T y)
+{
+    if constexpr (sizeof(T) == 4) return copysignf(x, y);
+    else return copysign(x, y);
+}
+template <class T> __device__ __forceinline__ V2<T> vcopysign(V2<T> x, V2<T> y)
+{
+    return V2<T>{vcopysign<T>(x.a, y.a), vcopysign<T>(x.b, y.b)};
+}
 template <class T> __device__ __forceinline__ M2 lt(V2<T> x, V2<T> y) { return M2{x.a < y.a, x.b < y.b}; }
 template <class T> __device__ __forceinline__ M2 gt(V2<T> x, V2<T> y) { return M2{x.a > y.a, x.b > y.b}; }
 template <class T> __device__ __forceinline__ M2 ge(V2<T> x, V2<T> y) { return M2{x.a >= y.a, x.b >= y.b}; }

@@ -182,18 +182,19 @@ __device__ __forceinline__ V hllc_v(V g, V CFLdelta, V epsi, V hm, V hp, V um, V
     const V half = cst<V>((T)0.5), zero = cst<V>((T)0.0), two = cst<V>((T)2.0);
     const V cmo = vsqrt(mul(g, hm));
     const V cp = vsqrt(mul(g, hp));
-    const V ustar = sub(add(mul(add(um, up), half), cmo), cp);
-    const V cstar = add(mul(add(cmo, cp), half), mul(sub(um, up), cst<V>((T)0.25)));
-    const V SL = sel(eq(hm, zero), sub(up, mul(two, cp)), vmin(sub(um, cmo), sub(ustar, cstar)));
-    const V SR = sel(eq(hp, zero), add(um, mul(two, cmo)), vmax(add(up, cp), add(ustar, cstar)));
+    const V ustar = sub(mad(add(um, up), half, cmo), cp);
+    const V cstar = mad(add(cmo, cp), half, mul(sub(um, up), cst<V>((T)0.25)));
+    const V SL = sel(eq(hm, zero), mad(cst<V>((T)-2.0), cp, up), vmin(sub(um, cmo), sub(ustar, cstar)));
+    const V SR = sel(eq(hp, zero), mad(two, cmo, um), vmax(add(up, cp), add(ustar, cstar)));
     const V fhm = mul(um, hm);
-    const V fum = mul(hm, add(mul(um, um), mul(mul(g, hm), half)));
+    const V fum = mul(hm, mad(um, um, mul(mul(g, hm), half)));
     const V fhp = mul(up, hp);
-    const V fup = mul(hp, add(mul(up, up), mul(mul(g, hp), half)));
+    const V fup = mul(hp, mad(up, up, mul(mul(g, hp), half)));
     const V SLSR = mul(SL, SR);
     const V den = sub(SR, SL);
-    const V nh = add(sub(mul(SR, fhm), mul(SL, fhp)), mul(SLSR, sub(hp, hm)));
-    const V nq = add(sub(mul(SR, fum), mul(SL, fup)), mul(SLSR, sub(mul(hp, up), mul(hm, um))));
+    const V nSL = mul(cst<V>((T)-1.0), SL);
+    const V nh = mad(SLSR, sub(hp, hm), mad(nSL, fhp, mul(SR, fhm)));
+    const V nq = mad(SLSR, sub(mul(hp, up), mul(hm, um)), mad(nSL, fup, mul(SR, fum)));
 #if BGF_FAST
     // one reciprocal of the wave-speed spread for both star-region fluxes
     const V rden = dv(cst<V>((T)1.0), den);
@@ -229,9 +230,9 @@ __device__ __forceinline__ V kurg_v(V g, V CFLdelta, V epsi, V hp, V hm, V up, V
     const V qp = mul(hp, up);
     const V ga = mul(g, cst<V>((T)0.5));
     const V apm = mul(ap, am);
-    const V fhl = mul(add(sub(mul(ap, qm), mul(am, qp)), mul(apm, sub(hp, hm))), ad);
-    const V ful = mul(add(sub(mul(ap, add(mul(qm, um), mul(ga, mul(hm, hm)))), mul(am, add(mul(qp, up), mul(ga, mul(hp, hp))))),
-                          mul(apm, sub(qp, qm))),
+    const V fhl = mul(mad(apm, sub(hp, hm), sub(mul(ap, qm), mul(am, qp))), ad);
+    const V ful = mul(mad(apm, sub(qp, qm),
+                          sub(mul(ap, mad(qm, um, mul(ga, mul(hm, hm)))), mul(am, mad(qp, up, mul(ga, mul(hp, hp)))))),
                       ad);
     fh = sel(live, fhl, zero);
     fu = sel(live, ful, zero);
@@ -250,25 +251,28 @@ __device__ __forceinline__ FaceOutV<V> face_v(const FaceV<V>& f, V g, V CFLdelta
     V fh, fu, fv, sl, sr;
     if constexpr (ENGINE == 2) {
         const V zi = sub(f.zsi, f.hi);
-        const V zl = sub(zi, mul(dx, sub(f.dzsi, f.dhi)));
+        const V ndx = mul(cst<V>((T)-1.0), dx);
+        const V zl = mad(ndx, sub(f.dzsi, f.dhi), zi);
         const V zn = sub(f.zsn, f.hn);
-        const V zr = add(zn, mul(dx, sub(f.dzsn, f.dhn)));
+        const V zr = mad(dx, sub(f.dzsn, f.dhn), zn);
         const V zlr = vmax(zl, zr);
-        const V hl = sub(f.hi, mul(dx, f.dhi));
-        const V up = sub(f.uni, mul(dx, f.duni));
+        const V hl = mad(ndx, f.dhi, f.hi);
+        const V up = mad(ndx, f.duni, f.uni);
         const V hp = vmax(zero, sub(add(hl, zl), zlr));
-        const V hr = add(f.hn, mul(dx, f.dhn));
-        const V um = add(f.unn, mul(dx, f.dunn));
+        const V hr = mad(dx, f.dhn, f.hn);
+        const V um = mad(dx, f.dunn, f.unn);
         const V hm = vmax(zero, sub(add(hr, zr), zlr));
         r.dt = kurg_v<V>(g, CFLdelta, epsi, hp, hm, up, um, fh, fu);
-        fv = mul(sel(gt(fh, zero), add(f.utn, mul(dx, f.dutn)), sub(f.uti, mul(dx, f.duti))), fh);
-        sl = mul(ga, add(sub(mul(hp, hp), mul(hl, hl)), mul(add(hl, f.hi), sub(zi, zl))));
-        sr = mul(ga, add(sub(mul(hm, hm), mul(hr, hr)), mul(add(hr, f.hn), sub(zn, zr))));
+        fv = mul(sel(gt(fh, zero), mad(dx, f.dutn, f.utn), mad(ndx, f.duti, f.uti)), fh);
+        sl = mul(ga, mad(add(hl, f.hi), sub(zi, zl), sub(mul(hp, hp), mul(hl, hl))));
+        sr = mul(ga, mad(add(hr, f.hn), sub(zn, zr), sub(mul(hm, hm), mul(hr, hr))));
     } else {
-        const V hr = sub(f.hi, mul(dx, f.dhi));
-        const V hl = add(f.hn, mul(dx, f.dhn));
-        const V etar = sub(f.zsi, mul(dx, f.dzsi));
-        const V etal = add(f.zsn, mul(dx, f.dzsn));
+        // products fused into the sums (exact build: separately rounded, the same values)
+        const V ndx = mul(cst<V>((T)-1.0), dx);
+        const V hr = mad(ndx, f.dhi, f.hi);
+        const V hl = mad(dx, f.dhn, f.hn);
+        const V etar = mad(ndx, f.dzsi, f.zsi);
+        const V etal = mad(dx, f.dzsn, f.zsn);
         const V zr = sub(etar, hr);
         const V zl = sub(etal, hl);
         const V zA = vmax(zr, zl);
@@ -276,12 +280,13 @@ __device__ __forceinline__ FaceOutV<V> face_v(const FaceV<V>& f, V g, V CFLdelta
         const V hCNr = vmax(zero, vmin(sub(etar, zCN), hr));
         const V hCNl = vmax(zero, vmin(sub(etal, zCN), hl));
         // Bouchut velocity reconstruction; a dry side keeps the plain slope
-        const V fr = sel(gt(f.hi, eps), mul(add(one, dv(mul(dx, f.dhi), f.hi)), dx), dx);
+        // (nfr is -fr exactly)
+        const V nfr = sel(gt(f.hi, eps), mul(add(one, dv(mul(dx, f.dhi), f.hi)), ndx), ndx);
         const V fl = sel(gt(f.hn, eps), mul(sub(one, dv(mul(dx, f.dhn), f.hn)), dx), dx);
-        const V ur = sub(f.uni, mul(fr, f.duni));
-        const V vr = sub(f.uti, mul(fr, f.duti));
-        const V ul = add(f.unn, mul(fl, f.dunn));
-        const V vl = add(f.utn, mul(fl, f.dutn));
+        const V ur = mad(nfr, f.duni, f.uni);
+        const V vr = mad(nfr, f.duti, f.uti);
+        const V ul = mad(fl, f.dunn, f.unn);
+        const V vl = mad(fl, f.dutn, f.utn);
         r.dt = hllc_v<V>(g, CFLdelta, epsi, hCNl, hCNr, ul, ur, fh, fu);
         fv = mul(sel(gt(fh, zero), vl, vr), fh);
         sl = mul(mul(ga, add(f.hi, hCNr)), sub(f.zbi, zCN));
@@ -669,8 +674,10 @@ __device__ __forceinline__ void divergence2(const Smem2<T>& s, const StepParams<
     const V Fquy_t{Fquy_i.b, s.fy[3][gt2]};
     const V cm{cmdinv, cmdinv}, fc{p.fc, p.fc};
     dh = mul(mul(V{(T)-1.0, (T)-1.0}, sub(add(sub(Fhu_r, Fhu_i), Fhv_t), Fhv_i)), cm);
-    dhu = add(mul(sub(sub(add(Fqux_i, Fquy_i), Su_r), Fquy_t), cm), mul(mul(fc, hi), vvi));
-    dhv = sub(mul(sub(sub(add(Fqvy_i, Fqvx_i), Sv_t), Fqvx_r), cm), mul(mul(fc, hi), uui));
+    // (the Coriolis products fused into the sums; -fc h u is -(fc h u) exactly)
+    const V nfc{-p.fc, -p.fc};
+    dhu = mad(sub(sub(add(Fqux_i, Fquy_i), Su_r), Fquy_t), cm, mul(mul(fc, hi), vvi));
+    dhv = mad(sub(sub(add(Fqvy_i, Fqvx_i), Sv_t), Fqvx_r), cm, mul(mul(nfc, hi), uui));
 }
 
 template <class T> __device__ __forceinline__ V2<T> finite_dt2(V2<T> h, V2<T> u, V2<T> v, V2<T> cdt)

@@ -165,6 +165,8 @@ struct bgf_handle {
     // device table work of bgf_adapt (bgf_adapt_dev.cu): 1 when the mesh allows it
     int adapt_mode = 1;
     int regular_nbx = 0;          // > 0: single-level mesh that is a full regular grid of blocks
+    int regular_nby = 0;
+    unsigned regular_magic = 0;   // multiply-high divisor of block ids by regular_nbx, or 0
     void* d_adapt = nullptr;      // scratch, carved into adapt::DevAdaptScratch
     int* d_agrids = nullptr;      // per-level block index grids
     long long agrids_cap = 0;
@@ -223,6 +225,9 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.datum = h->split ? (const T*)h->d_datum : nullptr;
     m.gen = h->gen;
     m.regular_nbx = h->amr ? 0 : h->regular_nbx;
+    m.regular_nby = h->regular_nby;
+    m.regular_magic = h->regular_magic;
+    m.l2_ahead = 0;
     return m;
 }
 
@@ -291,8 +296,15 @@ template <class T> static StepParams<T> step_params(const bgf_handle* h)
     return p;
 }
 
+// Makes the handle's device current.  A launch error that other code of this host
+// thread left pending (a host program whose own launches go unchecked -- the
+// reference's FlowGPU leaves "invalid configuration argument" pending after a step)
+// is taken off first, so that the check after each of this library's launches
+// reports this library's errors only.  A sticky error (a fault that ended the
+// context) is not cleared by this and fails the call all the same.
 static int set_device(bgf_handle* h)
 {
+    (void)cudaGetLastError();
     BGF_CUDA(cudaSetDevice(h->dev));
     return BGF_OK;
 }
@@ -914,6 +926,8 @@ static int upload_tables(bgf_handle* h)
     // a full regular grid of blocks in row-major ids: the two-cell kernels derive the
     // ids the tables hold instead of loading them
     h->regular_nbx = 0;
+    h->regular_nby = 0;
+    h->regular_magic = 0;
     if (!h->amr) {
         int nbx = 0;
         for (int k = 0; k < h->nblk && !nbx; k++)
@@ -928,7 +942,20 @@ static int upload_tables(bgf_handle* h)
             ok = h->active[k] == k;
             for (int q = 0; ok && q < 8; q++) ok = h->nbr[(size_t)q * nb + k] == want[q >> 1];
         }
-        if (ok) h->regular_nbx = nbx;
+        if (ok) {
+            h->regular_nbx = nbx;
+            h->regular_nby = nby;
+            // block row by = ib / nbx as the high word of ib * ceil(2^32 / nbx), kept only if
+            // it equals the quotient for every block id of this mesh
+            h->regular_magic = 0;
+            if (nbx > 1) {
+                const unsigned mg = (unsigned)((((unsigned long long)1 << 32) + nbx - 1) / nbx);
+                bool exact = true;
+                for (int k = 0; exact && k < h->nblk; k++)
+                    exact = (int)(((unsigned long long)(unsigned)k * mg) >> 32) == k / nbx;
+                if (exact) h->regular_magic = mg;
+            }
+        }
     }
     if (h->amr) {
         rc = alloc_amr(h);

@@ -156,10 +156,11 @@ template <class V> __device__ __forceinline__ V slope_v(V th, V thr, V hr, V s0,
 template <class V>
 __device__ __forceinline__ V wetslope_v(V hdelta, V zsi, V hi, V zsm, V zsp, V dzs, V dh, V dzb)
 {
+    using T = typename LaneOf<V>::T;
     const V base = sub(zsi, hi);
-    const V off = mul(hdelta, sub(dzs, dh));
-    const V mzs = sub(base, off);
-    const V pzs = add(base, off);
+    const V ddz = sub(dzs, dh);
+    const V mzs = mad(mul(cst<V>((T)-1.0), hdelta), ddz, base);  // base - hdelta (dzs - dh)
+    const V pzs = mad(hdelta, ddz, base);
     const auto reset = gt(mul(dzs, dzs), mul(dzb, dzb)) && (gt(mzs, zsm) || gt(pzs, zsp));
     return sel(reset, add(dh, dzb), dzs);
 }
@@ -349,8 +350,7 @@ __device__ __forceinline__ void friction_v(int model, T g, T eps, T dt, V2<T> cf
     else if (model == 1) cfi = V2<T>{smartfriction<T>(hi.a, cfv.a), smartfriction<T>(hi.b, cfv.b)};
     else if (model == -1) cfi = dv(mul(mul(V2<T>{g, g}, cfv), cfv), cbrt_v<T>(hi));
     else cfi = V2<T>{(T)0.0, (T)0.0};
-    const V2<T> tb = mul(dv(mul(cfi, normu), hi), V2<T>{dt, dt});
-    const V2<T> den = add(V2<T>{(T)1.0, (T)1.0}, tb);
+    const V2<T> den = mad(dv(mul(cfi, normu), hi), V2<T>{dt, dt}, V2<T>{(T)1.0, (T)1.0});
     const M2 wet = gt(hi, V2<T>{eps, eps});
     ui = sel(wet, dv(ui, den), ui);
     vi = sel(wet, dv(vi, den), vi);
@@ -366,7 +366,9 @@ __device__ __forceinline__ void ring_src2(const DevModel<T>& m, int ib, int r, i
 {
     ring_pos(r, x, y);
     if (m.regular_nbx > 0) {
-        const int nbx = m.regular_nbx, bx = ib % nbx, by = ib / nbx, nby = m.nblk / nbx;
+        const int nbx = m.regular_nbx, nby = m.regular_nby;
+        const int by = m.regular_magic ? (int)__umulhi((unsigned)ib, m.regular_magic) : ib / nbx;
+        const int bx = ib - by * nbx;
         sb = ib;
         sx = x;
         sy = y;
@@ -382,11 +384,24 @@ __device__ __forceinline__ void ring_src2(const DevModel<T>& m, int ib, int r, i
     }
 }
 
-// bed tile (324 values with halo) into the 18x18 pair layout
+// The bed tile (18 x 18 values with the halo) is kept in shared memory as it lies in
+// global memory, row-major (hi18): it arrives by 16-byte asynchronous copies
+// (cp.async, no registers, no index arithmetic), which each thread waits for with
+// bed_wait before the block's first barrier.  Both addresses are 16-byte aligned:
+// block pieces of the bed are 1296 (FP32) or 2592 (FP64) bytes from a 256-byte
+// aligned allocation, and s.zb starts on a 16-byte boundary of the CTA's shared memory.
 template <class T> __device__ __forceinline__ void load_bed2(Smem2<T>& s, const T* zbt, int tid)
 {
-    for (int k = tid; k < 324; k += NT2) s.zb[p2z(k % 18 - 1, k / 18 - 1)] = zbt[k];
+    static_assert(offsetof(Smem2<T>, zb) % 16 == 0 && (324 * sizeof(T)) % 16 == 0, "bed tile alignment");
+    constexpr int n16 = (int)(324 * sizeof(T) / 16);
+    if (tid < n16) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(s.zb) + 16 * tid);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst),
+                     "l"(reinterpret_cast<const char*>(zbt) + 16 * tid)
+                     : "memory");
+    }
 }
+__device__ __forceinline__ void bed_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Bed gradients the engine-1 wet-slope reset reads: the own pair's x and y values
 // and the one of this thread's ring cell, loaded with the tile (before the barrier).
@@ -494,9 +509,9 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
     V zbc{(T)0, (T)0}, zbx{(T)0, (T)0};
     T zby = (T)0;
     if (ENGINE == 1) {
-        zbc = ld2<T>(s.zb, p2z(x, y));
-        zbx = ld2<T>(s.zb, p2z(x - 1, y));
-        zby = s.zb[p2z(x, y - 1)];
+        zbc = V{s.zb[hi18(x, y)], s.zb[hi18(x, y + 1)]};
+        zbx = V{s.zb[hi18(x - 1, y)], s.zb[hi18(x - 1, y + 1)]};
+        zby = s.zb[hi18(x, y - 1)];
     }
     // X face pair (x-1 | x) at rows y, y+1
     FaceV<V> f;
@@ -541,13 +556,13 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         if (isx) {
             // faces x = 16 at rows 2q, 2q+1: i-side cells (16, .), n-side (15, .)
             ia = p2t(BW, 2 * q); ib2 = ia + 1; na = p2t(BW - 1, 2 * q); nb2 = na + 1;
-            za = p2z(BW, 2 * q); zb2 = za + 1; zna = p2z(BW - 1, 2 * q); znb = zna + 1;
+            za = hi18(BW, 2 * q); zb2 = za + 18; zna = hi18(BW - 1, 2 * q); znb = zna + 18;
             ga2 = p2gx(BW, 2 * q); gb2 = ga2 + 1; gna = p2gx(BW - 1, 2 * q); gnb = gna + 1;
             G[0] = s.gx[VH]; G[1] = s.gx[VZS]; G[2] = s.gx[VU]; G[3] = s.gx[VV];
         } else {
             // faces y = 16 at columns 2q, 2q+1: i-side cells (., 16), n-side (., 15)
             ia = p2t(2 * q, BW); ib2 = p2t(2 * q + 1, BW); na = p2t(2 * q, BW - 1); nb2 = p2t(2 * q + 1, BW - 1);
-            za = p2z(2 * q, BW); zb2 = p2z(2 * q + 1, BW); zna = p2z(2 * q, BW - 1); znb = p2z(2 * q + 1, BW - 1);
+            za = hi18(2 * q, BW); zb2 = za + 1; zna = hi18(2 * q, BW - 1); znb = zna + 1;
             ga2 = p2gy(2 * q, BW); gb2 = p2gy(2 * q + 1, BW); gna = p2gy(2 * q, BW - 1); gnb = p2gy(2 * q + 1, BW - 1);
             G[0] = s.gy[VH]; G[1] = s.gy[VZS]; G[2] = s.gy[VV]; G[3] = s.gy[VU];
         }
@@ -609,8 +624,8 @@ __device__ __forceinline__ void boundaries2(Smem2<T>& s, const DevModel<T>& m, c
     auto H0 = [&](int xx, int yy) -> T { return CORR ? s.h0[p2z(xx, yy)] : s.t[VH][p2t(xx, yy)]; };
     auto U0 = [&](int xx, int yy) -> T { return CORR ? s.u0[p2z(xx, yy)] : s.t[VU][p2t(xx, yy)]; };
     auto W0 = [&](int xx, int yy) -> T { return CORR ? s.v0[p2z(xx, yy)] : s.t[VV][p2t(xx, yy)]; };
-    const T zsi = s.zb[p2z(ix, iy)] + H0(ix, iy);
-    const T zsinside = s.zb[p2z(inx, iny)] + H0(inx, iny);
+    const T zsi = s.zb[hi18(ix, iy)] + H0(ix, iy);
+    const T zsinside = s.zb[hi18(inx, iny)] + H0(inx, iny);
     const T hinside = H0(inx, iny);
     const T uninside = isright != 0 ? U0(inx, iny) : W0(inx, iny);
     const T hface = H0(ix, iy);
@@ -682,8 +697,48 @@ __device__ __forceinline__ void divergence2(const Smem2<T>& s, const StepParams<
 
 template <class T> __device__ __forceinline__ V2<T> finite_dt2(V2<T> h, V2<T> u, V2<T> v, V2<T> cdt)
 {
+#if BGF_FAST
+    if constexpr (sizeof(T) == 4) {
+        // one test per cell: the sum is finite exactly when h, u and v are (a NaN or an
+        // infinity carries through it; finite states are far below the float range)
+        const V2<T> t = add(add(h, u), v);
+        return V2<T>{isfinite(t.a) ? cdt.a : (T)0, isfinite(t.b) ? cdt.b : (T)0};
+    }
+#endif
     return V2<T>{isfinite(h.a) && isfinite(u.a) && isfinite(v.a) ? cdt.a : (T)0,
                  isfinite(h.b) && isfinite(u.b) && isfinite(v.b) ? cdt.b : (T)0};
+}
+
+// L2 prefetch of the inputs of block w + m.l2_ahead: the block a CTA starting about
+// one wave of resident CTAs later (or this CTA's next block, in a grid-stride loop)
+// will read, so that its first loads find the data in L2 instead of waiting on HBM.
+// One bulk prefetch per array piece (cp.async.bulk.prefetch.L2: addresses and sizes are
+// multiples of 16 bytes, the pieces are 256 or 324 values of a 256-byte aligned array).
+// A hint only: it returns nothing and the addresses are those of an existing block.
+// Single scenarios only (a pool's blocks may belong to scenarios on the other state
+// buffer).
+template <class T, int ENGINE, bool CORR>
+__device__ __forceinline__ void prefetch_l2(const DevModel<T>& m, int w, int cur, int tid)
+{
+    constexpr int NP = (CORR ? 6 : 3) + (ENGINE == 1 ? 3 : 1);
+    if (m.l2_ahead <= 0 || tid >= NP) return;
+    const int wn = w + m.l2_ahead;
+    if (wn >= m.nblk) return;
+    const size_t ib = (size_t)(m.regular_nbx > 0 ? wn : m.active[wn]);
+    const T* p;
+    size_t n = 256;
+    if (tid == 0) p = m.h[cur];
+    else if (tid == 1) p = m.u[cur];
+    else if (tid == 2) p = m.v[cur];
+    else if (tid == 3) { p = m.zb; n = 324; }
+    else if (ENGINE == 1 && tid == 4) { p = m.dzbdx; n = 324; }
+    else if (ENGINE == 1 && tid == 5) { p = m.dzbdy; n = 324; }
+    else {
+        const int k = tid - (ENGINE == 1 ? 6 : 4);
+        p = k == 0 ? m.dh : k == 1 ? m.dhu : m.dhv;
+    }
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + ib * n), "r"((unsigned)(n * sizeof(T)))
+                 : "memory");
 }
 
 // ---------------------------------------------------------------- kernels
@@ -711,6 +766,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
         const T* U = m.u[cur];
         const T* Vv = m.v[cur];
         const T* zbt = m.zb + (size_t)ib * 324;
+        if constexpr (!POOL) prefetch_l2<T, ENGINE, false>(m, w, cur, tid);
         // the ring cell's source lookup first (its latency overlaps the pair loads)
         int rx, ry, sb, sx, sy;
         ring_src2<T>(m, ib, tid, rx, ry, sb, sx, sy);
@@ -734,6 +790,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
         for (int k = 0; k < 4; k++) st2<T>(s.t[k], ct, c[k]);
         load_bed2<T>(s, zbt, tid);
         const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
+        bed_wait();
         __syncthreads();
         V xm[4], gxo[4], gyo[4];
         T ym[4];
@@ -799,6 +856,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
         const T* U = m.u[cur];
         const T* Vv = m.v[cur];
         const T* zbt = m.zb + (size_t)ib * 324;
+        if constexpr (!POOL) prefetch_l2<T, ENGINE, true>(m, w, cur, tid);
         int rx, ry, sb, sx, sy;
         ring_src2<T>(m, ib, tid, rx, ry, sb, sx, sy);
         const size_t g0 = (size_t)ib * 256 + y * 16 + x;
@@ -814,7 +872,8 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
         const T rzb = ring2 ? m.zb[(size_t)sb * 324 + hi18(sx, sy)] : zbt[hi18(rx, ry)];
         load_bed2<T>(s, zbt, tid);
         const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
-        __syncthreads();  // s.dtv
+        bed_wait();
+        __syncthreads();  // s.dtv, s.zb
         const T dt = s.dtv;
         const double dtd = (double)dt;
         const T halfdt = dt * (T)0.5;

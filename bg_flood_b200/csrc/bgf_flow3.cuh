@@ -265,9 +265,10 @@ __device__ __forceinline__ T ring_val(const T* S, int v, int r)
     return S[L::rt + v * 32 + ring * 16 + t];
 }
 
+// the bed tile keeps its global (row-major, hi18) layout in Smem2
 template <class T> __device__ __forceinline__ void unpack_bed(Smem2<T>& s, const T* zbt, int tid)
 {
-    for (int k = tid; k < 324; k += NT2) s.zb[p2z(k % 18 - 1, k / 18 - 1)] = zbt[k];
+    for (int k = tid; k < 324; k += NT2) s.zb[k] = zbt[k];
 }
 
 template <class T, int ENGINE, bool POOL>

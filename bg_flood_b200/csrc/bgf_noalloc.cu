@@ -242,6 +242,7 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* a, bgf_loo
         return BGF_EINVAL;
     }
     int caller_dev = 0;
+    (void)cudaGetLastError();  // a launch error other code left pending is not this call's
     if (cudaGetDevice(&caller_dev) != cudaSuccess) return BGF_ECUDA;
     if (cudaSetDevice(p->GPUDEVICE) != cudaSuccess) return BGF_ECUDA;
     unsigned char* sc = nullptr;

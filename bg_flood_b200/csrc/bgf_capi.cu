@@ -227,7 +227,6 @@ template <class T> static DevModel<T> dev_model(bgf_handle* h)
     m.regular_nbx = h->amr ? 0 : h->regular_nbx;
     m.regular_nby = h->regular_nby;
     m.regular_magic = h->regular_magic;
-    m.l2_ahead = 0;
     return m;
 }
 

@@ -387,16 +387,6 @@ template <class T, int ENGINE, bool SPLIT, bool POOL> cudaError_t configure_one(
 
 // Persistent grid of the staged kernels: CTAs resident on all SMs at once (from the
 // occupancy of the kernel at its shared memory), at most one per block.
-// CTAs of kernel k resident on the whole GPU at once: SM count x CTAs per SM.
-template <class KERN> static int resident_ctas(KERN k, int threads, size_t smem)
-{
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, smem) != cudaSuccess || per <= 0) per = 1;
-    return sms * per;
-}
-
 template <class KERN> static int resident_grid(KERN k, size_t smem, int nblk)
 {
     static int sms = 0;
@@ -452,29 +442,13 @@ static void launch_step_kernel(const DevModel<T>& m, const StepParams<T>& p, int
         return;
     }
     if (!split && m.gen != 1) {
-        // two cells per thread; a single scenario's kernels prefetch into L2 the block
-        // that the CTA starting one resident wave later (grid-stride loop: this CTA's
-        // next block) will process
+        // two cells per thread
         if constexpr (FLUX) {
-            if (pool) {
-                flux2_kernel<T, ENGINE, true><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);
-            } else {
-                static int resident = 0;
-                if (!resident) resident = resident_ctas(flux2_kernel<T, ENGINE, false>, NT2, smem2_pred<T>());
-                DevModel<T> mm = m;
-                mm.l2_ahead = g < m.nblk ? g : resident;
-                flux2_kernel<T, ENGINE, false><<<g, NT2, smem2_pred<T>(), st>>>(mm, p, parity);
-            }
+            if (pool) flux2_kernel<T, ENGINE, true><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);
+            else flux2_kernel<T, ENGINE, false><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);
         } else {
-            if (pool) {
-                update2_kernel<T, ENGINE, true><<<g, NT2, smem2_corr<T>(), st>>>(m, p, parity);
-            } else {
-                static int resident = 0;
-                if (!resident) resident = resident_ctas(update2_kernel<T, ENGINE, false>, NT2, smem2_corr<T>());
-                DevModel<T> mm = m;
-                mm.l2_ahead = g < m.nblk ? g : resident;
-                update2_kernel<T, ENGINE, false><<<g, NT2, smem2_corr<T>(), st>>>(mm, p, parity);
-            }
+            if (pool) update2_kernel<T, ENGINE, true><<<g, NT2, smem2_corr<T>(), st>>>(m, p, parity);
+            else update2_kernel<T, ENGINE, false><<<g, NT2, smem2_corr<T>(), st>>>(m, p, parity);
         }
         return;
     }

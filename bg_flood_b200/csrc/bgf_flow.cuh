@@ -133,9 +133,6 @@ template <class T> struct DevModel {
     int regular_nby;                  // rows of that grid (nblk / regular_nbx)
     unsigned regular_magic;           // > 0: ib / regular_nbx == umulhi(ib, regular_magic) for every
                                       // block id (checked on the host), else a division
-    int l2_ahead;                     // > 0: the two-cell kernels prefetch into L2 the inputs of the
-                                      // block this many positions ahead in the block list (set per
-                                      // launch: the CTAs resident at once, or the grid-stride step)
 };
 
 // Device ring of gauge samples (bgf_gauge.cu): row k % cap holds, for each of the n

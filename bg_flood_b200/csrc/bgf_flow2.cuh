@@ -393,11 +393,11 @@ __device__ __forceinline__ void ring_src2(const DevModel<T>& m, int ib, int r, i
 template <class T> __device__ __forceinline__ void load_bed2(Smem2<T>& s, const T* zbt, int tid)
 {
     static_assert(offsetof(Smem2<T>, zb) % 16 == 0 && (324 * sizeof(T)) % 16 == 0, "bed tile alignment");
-    constexpr int n16 = (int)(324 * sizeof(T) / 16);
-    if (tid < n16) {
-        const unsigned dst = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(s.zb) + 16 * tid);
+    constexpr int n16 = (int)(324 * sizeof(T) / 16);  // 81 pieces in FP32, 162 in FP64
+    for (int k = tid; k < n16; k += NT2) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(s.zb) + 16 * k);
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst),
-                     "l"(reinterpret_cast<const char*>(zbt) + 16 * tid)
+                     "l"(reinterpret_cast<const char*>(zbt) + 16 * k)
                      : "memory");
     }
 }
@@ -709,38 +709,6 @@ template <class T> __device__ __forceinline__ V2<T> finite_dt2(V2<T> h, V2<T> u,
                  isfinite(h.b) && isfinite(u.b) && isfinite(v.b) ? cdt.b : (T)0};
 }
 
-// L2 prefetch of the inputs of block w + m.l2_ahead: the block a CTA starting about
-// one wave of resident CTAs later (or this CTA's next block, in a grid-stride loop)
-// will read, so that its first loads find the data in L2 instead of waiting on HBM.
-// One bulk prefetch per array piece (cp.async.bulk.prefetch.L2: addresses and sizes are
-// multiples of 16 bytes, the pieces are 256 or 324 values of a 256-byte aligned array).
-// A hint only: it returns nothing and the addresses are those of an existing block.
-// Single scenarios only (a pool's blocks may belong to scenarios on the other state
-// buffer).
-template <class T, int ENGINE, bool CORR>
-__device__ __forceinline__ void prefetch_l2(const DevModel<T>& m, int w, int cur, int tid)
-{
-    constexpr int NP = (CORR ? 6 : 3) + (ENGINE == 1 ? 3 : 1);
-    if (m.l2_ahead <= 0 || tid >= NP) return;
-    const int wn = w + m.l2_ahead;
-    if (wn >= m.nblk) return;
-    const size_t ib = (size_t)(m.regular_nbx > 0 ? wn : m.active[wn]);
-    const T* p;
-    size_t n = 256;
-    if (tid == 0) p = m.h[cur];
-    else if (tid == 1) p = m.u[cur];
-    else if (tid == 2) p = m.v[cur];
-    else if (tid == 3) { p = m.zb; n = 324; }
-    else if (ENGINE == 1 && tid == 4) { p = m.dzbdx; n = 324; }
-    else if (ENGINE == 1 && tid == 5) { p = m.dzbdy; n = 324; }
-    else {
-        const int k = tid - (ENGINE == 1 ? 6 : 4);
-        p = k == 0 ? m.dh : k == 1 ? m.dhu : m.dhv;
-    }
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + ib * n), "r"((unsigned)(n * sizeof(T)))
-                 : "memory");
-}
-
 // ---------------------------------------------------------------- kernels
 
 template <class T, int ENGINE, bool POOL>
@@ -766,7 +734,6 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
         const T* U = m.u[cur];
         const T* Vv = m.v[cur];
         const T* zbt = m.zb + (size_t)ib * 324;
-        if constexpr (!POOL) prefetch_l2<T, ENGINE, false>(m, w, cur, tid);
         // the ring cell's source lookup first (its latency overlaps the pair loads)
         int rx, ry, sb, sx, sy;
         ring_src2<T>(m, ib, tid, rx, ry, sb, sx, sy);
@@ -856,7 +823,6 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
         const T* U = m.u[cur];
         const T* Vv = m.v[cur];
         const T* zbt = m.zb + (size_t)ib * 324;
-        if constexpr (!POOL) prefetch_l2<T, ENGINE, true>(m, w, cur, tid);
         int rx, ry, sb, sx, sy;
         ring_src2<T>(m, ib, tid, rx, ry, sb, sx, sy);
         const size_t g0 = (size_t)ib * 256 + y * 16 + x;

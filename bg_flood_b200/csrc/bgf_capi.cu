@@ -131,6 +131,11 @@ struct bgf_handle {
     // pinned staging buffer for host <-> device copies of BUQ fields
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // page-locked staging of table uploads (pool rebuilds): while tstage_on, uploads
+    // go through it and are queued without a wait per copy
+    unsigned char* tstage = nullptr;
+    size_t tstage_bytes = 0, tstage_used = 0;
+    bool tstage_on = false;
     // device tile scratch for the layout kernels (pinned caller arrays)
     void* d_tiles = nullptr;
     size_t tiles_bytes = 0;
@@ -440,6 +445,39 @@ static cudaError_t copy_on(cudaStream_t st, void* dst, const void* src, size_t b
 {
     cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
     return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+}
+
+// Host -> device upload of a table.  Normally an asynchronous copy from the
+// caller's (pageable) array, which the driver stages before it returns.  While the
+// handle's table staging is on (a pool rebuild), the bytes are first copied into the
+// handle's page-locked staging area and the copy is queued without any wait: the
+// area is not reused before the stream has passed the copies (staging is reset only
+// on an idle stream, and a full area is replaced only after a synchronisation).
+static cudaError_t upload(bgf_handle* h, void* dst, const void* src, size_t bytes)
+{
+    if (bytes == 0) return cudaSuccess;
+    if (!h->tstage_on) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+    size_t off = (h->tstage_used + 255) & ~(size_t)255;
+    if (off + bytes > h->tstage_bytes) {
+        cudaError_t e = cudaStreamSynchronize(h->stream);  // the copies queued from the old area
+        if (e != cudaSuccess) return e;
+        stage_release(h->tstage, h->tstage_bytes);
+        size_t got = 0;
+        h->tstage = (unsigned char*)stage_acquire(std::max(2 * h->tstage_bytes, bytes), &got);
+        h->tstage_bytes = h->tstage ? got : 0;
+        h->tstage_used = 0;
+        off = 0;
+        if (!h->tstage) return cudaErrorMemoryAllocation;
+    }
+    memcpy(h->tstage + off, src, bytes);
+    h->tstage_used = off + bytes;
+    return cudaMemcpyAsync(dst, h->tstage + off, bytes, cudaMemcpyHostToDevice, h->stream);
+}
+
+// copy_on for host -> device table uploads: queued without a wait while staging is on.
+static cudaError_t upload_on(bgf_handle* h, void* dst, const void* src, size_t bytes)
+{
+    return h->tstage_on ? upload(h, dst, src, bytes) : copy_on(h->stream, dst, src, bytes, cudaMemcpyHostToDevice);
 }
 
 static cudaError_t fill_on(cudaStream_t st, void* p, int value, size_t bytes)
@@ -856,6 +894,7 @@ int bgf_destroy(bgf_handle* h)
     for (int k = 0; k < 3; k++)
         if (h->pev[k]) cudaEventDestroy(h->pev[k]);
     stage_release(h->pinned, h->pinned_bytes);
+    stage_release(h->tstage, h->tstage_bytes);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return BGF_OK;
@@ -902,13 +941,11 @@ static int upload_tables(bgf_handle* h)
     h->ntab = nt;
     // gauge cells name block slots of the previous mesh
     if (h->gauges.n) gauge_free(h, h->gauges);
-    BGF_CUDA(cudaMemcpyAsync(h->d_active, h->active.data(), sizeof(int) * h->nblk, cudaMemcpyHostToDevice, h->stream));
-    BGF_CUDA(cudaMemcpyAsync(h->d_level, h->level.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, h->stream));
-    for (int k = 0; k < 8; k++)
-        BGF_CUDA(cudaMemcpyAsync(h->d_nbr + (size_t)k * nb, h->nbr.data() + (size_t)k * nb, sizeof(int) * nt,
-                                 cudaMemcpyHostToDevice, h->stream));
-    BGF_CUDA(cudaMemcpyAsync(h->d_bxo, h->bxo.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, h->stream));
-    BGF_CUDA(cudaMemcpyAsync(h->d_byo, h->byo.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, h->stream));
+    BGF_CUDA(upload(h, h->d_active, h->active.data(), sizeof(int) * h->nblk));
+    BGF_CUDA(upload(h, h->d_level, h->level.data(), sizeof(int) * nt));
+    for (int k = 0; k < 8; k++) BGF_CUDA(upload(h, h->d_nbr + (size_t)k * nb, h->nbr.data() + (size_t)k * nb, sizeof(int) * nt));
+    BGF_CUDA(upload(h, h->d_bxo, h->bxo.data(), sizeof(double) * nt));
+    BGF_CUDA(upload(h, h->d_byo, h->byo.data(), sizeof(double) * nt));
     // a mesh is multi-level when some active block has a neighbour on another level
     h->amr = false;
     h->minlev = h->maxlev = h->level[h->active[0]];
@@ -961,7 +998,7 @@ static int upload_tables(bgf_handle* h)
         if (rc) return rc;
         std::vector<int> rank(nt, 0);
         for (int ibl = 0; ibl < h->nblk; ibl++) rank[h->active[ibl]] = ibl;
-        BGF_CUDA(cudaMemcpyAsync(h->d_rank, rank.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, h->stream));
+        BGF_CUDA(upload(h, h->d_rank, rank.data(), sizeof(int) * nt));
         // chain: blocks with a side facing another level; pure: the rest, in active order
         std::vector<int> chain, pure;
         for (int ibl = 0; ibl < h->nblk; ibl++) {
@@ -972,15 +1009,11 @@ static int upload_tables(bgf_handle* h)
         }
         h->nchain = (int)chain.size();
         h->npure = (int)pure.size();
-        if (h->nchain)
-            BGF_CUDA(cudaMemcpyAsync(h->d_active_chain, chain.data(), sizeof(int) * h->nchain, cudaMemcpyHostToDevice,
-                                     h->stream));
-        if (h->npure)
-            BGF_CUDA(cudaMemcpyAsync(h->d_active_pure, pure.data(), sizeof(int) * h->npure, cudaMemcpyHostToDevice,
-                                     h->stream));
-        BGF_CUDA(cudaStreamSynchronize(h->stream));
+        if (h->nchain) BGF_CUDA(upload(h, h->d_active_chain, chain.data(), sizeof(int) * h->nchain));
+        if (h->npure) BGF_CUDA(upload(h, h->d_active_pure, pure.data(), sizeof(int) * h->npure));
     }
-    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    // (staged uploads need no wait: their bytes are in the staging area already)
+    if (!h->tstage_on) BGF_CUDA(cudaStreamSynchronize(h->stream));
     h->has_blocks = true;
     free_graphs(h);
     return BGF_OK;
@@ -1125,7 +1158,7 @@ static int rebuild_segments(bgf_handle* h)
     }
     int rc = set_device(h);
     if (rc) return rc;
-    BGF_CUDA(cudaStreamSynchronize(h->stream));
+    if (!h->tstage_on) BGF_CUDA(cudaStreamSynchronize(h->stream));
     // segment buffers only grow (pools rebuild them on every admission)
     size_t ns = std::max<size_t>(1, sd.size()), nser = std::max<size_t>(1, st.size());
     if (ns > h->seg_cap || !h->d_segs) {
@@ -1140,12 +1173,12 @@ static int rebuild_segments(bgf_handle* h)
         BGF_CUDA(dalloc(h, (void**)&h->d_seg_t, h->ser_cap * sizeof(double)));
         BGF_CUDA(dalloc(h, (void**)&h->d_seg_wl, h->ser_cap * sizeof(double)));
     }
-    if (!sd.empty()) BGF_CUDA(copy_on(h->stream, h->d_segs, sd.data(), sd.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
+    if (!sd.empty()) BGF_CUDA(upload_on(h, h->d_segs, sd.data(), sd.size() * sizeof(SegDev)));
     if (!st.empty()) {
-        BGF_CUDA(copy_on(h->stream, h->d_seg_t, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
-        BGF_CUDA(copy_on(h->stream, h->d_seg_wl, swl.data(), swl.size() * sizeof(double), cudaMemcpyHostToDevice));
+        BGF_CUDA(upload_on(h, h->d_seg_t, st.data(), st.size() * sizeof(double)));
+        BGF_CUDA(upload_on(h, h->d_seg_wl, swl.data(), swl.size() * sizeof(double)));
     }
-    BGF_CUDA(copy_on(h->stream, h->d_bndseg, side.data(), side.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BGF_CUDA(upload_on(h, h->d_bndseg, side.data(), side.size() * sizeof(int)));
     h->nseg_dev = (int)sd.size();
     free_graphs(h);
     return BGF_OK;

@@ -71,6 +71,7 @@ SIGNATURES = {
     "bgf_pool_run_async": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "bgf_set_adapt_mode": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "bgf_pool_wait": (ctypes.c_int, [c_void_p, c_int_p]),
+    "bgf_pool_prepare": (ctypes.c_int, [c_void_p]),
     "bgf_pool_finish": (ctypes.c_int, [c_void_p, ctypes.c_int, c_int_p, c_void_p, c_void_p, c_void_p,
                                        ctypes.POINTER(ctypes.c_int64), c_int_p]),
     "bgf_autotune": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_double_p]),

@@ -133,8 +133,13 @@ struct bgf_handle {
     size_t pinned_bytes = 0;
     // page-locked staging of table uploads (pool rebuilds): while tstage_on, uploads
     // go through it and are queued without a wait per copy
-    unsigned char* tstage = nullptr;
-    size_t tstage_bytes = 0, tstage_used = 0;
+    // Two areas used in turn by consecutive rebuilds: a rebuild queued behind a run in
+    // flight (bgf_pool_prepare) must not overwrite the bytes of the previous rebuild's
+    // copies, which may still wait in the stream ahead of that run.
+    unsigned char* tstage[2] = {nullptr, nullptr};
+    size_t tstage_bytes[2] = {0, 0};
+    size_t tstage_used = 0;
+    int tstage_sel = 0;
     bool tstage_on = false;
     // device tile scratch for the layout kernels (pinned caller arrays)
     void* d_tiles = nullptr;
@@ -457,21 +462,30 @@ static cudaError_t upload(bgf_handle* h, void* dst, const void* src, size_t byte
 {
     if (bytes == 0) return cudaSuccess;
     if (!h->tstage_on) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+    const int a = h->tstage_sel;
     size_t off = (h->tstage_used + 255) & ~(size_t)255;
-    if (off + bytes > h->tstage_bytes) {
-        cudaError_t e = cudaStreamSynchronize(h->stream);  // the copies queued from the old area
+    if (off + bytes > h->tstage_bytes[a]) {
+        // a larger area: wait for every copy queued so far, then replace it
+        cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) return e;
-        stage_release(h->tstage, h->tstage_bytes);
+        stage_release(h->tstage[a], h->tstage_bytes[a]);
         size_t got = 0;
-        h->tstage = (unsigned char*)stage_acquire(std::max(2 * h->tstage_bytes, bytes), &got);
-        h->tstage_bytes = h->tstage ? got : 0;
-        h->tstage_used = 0;
+        h->tstage[a] = (unsigned char*)stage_acquire(std::max(2 * h->tstage_bytes[a], bytes), &got);
+        h->tstage_bytes[a] = h->tstage[a] ? got : 0;
         off = 0;
-        if (!h->tstage) return cudaErrorMemoryAllocation;
+        if (!h->tstage[a]) return cudaErrorMemoryAllocation;
     }
-    memcpy(h->tstage + off, src, bytes);
+    memcpy(h->tstage[a] + off, src, bytes);
     h->tstage_used = off + bytes;
-    return cudaMemcpyAsync(dst, h->tstage + off, bytes, cudaMemcpyHostToDevice, h->stream);
+    return cudaMemcpyAsync(dst, h->tstage[a] + off, bytes, cudaMemcpyHostToDevice, h->stream);
+}
+
+// Starts a staged rebuild in the area the previous rebuild did not use.
+static void staging_begin(bgf_handle* h)
+{
+    h->tstage_sel ^= 1;
+    h->tstage_used = 0;
+    h->tstage_on = true;
 }
 
 // copy_on for host -> device table uploads: queued without a wait while staging is on.
@@ -894,7 +908,7 @@ int bgf_destroy(bgf_handle* h)
     for (int k = 0; k < 3; k++)
         if (h->pev[k]) cudaEventDestroy(h->pev[k]);
     stage_release(h->pinned, h->pinned_bytes);
-    stage_release(h->tstage, h->tstage_bytes);
+    for (int k = 0; k < 2; k++) stage_release(h->tstage[k], h->tstage_bytes[k]);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return BGF_OK;

@@ -70,6 +70,12 @@ class ScenarioPool:
         """Enqueues maxsteps (<= 512) pool steps and returns at once; wait() completes them."""
         _check(lib().bgf_pool_run_async(self.handle, int(maxsteps)), "bgf_pool_run_async")
 
+    def prepare(self) -> None:
+        """While a run_async run is in flight: applies the admissions and retirements
+        made since it started to the tables now (uploads queued behind the run), so the
+        next run_async launches at once (bgf_pool_prepare)."""
+        _check(lib().bgf_pool_prepare(self.handle), "bgf_pool_prepare")
+
     def wait(self) -> int:
         """Waits for the steps run_async enqueued; returns the number still running."""
         n = ctypes.c_int(0)

@@ -83,9 +83,10 @@ class FloodServer:
         by `builders` background threads while the pool computes, at most `prefetch`
         ahead; they are admitted in the order they become ready.  Each chunk of pool
         steps is enqueued before the host retires the scenarios that finished in
-        the previous chunk (their fields gathered on the pool's copy stream) and
-        admits ready requests (queued behind the chunk), so both overlap the device
-        work."""
+        the previous chunk (their fields gathered on the pool's copy stream),
+        admits ready requests (queued behind the chunk) and builds the next chunk's
+        tables (their uploads also queued behind the chunk), so all of it overlaps
+        the device work and the next chunk launches as soon as this one ends."""
         self.gpu_ms = 0.0
         self.host_s = {k: 0.0 for k in self.host_s}
         pending = sorted(requests, key=lambda r: r.arrival)
@@ -179,6 +180,11 @@ class FloodServer:
                     retire(finished)
                     finished = []
                 admit_ready()
+                if running:
+                    # the next chunk's tables, built while this chunk runs
+                    ta = time.perf_counter()
+                    self.pool.prepare()
+                    self.host_s["enqueue"] += time.perf_counter() - ta
                 if not running:
                     if not live and len(out) < nreq:
                         with lock:

@@ -423,6 +423,14 @@ int bgf_pool_timing(bgf_pool* pool, double* gpu_ms, int64_t* steps, int* free_bl
  * staging); retire, run and get_depth return BGF_ESTATE. */
 int bgf_pool_run_async(bgf_pool* pool, int maxsteps);
 int bgf_pool_wait(bgf_pool* pool, int* nlive);
+/* While a run from bgf_pool_run_async is in flight: applies the admissions and
+ * retirements made since it started to the pool's tables now, with their uploads
+ * queued behind the run, so that the next bgf_pool_run_async launches at once
+ * instead of rebuilding the tables after the run.  Does nothing with no run in
+ * flight, nothing pending, or gauges set in the pool (the next run then rebuilds).
+ * Admissions and retirements after it are applied by the next run.  No counterpart
+ * in the reference (its loop steps one model). */
+int bgf_pool_prepare(bgf_pool* pool);
 /* Retirement of n finished scenarios (bgf_pool_query status != 0) for a caller
  * that needs only their fields: final depth h and maximum depth hmax (either may
  * be NULL; per scenario an array of nblk * 256 values of the field type in the

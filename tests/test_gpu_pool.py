@@ -130,12 +130,14 @@ def test_pool_with_multilevel_scenarios():
             assert np.array_equal(interior(a), interior(b))
 
 
-def test_async_run_and_batched_finish():
+@pytest.mark.parametrize("prepare", [False, True], ids=["rebuild_at_run", "prepare_behind_run"])
+def test_async_run_and_batched_finish(prepare):
     """Chunks enqueued with run_async while the scenarios that finished in the last
     chunk are retired with finish (fields gathered on the pool's copy stream): every
     scenario's final depth, maximum depth, time and step count equal its run alone,
     a later admission reuses freed slots, and a scenario still running cannot be
-    finished."""
+    finished.  With prepare, the tables after each retirement are rebuilt while the
+    chunk runs (bgf_pool_prepare) instead of by the next run_async."""
     from bg_flood_b200.flow import BGFError
     ref = [alone(mk, n) for mk, n in zip(MIX, BUDGET)]
     case0 = MIX[0]()
@@ -158,6 +160,8 @@ def test_async_run_and_batched_finish():
             finished = []
         if not running:
             continue
+        if prepare:
+            pool.prepare()
         pool.wait()
         for s in slots:
             _, status, _ = pool.query(s)
@@ -176,6 +180,36 @@ def test_async_run_and_batched_finish():
     assert pool.run(1000) == 0
     (_, h, _, loop_p, n_p, _), = pool.finish([s], [mesh.nblk])
     assert n_p == n_a and np.array_equal(h, interior(st[1])[: mesh.nblk])
+    pool.close()
+
+
+def test_admission_prepared_behind_a_running_chunk():
+    """Scenarios admitted while a chunk is in flight, with the next chunk's tables
+    built at once (bgf_pool_prepare, uploads queued behind the chunk): they join
+    the next chunk, which run_async launches without a rebuild, and every scenario
+    ends as it does alone; a second prepare with nothing pending changes nothing."""
+    ref = [alone(mk, n) for mk, n in zip(MIX[:3], [60, 45, 50])]
+    case0 = MIX[0]()
+    pool = ScenarioPool(case0.param, 4096, 8, track_hmax=True)
+    built = [make_gpu(mk()) for mk in MIX[:3]]
+    s0 = pool.admit(built[0][0], built[0][2], ENDTIME, maxsteps=60)
+    pool.run_async(16)
+    s1 = pool.admit(built[1][0], built[1][2], ENDTIME, maxsteps=45)   # queued behind the chunk
+    s2 = pool.admit(built[2][0], built[2][2], ENDTIME, maxsteps=50)
+    pool.prepare()
+    pool.prepare()
+    assert pool.wait() >= 1
+    _, st1, n1 = pool.query(s1)
+    assert st1 == 0 and n1 == 0   # not yet stepped
+    while True:
+        pool.run_async(16)
+        pool.prepare()            # nothing pending: no effect
+        if pool.wait() == 0:
+            break
+    for s, (st, loop_a, n_a), (f, mesh, _) in zip((s0, s1, s2), ref, built):
+        loop, status, n = pool.query(s)
+        assert n == n_a and loop.totaltime == loop_a.totaltime
+        assert np.array_equal(pool.depth(s, mesh.nblk), interior(st[1])[: mesh.nblk])
     pool.close()
 
 

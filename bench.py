@@ -670,10 +670,10 @@ def _serving_at_rate(nreq: int, seed: int, rate: float, dev: int, fastmath: int,
     # separately, not charged to the stream
     ts = time.perf_counter()
     if srv is None:
-        srv = FloodServer(param, budget_gb * 1e9, max_scenarios=64, chunk_steps=32, keep_fields=True)
+        srv = FloodServer(param, budget_gb * 1e9, max_scenarios=64, chunk_steps=64, keep_fields=True)
         # short untimed streams prime what a long-lived process has warm (kernel
         # modules, the memory pool, page-locked staging), for both paths
-        srv.serve(reqs[:4], realtime=False)
+        srv.serve(reqs[:12], realtime=False)
         serve_sequential(reqs[:4], realtime=False)
     startup_s = time.perf_counter() - ts
     for name, fn in (("served", None), ("plain", serve_sequential)):

@@ -369,14 +369,14 @@ template <class T, int ENGINE, bool SPLIT, bool POOL> cudaError_t configure_one(
     cudaError_t e = cudaFuncSetAttribute(flux_kernel<T, ENGINE, SPLIT, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(update_kernel<T, ENGINE, SPLIT, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e != cudaSuccess || SPLIT) return e;
-    // two cells per thread (split precision keeps the one-cell kernels)
-    e = cudaFuncSetAttribute(flux2_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (e != cudaSuccess) return e;
+    // two cells per thread
+    e = cudaFuncSetAttribute(flux2_kernel<T, ENGINE, POOL, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem2_pred<T>());
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(update2_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(update2_kernel<T, ENGINE, POOL, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem2_corr<T>());
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess || SPLIT) return e;  // (the staged layout has no split mode)
     // staged tiles (persistent CTAs with a producer warp)
     e = cudaFuncSetAttribute(flux3_kernel<T, ENGINE, POOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem3_pred<T>());
@@ -441,8 +441,20 @@ static void launch_step_kernel(const DevModel<T>& m, const StepParams<T>& p, int
         }
         return;
     }
-    if (!split && m.gen != 1) {
-        // two cells per thread
+    if (m.gen != 1) {
+        // two cells per thread (split precision too; the staged layout falls back here)
+        if constexpr (sizeof(T) == 4) {
+            if (split) {
+                if constexpr (FLUX) {
+                    if (pool) flux2_kernel<T, ENGINE, true, true><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);
+                    else flux2_kernel<T, ENGINE, false, true><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);
+                } else {
+                    if (pool) update2_kernel<T, ENGINE, true, true><<<g, NT2, smem2_corr<T>(), st>>>(m, p, parity);
+                    else update2_kernel<T, ENGINE, false, true><<<g, NT2, smem2_corr<T>(), st>>>(m, p, parity);
+                }
+                return;
+            }
+        }
         if constexpr (FLUX) {
             if (pool) flux2_kernel<T, ENGINE, true><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);
             else flux2_kernel<T, ENGINE, false><<<g, NT2, smem2_pred<T>(), st>>>(m, p, parity);

@@ -301,6 +301,104 @@ __device__ __forceinline__ FaceOutV<V> face_v(const FaceV<V>& f, V g, V CFLdelta
     return r;
 }
 
+// face_flux_split (bgf_split.cuh) on pairs: split precision, each operation in the
+// scalar routine's order (the exact build reproduces it bit for bit).  The FaceV
+// depths hi, hn are deviations from the block datum D; zsi, zsn surface elevations;
+// zbi, zbn beds as deviations zb + D (engine 1).  Momentum fluxes carry the datum's
+// hydrostatic shift -g D^2 / 2, which a dry face carries alone.
+template <class V, int ENGINE>
+__device__ __forceinline__ FaceOutV<V> face_v_split(const FaceV<V>& f, V D, V g, V CFLdelta, V epsi, V eps, V dx,
+                                                    V ga)
+{
+    using T = typename LaneOf<V>::T;
+    const V zero = cst<V>((T)0.0), one = cst<V>((T)1.0), two = cst<V>((T)2.0), mone = cst<V>((T)-1.0);
+    const V half = cst<V>((T)0.5), quarter = cst<V>((T)0.25);
+    const V nD = mul(mone, D), ndx = mul(mone, dx);
+    const V shift = mul(mul(mul(mone, ga), D), D);  // -ga * D * D
+    FaceOutV<V> r;
+    const V Hi = add(D, f.hi), Hn = add(D, f.hn);  // full depths
+    r.wet = gt(Hi, eps) || gt(Hn, eps);
+    V fh, fu, fv, sl, sr;
+    if constexpr (ENGINE == 2) {
+        const V zi = sub(f.zsi, f.hi);  // bed deviations
+        const V zl = mad(ndx, sub(f.dzsi, f.dhi), zi);
+        const V zn = sub(f.zsn, f.hn);
+        const V zr = mad(dx, sub(f.dzsn, f.dhn), zn);
+        const V zlr = vmax(zl, zr);
+        const V hl = mad(ndx, f.dhi, f.hi);
+        const V up = mad(ndx, f.duni, f.uni);
+        const V hp = vmax(nD, sub(add(hl, zl), zlr));
+        const V hr = mad(dx, f.dhn, f.hn);
+        const V um = mad(dx, f.dunn, f.unn);
+        const V hm = vmax(nD, sub(add(hr, zr), zlr));
+        const V Hp = add(D, hp), Hm = add(D, hm), Hl = add(D, hl), Hr = add(D, hr);
+        const V cp = vsqrt(mul(g, Hp)), cmo = vsqrt(mul(g, Hm));
+        const V ap = vmax(vmax(add(up, cp), add(um, cmo)), zero);
+        const V am = vmin(vmin(sub(up, cp), sub(um, cmo)), zero);
+        const V a = vmax(ap, mul(mone, am));
+        const auto live = gt(a, epsi);
+        const V ad = dv(one, sub(ap, am));
+        const V qm = mul(Hm, um), qp = mul(Hp, up), apm = mul(ap, am);
+        const V pm = mul(mul(ga, hm), mad(two, D, hm)), pp = mul(mul(ga, hp), mad(two, D, hp));
+        const V fhl = mul(mad(apm, sub(hp, hm), sub(mul(ap, qm), mul(am, qp))), ad);
+        const V ful = mul(mad(apm, sub(qp, qm), sub(mul(ap, mad(qm, um, pm)), mul(am, mad(qp, up, pp)))), ad);
+        fh = sel(live, fhl, zero);
+        fu = sel(live, ful, shift);
+        r.dt = sel(live, dv(CFLdelta, a), cst<V>(inv_epsi<T>()));
+        fv = sel(gt(fh, zero), mul(mad(dx, f.dutn, f.utn), fh), mul(mad(ndx, f.duti, f.uti), fh));
+        sl = mul(ga, mad(sub(hp, hl), add(Hp, Hl), mul(add(Hl, Hi), sub(zi, zl))));
+        sr = mul(ga, mad(sub(hm, hr), add(Hm, Hr), mul(add(Hr, Hn), sub(zn, zr))));
+    } else {
+        const V hr = mad(ndx, f.dhi, f.hi);
+        const V hl = mad(dx, f.dhn, f.hn);
+        const V etar = mad(ndx, f.dzsi, f.zsi);
+        const V etal = mad(dx, f.dzsn, f.zsn);
+        const V zr = sub(etar, hr);
+        const V zl = sub(etal, hl);
+        const V zA = vmax(zr, zl);
+        const V zCN = vmin(zA, add(vmin(etal, etar), D));
+        const V hCNr = vmax(nD, vmin(sub(etar, zCN), hr));
+        const V hCNl = vmax(nD, vmin(sub(etal, zCN), hl));
+        // Bouchut velocity reconstruction on the full depths (nfr is -fr exactly)
+        const V nfr = sel(gt(Hi, eps), mul(add(one, dv(mul(dx, f.dhi), Hi)), ndx), ndx);
+        const V fl = sel(gt(Hn, eps), mul(sub(one, dv(mul(dx, f.dhn), Hn)), dx), dx);
+        const V ur = mad(nfr, f.duni, f.uni);
+        const V vr = mad(nfr, f.duti, f.uti);
+        const V ul = mad(fl, f.dunn, f.unn);
+        const V vl = mad(fl, f.dutn, f.utn);
+        // hllc on the reconstructed states, pressures shifted by the datum
+        const V hm = add(D, hCNl), hp = add(D, hCNr), um = ul, up = ur;
+        const V cmo = vsqrt(mul(g, hm)), cp = vsqrt(mul(g, hp));
+        const V ustar = sub(mad(add(um, up), half, cmo), cp);
+        const V cstar = mad(add(cmo, cp), half, mul(sub(um, up), quarter));
+        const V SL = sel(eq(hm, zero), mad(cst<V>((T)-2.0), cp, up), vmin(sub(um, cmo), sub(ustar, cstar)));
+        const V SR = sel(eq(hp, zero), mad(two, cmo, um), vmax(add(up, cp), add(ustar, cstar)));
+        const V fum = mad(mul(hm, um), um, mul(mul(ga, hCNl), mad(two, D, hCNl)));
+        const V fup = mad(mul(hp, up), up, mul(mul(ga, hCNr), mad(two, D, hCNr)));
+        const V fhm = mul(um, hm), fhp = mul(up, hp);
+        const V rs = dv(one, sub(SR, SL));
+        const V SLSR = mul(SL, SR);
+        const V nSL = mul(mone, SL);
+        const V fhM = mul(mad(SLSR, sub(hCNr, hCNl), mad(nSL, fhp, mul(SR, fhm))), rs);
+        const V fqM = mul(mad(SLSR, sub(mul(hp, up), mul(hm, um)), mad(nSL, fup, mul(SR, fum))), rs);
+        const auto caseL = le(zero, SL);
+        const auto caseR = ge(zero, SR);
+        fh = sel(caseL, fhm, sel(caseR, fhp, fhM));
+        fu = sel(caseL, fum, sel(caseR, fup, fqM));
+        const V a = vmax(vabs(SL), vabs(SR));
+        r.dt = sel(gt(a, epsi), dv(CFLdelta, a), cst<V>(inv_epsi<T>()));
+        fv = mul(sel(gt(fh, zero), vl, vr), fh);
+        sl = mul(mul(ga, add(Hi, add(D, hCNr))), sub(f.zbi, zCN));
+        sr = mul(mul(ga, add(add(D, hCNl), Hn)), sub(f.zbn, zCN));
+    }
+    r.Fh = sel(r.wet, fh, zero);
+    r.Fq = sel(r.wet, sub(fu, sl), shift);
+    r.S = sel(r.wet, sub(fu, sr), shift);
+    r.Ft = sel(r.wet, fv, zero);
+    r.dt = sel(r.wet, r.dt, cst<V>(inv_epsi<T>()));
+    return r;
+}
+
 // AdvkernelCPU / AdvkernelGPU (src/Advection.cu:272-385) on pairs.
 template <class T>
 __device__ __forceinline__ T edt_lane(T dt, double eps_d, bool forcemass, T hold, T dhi)
@@ -338,6 +436,26 @@ template <class T> __device__ __forceinline__ V2<T> cbrt_v(V2<T> h)
     if constexpr (sizeof(T) == 4) return V2<T>{cbrta(h.a), cbrta(h.b)};
 #endif
     return V2<T>{M<T>::cbrt_(h.a), M<T>::cbrt_(h.b)};
+}
+
+// advance_split (bgf_split.cuh) on pairs: depths as deviations from the datum D,
+// full depths for the limiter and the velocities.
+template <class T> __device__ __forceinline__ T edt_split_lane(T dt, T eps, bool forcemass, T Hold, T dhi)
+{
+    return forcemass ? dt : dhi >= (T)0.0 ? dt : M<T>::fmin_(dt, dv(M<T>::fmax_(Hold, eps), M<T>::fabs_(dhi)));
+}
+template <class T>
+__device__ __forceinline__ void advance_split_v(T dt, T eps, bool forcemass, V2<T> D, V2<T> hold, V2<T> uold,
+                                                V2<T> vold, V2<T> dhi, V2<T> dhui, V2<T> dhvi, V2<T>& ho, V2<T>& uo,
+                                                V2<T>& vo)
+{
+    const V2<T> Hold = add(D, hold);
+    const V2<T> edt{edt_split_lane<T>(dt, eps, forcemass, Hold.a, dhi.a), edt_split_lane<T>(dt, eps, forcemass, Hold.b, dhi.b)};
+    ho = mad(edt, dhi, hold);
+    const V2<T> Ho = add(D, ho);
+    const M2 wet = gt(Ho, V2<T>{eps, eps});
+    uo = sel(wet, dv(mad(Hold, uold, mul(edt, dhui)), Ho), V2<T>{(T)0.0, (T)0.0});
+    vo = sel(wet, dv(mad(Hold, vold, mul(edt, dhvi)), Ho), V2<T>{(T)0.0, (T)0.0});
 }
 
 // bottomfriction (src/Friction.cu:17-143) on a pair; model is uniform.
@@ -429,10 +547,10 @@ __device__ __forceinline__ BedGrad<T> load_bedgrad(const DevModel<T>& m, int ib,
 // Gradients of the own pair (registers and shared) and two ring gradients per thread,
 // with the engine-1 wet-slope reset.  c holds the pair's h, zs, u, v; xm / ym the
 // left and lower neighbours (kept for the faces).
-template <class T, int ENGINE>
+template <class T, int ENGINE, bool SPLIT = false>
 __device__ __forceinline__ void gradients2(Smem2<T>& s, const BedGrad<T>& bg, T theta, T delta, int tid, int x,
                                            int py, const V2<T> (&c)[4], V2<T> (&xm)[4], T (&ym)[4], V2<T> (&gxo)[4],
-                                           V2<T> (&gyo)[4])
+                                           V2<T> (&gyo)[4], T D = (T)0)
 {
     using V = V2<T>;
     const T rdelta = (T)1.0 / delta;
@@ -472,14 +590,17 @@ __device__ __forceinline__ void gradients2(Smem2<T>& s, const BedGrad<T>& bg, T 
         // lower neighbour twice (WetsloperesetCPU)
         const V zsxp = ld2<T>(s.t[VZS], ct + 2);
         const V zsym{ym[VZS], c[VZS].a};
-        gxo[VZS] = wetslope_v<V>(V{hd, hd}, c[VZS], c[VH], xm[VZS], zsxp, gxo[VZS], gxo[VH], bg.gx);
-        gyo[VZS] = wetslope_v<V>(V{hd, hd}, c[VZS], c[VH], zsym, zsym, gyo[VZS], gyo[VH], bg.gy);
+        // (split precision: the reset tests the full depth D + h')
+        const V hc = SPLIT ? add(V{D, D}, c[VH]) : c[VH];
+        gxo[VZS] = wetslope_v<V>(V{hd, hd}, c[VZS], hc, xm[VZS], zsxp, gxo[VZS], gxo[VH], bg.gx);
+        gyo[VZS] = wetslope_v<V>(V{hd, hd}, c[VZS], hc, zsym, zsym, gyo[VZS], gyo[VH], bg.gy);
         if (k0 == 0) {
             // ring cell: rg[0] = h gradient, rg[1] = zs gradient
             const T* zs = s.t[VZS];
             const T zm = isx ? zs[cr - 2] : zs[cm];
             const T zp = isx ? zs[cr + 2] : zs[cp];
-            rg[1] = wetslope_v<T>(hd, zs[cr], s.t[VH][cr], zm, zp, rg[1], rg[0], bg.ring);
+            const T hr = SPLIT ? D + s.t[VH][cr] : s.t[VH][cr];
+            rg[1] = wetslope_v<T>(hd, zs[cr], hr, zm, zp, rg[1], rg[0], bg.ring);
         }
     }
     T* go = isx ? s.gx[0] : s.gy[0];
@@ -496,10 +617,10 @@ __device__ __forceinline__ void gradients2(Smem2<T>& s, const BedGrad<T>& bg, T 
 // The own pair's X faces (left of each cell) and Y faces (below each cell), and the
 // 16 + 16 faces on the right column and the top row (warp 0, lanes 0..7 X, 8..15 Y).
 // Returns the pair's cell dtmax as the one-cell kernels leave it.
-template <class T, int ENGINE>
+template <class T, int ENGINE, bool SPLIT = false>
 __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T delta, int tid, int x, int py,
                                         const V2<T> (&c)[4], const V2<T> (&xm)[4], const T (&ym)[4],
-                                        const V2<T> (&gxo)[4], const V2<T> (&gyo)[4])
+                                        const V2<T> (&gxo)[4], const V2<T> (&gyo)[4], T D = (T)0)
 {
     using V = V2<T>;
     const V g{p.g, p.g}, epsi{p.epsi, p.epsi}, eps{p.epsface, p.epsface};
@@ -512,7 +633,18 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         zbc = V{s.zb[hi18(x, y)], s.zb[hi18(x, y + 1)]};
         zbx = V{s.zb[hi18(x - 1, y)], s.zb[hi18(x - 1, y + 1)]};
         zby = s.zb[hi18(x, y - 1)];
+        if (SPLIT) {
+            // split precision: beds as deviations zb + D of the block's datum
+            zbc = add(zbc, V{D, D});
+            zbx = add(zbx, V{D, D});
+            zby = zby + D;
+        }
     }
+    const V Dv{D, D};
+    auto face = [&](const FaceV<V>& ff) {
+        if constexpr (SPLIT) return face_v_split<V, ENGINE>(ff, Dv, g, CFLd, epsi, eps, dx, ga);
+        else return face_v<V, ENGINE>(ff, g, CFLd, epsi, eps, dx, ga);
+    };
     // X face pair (x-1 | x) at rows y, y+1
     FaceV<V> f;
     f.hi = c[VH]; f.zsi = c[VZS]; f.uni = c[VU]; f.uti = c[VV];
@@ -524,7 +656,7 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         f.dunn = ld2<T>(s.gx[VU], gn); f.dutn = ld2<T>(s.gx[VV], gn);
     }
     f.zbi = zbc; f.zbn = zbx;
-    const FaceOutV<V> fx = face_v<V, ENGINE>(f, g, CFLd, epsi, eps, dx, ga);
+    const FaceOutV<V> fx = face(f);
     {
         const int o = p2fx(x, y);
         st2<T>(s.fx[0], o, fx.Fh); st2<T>(s.fx[1], o, fx.Fq); st2<T>(s.fx[2], o, fx.S); st2<T>(s.fx[3], o, fx.Ft);
@@ -539,7 +671,7 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         f.dunn = V{s.gy[VV][gn], gyo[VV].a}; f.dutn = V{s.gy[VU][gn], gyo[VU].a};
     }
     f.zbi = zbc; f.zbn = V{zby, zbc.a};
-    const FaceOutV<V> fy = face_v<V, ENGINE>(f, g, CFLd, epsi, eps, dx, ga);
+    const FaceOutV<V> fy = face(f);
     {
         const int o = p2fy(x, y);
         st2<T>(s.fy[0], o, fy.Fh); st2<T>(s.fy[1], o, fy.Fq); st2<T>(s.fy[2], o, fy.S); st2<T>(s.fy[3], o, fy.Ft);
@@ -577,7 +709,11 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         e.duni = V{G[2][ga2], G[2][gb2]}; e.dunn = V{G[2][gna], G[2][gnb]};
         e.duti = V{G[3][ga2], G[3][gb2]}; e.dutn = V{G[3][gna], G[3][gnb]};
         e.zbi = V{s.zb[za], s.zb[zb2]}; e.zbn = V{s.zb[zna], s.zb[znb]};
-        const FaceOutV<V> fe = face_v<V, ENGINE>(e, g, CFLd, epsi, eps, dx, ga);
+        if (SPLIT) {
+            e.zbi = add(e.zbi, Dv);
+            e.zbn = add(e.zbn, Dv);
+        }
+        const FaceOutV<V> fe = face(e);
         if (isx) {
             const int o = p2fx(BW, 2 * q);
             st2<T>(s.fx[0], o, fe.Fh); st2<T>(s.fx[1], o, fe.Fq); st2<T>(s.fx[2], o, fe.S); st2<T>(s.fx[3], o, fe.Ft);
@@ -592,9 +728,9 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
 
 // bndFluxGPUSideCPU (src/Boundary.cu:587-745) on the pair layouts; CORR: state n
 // from the corrector's h0/u0/v0, else from the predictor's tile (which is state n).
-template <class T, bool CORR>
+template <class T, bool CORR, bool SPLIT = false>
 __device__ __forceinline__ void boundaries2(Smem2<T>& s, const DevModel<T>& m, const StepParams<T>& p, int ib,
-                                            double tbnd, int tid)
+                                            double tbnd, int tid, T D = (T)0)
 {
     if (tid >= 64) return;
     const int side = tid >> 4, t = tid & 15;
@@ -624,11 +760,12 @@ __device__ __forceinline__ void boundaries2(Smem2<T>& s, const DevModel<T>& m, c
     auto H0 = [&](int xx, int yy) -> T { return CORR ? s.h0[p2z(xx, yy)] : s.t[VH][p2t(xx, yy)]; };
     auto U0 = [&](int xx, int yy) -> T { return CORR ? s.u0[p2z(xx, yy)] : s.t[VU][p2t(xx, yy)]; };
     auto W0 = [&](int xx, int yy) -> T { return CORR ? s.v0[p2z(xx, yy)] : s.t[VV][p2t(xx, yy)]; };
-    const T zsi = s.zb[hi18(ix, iy)] + H0(ix, iy);
-    const T zsinside = s.zb[hi18(inx, iny)] + H0(inx, iny);
-    const T hinside = H0(inx, iny);
+    // (split precision: beds zb + D and depths D + h'; zs is the surface either way)
+    const T zsi = (SPLIT ? s.zb[hi18(ix, iy)] + D : s.zb[hi18(ix, iy)]) + H0(ix, iy);
+    const T zsinside = (SPLIT ? s.zb[hi18(inx, iny)] + D : s.zb[hi18(inx, iny)]) + H0(inx, iny);
+    const T hinside = SPLIT ? D + H0(inx, iny) : H0(inx, iny);
     const T uninside = isright != 0 ? U0(inx, iny) : W0(inx, iny);
-    const T hface = H0(ix, iy);
+    const T hface = SPLIT ? D + H0(ix, iy) : H0(ix, iy);
     const T zsX = (T)(((double)((T)zsb + (T)0.0) - 0.5 * (double)(zsi + zsinside)) * (double)taper +
                       0.5 * (double)(zsi + zsinside));
     float* qm = m.qmean + ib * 64 + side * 16 + t;
@@ -711,7 +848,7 @@ template <class T> __device__ __forceinline__ V2<T> finite_dt2(V2<T> h, V2<T> u,
 
 // ---------------------------------------------------------------- kernels
 
-template <class T, int ENGINE, bool POOL>
+template <class T, int ENGINE, bool POOL, bool SPLIT = false>
 __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     using V = V2<T>;
@@ -729,6 +866,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
         if (!step_live(ts)) continue;
         const StepParams<T>& p = params_ref<POOL>(m, p0, sc);
         const T delta = calcres<T>(p.delta0, m.level[ib]);
+        const T D = SPLIT ? m.datum[ib] : (T)0;  // split precision: the block's datum
         const int cur = ts.cur;
         const T* H = m.h[cur];
         const T* U = m.u[cur];
@@ -743,14 +881,17 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
         c[VU] = V{U[g0], U[g0 + 16]};
         c[VV] = V{Vv[g0], Vv[g0 + 16]};
         const V zbo{zbt[hi18(x, y)], zbt[hi18(x, y + 1)]};
-        c[VZS] = add(zbo, c[VH]);
+        c[VZS] = SPLIT ? add(add(zbo, V{D, D}), c[VH]) : add(zbo, c[VH]);
         {
             const size_t gr = (size_t)sb * 256 + sy * 16 + sx;
-            const T hv = H[gr];
+            T hv = H[gr];
+            // split precision: a neighbour's deviation in this block's datum (datums are
+            // whole metres, so the difference is exact)
+            if (SPLIT && sb != ib) hv = hv + (m.datum[sb] - D);
             const bool ring2 = rx < -1 || rx > BW || ry < -1 || ry > BW;
             const T zr = ring2 ? m.zb[(size_t)sb * 324 + hi18(sx, sy)] : zbt[hi18(rx, ry)];
             const int o = p2t(rx, ry);
-            s.t[VH][o] = hv; s.t[VU][o] = U[gr]; s.t[VV][o] = Vv[gr]; s.t[VZS][o] = zr + hv;
+            s.t[VH][o] = hv; s.t[VU][o] = U[gr]; s.t[VV][o] = Vv[gr]; s.t[VZS][o] = (SPLIT ? zr + D : zr) + hv;
         }
         const int ct = p2t(x, y);
 #pragma unroll
@@ -761,9 +902,9 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
         __syncthreads();
         V xm[4], gxo[4], gyo[4];
         T ym[4];
-        gradients2<T, ENGINE>(s, bg, p.theta, delta, tid, x, py, c, xm, ym, gxo, gyo);
+        gradients2<T, ENGINE, SPLIT>(s, bg, p.theta, delta, tid, x, py, c, xm, ym, gxo, gyo, D);
         __syncthreads();
-        V cdt = faces2<T, ENGINE>(s, p, delta, tid, x, py, c, xm, ym, gxo, gyo);
+        V cdt = faces2<T, ENGINE, SPLIT>(s, p, delta, tid, x, py, c, xm, ym, gxo, gyo, D);
         cdt = finite_dt2<T>(c[VH], c[VU], c[VV], cdt);
         T v = cdt.b < cdt.a ? cdt.b : cdt.a;
         for (int o = 16; o > 0; o >>= 1) {
@@ -774,7 +915,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
         __syncthreads();
         // boundary segments (FlowbndFlux) after the dt, at t + dt_prev / 2 as FlowCPU does
         if (block_has_segments<T>(m, ib)) {
-            boundaries2<T, false>(s, m, p, ib, ts.totaltime + ts.dt * 0.5, tid);
+            boundaries2<T, false, SPLIT>(s, m, p, ib, ts.totaltime + ts.dt * 0.5, tid, D);
             __syncthreads();
         }
         if (tid == 0) {
@@ -783,7 +924,8 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
             atomicMin(&m.dtmin[2 * sc + parity], dt_bits(b));
         }
         V dh, dhu, dhv;
-        divergence2<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, py, c[VH], c[VU], c[VV], dh, dhu, dhv);
+        divergence2<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, py, SPLIT ? add(V{D, D}, c[VH]) : c[VH], c[VU], c[VV], dh,
+                       dhu, dhv);
         m.dh[g0] = dh.a; m.dh[g0 + 16] = dh.b;
         m.dhu[g0] = dhu.a; m.dhu[g0 + 16] = dhu.b;
         m.dhv[g0] = dhv.a; m.dhv[g0 + 16] = dhv.b;
@@ -791,7 +933,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevM
     }
 }
 
-template <class T, int ENGINE, bool POOL>
+template <class T, int ENGINE, bool POOL, bool SPLIT = false>
 __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     using V = V2<T>;
@@ -818,6 +960,8 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
         const StepParams<T>& p = params_ref<POOL>(m, p0, sc);
         if (tid == 0) s.dtv = step_dt<T>(ts, m.dtmin[2 * sc + parity]);
         const T delta = calcres<T>(p.delta0, m.level[ib]);
+        const T D = SPLIT ? m.datum[ib] : (T)0;  // split precision: the block's datum
+        const V Dv{D, D};
         const int cur = ts.cur;
         const T* H = m.h[cur];
         const T* U = m.u[cur];
@@ -849,16 +993,34 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
             rdh = add_rivers<T>(m, p, sb, sx, sy, rdh, ts.totaltime);
         }
         V c[4];
-        advance_v<V>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, ddh, ddhu, ddhv, c[VH], c[VU], c[VV]);
-        c[VZS] = add(zbo, c[VH]);
+        if constexpr (SPLIT) {
+            advance_split_v<T>(halfdt, p.eps, p.forcemass != 0, Dv, hold, uold, vold, ddh, ddhu, ddhv, c[VH], c[VU],
+                               c[VV]);
+            c[VZS] = add(add(zbo, Dv), c[VH]);
+        } else {
+            advance_v<V>(halfdt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, ddh, ddhu, ddhv, c[VH], c[VU],
+                         c[VV]);
+            c[VZS] = add(zbo, c[VH]);
+        }
         {
-            T ho, uo, vo;
-            advance_v<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, rh, ru, rv, rdh, rdhu, rdhv, ho, uo, vo);
+            T ho, uo, vo, rh0 = rh;
+            if constexpr (SPLIT) {
+                // the source cell's half step in its own datum, then both states in this
+                // block's datum (whole metres: the difference is exact)
+                const T Ds = sb == ib ? D : m.datum[sb];
+                advance_split<T>(halfdt, p.eps, p.forcemass != 0, Ds, rh, ru, rv, rdh, rdhu, rdhv, ho, uo, vo);
+                if (sb != ib) {
+                    rh0 = rh + (m.datum[sb] - D);
+                    ho = ho + (m.datum[sb] - D);
+                }
+            } else {
+                advance_v<T>(halfdt, p.eps, p.eps_d, p.forcemass != 0, rh, ru, rv, rdh, rdhu, rdhv, ho, uo, vo);
+            }
             const int o = p2t(rx, ry);
-            s.t[VH][o] = ho; s.t[VU][o] = uo; s.t[VV][o] = vo; s.t[VZS][o] = rzb + ho;
+            s.t[VH][o] = ho; s.t[VU][o] = uo; s.t[VV][o] = vo; s.t[VZS][o] = (SPLIT ? rzb + D : rzb) + ho;
             if (!ring2) {
                 const int o2 = p2z(rx, ry);
-                s.h0[o2] = rh; s.u0[o2] = ru; s.v0[o2] = rv;
+                s.h0[o2] = rh0; s.u0[o2] = ru; s.v0[o2] = rv;
             }
         }
         const int ct = p2t(x, y);
@@ -871,23 +1033,26 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
         __syncthreads();
         V xm[4], gxo[4], gyo[4];
         T ym[4];
-        gradients2<T, ENGINE>(s, bg, p.theta, delta, tid, x, py, c, xm, ym, gxo, gyo);
+        gradients2<T, ENGINE, SPLIT>(s, bg, p.theta, delta, tid, x, py, c, xm, ym, gxo, gyo, D);
         __syncthreads();
-        (void)faces2<T, ENGINE>(s, p, delta, tid, x, py, c, xm, ym, gxo, gyo);
+        (void)faces2<T, ENGINE, SPLIT>(s, p, delta, tid, x, py, c, xm, ym, gxo, gyo, D);
         __syncthreads();
         if (block_has_segments<T>(m, ib)) {  // interior blocks skip the step and its barrier
-            boundaries2<T, true>(s, m, p, ib, ts.totaltime + dtd, tid);
+            boundaries2<T, true, SPLIT>(s, m, p, ib, ts.totaltime + dtd, tid, D);
             __syncthreads();
         }
         V dh, dhu, dhv;
-        divergence2<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, py, c[VH], c[VU], c[VV], dh, dhu, dhv);
+        divergence2<T>(s, p, (T)1.0 / ((T)1.0 * delta), x, py, SPLIT ? add(Dv, c[VH]) : c[VH], c[VU], c[VV], dh, dhu,
+                       dhv);
         if (p.nriver > 0)
             dh = V{add_rivers<T>(m, p, ib, x, y, dh.a, ts.totaltime), add_rivers<T>(m, p, ib, x, y + 1, dh.b, ts.totaltime)};
         // full step from state n (AdvkernelCPU with evolv), then friction on the result
         V ho, uo, vo;
-        advance_v<V>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+        if constexpr (SPLIT) advance_split_v<T>(dt, p.eps, p.forcemass != 0, Dv, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+        else advance_v<V>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
         const V cfv = p.has_cf ? V{m.cf[g0], m.cf[g0 + 16]} : V{p.cf, p.cf};
-        friction_v<T>(p.frictionmodel, p.g, p.eps, dt, cfv, ho, uo, vo);
+        // (split precision: friction on the full depth; the deviation is not changed by it)
+        friction_v<T>(p.frictionmodel, p.g, p.eps, dt, cfv, SPLIT ? add(Dv, ho) : ho, uo, vo);
         if (p.has_rain) {
             // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): the rain rate at
             // the start of the step, uniform or gridded
@@ -906,9 +1071,9 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
             const T rs = (T)dtd;
             const V rr = dv(dv(Rainhh, V{(T)1000.0, (T)1000.0}), V{(T)3600.0, (T)3600.0});
             Rainhh = mul(vmax(mul(rr, V{rs, rs}), V{(T)0.0, (T)0.0}), mask);
-            const V hi = ho;
+            const V hi = SPLIT ? add(Dv, ho) : ho;
             const V qvol = dv(hi, add(hi, Rainhh));
-            ho = add(hi, Rainhh);
+            ho = add(ho, Rainhh);
             const M2 wet{(double)hi.a > p.eps_d, (double)hi.b > p.eps_d};
             uo = sel(wet, mul(uo, qvol), uo);
             vo = sel(wet, mul(vo, qvol), vo);
@@ -918,8 +1083,9 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
         m.u[nxt][g0] = uo.a; m.u[nxt][g0 + 16] = uo.b;
         m.v[nxt][g0] = vo.a; m.v[nxt][g0 + 16] = vo.b;
         if (m.hmax) {
-            m.hmax[g0] = ho.a > m.hmax[g0] ? ho.a : m.hmax[g0];
-            m.hmax[g0 + 16] = ho.b > m.hmax[g0 + 16] ? ho.b : m.hmax[g0 + 16];
+            const V hf = SPLIT ? add(Dv, ho) : ho;  // the full depth
+            m.hmax[g0] = hf.a > m.hmax[g0] ? hf.a : m.hmax[g0];
+            m.hmax[g0 + 16] = hf.b > m.hmax[g0 + 16] ? hf.b : m.hmax[g0 + 16];
         }
         if (lead && tid == 0)
             m.time[2 * sc + (parity ^ 1)] = next_time_state<T>(ts, p, dtd, nxt, m.dtmin + 2 * sc, parity);

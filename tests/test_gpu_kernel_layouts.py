@@ -120,3 +120,71 @@ def test_layout_rejects_other_values():
     for bad in (0, 4):
         with pytest.raises(BGFError):
             f.set_kernel_layout(bad)
+
+
+# ---------------------------------------------------------------- split precision
+
+def _split(mk):
+    def make():
+        case = mk()
+        case.param.splitprecision = 1
+        return case
+    return make
+
+
+SPLIT_CASES = [
+    ("tsunami3", _split(lambda: cases.ensemble_member(3, 2024, 64, 512)), 40),
+    ("tsunami7", _split(lambda: cases.ensemble_member(7, 2024, 64, 512)), 40),
+    ("island64_e1", _split(lambda: cases.conical_island(64, 1)), 40),
+    ("hump64_e2", _split(lambda: cases.hump_walls(64, 2)), 30),
+    ("rain48_e1", _split(lambda: cases.rain_on_terrain(48, 1)), 30),
+]
+
+
+@pytest.mark.parametrize("name,mk,nsteps", SPLIT_CASES, ids=[c[0] for c in SPLIT_CASES])
+def test_split_layouts_bit_identical_exact(name, mk, nsteps):
+    """Split precision (FP32 deviations from per-block datums) in the two-cell kernels
+    reproduces the one-cell split kernels bit for bit in the exact build: datum
+    conversion of neighbour cells, full depths in the wet tests, the limiter and
+    friction, and the datum's pressure shift."""
+    d1, s1 = _run(mk, 1, 0, nsteps)
+    d2, s2 = _run(mk, 2, 0, nsteps)
+    assert d1 == d2
+    for k, a, b in zip("zs h u v".split(), s1, s2):
+        assert np.array_equal(interior(a), interior(b)), (k, float(np.abs(interior(a) - interior(b)).max()))
+
+
+@pytest.mark.parametrize("name,mk,nsteps", SPLIT_CASES, ids=[c[0] for c in SPLIT_CASES])
+def test_split_layouts_close_fast(name, mk, nsteps):
+    d1, s1 = _run(mk, 1, 1, nsteps)
+    d2, s2 = _run(mk, 2, 1, nsteps)
+    for a, b in zip(d1, d2):
+        assert abs(a - b) <= FAST_DT_RTOL * a
+    for k, a, b in zip("zs h u v".split(), s1, s2):
+        assert float(np.abs(interior(a).astype(np.float64) - interior(b)).max()) <= FAST_TOL, k
+
+
+def test_split_pool_equals_alone():
+    """Two split-precision tsunami members batched in one pool (two-cell kernels,
+    per-block datums in the pool's slots) end exactly as each does alone."""
+    from bg_flood_b200.pool import ScenarioPool
+    mks = [SPLIT_CASES[0][1], SPLIT_CASES[1][1]]
+    ref = []
+    for mk in mks:
+        f, mesh, loop = make_gpu(mk())
+        n = f.run(loop, endtime=1e30, maxsteps=30)
+        ref.append((f.get_state(), loop, n, mesh.nblk))
+    pool = ScenarioPool(mks[0]().param, sum(r[3] for r in ref), 2)
+    slots = []
+    for mk in mks:
+        f, mesh, loop = make_gpu(mk())
+        slots.append((pool.admit(f, loop, 1e30, maxsteps=30), mesh.nblk))
+    assert pool.run(1000) == 0
+    for (s, nblk), (st, loop_a, n_a, _) in zip(slots, ref):
+        loop, status, n = pool.query(s)
+        assert n == n_a == 30 and loop.totaltime == loop_a.totaltime
+        # full depths D + h' (the handle forms the sum in FP64, the pool in FP32: both
+        # round the same exact sum to FP32)
+        got = np.asarray(pool.depth(s, nblk), np.float64).astype(np.float32)
+        assert np.array_equal(got, interior(st[1])[:nblk].astype(np.float32))
+    pool.close()

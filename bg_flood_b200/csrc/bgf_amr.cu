@@ -465,6 +465,14 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::update) amr_update_kernel
     load_tile(tid);
     if (tid >= 240) load_faces(tid + 16);
     if (tid >= 128 && tid < 196) load_tile(tid + 128);
+    // uniform rain: the depth of the step is the same for every cell of the scenario;
+    // one thread evaluates the series (AddrainforcingImplicitCPU) for the block
+    __shared__ T rain_step;
+    if (stage == 1 && p.has_rain && !p.rain_map && tid == 0) {
+        const T r = (T)series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime,
+                                 p.rain_sorted != 0);
+        rain_step = M<T>::fmax_(r / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0);
+    }
     __syncthreads();
     // HaloFluxCPULR / HaloFluxCPUBT (src/Halo.cu:1441-1540, 1766-1850): the faces of
     // a side with finer neighbours take the mean of the two fine faces
@@ -515,16 +523,15 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::update) amr_update_kernel
         // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): the rain rate at the
         // start of the step, uniform or gridded
         T Rainhh;
+        const T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
         if (p.rain_map) {
             const T xc = (T)p.xo_d + (T)m.bxo[ib] + (T)x * delta;
             const T yc = (T)p.yo_d + (T)m.byo[ib] + (T)y * delta;
             Rainhh = rain_map_at<T>(m.rmap, xc, yc, ts.totaltime);
+            Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
         } else {
-            Rainhh = (T)series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime,
-                                  p.rain_sorted != 0);
+            Rainhh = rain_step * mask;
         }
-        const T mask = m.rainmask ? (T)m.rainmask[g] : (T)1;
-        Rainhh = M<T>::fmax_(Rainhh / (T)1000.0 / (T)3600.0 * (T)dtd, (T)0.0) * mask;
         const T hi = ho;
         const T qvol = hi / (hi + Rainhh);
         ho = hi + Rainhh;

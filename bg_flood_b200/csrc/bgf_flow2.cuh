@@ -55,7 +55,7 @@ template <class T> struct Smem2 {
     T fy[4][288];   // Fhv, Fqvy, Sv, Fquy
     T red[NT2 / 32];
     T dtv;          // dt of the step (corrector), evaluated once per block
-    T pad_;
+    T rainv;        // uniform rain depth of the step (corrector), evaluated once per block
     // corrector only (the predictor's launch leaves these out of its shared memory)
     T h0[360], u0[360], v0[360];  // state n on the 18x18 tile (boundary fluxes)
 };
@@ -958,7 +958,18 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
             continue;
         }
         const StepParams<T>& p = params_ref<POOL>(m, p0, sc);
-        if (tid == 0) s.dtv = step_dt<T>(ts, m.dtmin[2 * sc + parity]);
+        if (tid == 0) {
+            const T dt0 = step_dt<T>(ts, m.dtmin[2 * sc + parity]);
+            s.dtv = dt0;
+            if (p.has_rain && !p.rain_map) {
+                // uniform rain (AddrainforcingImplicitCPU, src/Updateforcing.cu:530-580): the
+                // rate at the start of the step and its depth over the step, the same for
+                // every cell of the scenario, once per block instead of once per thread
+                const T r = (T)series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime,
+                                         p.rain_sorted != 0);
+                s.rainv = M<T>::fmax_(dv(dv(r, (T)1000.0), (T)3600.0) * dt0, (T)0.0);
+            }
+        }
         const T delta = calcres<T>(p.delta0, m.level[ib]);
         const T D = SPLIT ? m.datum[ib] : (T)0;  // split precision: the block's datum
         const V Dv{D, D};
@@ -1057,20 +1068,18 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
             // AddrainforcingImplicitCPU (src/Updateforcing.cu:530-580): the rain rate at
             // the start of the step, uniform or gridded
             V Rainhh;
+            const V mask = m.rainmask ? V{(T)m.rainmask[g0], (T)m.rainmask[g0 + 16]} : V{(T)1, (T)1};
             if (p.rain_map) {
                 const T xc = (T)p.xo_d + (T)m.bxo[ib] + (T)x * delta;
                 const T yc0 = (T)p.yo_d + (T)m.byo[ib] + (T)y * delta;
                 const T yc1 = (T)p.yo_d + (T)m.byo[ib] + (T)(y + 1) * delta;
                 Rainhh = V{rain_map_at<T>(m.rmap, xc, yc0, ts.totaltime), rain_map_at<T>(m.rmap, xc, yc1, ts.totaltime)};
+                const T rs = (T)dtd;
+                const V rr = dv(dv(Rainhh, V{(T)1000.0, (T)1000.0}), V{(T)3600.0, (T)3600.0});
+                Rainhh = mul(vmax(mul(rr, V{rs, rs}), V{(T)0.0, (T)0.0}), mask);
             } else {
-                const T r = (T)series_at(m.rain_t + p.rain_off, m.rain_r + p.rain_off, p.rain_n, ts.totaltime,
-                                         p.rain_sorted != 0);
-                Rainhh = V{r, r};
+                Rainhh = mul(V{s.rainv, s.rainv}, mask);  // (the block's uniform depth, above)
             }
-            const V mask = m.rainmask ? V{(T)m.rainmask[g0], (T)m.rainmask[g0 + 16]} : V{(T)1, (T)1};
-            const T rs = (T)dtd;
-            const V rr = dv(dv(Rainhh, V{(T)1000.0, (T)1000.0}), V{(T)3600.0, (T)3600.0});
-            Rainhh = mul(vmax(mul(rr, V{rs, rs}), V{(T)0.0, (T)0.0}), mask);
             const V hi = SPLIT ? add(Dv, ho) : ho;
             const V qvol = dv(hi, add(hi, Rainhh));
             ho = add(ho, Rainhh);

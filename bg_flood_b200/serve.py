@@ -13,6 +13,7 @@ from arrival to retirement."""
 from __future__ import annotations
 
 import sys
+import queue
 import threading
 import time
 from dataclasses import dataclass, field
@@ -121,7 +122,20 @@ class FloodServer:
                     errors.append(e)
                     lock.notify_all()
 
+        # retired handles are released by a closer thread: their destruction (stream,
+        # events, memory back to the pool) stays off the loop that feeds the device
+        closeq: queue.Queue = queue.Queue()
+
+        def closer():
+            while True:
+                f = closeq.get()
+                if f is None:
+                    return
+                f.close()
+
         ths = [threading.Thread(target=builder, daemon=True) for _ in range(max(1, builders))]
+        reaper = threading.Thread(target=closer, daemon=True)
+        reaper.start()
         # the serving loop makes many short calls; a short interpreter switch interval
         # keeps the preparing threads from holding it off the GPU for milliseconds
         switch = sys.getswitchinterval()
@@ -140,7 +154,7 @@ class FloodServer:
             self.host_s["fields"] += tb - ta
             for slot, (f, h, hmax, loop, n, status) in zip(slots, res):
                 r, _, t_adm, series = live.pop(slot)
-                f.close()
+                closeq.put(f)
                 out.append(Result(r.rid, r.arrival, t_adm, now(), n, loop.totaltime,
                                   h if self.keep_fields else None, hmax if self.keep_fields else None, series, status))
             self.host_s["retire"] += time.perf_counter() - tb
@@ -212,6 +226,8 @@ class FloodServer:
                 lock.notify_all()
             for th in ths:
                 th.join(timeout=10)
+            closeq.put(None)
+            reaper.join(timeout=60)
             sys.setswitchinterval(switch)
         return sorted(out, key=lambda x: x.rid)
 

@@ -141,6 +141,7 @@ struct bgf_handle {
     size_t tstage_used = 0;
     int tstage_sel = 0;
     bool tstage_on = false;
+    cudaEvent_t tstage_ev[2] = {nullptr, nullptr};  // recorded after each area's copies
     // device tile scratch for the layout kernels (pinned caller arrays)
     void* d_tiles = nullptr;
     size_t tiles_bytes = 0;
@@ -470,7 +471,7 @@ static cudaError_t upload(bgf_handle* h, void* dst, const void* src, size_t byte
         if (e != cudaSuccess) return e;
         stage_release(h->tstage[a], h->tstage_bytes[a]);
         size_t got = 0;
-        h->tstage[a] = (unsigned char*)stage_acquire(std::max(2 * h->tstage_bytes[a], bytes), &got);
+        h->tstage[a] = (unsigned char*)stage_acquire(std::max(std::max(2 * h->tstage_bytes[a], bytes), (size_t)4 << 20), &got);
         h->tstage_bytes[a] = h->tstage[a] ? got : 0;
         off = 0;
         if (!h->tstage[a]) return cudaErrorMemoryAllocation;
@@ -480,12 +481,40 @@ static cudaError_t upload(bgf_handle* h, void* dst, const void* src, size_t byte
     return cudaMemcpyAsync(dst, h->tstage[a] + off, bytes, cudaMemcpyHostToDevice, h->stream);
 }
 
-// Starts a staged rebuild in the area the previous rebuild did not use.
+// Allocation of a table buffer during a rebuild.  While table staging is on, the
+// buffer is stream-ordered without a wait: it is used only by copies and kernels
+// queued later on the handle's stream, and the buffer it replaces is freed in the
+// same stream order (a rebuild queued behind a run must not wait for that run).
+static cudaError_t dalloc_table(bgf_handle* h, void** p, size_t bytes)
+{
+    if (!h->tstage_on) return dalloc(h, p, bytes);
+    cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
+    if (e == cudaSuccess && debug_fill()) e = cudaMemsetAsync(*p, 0xff, bytes, h->stream);
+    return e;
+}
+
+// Starts a staged rebuild in the area the previous rebuild did not use, once the
+// copies last queued from that area have run (its event; normally long done).
 static void staging_begin(bgf_handle* h)
 {
     h->tstage_sel ^= 1;
+    if (h->tstage_ev[h->tstage_sel]) cudaEventSynchronize(h->tstage_ev[h->tstage_sel]);
     h->tstage_used = 0;
     h->tstage_on = true;
+}
+
+// Ends a staged rebuild: marks the point in the stream after its copies.
+static void staging_end(bgf_handle* h)
+{
+    h->tstage_on = false;
+    cudaEvent_t& ev = h->tstage_ev[h->tstage_sel];
+    if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        ev = nullptr;
+        cudaGetLastError();
+        cudaStreamSynchronize(h->stream);  // no event: wait here instead
+        return;
+    }
+    cudaEventRecord(ev, h->stream);
 }
 
 // copy_on for host -> device table uploads: queued without a wait while staging is on.
@@ -908,7 +937,10 @@ int bgf_destroy(bgf_handle* h)
     for (int k = 0; k < 3; k++)
         if (h->pev[k]) cudaEventDestroy(h->pev[k]);
     stage_release(h->pinned, h->pinned_bytes);
-    for (int k = 0; k < 2; k++) stage_release(h->tstage[k], h->tstage_bytes[k]);
+    for (int k = 0; k < 2; k++) {
+        stage_release(h->tstage[k], h->tstage_bytes[k]);
+        if (h->tstage_ev[k]) cudaEventDestroy(h->tstage_ev[k]);
+    }
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return BGF_OK;
@@ -1178,14 +1210,14 @@ static int rebuild_segments(bgf_handle* h)
     if (ns > h->seg_cap || !h->d_segs) {
         dfree(h, h->d_segs);
         h->seg_cap = std::max(ns, 2 * h->seg_cap);
-        BGF_CUDA(dalloc(h, (void**)&h->d_segs, h->seg_cap * sizeof(SegDev)));
+        BGF_CUDA(dalloc_table(h, (void**)&h->d_segs, h->seg_cap * sizeof(SegDev)));
     }
     if (nser > h->ser_cap || !h->d_seg_t) {
         dfree(h, h->d_seg_t);
         dfree(h, h->d_seg_wl);
         h->ser_cap = std::max(nser, 2 * h->ser_cap);
-        BGF_CUDA(dalloc(h, (void**)&h->d_seg_t, h->ser_cap * sizeof(double)));
-        BGF_CUDA(dalloc(h, (void**)&h->d_seg_wl, h->ser_cap * sizeof(double)));
+        BGF_CUDA(dalloc_table(h, (void**)&h->d_seg_t, h->ser_cap * sizeof(double)));
+        BGF_CUDA(dalloc_table(h, (void**)&h->d_seg_wl, h->ser_cap * sizeof(double)));
     }
     if (!sd.empty()) BGF_CUDA(upload_on(h, h->d_segs, sd.data(), sd.size() * sizeof(SegDev)));
     if (!st.empty()) {

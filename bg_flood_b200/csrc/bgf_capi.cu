@@ -361,7 +361,9 @@ template <class T> static void buq_to(const void* src, int dbl, size_t n, std::v
 // Pinned staging area of at least `bytes` (grown on demand, kept for the handle).
 // Page-locked staging buffers are kept in a process-wide cache by power-of-two size
 // class: handles come and go per scenario when serving, and cudaMallocHost /
-// cudaFreeHost of megabytes cost milliseconds.  The cache holds at most 1 GB.
+// cudaFreeHost cost milliseconds each and synchronise the device; under load a
+// cudaFreeHost was measured holding every CUDA call of the process for up to two
+// seconds.  The cache holds at most 8 GB (only what has been used is kept).
 static std::mutex g_stage_mu;
 static std::vector<std::pair<size_t, void*>> g_stage_free;  // (bytes, buffer)
 static size_t g_stage_cached = 0;
@@ -370,7 +372,7 @@ static void stage_release(void* p, size_t bytes)
 {
     if (!p) return;
     std::lock_guard<std::mutex> lk(g_stage_mu);
-    if (g_stage_cached + bytes > ((size_t)1 << 30)) {
+    if (g_stage_cached + bytes > ((size_t)8 << 30)) {
         cudaFreeHost(p);
         return;
     }

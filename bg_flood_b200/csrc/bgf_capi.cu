@@ -831,9 +831,11 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
     // and destroyed per scenario when serving, and each cudaMalloc / cudaFree costs
     size_t total = 0;
     for (auto& a : allocs) total += (a.bytes + 255) & ~(size_t)255;
-    // stream-ordered allocation from the device's memory pool, which keeps up to 4 GB
-    // of freed memory for reuse instead of returning it to the driver at each
-    // synchronisation (larger releases, e.g. of a pool's slots, still go back)
+    // stream-ordered allocation from the device's memory pool, which keeps all freed
+    // memory for reuse until the process exits instead of returning it to the driver
+    // at synchronisation points: a release unmaps device memory, which waits for the
+    // running kernels and held every CUDA call of a serving process (other threads
+    // creating and destroying scenario handles) for tens of milliseconds to a second
     static std::mutex pool_mu;
     static bool pool_set[64] = {};
     {
@@ -841,7 +843,7 @@ int bgf_create(const bgf_param* p, int nblkmem, void* stream, bgf_handle** out)
         if (!pool_set[h->dev & 63]) {
             cudaMemPool_t mp;
             if (cudaDeviceGetDefaultMemPool(&mp, h->dev) == cudaSuccess) {
-                uint64_t keep = (uint64_t)4 << 30;
+                uint64_t keep = ~(uint64_t)0;
                 cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
             }
             cudaGetLastError();

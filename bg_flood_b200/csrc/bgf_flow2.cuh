@@ -849,7 +849,7 @@ template <class T> __device__ __forceinline__ V2<T> finite_dt2(V2<T> h, V2<T> u,
 // ---------------------------------------------------------------- kernels
 
 template <class T, int ENGINE, bool POOL, bool SPLIT = false>
-__global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 8 : 3) flux2_kernel(DevModel<T> m, StepParams<T> p0, int parity)
+__global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) flux2_kernel(DevModel<T> m, StepParams<T> p0, int parity)
 {
     using V = V2<T>;
     extern __shared__ __align__(16) unsigned char smem_raw2[];

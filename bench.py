@@ -671,10 +671,21 @@ def _serving_at_rate(nreq: int, seed: int, rate: float, dev: int, fastmath: int,
     ts = time.perf_counter()
     if srv is None:
         srv = FloodServer(param, budget_gb * 1e9, max_scenarios=64, chunk_steps=64, keep_fields=True)
-        # short untimed streams prime what a long-lived process has warm (kernel
-        # modules, the memory pool, page-locked staging), for both paths
-        srv.serve(reqs[:12], realtime=False)
-        serve_sequential(reqs[:4], realtime=False)
+        # short untimed streams of other scenarios over the same size range prime what
+        # a long-lived process has warm (kernel modules, the memory pool, page-locked
+        # staging of each size class), for both paths
+        prime = []
+        for k in range(16):
+            pc = cases.ensemble_member(k, seed + 1000, 16, 2048)
+            pc.param.GPUDEVICE = dev
+            pc.param.fastmath = fastmath
+
+            def pbuild(case=pc):
+                f, mesh, loop = make_gpu(case)
+                return f, loop
+            prime.append(Request(1000 + k, 0.0, (pc.nx // 16) * (pc.ny // 16), pbuild, maxsteps=20))
+        srv.serve(prime, realtime=False)
+        serve_sequential(prime[:4], realtime=False)
     startup_s = time.perf_counter() - ts
     for name, fn in (("served", None), ("plain", serve_sequential)):
         t0 = time.perf_counter()

@@ -213,6 +213,31 @@ def test_admission_prepared_behind_a_running_chunk():
     pool.close()
 
 
+def test_three_prepares_behind_one_chunk():
+    """Three admissions while one chunk is in flight, each followed by
+    bgf_pool_prepare: three table rebuilds queued behind the same chunk, so the third
+    reuses the staging area of the first before any wait (its copies must have run
+    first).  Every scenario still ends as it does alone."""
+    steps = [60, 45, 50, 35]
+    ref = [alone(mk, n) for mk, n in zip(MIX[:4], steps)]
+    pool = ScenarioPool(MIX[0]().param, 4096, 8)
+    built = [make_gpu(mk()) for mk in MIX[:4]]
+    slots = [pool.admit(built[0][0], built[0][2], ENDTIME, maxsteps=steps[0])]
+    pool.run_async(16)
+    for k in (1, 2, 3):
+        slots.append(pool.admit(built[k][0], built[k][2], ENDTIME, maxsteps=steps[k]))
+        pool.prepare()
+    while True:
+        if pool.wait() == 0:
+            break
+        pool.run_async(16)
+    for s, (st, loop_a, n_a), (f, mesh, _) in zip(slots, ref, built):
+        loop, status, n = pool.query(s)
+        assert n == n_a and loop.totaltime == loop_a.totaltime
+        assert np.array_equal(pool.depth(s, mesh.nblk), interior(st[1])[: mesh.nblk])
+    pool.close()
+
+
 def test_admission_queued_behind_a_running_chunk():
     """Scenarios admitted (with gauges) while a chunk is in flight join the next
     chunk and end as they do alone; the running scenario is unaffected."""

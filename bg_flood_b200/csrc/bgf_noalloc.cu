@@ -18,6 +18,7 @@
 // reference's qmean carries from step to step (src/Boundary.cu:481-537); they are
 // cleared at the first set-up on a device and when the caller asks (reset_means).
 #include <cuda_runtime.h>
+#include <stdint.h>
 #include <string.h>
 
 #include <mutex>
@@ -236,6 +237,11 @@ int bgf_flow_step_noalloc(const bgf_param* p, const bgf_noalloc_args* a, bgf_loo
         !a->h_out || !a->u_out || !a->v_out)
         return BGF_EINVAL;
     if (p->engine == 1 && (!a->dzbdx || !a->dzbdy)) return BGF_EINVAL;
+    // the kernels copy each block's bed tile into shared memory in 16-byte pieces
+    if (((uintptr_t)a->zb & 15) != 0) {
+        bgf::set_last_error("zb must be 16-byte aligned (as cudaMalloc returns it)");
+        return BGF_EINVAL;
+    }
     if (p->frictionmodel != 0 && p->frictionmodel != -1 && p->frictionmodel != 1) return BGF_EINVAL;
     if (p->splitprecision || p->conserveElevation) {
         bgf::set_last_error("the allocation-free step takes neither split precision nor conserveElevation");

@@ -269,6 +269,8 @@ int bgf_run_timing(bgf_handle* h, double* gpu_ms, int64_t* launches);
  *   with a neighbour; time series are not taken.
  * - active must hold nblk distinct ids < nblkmem and nbr ids < nblkmem: the
  *   kernels index with them unchecked.
+ * - zb must start on a 16-byte boundary (any cudaMalloc result does): the bed
+ *   tiles are copied in 16-byte pieces; BGF_EINVAL otherwise.
  * State layout here is the kernels' own: 256 values per block slot, cell
  * (i, j) at j * 16 + i; the output arrays must not alias the inputs.
  * Synchronises `stream` (dt is returned to the host, as bgf_flow_step does). */

@@ -123,3 +123,31 @@ def test_param_reader_follows_reference_rules():
     assert p.segments[0].side == "left" and p.segments[0].type == 2
     assert read_param_text("engine = 2").engine == 2
     assert read_param_text("engine = 9").engine == 5
+
+
+def test_noalloc_rejects_a_misaligned_bed():
+    """The allocation-free step copies bed tiles in 16-byte pieces: a bed pointer off
+    a 16-byte boundary is refused with BGF_EINVAL before any device work (so this
+    runs without a GPU; the other pointers are never dereferenced)."""
+    import ctypes
+    import cases
+    from bg_flood_b200._native import lib
+    from bg_flood_b200.flow import Loop
+
+    class NoallocArgs(ctypes.Structure):
+        _fields_ = [("nblk", ctypes.c_int), ("nblkmem", ctypes.c_int)] + \
+            [(n, ctypes.c_void_p) for n in ("active", "level", "nbr", "bndtype", "zb", "dzbdx", "dzbdy",
+                                            "h_in", "u_in", "v_in", "h_out", "u_out", "v_out")] + \
+            [("reset_means", ctypes.c_int)]
+
+    a = NoallocArgs()
+    a.nblk = a.nblkmem = 9
+    for k in ("active", "level", "nbr", "bndtype", "dzbdx", "dzbdy", "h_in", "u_in", "v_in",
+              "h_out", "u_out", "v_out"):
+        setattr(a, k, 0x10000)
+    a.zb = 0x10004
+    p = cases.gauss(48, 1, 3).param.to_c()
+    c = Loop().to_c()
+    rc = lib().bgf_flow_step_noalloc(ctypes.byref(p), ctypes.byref(a), ctypes.byref(c), None)
+    assert rc == 1, rc  # BGF_EINVAL
+    assert b"16-byte" in lib().bgf_last_error()

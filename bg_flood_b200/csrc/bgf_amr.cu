@@ -39,6 +39,8 @@ namespace bgf {
 namespace BGF_VARIANT {
 
 #include "bgf_stage.cuh"
+#include "bgf_pair.cuh"
+#include "bgf_flow2.cuh"
 
 __device__ __forceinline__ bool has_coarser_side(const int* nbr, int nbm, const int* lv, int ib)
 {
@@ -413,6 +415,127 @@ __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::flux) amr_flux_kernel(Dev
     }
 }
 
+// amr_flux_kernel in the two-cells-per-thread layout of the single-level kernels
+// (bgf_flow2.cuh): 128 threads per block, thread (x, p) owning cells (x, 2p) and
+// (x, 2p+1).  The tile comes from the stage tile W (interior and ring 1, whose
+// halos the chain filled) and the outer ring rules (ring 2); gradients, wet-slope
+// reset and faces are the single-level kernels' own, with the coarse/fine source
+// substitution on the sides whose neighbour is coarser.  The faces go to the stage
+// face arrays in the layout amr_update_kernel reads.  The same operations in the
+// same order as amr_flux_kernel: the exact build gives the same faces and dt.
+template <class T, int ENGINE>
+__global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 6 : 3) amr_flux2_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0,
+                                                                            int parity, int stage)
+{
+    using V = V2<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw2[];
+    Smem2<T>& s = *reinterpret_cast<Smem2<T>*>(smem_raw2);
+    __shared__ SubFaces<T> sub;
+    const int tid = threadIdx.x;
+    const int w4 = tid >> 5, lane = tid & 31;
+    const int x = lane & 15;
+    const int py = (w4 & 1) + 4 * (w4 >> 1) + 2 * (lane >> 4);
+    const int y = 2 * py;
+    const int ib = m.active[blockIdx.x];
+    const int sc = scen_of(m, ib);
+    const TimeState ts = m.time[2 * sc + parity];
+    if (!step_live(ts)) return;
+    const StepParams<T>& p = m.sparams ? m.sparams[sc] : p0;
+    const int nbm = m.nblkmem;
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    T* const* W = a.W[stage];
+    const size_t base = (size_t)ib * 324;
+    const T* zbt = m.zb + base;
+    // the own pair from the stage tile
+    V c[4];
+#pragma unroll
+    for (int v = 0; v < 4; v++) c[v] = V{W[v][base + hi18(x, y)], W[v][base + hi18(x, y + 1)]};
+    if (tid < 64) {
+        // ring 1 (the block's halo, corners excluded) and the coarse/fine substitution
+        const int sd = tid >> 4, t = tid & 15;
+        int hx, hy;
+        halo_xy(sd, t, hx, hy);
+        const int c18 = hi18(hx, hy), o = p2t(hx, hy);
+#pragma unroll
+        for (int v = 0; v < 4; v++) s.t[v][o] = W[v][base + c18];
+        int pb, px, pyy;
+        const bool coarse = parent_cell(m.nbr, nbm, m.level, ib, sd, t, pb, px, pyy);
+        if (t == 0) sub.on[sd] = coarse ? 1 : 0;
+        if (coarse) {
+            sub.h[sd][t] = W[0][(size_t)pb * 324 + hi18(px, pyy)];
+            sub.z[sd][t] = a.zb[(size_t)pb * 324 + hi18(px, pyy)];
+        }
+    } else {
+        // ring 2: the outer stencil values of the halo gradients
+        const int k = tid - 64;
+        const int sd = k >> 4, t = k & 15;
+        const CellRule<T> r = outer_rule<T>(m.nbr, nbm, m.level, ib, sd, t);
+        int rx, ry;
+        halo_xy(sd, t, rx, ry);
+        if (sd == 0) rx = -2;
+        else if (sd == 1) rx = BW + 1;
+        else if (sd == 2) ry = -2;
+        else ry = BW + 1;
+        const int o = p2t(rx, ry);
+        if (r.kind == 3) {
+            // inside a coarser neighbour's 2x2 patch (see amr_flux_kernel)
+#pragma unroll
+            for (int v = 0; v < 4; v++) s.t[v][o] = rule_eval(r, Acc324<T>{W[v]});
+        } else {
+            const T halfdt = stage == 0 ? (T)0 : step_dt<T>(ts, m.dtmin[2 * sc + parity]) * (T)0.5;
+            const StageState<T> S{m, p, ts.cur, stage != 0, halfdt, ts.totaltime};
+            T cv[4][4];  // per rule cell: h, zs, u, v
+            const int nc = r.kind == 0 ? 1 : 4;
+            for (int q = 0; q < nc; q++) {
+                S.get(r.b[q], r.x[q], r.y[q], cv[q][0], cv[q][2], cv[q][3]);
+                cv[q][1] = a.zb[(size_t)r.b[q] * 324 + hi18(r.x[q], r.y[q])] + cv[q][0];
+            }
+#pragma unroll
+            for (int v = 0; v < 4; v++)
+                s.t[v][o] = r.kind == 0 ? cv[0][v] : (T)0.25 * (cv[0][v] + cv[1][v] + cv[2][v] + cv[3][v]);
+        }
+    }
+    const int ct = p2t(x, y);
+#pragma unroll
+    for (int k = 0; k < 4; k++) st2<T>(s.t[k], ct, c[k]);
+    load_bed2<T>(s, zbt, tid);
+    const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
+    bed_wait();
+    __syncthreads();
+    V xm[4], gxo[4], gyo[4];
+    T ym[4];
+    gradients2<T, ENGINE>(s, bg, p.theta, delta, tid, x, py, c, xm, ym, gxo, gyo);
+    __syncthreads();
+    V cdt = faces2<T, ENGINE, false, true>(s, p, delta, tid, x, py, c, xm, ym, gxo, gyo, (T)0, &sub);
+    if (stage == 0) {
+        cdt = finite_dt2<T>(c[VH], c[VU], c[VV], cdt);
+        T v = cdt.b < cdt.a ? cdt.b : cdt.a;
+        for (int o = 16; o > 0; o >>= 1) {
+            const T q = __shfl_xor_sync(0xffffffffu, v, o);
+            v = q < v ? q : v;
+        }
+        if (lane == 0) s.red[w4] = v;
+    }
+    __syncthreads();  // every face written (the right column and top row by warp 0)
+    // faces to the stage face arrays: X faces at fxi(x, y) (x = 16 after the 256
+    // interior faces), Y faces at fyi(x, y)
+    const size_t fb = (size_t)ib * NFX;
+    for (int k = tid; k < NFX; k += NT2) {
+        const int ox = k < 256 ? p2fx(k & 15, k >> 4) : p2fx(BW, k - 256);
+        const int oy = p2fy(k & 15, k >> 4);
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            a.F[v][fb + k] = s.fx[v][ox];
+            a.F[4 + v][fb + k] = s.fy[v][oy];
+        }
+    }
+    if (stage == 0 && tid == 0) {
+        T b = s.red[0];
+        for (int k = 1; k < NT2 / 32; k++) b = s.red[k] < b ? s.red[k] : b;
+        atomicMin(&m.dtmin[2 * sc + parity], dt_bits(b));
+    }
+}
+
 template <class T, int ENGINE>
 __global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::update) amr_update_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
                                                                  int stage)
@@ -616,6 +739,9 @@ template <class T, int ENGINE> static cudaError_t amr_configure_engine()
     cudaError_t e = cudaFuncSetAttribute(amr_flux_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)amr_smem<T>());
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(amr_flux2_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem2_pred<T>());
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(amr_update_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)amr_smem<T>());
 }
@@ -644,10 +770,10 @@ int launch_amr_stage(const DevModel<T>& m, const AmrDev<T>& a, const StepParams<
     }
     amr_apply_kernel<T><<<n, 64, 0, st>>>(m, a, p, parity, stage);
     if (engine == 1) {
-        amr_flux_kernel<T, 1><<<n, NTHREADS, amr_smem<T>(), st>>>(m, a, p, parity, stage);
+        amr_flux2_kernel<T, 1><<<n, NT2, smem2_pred<T>(), st>>>(m, a, p, parity, stage);
         amr_update_kernel<T, 1><<<n, NTHREADS, amr_smem<T>(), st>>>(m, a, p, parity, stage);
     } else {
-        amr_flux_kernel<T, 2><<<n, NTHREADS, amr_smem<T>(), st>>>(m, a, p, parity, stage);
+        amr_flux2_kernel<T, 2><<<n, NT2, smem2_pred<T>(), st>>>(m, a, p, parity, stage);
         amr_update_kernel<T, 2><<<n, NTHREADS, amr_smem<T>(), st>>>(m, a, p, parity, stage);
     }
     return launches + 3;

@@ -169,6 +169,9 @@ template <class V> struct FaceV {
     V hi, hn, zsi, zsn, uni, unn, uti, utn;
     V dhi, dhn, dzsi, dzsn, duni, dunn, duti, dutn;
     V zbi, zbn;
+    // source-term depth and bed of each side: the cells' own (engine 1: zb; engine 2:
+    // zs - h) except at a coarse/fine face, where the coarser side's cell is used
+    V hsi, hsn, zri, zrn;
 };
 template <class V> struct FaceOutV {
     V Fh, Fq, S, Ft, dt;
@@ -265,8 +268,8 @@ __device__ __forceinline__ FaceOutV<V> face_v(const FaceV<V>& f, V g, V CFLdelta
         const V hm = vmax(zero, sub(add(hr, zr), zlr));
         r.dt = kurg_v<V>(g, CFLdelta, epsi, hp, hm, up, um, fh, fu);
         fv = mul(sel(gt(fh, zero), mad(dx, f.dutn, f.utn), mad(ndx, f.duti, f.uti)), fh);
-        sl = mul(ga, mad(add(hl, f.hi), sub(zi, zl), sub(mul(hp, hp), mul(hl, hl))));
-        sr = mul(ga, mad(add(hr, f.hn), sub(zn, zr), sub(mul(hm, hm), mul(hr, hr))));
+        sl = mul(ga, mad(add(hl, f.hsi), sub(f.zri, zl), sub(mul(hp, hp), mul(hl, hl))));
+        sr = mul(ga, mad(add(hr, f.hsn), sub(f.zrn, zr), sub(mul(hm, hm), mul(hr, hr))));
     } else {
         // products fused into the sums (exact build: separately rounded, the same values)
         const V ndx = mul(cst<V>((T)-1.0), dx);
@@ -290,8 +293,8 @@ __device__ __forceinline__ FaceOutV<V> face_v(const FaceV<V>& f, V g, V CFLdelta
         const V vl = mad(fl, f.dutn, f.utn);
         r.dt = hllc_v<V>(g, CFLdelta, epsi, hCNl, hCNr, ul, ur, fh, fu);
         fv = mul(sel(gt(fh, zero), vl, vr), fh);
-        sl = mul(mul(ga, add(f.hi, hCNr)), sub(f.zbi, zCN));
-        sr = mul(mul(ga, add(hCNl, f.hn)), sub(f.zbn, zCN));
+        sl = mul(mul(ga, add(f.hsi, hCNr)), sub(f.zri, zCN));
+        sr = mul(mul(ga, add(hCNl, f.hsn)), sub(f.zrn, zCN));
     }
     r.Fh = sel(r.wet, fh, zero);
     r.Fq = sel(r.wet, sub(fu, sl), zero);
@@ -617,10 +620,13 @@ __device__ __forceinline__ void gradients2(Smem2<T>& s, const BedGrad<T>& bg, T 
 // The own pair's X faces (left of each cell) and Y faces (below each cell), and the
 // 16 + 16 faces on the right column and the top row (warp 0, lanes 0..7 X, 8..15 Y).
 // Returns the pair's cell dtmax as the one-cell kernels leave it.
-template <class T, int ENGINE, bool SPLIT = false>
+// SUB: faces on a side whose neighbour is coarser take the neighbour's parent cell
+// (subf, filled by the multi-level flux kernel) as their source-term depth and bed.
+template <class T, int ENGINE, bool SPLIT = false, bool SUB = false>
 __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T delta, int tid, int x, int py,
                                         const V2<T> (&c)[4], const V2<T> (&xm)[4], const T (&ym)[4],
-                                        const V2<T> (&gxo)[4], const V2<T> (&gyo)[4], T D = (T)0)
+                                        const V2<T> (&gxo)[4], const V2<T> (&gyo)[4], T D = (T)0,
+                                        const SubFaces<T>* subf = nullptr)
 {
     using V = V2<T>;
     const V g{p.g, p.g}, epsi{p.epsi, p.epsi}, eps{p.epsface, p.epsface};
@@ -641,6 +647,18 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         }
     }
     const V Dv{D, D};
+    // the cells' own source-term depth and bed
+    auto own_sources = [&](FaceV<V>& ff) {
+        ff.hsi = ff.hi;
+        ff.hsn = ff.hn;
+        if constexpr (ENGINE == 1) {
+            ff.zri = ff.zbi;
+            ff.zrn = ff.zbn;
+        } else {
+            ff.zri = sub(ff.zsi, ff.hi);
+            ff.zrn = sub(ff.zsn, ff.hn);
+        }
+    };
     auto face = [&](const FaceV<V>& ff) {
         if constexpr (SPLIT) return face_v_split<V, ENGINE>(ff, Dv, g, CFLd, epsi, eps, dx, ga);
         else return face_v<V, ENGINE>(ff, g, CFLd, epsi, eps, dx, ga);
@@ -656,6 +674,13 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         f.dunn = ld2<T>(s.gx[VU], gn); f.dutn = ld2<T>(s.gx[VV], gn);
     }
     f.zbi = zbc; f.zbn = zbx;
+    own_sources(f);
+    if constexpr (SUB) {
+        if (x == 0 && subf->on[0]) {  // left side coarser: the n-side sources
+            f.hsn = V{subf->h[0][y], subf->h[0][y + 1]};
+            f.zrn = V{subf->z[0][y], subf->z[0][y + 1]};
+        }
+    }
     const FaceOutV<V> fx = face(f);
     {
         const int o = p2fx(x, y);
@@ -671,6 +696,13 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         f.dunn = V{s.gy[VV][gn], gyo[VV].a}; f.dutn = V{s.gy[VU][gn], gyo[VU].a};
     }
     f.zbi = zbc; f.zbn = V{zby, zbc.a};
+    own_sources(f);
+    if constexpr (SUB) {
+        if (y == 0 && subf->on[2]) {  // bottom side coarser: the lower face's n-side sources
+            f.hsn.a = subf->h[2][x];
+            f.zrn.a = subf->z[2][x];
+        }
+    }
     const FaceOutV<V> fy = face(f);
     {
         const int o = p2fy(x, y);
@@ -712,6 +744,14 @@ __device__ __forceinline__ V2<T> faces2(Smem2<T>& s, const StepParams<T>& p, T d
         if (SPLIT) {
             e.zbi = add(e.zbi, Dv);
             e.zbn = add(e.zbn, Dv);
+        }
+        own_sources(e);
+        if constexpr (SUB) {
+            const int sd = isx ? 1 : 3;  // right / top side coarser: the i-side sources
+            if (subf->on[sd]) {
+                e.hsi = V{subf->h[sd][2 * q], subf->h[sd][2 * q + 1]};
+                e.zri = V{subf->z[sd][2 * q], subf->z[sd][2 * q + 1]};
+            }
         }
         const FaceOutV<V> fe = face(e);
         if (isx) {

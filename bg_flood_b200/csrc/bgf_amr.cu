@@ -15,7 +15,7 @@
 //                       same pass already changed)
 //   amr_apply_kernel    the decisions applied (depth and bed of the parent), zs
 //                       recomputed on the prolongated halo
-//   amr_flux_kernel     tile with its outer stencil ring, gradients, wet-slope
+//   amr_flux2_kernel    tile with its outer stencil ring, gradients, wet-slope
 //                       reset, faces with the coarse/fine source substitution,
 //                       cell dtmax and the block minimum (predictor only);
 //                       faces written to the stage face arrays
@@ -306,125 +306,16 @@ template <class T> struct AmrOcc {
     static constexpr int flux = sizeof(T) == 4 ? 6 : 3;
 };
 
-template <class T, int ENGINE>
-__global__ void __launch_bounds__(NTHREADS, AmrOcc<T>::flux) amr_flux_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0, int parity,
-                                                               int stage)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem<T>& s = *reinterpret_cast<Smem<T>*>(smem_raw);
-    __shared__ SubFaces<T> sub;
-    const int tid = threadIdx.x;
-    const int ib = m.active[blockIdx.x];
-    const int sc = scen_of(m, ib);
-    const TimeState ts = m.time[2 * sc + parity];
-    if (!step_live(ts)) return;
-    const StepParams<T>& p = m.sparams ? m.sparams[sc] : p0;
-    const int nbm = m.nblkmem;
-    const T delta = calcres<T>(p.delta0, m.level[ib]);
-    T* const* W = a.W[stage];
-    const size_t base = (size_t)ib * 324;
-
-    load_bed<T, ENGINE, false, true>(s, m, ib, tid);  // entries beyond 256 on threads 128..
-    {
-        // interior and ring 1 (the block's halo, corners excluded)
-        const int x = tid & 15, y = tid >> 4;
-        const int c18 = hi18(x, y), c = ti(x, y);
-#pragma unroll
-        for (int v = 0; v < 4; v++) s.t[v][c] = W[v][base + c18];
-    }
-    if (tid < 64) {
-        const int sd = tid >> 4, t = tid & 15;
-        int hx, hy;
-        halo_xy(sd, t, hx, hy);
-        const int c18 = hi18(hx, hy), c = ti(hx, hy);
-#pragma unroll
-        for (int v = 0; v < 4; v++) s.t[v][c] = W[v][base + c18];
-        // coarse/fine source substitution for the faces on this side
-        int pb, px, py;
-        const bool coarse = parent_cell(m.nbr, nbm, m.level, ib, sd, t, pb, px, py);
-        if (t == 0) sub.on[sd] = coarse ? 1 : 0;
-        if (coarse) {
-            sub.h[sd][t] = W[0][(size_t)pb * 324 + hi18(px, py)];
-            sub.z[sd][t] = a.zb[(size_t)pb * 324 + hi18(px, py)];
-        }
-    } else if (tid < 128) {
-        // ring 2: the outer stencil values of the halo gradients
-        const int k = tid - 64;
-        const int sd = k >> 4, t = k & 15;
-        const CellRule<T> r = outer_rule<T>(m.nbr, nbm, m.level, ib, sd, t);
-        int x, y;
-        halo_xy(sd, t, x, y);
-        if (sd == 0) x = -2;
-        else if (sd == 1) x = BW + 1;
-        else if (sd == 2) y = -2;
-        else y = BW + 1;
-        const int c = ti(x, y);
-        if (r.kind == 3) {
-            // inside a coarser neighbour's 2x2 patch, which may reach into its halo:
-            // that neighbour has a finer neighbour, so it runs this chain and its
-            // stage tile is filled
-#pragma unroll
-            for (int v = 0; v < 4; v++) s.t[v][c] = rule_eval(r, Acc324<T>{W[v]});
-        } else {
-            // interior cells of this block or of a same-level or finer neighbour,
-            // read as the stage reads any cell (the neighbour may run the single-level
-            // kernels and have no stage tile)
-            const T halfdt = stage == 0 ? (T)0 : step_dt<T>(ts, m.dtmin[2 * sc + parity]) * (T)0.5;
-            const StageState<T> S{m, p, ts.cur, stage != 0, halfdt, ts.totaltime};
-            T cv[4][4];  // per rule cell: h, zs, u, v
-            const int nc = r.kind == 0 ? 1 : 4;
-            for (int q = 0; q < nc; q++) {
-                S.get(r.b[q], r.x[q], r.y[q], cv[q][0], cv[q][2], cv[q][3]);
-                cv[q][1] = a.zb[(size_t)r.b[q] * 324 + hi18(r.x[q], r.y[q])] + cv[q][0];
-            }
-#pragma unroll
-            for (int v = 0; v < 4; v++)
-                s.t[v][c] = r.kind == 0 ? cv[0][v] : (T)0.25 * (cv[0][v] + cv[1][v] + cv[2][v] + cv[3][v]);
-        }
-    }
-    __syncthreads();
-    const T celldt = tile_fluxes<T, ENGINE, true>(s, p, delta, tid, &sub);
-    __syncthreads();
-    if (stage == 0) {
-        T v = finite_state_dt<T>(s, tid, celldt);
-        for (int o = 16; o > 0; o >>= 1) {
-            T w = __shfl_xor_sync(0xffffffffu, v, o);
-            v = w < v ? w : v;
-        }
-        if ((tid & 31) == 0) s.red[tid >> 5] = v;
-    }
-    // faces to the stage face arrays
-    const size_t fb = (size_t)ib * NFX;
-    for (int k = tid; k < NFX; k += NTHREADS) {
-        a.F[0][fb + k] = s.Fhu[k];
-        a.F[1][fb + k] = s.Fqux[k];
-        a.F[2][fb + k] = s.Su[k];
-        a.F[3][fb + k] = s.Fqvx[k];
-        a.F[4][fb + k] = s.Fhv[k];
-        a.F[5][fb + k] = s.Fqvy[k];
-        a.F[6][fb + k] = s.Sv[k];
-        a.F[7][fb + k] = s.Fquy[k];
-    }
-    if (stage == 0) {
-        __syncthreads();
-        if (tid == 0) {
-            T b = s.red[0];
-            for (int k = 1; k < NTHREADS / 32; k++) b = s.red[k] < b ? s.red[k] : b;
-            atomicMin(&m.dtmin[2 * sc + parity], dt_bits(b));
-        }
-    }
-}
-
-// amr_flux_kernel in the two-cells-per-thread layout of the single-level kernels
+// The multi-level flux kernel, in the two-cells-per-thread layout of the single-level kernels
 // (bgf_flow2.cuh): 128 threads per block, thread (x, p) owning cells (x, 2p) and
 // (x, 2p+1).  The tile comes from the stage tile W (interior and ring 1, whose
 // halos the chain filled) and the outer ring rules (ring 2); gradients, wet-slope
 // reset and faces are the single-level kernels' own, with the coarse/fine source
 // substitution on the sides whose neighbour is coarser.  The faces go to the stage
 // face arrays in the layout amr_update_kernel reads.  The same operations in the
-// same order as amr_flux_kernel: the exact build gives the same faces and dt.
+// same order as the reference's FlowCPU: the exact build matches the oracle bit for bit.
 template <class T, int ENGINE>
-__global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 6 : 3) amr_flux2_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0,
+__global__ void __launch_bounds__(NT2, AmrOcc<T>::flux) amr_flux2_kernel(DevModel<T> m, AmrDev<T> a, StepParams<T> p0,
                                                                             int parity, int stage)
 {
     using V = V2<T>;
@@ -478,10 +369,15 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 6 : 3) amr_flux2_kernel(
         else ry = BW + 1;
         const int o = p2t(rx, ry);
         if (r.kind == 3) {
-            // inside a coarser neighbour's 2x2 patch (see amr_flux_kernel)
+            // inside a coarser neighbour's 2x2 patch, which may reach into its halo:
+            // that neighbour has a finer neighbour, so it runs this chain and its
+            // stage tile is filled
 #pragma unroll
             for (int v = 0; v < 4; v++) s.t[v][o] = rule_eval(r, Acc324<T>{W[v]});
         } else {
+            // interior cells of this block or of a same-level or finer neighbour,
+            // read as the stage reads any cell (the neighbour may run the single-level
+            // kernels and have no stage tile)
             const T halfdt = stage == 0 ? (T)0 : step_dt<T>(ts, m.dtmin[2 * sc + parity]) * (T)0.5;
             const StageState<T> S{m, p, ts.cur, stage != 0, halfdt, ts.totaltime};
             T cv[4][4];  // per rule cell: h, zs, u, v
@@ -736,11 +632,8 @@ template <class T> static size_t amr_smem() { return sizeof(Smem<T>); }
 
 template <class T, int ENGINE> static cudaError_t amr_configure_engine()
 {
-    cudaError_t e = cudaFuncSetAttribute(amr_flux_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)amr_smem<T>());
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(amr_flux2_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem2_pred<T>());
+    cudaError_t e = cudaFuncSetAttribute(amr_flux2_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem2_pred<T>());
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(amr_update_kernel<T, ENGINE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)amr_smem<T>());

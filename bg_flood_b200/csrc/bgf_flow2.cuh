@@ -901,9 +901,23 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) flux2_kernel(DevM
     const int y = 2 * py;
     for (int w = blockIdx.x; w < m.nblk; w += gridDim.x) {
         const int ib = m.regular_nbx > 0 ? w : m.active[w];
+        // the bed tile, the own pair's bed and the bed gradients do not depend on the
+        // time slot: their loads are in flight while it arrives
+        const T* zbt = m.zb + (size_t)ib * 324;
+        load_bed2<T>(s, zbt, tid);
+        const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
+        const V zbo{zbt[hi18(x, y)], zbt[hi18(x, y + 1)]};
+        // the ring cell's source lookup and its bed too
+        int rx, ry, sb, sx, sy;
+        ring_src2<T>(m, ib, tid, rx, ry, sb, sx, sy);
+        const bool ring2 = rx < -1 || rx > BW || ry < -1 || ry > BW;
+        const T zr = ring2 ? m.zb[(size_t)sb * 324 + hi18(sx, sy)] : zbt[hi18(rx, ry)];
         const int sc = POOL ? m.scen[ib] : 0;
         const TimeState ts = m.time[2 * sc + parity];
-        if (!step_live(ts)) continue;
+        if (!step_live(ts)) {
+            bed_wait();  // the next block's copies go to the same shared words
+            continue;
+        }
         const StepParams<T>& p = params_ref<POOL>(m, p0, sc);
         const T delta = calcres<T>(p.delta0, m.level[ib]);
         const T D = SPLIT ? m.datum[ib] : (T)0;  // split precision: the block's datum
@@ -911,16 +925,11 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) flux2_kernel(DevM
         const T* H = m.h[cur];
         const T* U = m.u[cur];
         const T* Vv = m.v[cur];
-        const T* zbt = m.zb + (size_t)ib * 324;
-        // the ring cell's source lookup first (its latency overlaps the pair loads)
-        int rx, ry, sb, sx, sy;
-        ring_src2<T>(m, ib, tid, rx, ry, sb, sx, sy);
         V c[4];
         const size_t g0 = (size_t)ib * 256 + y * 16 + x;
         c[VH] = V{H[g0], H[g0 + 16]};
         c[VU] = V{U[g0], U[g0 + 16]};
         c[VV] = V{Vv[g0], Vv[g0 + 16]};
-        const V zbo{zbt[hi18(x, y)], zbt[hi18(x, y + 1)]};
         c[VZS] = SPLIT ? add(add(zbo, V{D, D}), c[VH]) : add(zbo, c[VH]);
         {
             const size_t gr = (size_t)sb * 256 + sy * 16 + sx;
@@ -928,16 +937,12 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) flux2_kernel(DevM
             // split precision: a neighbour's deviation in this block's datum (datums are
             // whole metres, so the difference is exact)
             if (SPLIT && sb != ib) hv = hv + (m.datum[sb] - D);
-            const bool ring2 = rx < -1 || rx > BW || ry < -1 || ry > BW;
-            const T zr = ring2 ? m.zb[(size_t)sb * 324 + hi18(sx, sy)] : zbt[hi18(rx, ry)];
             const int o = p2t(rx, ry);
             s.t[VH][o] = hv; s.t[VU][o] = U[gr]; s.t[VV][o] = Vv[gr]; s.t[VZS][o] = (SPLIT ? zr + D : zr) + hv;
         }
         const int ct = p2t(x, y);
 #pragma unroll
         for (int k = 0; k < 4; k++) st2<T>(s.t[k], ct, c[k]);
-        load_bed2<T>(s, zbt, tid);
-        const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
         bed_wait();
         __syncthreads();
         V xm[4], gxo[4], gyo[4];
@@ -986,10 +991,30 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
     const int y = 2 * py;
     for (int w = blockIdx.x; w < m.nblk; w += gridDim.x) {
         const int ib = m.regular_nbx > 0 ? w : m.active[w];
+        // the bed, the predictor's tendencies and the ring cell's source do not depend
+        // on the time slot (only the state buffer does): their loads are in flight
+        // while it arrives
+        const T* zbt = m.zb + (size_t)ib * 324;
+        load_bed2<T>(s, zbt, tid);
+        const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
+        const V zbo{zbt[hi18(x, y)], zbt[hi18(x, y + 1)]};
+        int rx, ry, sb, sx, sy;
+        ring_src2<T>(m, ib, tid, rx, ry, sb, sx, sy);
+        const size_t g0 = (size_t)ib * 256 + y * 16 + x;
+        V ddh{m.dh[g0], m.dh[g0 + 16]};
+        const V ddhu{m.dhu[g0], m.dhu[g0 + 16]}, ddhv{m.dhv[g0], m.dhv[g0 + 16]};
+        const size_t gr = (size_t)sb * 256 + sy * 16 + sx;
+        T rdh = m.dh[gr];
+        const T rdhu = m.dhu[gr], rdhv = m.dhv[gr];
+        const bool ring2 = rx < -1 || rx > BW || ry < -1 || ry > BW;
+        const T rzb = ring2 ? m.zb[(size_t)sb * 324 + hi18(sx, sy)] : zbt[hi18(rx, ry)];
         const int sc = POOL ? m.scen[ib] : 0;
+        // the predictor's dt minimum (read by thread 0) does not depend on it either
+        const unsigned long long dtbits = tid == 0 ? m.dtmin[2 * sc + parity] : 0ull;
         const TimeState ts = m.time[2 * sc + parity];
         const bool lead = POOL ? m.lead[ib] != 0 : w == 0;
         if (!step_live(ts)) {
+            bed_wait();  // the next block's copies go to the same shared words
             if (lead && tid == 0) {
                 TimeState nt = ts;
                 nt.done = 1;
@@ -999,7 +1024,7 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
         }
         const StepParams<T>& p = params_ref<POOL>(m, p0, sc);
         if (tid == 0) {
-            const T dt0 = step_dt<T>(ts, m.dtmin[2 * sc + parity]);
+            const T dt0 = step_dt<T>(ts, dtbits);
             s.dtv = dt0;
             if (p.has_rain && !p.rain_map) {
                 // uniform rain (AddrainforcingImplicitCPU, src/Updateforcing.cu:530-580): the
@@ -1017,22 +1042,8 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
         const T* H = m.h[cur];
         const T* U = m.u[cur];
         const T* Vv = m.v[cur];
-        const T* zbt = m.zb + (size_t)ib * 324;
-        int rx, ry, sb, sx, sy;
-        ring_src2<T>(m, ib, tid, rx, ry, sb, sx, sy);
-        const size_t g0 = (size_t)ib * 256 + y * 16 + x;
         const V hold{H[g0], H[g0 + 16]}, uold{U[g0], U[g0 + 16]}, vold{Vv[g0], Vv[g0 + 16]};
-        V ddh{m.dh[g0], m.dh[g0 + 16]};
-        const V ddhu{m.dhu[g0], m.dhu[g0 + 16]}, ddhv{m.dhv[g0], m.dhv[g0 + 16]};
-        const V zbo{zbt[hi18(x, y)], zbt[hi18(x, y + 1)]};
-        const size_t gr = (size_t)sb * 256 + sy * 16 + sx;
         const T rh = H[gr], ru = U[gr], rv = Vv[gr];
-        T rdh = m.dh[gr];
-        const T rdhu = m.dhu[gr], rdhv = m.dhv[gr];
-        const bool ring2 = rx < -1 || rx > BW || ry < -1 || ry > BW;
-        const T rzb = ring2 ? m.zb[(size_t)sb * 324 + hi18(sx, sy)] : zbt[hi18(rx, ry)];
-        load_bed2<T>(s, zbt, tid);
-        const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
         bed_wait();
         __syncthreads();  // s.dtv, s.zb
         const T dt = s.dtv;
@@ -1097,10 +1108,15 @@ __global__ void __launch_bounds__(NT2, sizeof(T) == 4 ? 7 : 3) update2_kernel(De
                        dhv);
         if (p.nriver > 0)
             dh = V{add_rivers<T>(m, p, ib, x, y, dh.a, ts.totaltime), add_rivers<T>(m, p, ib, x, y + 1, dh.b, ts.totaltime)};
-        // full step from state n (AdvkernelCPU with evolv), then friction on the result
+        // full step from state n (AdvkernelCPU with evolv), then friction on the result;
+        // state n comes back from its shared tile (fewer registers held over the faces)
         V ho, uo, vo;
-        if constexpr (SPLIT) advance_split_v<T>(dt, p.eps, p.forcemass != 0, Dv, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
-        else advance_v<V>(dt, p.eps, p.eps_d, p.forcemass != 0, hold, uold, vold, dh, dhu, dhv, ho, uo, vo);
+        {
+            const int o2 = p2z(x, y);
+            const V hn = ld2<T>(s.h0, o2), un = ld2<T>(s.u0, o2), vn = ld2<T>(s.v0, o2);
+            if constexpr (SPLIT) advance_split_v<T>(dt, p.eps, p.forcemass != 0, Dv, hn, un, vn, dh, dhu, dhv, ho, uo, vo);
+            else advance_v<V>(dt, p.eps, p.eps_d, p.forcemass != 0, hn, un, vn, dh, dhu, dhv, ho, uo, vo);
+        }
         const V cfv = p.has_cf ? V{m.cf[g0], m.cf[g0 + 16]} : V{p.cf, p.cf};
         // (split precision: friction on the full depth; the deviation is not changed by it)
         friction_v<T>(p.frictionmodel, p.g, p.eps, dt, cfv, SPLIT ? add(Dv, ho) : ho, uo, vo);

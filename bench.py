@@ -802,6 +802,10 @@ def main():
     dom = max(kern, key=lambda k: kern[k][0])
     dom_ms, dom_b = kern[dom]
     achieved = dom_b * ncell / (dom_ms / 1e3) / 1e9
+    # both stage kernels (their times are within a few per cent of each other, so the
+    # one named dominant can change from run to run)
+    per_kernel = {k: {"us_per_launch": ms * 1e3, "alg_bytes_per_cell": b,
+                      "achieved": b * ncell / (ms / 1e3) / 1e9} for k, (ms, b) in kern.items()}
     traffic = None
     variant = "fastmath" if args.fastmath else "exact"
     tfile = os.path.join(ROOT, "profiles", f"{dom}_runup{args.n}_{variant}.md")
@@ -920,6 +924,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "alg_bytes_per_cell": dom_b,
+                         "kernels": {k: {**v, "frac": v["achieved"] / peak} for k, v in per_kernel.items()},
                          "step": {"alg_bytes_per_cell_update": ALG_BYTES_FLUX + ALG_BYTES_UPDATE,
                                   "achieved": (ALG_BYTES_FLUX + ALG_BYTES_UPDATE) * value / world / 1e9,
                                   "frac": (ALG_BYTES_FLUX + ALG_BYTES_UPDATE) * value / world / 1e9 / peak}},

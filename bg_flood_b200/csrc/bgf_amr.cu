@@ -329,18 +329,21 @@ __global__ void __launch_bounds__(NT2, AmrOcc<T>::flux) amr_flux2_kernel(DevMode
     const int y = 2 * py;
     const int ib = m.active[blockIdx.x];
     const int sc = scen_of(m, ib);
-    const TimeState ts = m.time[2 * sc + parity];
-    if (!step_live(ts)) return;
     const StepParams<T>& p = m.sparams ? m.sparams[sc] : p0;
     const int nbm = m.nblkmem;
-    const T delta = calcres<T>(p.delta0, m.level[ib]);
     T* const* W = a.W[stage];
     const size_t base = (size_t)ib * 324;
     const T* zbt = m.zb + base;
-    // the own pair from the stage tile
+    // every load that does not depend on the block's time slot is issued before it
+    // arrives: the bed tile and gradients, the own pair and ring 1 from the stage
+    // tile, the coarse/fine sources, and ring 2 inside a coarser neighbour's patch
+    load_bed2<T>(s, zbt, tid);
+    const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
     V c[4];
 #pragma unroll
     for (int v = 0; v < 4; v++) c[v] = V{W[v][base + hi18(x, y)], W[v][base + hi18(x, y + 1)]};
+    CellRule<T> r{};  // ring 2 (threads 64..127)
+    int o2 = 0;
     if (tid < 64) {
         // ring 1 (the block's halo, corners excluded) and the coarse/fine substitution
         const int sd = tid >> 4, t = tid & 15;
@@ -360,42 +363,47 @@ __global__ void __launch_bounds__(NT2, AmrOcc<T>::flux) amr_flux2_kernel(DevMode
         // ring 2: the outer stencil values of the halo gradients
         const int k = tid - 64;
         const int sd = k >> 4, t = k & 15;
-        const CellRule<T> r = outer_rule<T>(m.nbr, nbm, m.level, ib, sd, t);
+        r = outer_rule<T>(m.nbr, nbm, m.level, ib, sd, t);
         int rx, ry;
         halo_xy(sd, t, rx, ry);
         if (sd == 0) rx = -2;
         else if (sd == 1) rx = BW + 1;
         else if (sd == 2) ry = -2;
         else ry = BW + 1;
-        const int o = p2t(rx, ry);
+        o2 = p2t(rx, ry);
         if (r.kind == 3) {
             // inside a coarser neighbour's 2x2 patch, which may reach into its halo:
             // that neighbour has a finer neighbour, so it runs this chain and its
             // stage tile is filled
 #pragma unroll
-            for (int v = 0; v < 4; v++) s.t[v][o] = rule_eval(r, Acc324<T>{W[v]});
-        } else {
-            // interior cells of this block or of a same-level or finer neighbour,
-            // read as the stage reads any cell (the neighbour may run the single-level
-            // kernels and have no stage tile)
-            const T halfdt = stage == 0 ? (T)0 : step_dt<T>(ts, m.dtmin[2 * sc + parity]) * (T)0.5;
-            const StageState<T> S{m, p, ts.cur, stage != 0, halfdt, ts.totaltime};
-            T cv[4][4];  // per rule cell: h, zs, u, v
-            const int nc = r.kind == 0 ? 1 : 4;
-            for (int q = 0; q < nc; q++) {
-                S.get(r.b[q], r.x[q], r.y[q], cv[q][0], cv[q][2], cv[q][3]);
-                cv[q][1] = a.zb[(size_t)r.b[q] * 324 + hi18(r.x[q], r.y[q])] + cv[q][0];
-            }
-#pragma unroll
-            for (int v = 0; v < 4; v++)
-                s.t[v][o] = r.kind == 0 ? cv[0][v] : (T)0.25 * (cv[0][v] + cv[1][v] + cv[2][v] + cv[3][v]);
+            for (int v = 0; v < 4; v++) s.t[v][o2] = rule_eval(r, Acc324<T>{W[v]});
         }
+    }
+    const TimeState ts = m.time[2 * sc + parity];
+    if (!step_live(ts)) {
+        bed_wait();  // (no bed copy outlives the block)
+        return;
+    }
+    const T delta = calcres<T>(p.delta0, m.level[ib]);
+    if (tid >= 64 && r.kind != 3) {
+        // ring 2 at interior cells of this block or of a same-level or finer
+        // neighbour, read as the stage reads any cell (the neighbour may run the
+        // single-level kernels and have no stage tile): the state of the step
+        const T halfdt = stage == 0 ? (T)0 : step_dt<T>(ts, m.dtmin[2 * sc + parity]) * (T)0.5;
+        const StageState<T> S{m, p, ts.cur, stage != 0, halfdt, ts.totaltime};
+        T cv[4][4];  // per rule cell: h, zs, u, v
+        const int nc = r.kind == 0 ? 1 : 4;
+        for (int q = 0; q < nc; q++) {
+            S.get(r.b[q], r.x[q], r.y[q], cv[q][0], cv[q][2], cv[q][3]);
+            cv[q][1] = a.zb[(size_t)r.b[q] * 324 + hi18(r.x[q], r.y[q])] + cv[q][0];
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++)
+            s.t[v][o2] = r.kind == 0 ? cv[0][v] : (T)0.25 * (cv[0][v] + cv[1][v] + cv[2][v] + cv[3][v]);
     }
     const int ct = p2t(x, y);
 #pragma unroll
     for (int k = 0; k < 4; k++) st2<T>(s.t[k], ct, c[k]);
-    load_bed2<T>(s, zbt, tid);
-    const BedGrad<T> bg = load_bedgrad<T, ENGINE>(m, ib, tid, x, y);
     bed_wait();
     __syncthreads();
     V xm[4], gxo[4], gyo[4];
